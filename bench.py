@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the flash hot path on B200: flash+Jacobian cells/s.
+
+Workload (one step): the batched flash of 1,048,576 independent cells, SRK,
+6 components, seeded synthetic inputs (osiris_b200.workloads), returning
+phase labels, phase fractions, compositions, compressibilities and the
+fugacity derivative blocks of both phases.  Inputs are resident in HBM when
+the timed region starts; L2 is flushed (256 MiB write) before every step.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W]`` prints one JSON line.
+Under torchrun each rank flashes its own 1,048,576 cells (weak scaling, no
+data-path collective); ``value`` is all ranks' cells over the slowest rank's
+time.  ``--impl reference`` times the reference's own CPU flash (SuccFalsh,
+compiled from the reference's sources into oracle/_ref) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "flash+Jacobian cells/s on 1 B200, batched vs plain, at 1e-10 rel err"
+UNIT = "cells/s"
+WORKLOAD = "batched flash: 1,048,576 cells, SRK, 6 components, P~U(5,40) MPa, T~U(300,450) K, z~Dirichlet(1), " \
+           "with fugacity derivatives of both phases"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cells", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- CPU (reference) side
+
+_W = {}
+
+
+def _cpu_worker_init(lo, hi, n_total):
+    import numpy as np
+    import oracle
+    from osiris_b200 import workloads
+    tc, pc, acf, kij, eos = workloads.flash_fluid_srk6()
+    P, T, z = workloads.flash_cells(n_total, 6, seed=3)
+    _W["fl"] = oracle.Fluid(tc, pc, acf, kij, eos)
+    _W["P"] = np.ascontiguousarray(P[lo:hi])
+    _W["T"] = np.ascontiguousarray(T[lo:hi])
+    _W["z"] = np.ascontiguousarray(z[:, lo:hi])
+
+
+def _cpu_worker_run(_):
+    import oracle
+    t = time.perf_counter()
+    oracle.ref_flash_batch(_W["fl"], _W["P"], _W["T"], _W["z"])
+    return time.perf_counter() - t
+
+
+class CpuReference:
+    """The reference's SuccFalsh on every host core: one spawned process per
+    core, each holding a contiguous shard of the cells (the reference keeps its
+    state in globals, so parallelism is by process, not thread)."""
+
+    def __init__(self, n_cells: int, cores: int | None = None):
+        self.cores = cores or len(os.sched_getaffinity(0))
+        self.n = n_cells
+        ctx = mp.get_context("spawn")
+        bounds = [(i * n_cells // self.cores, (i + 1) * n_cells // self.cores) for i in range(self.cores)]
+        self.pools = [ctx.Pool(1, initializer=_cpu_worker_init, initargs=(lo, hi, n_cells)) for lo, hi in bounds]
+
+    def step(self) -> float:
+        t = time.perf_counter()
+        rs = [p.apply_async(_cpu_worker_run, (0,)) for p in self.pools]
+        for r in rs:
+            r.get()
+        return time.perf_counter() - t
+
+    def close(self):
+        for p in self.pools:
+            p.terminate()
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    from osiris_b200 import workloads
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libosiris_ref.so not built"}))
+        return 0
+    n = args.cells or workloads.FLASH_CELLS
+    ref = CpuReference(n)
+    for _ in range(args.warmup):
+        ref.step()
+    times = [ref.step() for _ in range(args.steps)]
+    ref.close()
+    sec = sum(times) / len(times)
+    value = n / sec
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "cells": n, "nc": 6, "eos": "SRK"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.cores, "kind": "reference",
+                             "sample": f"all {n} cells per step, sharded over {ref.cores} processes"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str):
+        self.proc = None
+        self.bus = bus_id.lower()
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9 and parts[0].lower().endswith(self.bus):
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                except ValueError:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples for this GPU"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i in range(4) if r[i].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _gpu_id(torch, dev):
+    """'bb:dd.0' of this device's PCI address (the tail nvidia-smi prints)."""
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        return f"{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+    except Exception:
+        return ""
+
+
+# ----------------------------------------------------------------------------- GPU side
+
+def _traffic_from_profiles():
+    """dram bytes per launch of the flash kernel, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "flash_queue_srk6.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import osiris_b200 as osr
+    from osiris_b200 import flop_model, workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n = args.cells or workloads.FLASH_CELLS
+
+    # the CPU pool is spawned before the first GPU call
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            cpu = CpuReference(n)
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
+
+    tc, pc, acf, kij, eos = workloads.flash_fluid_srk6()
+    fl = osr.Fluid(tc, pc, acf, kij, eos)
+    nc = fl.nc
+    Pn, Tn, zn = workloads.flash_cells(n, nc, seed=3 + rank)
+    P = torch.from_numpy(Pn).to(dev)
+    T = torch.from_numpy(Tn).to(dev)
+    z = torch.from_numpy(zn).to(dev)
+    out = osr.alloc_flash_outputs(nc, n, True, dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for s, e in ev:
+            flush.zero_()
+            s.record(stream)
+            fn()
+            e.record(stream)
+        torch.cuda.synchronize(dev)
+        return [s.elapsed_time(e) for s, e in ev]
+
+    step = lambda: osr.flash(fl, P, T, z, derivs=True, out=out)  # noqa: E731
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    iters = out["iters"].cpu().numpy()
+    rr = out["rr_iters"].cpu().numpy()
+
+    import ctypes
+    pk = ctypes.c_double()
+    osr._check(osr.lib().osr_probe_fp64_peak(ctypes.byref(pk), ctypes.c_void_p(stream.cuda_stream)),
+               "osr_probe_fp64_peak")
+    fp64_peak = pk.value
+
+    barrier()
+    torch.cuda.synchronize(dev)
+    gpu_id = _gpu_id(torch, dev)
+    clocks = ClockSampler(gpu_id)
+    t_wall0 = time.perf_counter()
+    step_ms = timed(step, args.steps)
+    torch.cuda.synchronize(dev)
+    t_wall = time.perf_counter() - t_wall0
+    barrier()
+    # the iteration kernel alone (no derivative pass), for its roofline
+    out_nod = {k: v for k, v in out.items() if k not in ("dlnphi_dx", "dlnphi_dP")}
+    kern_ms = timed(lambda: osr.flash(fl, P, T, z, derivs=False, out=out_nod), args.steps)
+    clk = clocks.stop()
+
+    ms = sum(step_ms) / len(step_ms)
+    ms_max = max_over_ranks(ms)
+    value = world * n / (ms_max * 1e-3)
+    kms = sum(kern_ms) / len(kern_ms)
+    deriv_ms = max(ms - kms, 1e-9)
+
+    kflops = flop_model.flash_kernel_flops(nc, iters, rr)
+    achieved = kflops / (kms * 1e-3) / 1e12
+    dflops = flop_model.deriv_kernel_flops(nc, n)
+    # derivative pass: reads P, T once, x|y and Z per phase; writes both blocks
+    deriv_bytes = n * (16 + 2 * (nc * 8 + 8) + 2 * (nc * nc + nc) * 8)
+    traffic = _traffic_from_profiles()
+
+    # batched vs plain (same outputs; the plain form is the one-thread-per-cell kernel)
+    plain = None
+    if not args.no_plain:
+        step_plain = lambda: osr.flash(fl, P, T, z, derivs=True, out=out, form="plain")  # noqa: E731
+        step_plain()
+        pms = timed(step_plain, max(2, min(3, args.steps)))
+        pm = max_over_ranks(sum(pms) / len(pms))
+        plain = {"value": world * n / (pm * 1e-3), "ms_per_step": pm, "batched_over_plain": pm / ms_max}
+
+    # end to end through the public host API: pinned host inputs and outputs
+    e2e = None
+    if not args.no_e2e:
+        hP = torch.from_numpy(Pn).pin_memory()
+        hT = torch.from_numpy(Tn).pin_memory()
+        hz = torch.from_numpy(zn).pin_memory()
+        hout = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in out.items()}
+        host_step = lambda: osr.flash_host(fl, hP, hT, hz, derivs=True, out=hout)  # noqa: E731
+        host_step()
+        ems = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            host_step()
+            ems.append((time.perf_counter() - t0) * 1e3)
+        em = max_over_ranks(sum(ems) / len(ems))
+        h2d = n * (nc + 2) * 8
+        d2h = sum(v.numel() * v.element_size() for v in out.values())
+        e2e = {"value": world * n / (em * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": em}
+
+    cpu_line = None
+    if cpu is not None:
+        cpu.step()  # warm the workers (library load, first-touch)
+        sec = cpu.step()
+        cpu.close()
+        cpu_line = {"value": n / sec, "unit": UNIT, "cores": cpu.cores, "kind": "reference",
+                    "sample": f"all {n} cells of the workload, reference SuccFalsh, one process per core"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    two_phase = float((out["label"] == 0).float().mean().item())
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, numpy default_rng)",
+        "config": {"workload": WORKLOAD, "cells_per_gpu": n, "nc": nc, "eos": "SRK", "form": "batched",
+                   "l2": "flushed before every step (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "two_phase_fraction": two_phase, "mean_ss_iters": float(iters.mean()),
+                   "mean_rr_iters": float(rr.mean()), "max_ss_iters": int(iters.max()),
+                   "max_rr_iters": int(rr.max())},
+        "roofline": {"bound": "fp64", "kernel": "flash_queue_kernel<6>", "achieved": achieved,
+                     "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                     "peak_source": "measured: osr_probe_fp64_peak (dependent-FMA microbenchmark, this run)",
+                     "traffic": traffic, "flops_per_launch": kflops, "ms_per_launch": kms},
+        "deriv_kernel": {"bound": "hbm", "ms_per_launch": deriv_ms,
+                         "achieved_gbs": deriv_bytes / (deriv_ms * 1e-3) / 1e9, "bytes_per_launch": deriv_bytes,
+                         "flops_per_launch": dflops},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+        "timed_wall_s": t_wall,
+    }
+    if plain is not None:
+        line["plain"] = plain
+    if e2e is not None:
+        line["e2e"] = e2e
+    if cpu_line is not None:
+        line["cpu_baseline"] = cpu_line
+    try:
+        import json as _j
+        peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        line["deriv_kernel"]["hbm_peak_gbs"] = peaks.get("hbm_gbs")
+        line["deriv_kernel"]["frac"] = line["deriv_kernel"]["achieved_gbs"] / peaks["hbm_gbs"]
+    except Exception:
+        pass
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,198 @@
+"""CPU oracle for the flash hot path (test infrastructure only).
+
+Two libraries sit behind this module:
+
+* ``_ref/libosiris_ref.so`` -- the reference simulator compiled unmodified from
+  its own C++ sources (``oracle/Makefile``), driven through the C entry points
+  in ``oracle/ref_driver.cpp``.  It is only present where the reference sources
+  were available at build time.
+* ``_build/liboracle.so`` -- the plain-C restatement in ``oracle/flash_oracle.c``
+  (each function cites the reference file:line it restates).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module, and only as the checker.  The CUDA library
+never loads or calls it.
+
+Array conventions match the CUDA library: per-cell scalars ``[n]``,
+per-component fields ``[nc, n]``, derivative blocks ``[2, nc, nc, n]`` and
+``[2, nc, n]`` with phase 0 = liquid, 1 = vapour.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libosiris_ref.so")
+ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+_vp = ctypes.c_void_p
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+class _Fluid(ctypes.Structure):
+    _fields_ = [("nc", ctypes.c_int), ("eos", ctypes.c_int), ("tc", _vp), ("pc", _vp), ("acf", _vp),
+                ("kij", _vp)]
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise FileNotFoundError(f"{ORACLE_LIB} missing: run `make -C oracle oracle`")
+        lib = ctypes.CDLL(ORACLE_LIB)
+        lib.orc_solve_z.restype = ctypes.c_double
+        lib.orc_solve_z.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int]
+        lib.orc_flash_batch.restype = ctypes.c_int
+        lib.orc_flash_derivs_batch.restype = ctypes.c_int
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_LIB} missing: build with `make -C oracle ref`")
+        lib = ctypes.CDLL(REF_LIB)
+        lib.ref_flash_batch.restype = ctypes.c_int
+        lib.ref_solve_z.restype = ctypes.c_double
+        lib.ref_solve_z.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int]
+        lib.ref_eos_params.restype = ctypes.c_int
+        _ref = lib
+    return _ref
+
+
+class Fluid:
+    """Component table: critical temperature [K], critical pressure [Pa],
+    acentric factor, symmetric kij with zero diagonal; eos 0 = PR, 1 = SRK."""
+
+    def __init__(self, tc, pc, acf, kij, eos: int):
+        self.tc = np.ascontiguousarray(tc, dtype=np.float64)
+        self.pc = np.ascontiguousarray(pc, dtype=np.float64)
+        self.acf = np.ascontiguousarray(acf, dtype=np.float64)
+        self.kij = np.ascontiguousarray(kij, dtype=np.float64)
+        self.nc = int(self.tc.shape[0])
+        self.eos = int(eos)
+        self._c = _Fluid(self.nc, self.eos, _p(self.tc), _p(self.pc), _p(self.acf), _p(self.kij))
+
+    @property
+    def cstruct(self):
+        return ctypes.byref(self._c)
+
+
+def flash_batch(fl: Fluid, P, T, z):
+    """Restated flash (oracle/flash_oracle.c).  Returns a dict of arrays."""
+    lib = oracle_lib()
+    P = np.ascontiguousarray(P, np.float64)
+    T = np.ascontiguousarray(T, np.float64)
+    z = np.ascontiguousarray(z, np.float64)
+    n = P.shape[0]
+    nc = fl.nc
+    out = dict(label=np.zeros(n, np.int8), L=np.zeros(n), x=np.zeros((nc, n)), y=np.zeros((nc, n)),
+               Zl=np.zeros(n), Zg=np.zeros(n), iters=np.zeros(n, np.int32), rr_iters=np.zeros(n, np.int32))
+    rc = lib.orc_flash_batch(fl.cstruct, ctypes.c_long(n), _p(P), _p(T), _p(z), _p(out["label"]), _p(out["L"]),
+                             _p(out["x"]), _p(out["y"]), _p(out["Zl"]), _p(out["Zg"]), _p(out["iters"]),
+                             _p(out["rr_iters"]))
+    if rc:
+        raise RuntimeError(f"orc_flash_batch returned {rc}")
+    return out
+
+
+def flash_derivs(fl: Fluid, P, T, x, y, Zl, Zg):
+    lib = oracle_lib()
+    n = P.shape[0]
+    nc = fl.nc
+    dx = np.zeros((2, nc, nc, n))
+    dp = np.zeros((2, nc, n))
+    args = [np.ascontiguousarray(a, np.float64) for a in (P, T, x, y, Zl, Zg)]
+    rc = lib.orc_flash_derivs_batch(fl.cstruct, ctypes.c_long(n), *[_p(a) for a in args], _p(dx), _p(dp))
+    if rc:
+        raise RuntimeError(f"orc_flash_derivs_batch returned {rc}")
+    return dx, dp
+
+
+def fugacity(fl: Fluid, P: float, T: float, w, Z: float):
+    """ln(phi), d ln(phi)/dw [nc, nc], d ln(phi)/dP for one phase."""
+    lib = oracle_lib()
+    nc = fl.nc
+    w = np.ascontiguousarray(w, np.float64)
+    lnphi = np.zeros(nc)
+    dx = np.zeros((nc, nc))
+    dp = np.zeros(nc)
+    lib.orc_fugacity(fl.cstruct, ctypes.c_double(P), ctypes.c_double(T), _p(w), ctypes.c_double(Z), _p(lnphi),
+                     _p(dx), _p(dp))
+    return lnphi, dx, dp
+
+
+def eos_params(fl: Fluid, T: float):
+    lib = oracle_lib()
+    a = np.zeros(fl.nc)
+    b = np.zeros(fl.nc)
+    lib.orc_eos_params(fl.cstruct, ctypes.c_double(T), _p(a), _p(b))
+    return a, b
+
+
+def solve_z(a1, a2, a3, gas: bool) -> float:
+    return oracle_lib().orc_solve_z(a1, a2, a3, int(gas))
+
+
+def ref_flash_batch(fl: Fluid, P, T, z):
+    """The reference's own SuccFalsh over n cells (compsim/Init_Calcs.cpp:571)."""
+    lib = ref_lib()
+    P = np.ascontiguousarray(P, np.float64)
+    T = np.ascontiguousarray(T, np.float64)
+    z = np.ascontiguousarray(z, np.float64)
+    n = P.shape[0]
+    nc = fl.nc
+    out = dict(label=np.zeros(n, np.int8), x=np.zeros((nc, n)), y=np.zeros((nc, n)), sat_o=np.zeros(n),
+               sat_g=np.zeros(n), rho_o=np.zeros(n), rho_g=np.zeros(n))
+    rc = lib.ref_flash_batch(nc, fl.eos, _p(fl.tc), _p(fl.pc), _p(fl.acf), _p(fl.kij), ctypes.c_long(n), _p(P),
+                             _p(T), _p(z), _p(out["x"]), _p(out["y"]), _p(out["label"]), _p(out["sat_o"]),
+                             _p(out["sat_g"]), _p(out["rho_o"]), _p(out["rho_g"]))
+    if rc:
+        raise RuntimeError(f"ref_flash_batch returned {rc}")
+    return out
+
+
+def ref_solve_z(a1, a2, a3, gas: bool) -> float:
+    return ref_lib().ref_solve_z(a1, a2, a3, int(gas))
+
+
+def ref_eos_params(fl: Fluid, T: float):
+    lib = ref_lib()
+    a = np.zeros(fl.nc)
+    b = np.zeros(fl.nc)
+    rc = lib.ref_eos_params(fl.nc, fl.eos, _p(fl.tc), _p(fl.pc), _p(fl.acf), ctypes.c_double(T), _p(a), _p(b))
+    if rc:
+        raise RuntimeError("ref_eos_params failed")
+    return a, b
+
+
+R_GAS = 8.3144621
+
+
+def derived_sat_rho(fl_out, P, T):
+    """Oil/gas volume fractions and molar densities from L and Z, as the
+    reference's SuccFalsh forms them with zero water saturation
+    (compsim/Init_Calcs.cpp:730-736)."""
+    L, Zl, Zg = fl_out["L"], fl_out["Zl"], fl_out["Zg"]
+    newD = Zl * L / (Zl * L + Zg * (1 - L))
+    sat_o = newD * (1 - 0.0)
+    sat_g = (1 - newD) * (1 - 0.0)
+    rho_o = P / (Zl * R_GAS * T)
+    rho_g = P / (Zg * R_GAS * T)
+    return sat_o, sat_g, rho_o, rho_g

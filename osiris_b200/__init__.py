@@ -1,0 +1,176 @@
+"""osiris_b200: B200-native FP64 hot path of the Osiris reservoir simulator.
+
+The compute lives in the CUDA library ``_lib/libosiris_b200.so`` (C ABI:
+``include/osiris_b200.h``).  This module is a thin ctypes host mirror over
+that ABI; PyTorch only supplies device memory and streams.  There is no CPU
+fallback: every entry point raises if the library is missing or a call
+fails.
+
+Conventions (shared with the C ABI): per-cell scalars ``[n]``,
+per-component fields ``[nc, n]``, fugacity derivative blocks
+``[2, nc, nc, n]`` / ``[2, nc, n]`` with phase 0 = liquid, 1 = vapour; phase
+labels +1 liquid only, -1 vapour only, 0 two-phase.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from .build import INCLUDE, LIB
+
+__all__ = ["Fluid", "lib", "flash", "flash_host", "set_shape", "get_shape", "header_symbols", "OsrError",
+           "FLASH_OUTPUTS"]
+
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class OsrError(RuntimeError):
+    pass
+
+
+class _CFluid(ctypes.Structure):
+    _fields_ = [("nc", ctypes.c_int), ("eos", ctypes.c_int), ("tc", _vp), ("pc", _vp), ("acf", _vp),
+                ("kij", _vp)]
+
+
+class _CFlashOut(ctypes.Structure):
+    _fields_ = [("label", _vp), ("L", _vp), ("x", _vp), ("y", _vp), ("Zl", _vp), ("Zg", _vp), ("iters", _vp),
+                ("rr_iters", _vp), ("dlnphi_dx", _vp), ("dlnphi_dP", _vp)]
+
+
+FLASH_OUTPUTS = ("label", "L", "x", "y", "Zl", "Zg", "iters", "rr_iters", "dlnphi_dx", "dlnphi_dP")
+
+
+def header_symbols():
+    """Every function the public header declares."""
+    names = []
+    for h in sorted(os.listdir(INCLUDE)):
+        if h.endswith(".h"):
+            text = open(os.path.join(INCLUDE, h)).read()
+            names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z_0-9]*\s*\**\s*(osr_[a-z0-9_]+)\s*\(", text,
+                                flags=re.M)
+    return sorted(set(names))
+
+
+def lib():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise OsrError(f"{LIB} is missing: run `python -m osiris_b200.build` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB)
+        for name in header_symbols():
+            getattr(L, name)  # every declared entry point must resolve
+        L.osr_status_string.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        L = lib()
+        msg = L.osr_status_string(rc).decode()
+        raise OsrError(f"{what}: status {rc} ({msg}), cuda error {L.osr_last_cuda_error()}")
+
+
+class Fluid:
+    """Component table: Tc [K], Pc [Pa], acentric factor, kij (symmetric, zero
+    diagonal); eos 0 = Peng-Robinson, 1 = Soave-Redlich-Kwong."""
+
+    def __init__(self, tc, pc, acf, kij, eos: int):
+        self.tc = np.ascontiguousarray(tc, dtype=np.float64)
+        self.pc = np.ascontiguousarray(pc, dtype=np.float64)
+        self.acf = np.ascontiguousarray(acf, dtype=np.float64)
+        self.kij = np.ascontiguousarray(kij, dtype=np.float64)
+        self.nc = int(self.tc.shape[0])
+        self.eos = int(eos)
+        if self.kij.shape != (self.nc, self.nc):
+            raise ValueError("kij must be [nc, nc]")
+        self._c = _CFluid(self.nc, self.eos, self.tc.ctypes.data, self.pc.ctypes.data, self.acf.ctypes.data,
+                          self.kij.ctypes.data)
+
+    @property
+    def cref(self):
+        return ctypes.byref(self._c)
+
+
+def _out_struct(outs: dict, ptr):
+    return _CFlashOut(*[ptr(outs[k]) if outs.get(k) is not None else None for k in FLASH_OUTPUTS])
+
+
+def alloc_flash_outputs(nc: int, n: int, derivs: bool, device, iters: bool = True):
+    import torch
+    f64 = dict(dtype=torch.float64, device=device)
+    o = dict(label=torch.empty(n, dtype=torch.int8, device=device), L=torch.empty(n, **f64),
+             x=torch.empty(nc, n, **f64), y=torch.empty(nc, n, **f64), Zl=torch.empty(n, **f64),
+             Zg=torch.empty(n, **f64))
+    if iters:
+        o["iters"] = torch.empty(n, dtype=torch.int32, device=device)
+        o["rr_iters"] = torch.empty(n, dtype=torch.int32, device=device)
+    if derivs:
+        o["dlnphi_dx"] = torch.empty(2, nc, nc, n, **f64)
+        o["dlnphi_dP"] = torch.empty(2, nc, n, **f64)
+    return o
+
+
+def flash(fluid: Fluid, P, T, z, derivs: bool = True, form: str = "batched", out: dict | None = None,
+          stream=None, iters: bool = True):
+    """Flash cells held in device memory (torch CUDA float64 tensors P [n],
+    T [n], z [nc, n]).  Returns (or fills) a dict of device tensors.
+    Asynchronous on the current torch stream unless ``stream`` is given."""
+    import torch
+    n = int(P.shape[0])
+    for t in (P, T, z):
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise OsrError("P, T, z must be contiguous float64 CUDA tensors")
+    if z.shape != (fluid.nc, n):
+        raise OsrError("z must be [nc, n]")
+    if out is None:
+        out = alloc_flash_outputs(fluid.nc, n, derivs, P.device, iters)
+    if stream is None:
+        stream = torch.cuda.current_stream(P.device)
+    co = _out_struct(out, lambda t: t.data_ptr())
+    fn = {"batched": lib().osr_flash_batch, "plain": lib().osr_flash_batch_plain}[form]
+    rc = fn(fluid.cref, _vp(P.data_ptr()), _vp(T.data_ptr()), _vp(z.data_ptr()), ctypes.c_long(n),
+            ctypes.byref(co), _vp(stream.cuda_stream))
+    _check(rc, f"osr_flash_batch ({form})")
+    return out
+
+
+def flash_host(fluid: Fluid, P, T, z, derivs: bool = True, out: dict | None = None, iters: bool = True):
+    """End-to-end flash of host (numpy) arrays through osr_flash_batch_host.
+    Inputs may be pinned torch CPU tensors or numpy arrays."""
+    def host_ptr(a):
+        if hasattr(a, "data_ptr"):
+            return a.data_ptr()
+        return a.ctypes.data
+    n = int(P.shape[0])
+    nc = fluid.nc
+    if out is None:
+        out = dict(label=np.empty(n, np.int8), L=np.empty(n), x=np.empty((nc, n)), y=np.empty((nc, n)),
+                   Zl=np.empty(n), Zg=np.empty(n))
+        if iters:
+            out["iters"] = np.empty(n, np.int32)
+            out["rr_iters"] = np.empty(n, np.int32)
+        if derivs:
+            out["dlnphi_dx"] = np.empty((2, nc, nc, n))
+            out["dlnphi_dP"] = np.empty((2, nc, n))
+    co = _out_struct(out, host_ptr)
+    rc = lib().osr_flash_batch_host(fluid.cref, _vp(host_ptr(P)), _vp(host_ptr(T)), _vp(host_ptr(z)),
+                                    ctypes.c_long(n), ctypes.byref(co), None)
+    _check(rc, "osr_flash_batch_host")
+    return out
+
+
+def set_shape(ss_batch: int, ctas_per_sm: int):
+    _check(lib().osr_flash_set_shape(int(ss_batch), int(ctas_per_sm)), "osr_flash_set_shape")
+
+
+def get_shape():
+    a, b = ctypes.c_int(), ctypes.c_int()
+    _check(lib().osr_flash_get_shape(ctypes.byref(a), ctypes.byref(b)), "osr_flash_get_shape")
+    return a.value, b.value

@@ -1,0 +1,305 @@
+// Host side of the flash hot path: component-table preparation, template
+// dispatch on the component count, launches, and the C-ABI entry points
+// declared in include/osiris_b200.h.
+#include <cuda_runtime.h>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include "osiris_b200.h"
+#include "flash_kernels.cuh"
+
+namespace osr {
+
+static std::atomic<int> g_last_cuda{0};
+static std::atomic<int> g_ss_batch{20};
+static std::atomic<int> g_ctas_per_sm{4};
+
+static osr_status cuda_fail(cudaError_t e) {
+    g_last_cuda.store((int)e);
+    return OSR_ERR_CUDA;
+}
+
+#define OSR_CUDA(call)                              \
+    do {                                            \
+        cudaError_t e_ = (call);                    \
+        if (e_ != cudaSuccess) return cuda_fail(e_); \
+    } while (0)
+
+// Component table in the form the kernels read (see FluidTable).  The
+// temperature-independent EOS constants are formed here with the reference's
+// expressions (compsim/Init_Calcs.cpp:81-96).
+template <int N>
+static void make_table(const osr_fluid &fl, FluidTable<N> &t) {
+    std::memset(&t, 0, sizeof(t));
+    t.srk = fl.eos == OSR_EOS_SRK;
+    for (int i = 0; i < N; i++) {
+        double tc = fl.tc[i], pc = fl.pc[i], w = fl.acf[i];
+        t.pc[i] = pc;
+        t.tc[i] = tc;
+        t.wil[i] = 5.37 * (1 + w);
+        if (t.srk) {
+            t.ac[i] = 0.42747 * kR * kR * tc * tc / pc;
+            t.m[i] = 0.48508 + 1.55171 * w - 0.15613 * w * w;
+            t.b[i] = 0.08664 * kR * tc / pc;
+        } else {
+            t.ac[i] = 0.457235 * kR * kR * tc * tc / pc;
+            t.m[i] = 0.3796 + 1.485 * w - 0.1644 * w * w + 0.01667 * w * w * w;
+            t.b[i] = 0.077796 * kR * tc / pc;
+        }
+        for (int j = 0; j < N; j++) t.bic[i * N + j] = 1 - fl.kij[i * N + j];
+    }
+}
+
+static osr_status check_fluid(const osr_fluid *fl) {
+    if (!fl || !fl->tc || !fl->pc || !fl->acf || !fl->kij) return OSR_ERR_ARG;
+    if (fl->nc < 1 || fl->nc > OSR_MAX_NC) return OSR_ERR_NC;
+    if (fl->eos != OSR_EOS_PR && fl->eos != OSR_EOS_SRK) return OSR_ERR_ARG;
+    return OSR_OK;
+}
+
+static osr_status check_out(const osr_flash_out *o) {
+    if (!o || !o->label || !o->L || !o->x || !o->y || !o->Zl || !o->Zg) return OSR_ERR_ARG;
+    if ((o->dlnphi_dx == nullptr) != (o->dlnphi_dP == nullptr)) return OSR_ERR_ARG;
+    return OSR_OK;
+}
+
+// Library-private stream-ordered pool per device, keeping freed blocks for
+// reuse (release threshold = unlimited) so that repeated calls do not map and
+// unmap device memory; the process's default pool is left untouched.
+static cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&pools[dev], &props)) != cudaSuccess) return e;
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pools[dev], s);
+}
+
+static int sm_count() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) ==
+                                                       cudaSuccess)
+            cached = n;
+        else
+            cached = 148;
+    }
+    return cached;
+}
+
+enum class Form { kQueue, kPlain };
+
+template <int N>
+static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double *T, const double *z, long n,
+                              const osr_flash_out &o, cudaStream_t s, Form form,
+                              unsigned long long *counter) {
+    FlashArgs<N> a;
+    make_table<N>(fl, a.f);
+    a.io = FlashIO{P, T, z, n, o.label, o.L, o.x, o.y, o.Zl, o.Zg, o.iters, o.rr_iters};
+    a.counter = counter;
+    a.ss_batch = g_ss_batch.load();
+    if (n > 0) {
+        if (form == Form::kPlain) {
+            unsigned blocks = (unsigned)((n + 127) / 128);
+            flash_plain_kernel<N><<<blocks, 128, 0, s>>>(a);
+        } else {
+            long warps_needed = (n + 31) / 32;
+            int per_sm = g_ctas_per_sm.load(), fit = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N>, 128, 0) ==
+                    cudaSuccess && fit > 0 && per_sm > fit)
+                per_sm = fit;
+            long blocks = (long)sm_count() * per_sm;
+            long max_blocks = (warps_needed + 3) / 4;
+            if (blocks > max_blocks) blocks = max_blocks;
+            if (blocks < 1) blocks = 1;
+            flash_queue_kernel<N><<<(unsigned)blocks, 128, 0, s>>>(a);
+        }
+        OSR_CUDA(cudaGetLastError());
+        if (o.dlnphi_dx) {
+            DerivArgs<N> d;
+            d.f = a.f;
+            d.P = P;
+            d.T = T;
+            d.x = o.x;
+            d.y = o.y;
+            d.Zl = o.Zl;
+            d.Zg = o.Zg;
+            d.n = n;
+            d.dlnphi_dx = o.dlnphi_dx;
+            d.dlnphi_dP = o.dlnphi_dP;
+            long blocks = (n + 127) / 128;
+            long cap = (long)sm_count() * 8;
+            if (blocks > cap) blocks = cap;
+            flash_deriv_kernel<N><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+            OSR_CUDA(cudaGetLastError());
+        }
+    }
+    return OSR_OK;
+}
+
+static osr_status run_flash(const osr_fluid &fl, const double *P, const double *T, const double *z, long n,
+                            const osr_flash_out &o, cudaStream_t s, Form form, unsigned long long *counter) {
+    switch (fl.nc) {
+#define OSR_NC_CASE(K) \
+    case K: return run_flash_n<K>(fl, P, T, z, n, o, s, form, counter);
+        OSR_NC_CASE(1) OSR_NC_CASE(2) OSR_NC_CASE(3) OSR_NC_CASE(4) OSR_NC_CASE(5) OSR_NC_CASE(6)
+        OSR_NC_CASE(7) OSR_NC_CASE(8) OSR_NC_CASE(9) OSR_NC_CASE(10) OSR_NC_CASE(11) OSR_NC_CASE(12)
+        OSR_NC_CASE(13) OSR_NC_CASE(14) OSR_NC_CASE(15) OSR_NC_CASE(16)
+#undef OSR_NC_CASE
+        default: return OSR_ERR_NC;
+    }
+}
+
+static osr_status flash_device(const osr_fluid *fluid, const double *P, const double *T, const double *z, long n,
+                               const osr_flash_out *out, void *stream, Form form) {
+    osr_status st = check_fluid(fluid);
+    if (st) return st;
+    if ((st = check_out(out))) return st;
+    if (n < 0 || (n > 0 && (!P || !T || !z))) return OSR_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long *counter = nullptr;
+    if (form == Form::kQueue && n > 0) {
+        OSR_CUDA(pool_alloc((void **)&counter, sizeof(unsigned long long), s));
+        cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(counter, s);
+            return cuda_fail(e);
+        }
+    }
+    st = run_flash(*fluid, P, T, z, n, *out, s, form, counter);
+    if (counter) {
+        cudaError_t e = cudaFreeAsync(counter, s);
+        if (st == OSR_OK && e != cudaSuccess) return cuda_fail(e);
+    }
+    return st;
+}
+
+}  // namespace osr
+
+using namespace osr;
+
+extern "C" {
+
+osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z, long n,
+                           const osr_flash_out *out, void *stream) {
+    return flash_device(fluid, d_P, d_T, d_z, n, out, stream, Form::kQueue);
+}
+
+osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
+                                 long n, const osr_flash_out *out, void *stream) {
+    return flash_device(fluid, d_P, d_T, d_z, n, out, stream, Form::kPlain);
+}
+
+osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const double *T, const double *z, long n,
+                                const osr_flash_out *out, void *stream) {
+    osr_status st = check_fluid(fluid);
+    if (st) return st;
+    if ((st = check_out(out))) return st;
+    if (n < 0 || (n > 0 && (!P || !T || !z))) return OSR_ERR_ARG;
+    if (n == 0) return OSR_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nc = fluid->nc;
+    const bool derivs = out->dlnphi_dx != nullptr;
+    // one device block: inputs, then outputs, 256-byte aligned pieces
+    size_t nd = (size_t)n;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t szP = al(nd * 8), szz = al(nd * nc * 8), szl = al(nd), szi = al(nd * 4);
+    size_t szdx = derivs ? al(nd * 2 * nc * nc * 8) : 0, szdp = derivs ? al(nd * 2 * nc * 8) : 0;
+    size_t total = 2 * szP + szz + szl + szP + 2 * szz + 2 * szP + 2 * szi + szdx + szdp;
+    char *base = nullptr;
+    OSR_CUDA(pool_alloc((void **)&base, total, s));
+    char *p = base;
+    auto take = [&](size_t sz) { char *r = p; p += sz; return r; };
+    double *dP = (double *)take(szP), *dT = (double *)take(szP), *dz = (double *)take(szz);
+    osr_flash_out d{};
+    d.label = (signed char *)take(szl);
+    d.L = (double *)take(szP);
+    d.x = (double *)take(szz);
+    d.y = (double *)take(szz);
+    d.Zl = (double *)take(szP);
+    d.Zg = (double *)take(szP);
+    int *di = (int *)take(szi), *dr = (int *)take(szi);
+    d.iters = out->iters ? di : nullptr;
+    d.rr_iters = out->rr_iters ? dr : nullptr;
+    if (derivs) {
+        d.dlnphi_dx = (double *)take(szdx);
+        d.dlnphi_dP = (double *)take(szdp);
+    }
+    cudaError_t e = cudaSuccess;
+    auto h2d = [&](void *dst, const void *src, size_t b) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, s);
+    };
+    auto d2h = [&](void *dst, const void *src, size_t b) {
+        if (e == cudaSuccess && dst) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s);
+    };
+    h2d(dP, P, nd * 8);
+    h2d(dT, T, nd * 8);
+    h2d(dz, z, nd * nc * 8);
+    if (e == cudaSuccess) st = flash_device(fluid, dP, dT, dz, n, &d, stream, Form::kQueue);
+    d2h(out->label, d.label, nd);
+    d2h(out->L, d.L, nd * 8);
+    d2h(out->x, d.x, nd * nc * 8);
+    d2h(out->y, d.y, nd * nc * 8);
+    d2h(out->Zl, d.Zl, nd * 8);
+    d2h(out->Zg, d.Zg, nd * 8);
+    if (out->iters) d2h(out->iters, d.iters, nd * 4);
+    if (out->rr_iters) d2h(out->rr_iters, d.rr_iters, nd * 4);
+    if (derivs) {
+        d2h(out->dlnphi_dx, d.dlnphi_dx, nd * 2 * nc * nc * 8);
+        d2h(out->dlnphi_dP, d.dlnphi_dP, nd * 2 * nc * 8);
+    }
+    cudaError_t ef = cudaFreeAsync(base, s);
+    cudaError_t es = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (st != OSR_OK) return st;
+    if (ef != cudaSuccess) return cuda_fail(ef);
+    if (es != cudaSuccess) return cuda_fail(es);
+    return OSR_OK;
+}
+
+osr_status osr_flash_set_shape(int ss_batch, int ctas_per_sm) {
+    if (ss_batch < 1 || ss_batch > 32 || ctas_per_sm < 1 || ctas_per_sm > 16) return OSR_ERR_ARG;
+    g_ss_batch.store(ss_batch);
+    g_ctas_per_sm.store(ctas_per_sm);
+    return OSR_OK;
+}
+
+osr_status osr_flash_get_shape(int *ss_batch, int *ctas_per_sm) {
+    if (!ss_batch || !ctas_per_sm) return OSR_ERR_ARG;
+    *ss_batch = g_ss_batch.load();
+    *ctas_per_sm = g_ctas_per_sm.load();
+    return OSR_OK;
+}
+
+const char *osr_status_string(osr_status s) {
+    switch (s) {
+        case OSR_OK: return "ok";
+        case OSR_ERR_ARG: return "invalid argument";
+        case OSR_ERR_NC: return "component count outside 1..16";
+        case OSR_ERR_CUDA: return "CUDA runtime error";
+        case OSR_ERR_NODEVICE: return "no suitable CUDA device";
+        case OSR_ERR_SIZE: return "request exceeds the entry point's size limit";
+    }
+    return "unknown status";
+}
+
+int osr_last_cuda_error(void) { return g_last_cuda.load(); }
+int osr_version(void) { return OSR_VERSION; }
+
+}  // extern "C"

@@ -1,0 +1,378 @@
+// Successive-substitution flash with an inner Rachford-Rice Newton, and the
+// fugacity-derivative pass, as FP64 CUDA kernels for sm_100a.
+//
+// Algorithm: the reference's SuccFalsh (compsim/Init_Calcs.cpp:571-738):
+//   K_i = Pc_i/P exp(5.37 (1 + w_i)(1 - Tc_i/T))                (Wilson)
+//   repeat (at most 500 times, until |L_k - L_{k-1}| <= 1e-14):
+//     L = 0.6; Newton on sum_i z_i (1-K_i)/(L + (1-L) K_i) = 0
+//       (at most 100 steps, until step^2 <= 1e-8); clamp L to [0,1]
+//     x_i = z_i/(L + K_i (1-L)), y_i = K_i x_i    (K_i < 0 flags a component
+//       the vapour cannot hold: x_i = 0, y_i = z_i/(1-L))
+//     Z_l, Z_v from the cubic; K_i *= x_i phi_i^L / (y_i phi_i^V)
+//   label = -1 (vapour only) if |L| < 1e-20, +1 (liquid only) if |1-L| < 1e-20,
+//   else 0 (two-phase).
+//
+// Work distribution.  Per-cell cost is heavy-tailed (most single-phase cells
+// need 2-3 substitution steps, two-phase cells tens to hundreds, and each step
+// runs 1 to 100 Newton steps), so a thread-per-cell grid would idle most lanes
+// of a warp behind its slowest cell.  The batched kernel is persistent: every
+// lane runs a small state machine (fetch cell -> Newton steps -> substitution
+// step -> ...), claims a new cell from a global work counter as soon as its
+// cell converges, and the warp runs the expensive substitution step only when
+// enough lanes are ready for it, so that step executes with most lanes busy.
+// The plain kernel (one thread per cell, no queue) is kept as the baseline the
+// batched form is measured against.
+#pragma once
+#include "eos_device.cuh"
+
+namespace osr {
+
+// Device pointers of one flash batch.  Per-component fields are [nc][n].
+struct FlashIO {
+    const double *P, *T, *z;
+    long n;
+    signed char *label;
+    double *L, *x, *y, *Zl, *Zg;
+    int *iters, *rr_iters;  // optional (may be null)
+};
+
+template <int N>
+struct FlashArgs {
+    FluidTable<N> f;
+    FlashIO io;
+    unsigned long long *counter;  // work-queue head; must be zero at launch
+    int ss_batch;                 // ready lanes needed before a substitution step runs
+};
+
+// One Rachford-Rice Newton step (compsim/Init_Calcs.cpp:595-605).  Returns
+// the step t; L is updated in place.
+template <int N>
+__device__ __forceinline__ double rr_step(const double *K, const double *z, double &L) {
+    double F = 0, dF = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        double td = (K[i] >= 0) ? (1 - K[i]) / (L + (1 - L) * K[i]) : 1 / (L - 1);
+        double zt = z[i] * td;
+        F += zt;
+        dF -= zt * td;
+    }
+    double t = F / dF;
+    L -= t;
+    return t;
+}
+
+// One substitution step after the Newton loop: clamp L, form x, y, solve both
+// cubics and update K (compsim/Init_Calcs.cpp:608-712).  Returns |Lb - L|.
+template <int N>
+__device__ __forceinline__ double ss_update(const FluidTable<N> &f, const double *sa, double P, double T,
+                                            const double *z, double *K, double &L, double &Lb, double *x,
+                                            double *y, double &Zl, double &Zg) {
+    if (L > 1) L = 1;
+    else if (L < 0) L = 0;
+    double es = fabs(Lb - L);
+    Lb = L;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (K[i] >= 0) {
+            x[i] = z[i] / (L + K[i] * (1 - L));
+            y[i] = K[i] * x[i];
+        } else {
+            x[i] = 0;
+            y[i] = z[i] / (1 - L);
+        }
+    }
+    // Mixing rule: with u_i = w_i sqrt(a_i) and v_i = sum_j (1-k_ij) u_j,
+    // sum_i sum_j w_i w_j sqrt(a_i a_j)(1-k_ij) = sum_i u_i v_i and the
+    // per-component sums sum_j w_j sqrt(a_i a_j)(1-k_ij) = sqrt(a_i) v_i.
+    double ul[N], ug[N], vl[N], vg[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        ul[i] = x[i] * sa[i];
+        ug[i] = y[i] * sa[i];
+    }
+    double Cal = 0, Cag = 0, Cbl = 0, Cbg = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        double sl = 0, sg = 0;
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            sl += f.bic[i * N + j] * ul[j];
+            sg += f.bic[i * N + j] * ug[j];
+        }
+        vl[i] = sl;
+        vg[i] = sg;
+        Cal += ul[i] * sl;
+        Cag += ug[i] * sg;
+        Cbl += x[i] * f.b[i];
+        Cbg += y[i] * f.b[i];
+    }
+    const double pa = P / (kR * kR * T * T), pb = P / (kR * T);
+    double Al = Cal * pa, Bl = Cbl * pb, Ag = Cag * pa, Bg = Cbg * pb;
+    const bool srk = f.srk != 0;
+    Zl = phase_z(Al, Bl, srk, false);
+    Zg = phase_z(Ag, Bg, srk, true);
+    const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
+    // i-independent parts of ln(phi_i) (the reference re-evaluates them per i)
+    double DDl = Al / (Bl * (d1 - d2)), DDg = Ag / (Bg * (d1 - d2));
+    double FFl = log((Zl + d2 * Bl) / (Zl + d1 * Bl)), FFg = log((Zg + d2 * Bg) / (Zg + d1 * Bg));
+    double cl = log(Zl - Bl), cg = log(Zg - Bg);
+    double rCal = 2 / Cal, rCag = 2 / Cag, rCbl = 1 / Cbl, rCbg = 1 / Cbg;
+    double DFl = DDl * FFl, DFg = DDg * FFg;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        double t1l = f.b[i] * rCbl, t1g = f.b[i] * rCbg;
+        double EEl = sa[i] * vl[i] * rCal - t1l;
+        double EEg = sa[i] * vg[i] * rCag - t1g;
+        double phiL = exp(t1l * (Zl - 1) - cl + DFl * EEl);
+        double phiG = exp(t1g * (Zg - 1) - cg + DFg * EEg);
+        double fL = x[i] * phiL, fG = y[i] * phiG;
+        if (z[i] != 0) {
+            if (fG != 0) K[i] *= fL / fG;
+            else K[i] = -1;
+            if (fL != fL) K[i] = -1;
+            if (fG != fG) K[i] = 1;
+        }
+    }
+    return es;
+}
+
+template <int N>
+__device__ __forceinline__ void flash_init(const FluidTable<N> &f, double P, double T, double *K, double *sa) {
+#pragma unroll
+    for (int i = 0; i < N; i++) K[i] = (f.pc[i] / P) * exp(f.wil[i] * (1 - f.tc[i] / T));
+    sqrt_a<N>(f, T, sa);
+}
+
+__device__ __forceinline__ signed char flash_label(double L) {
+    if (fabs(L) < kLZero) return -1;
+    if (fabs(1 - L) < kLZero) return 1;
+    return 0;
+}
+
+template <int N>
+__device__ __forceinline__ void flash_store(const FlashIO &io, long c, double L, const double *x, const double *y,
+                                            double Zl, double Zg, int k, int rr) {
+    io.label[c] = flash_label(L);
+    io.L[c] = L;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        io.x[(long)i * io.n + c] = x[i];
+        io.y[(long)i * io.n + c] = y[i];
+    }
+    io.Zl[c] = Zl;
+    io.Zg[c] = Zg;
+    if (io.iters) io.iters[c] = k;
+    if (io.rr_iters) io.rr_iters[c] = rr;
+}
+
+// Plain form: one thread per cell, the whole iteration in one thread.
+template <int N>
+__global__ void __launch_bounds__(128) flash_plain_kernel(const __grid_constant__ FlashArgs<N> a) {
+    long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.io.n) return;
+    const FlashIO &io = a.io;
+    double P = io.P[c], T = io.T[c];
+    double z[N], K[N], sa[N], x[N], y[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
+    flash_init<N>(a.f, P, T, K, sa);
+    double L = 0, Lb = 10, Zl = 0, Zg = 0, es;
+    int k = 0, rr = 0;
+    do {
+        L = 0.6;
+        int j = 0;
+        double t;
+        do {
+            t = rr_step<N>(K, z, L);
+            j++;
+        } while ((t * t > kRRTol) && (j < kRRMaxIt));
+        rr += j;
+        es = ss_update<N>(a.f, sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
+        k++;
+    } while ((es > kSSTol) && (k < kSSMaxIt));
+    flash_store<N>(io, c, L, x, y, Zl, Zg, k, rr);
+}
+
+enum : int { kFetch = 0, kNewton = 1, kReady = 2, kDone = 3 };
+
+// Batched form: persistent warps, per-lane state machine, global work queue.
+template <int N>
+__global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant__ FlashArgs<N> a) {
+    constexpr unsigned kFull = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const FlashIO &io = a.io;
+    int mode = kFetch;
+    long c = -1;
+    double P = 0, T = 0, L = 0, Lb = 10;
+    double z[N], K[N], sa[N];
+    int j = 0, k = 0, rr = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) z[i] = K[i] = sa[i] = 0;
+    for (;;) {
+        unsigned need = __ballot_sync(kFull, mode == kFetch);
+        if (need) {
+            int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(a.counter, (unsigned long long)__popc(need));
+            base = __shfl_sync(kFull, base, leader);
+            if (mode == kFetch) {
+                long cc = (long)base + __popc(need & ((1u << lane) - 1));
+                if (cc < io.n) {
+                    c = cc;
+                    P = io.P[c];
+                    T = io.T[c];
+#pragma unroll
+                    for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
+                    flash_init<N>(a.f, P, T, K, sa);
+                    L = 0.6;
+                    Lb = 10;
+                    j = 0;
+                    k = 0;
+                    rr = 0;
+                    mode = kNewton;
+                } else {
+                    mode = kDone;
+                }
+            }
+        }
+        if (__ballot_sync(kFull, mode != kDone) == 0) break;
+        if (mode == kNewton) {
+            double t = rr_step<N>(K, z, L);
+            j++;
+            if (!((t * t > kRRTol) && (j < kRRMaxIt))) mode = kReady;
+        }
+        unsigned ready = __ballot_sync(kFull, mode == kReady);
+        unsigned newton = __ballot_sync(kFull, mode == kNewton);
+        if (ready != 0 && (__popc(ready) >= a.ss_batch || newton == 0)) {
+            if (mode == kReady) {
+                double x[N], y[N], Zl, Zg;
+                double es = ss_update<N>(a.f, sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
+                rr += j;
+                k++;
+                if ((es > kSSTol) && (k < kSSMaxIt)) {
+                    L = 0.6;
+                    j = 0;
+                    mode = kNewton;
+                } else {
+                    flash_store<N>(io, c, L, x, y, Zl, Zg, k, rr);
+                    mode = kFetch;
+                }
+            }
+        }
+    }
+}
+
+// Fugacity derivatives for both phases of every cell, following the
+// reference's fugacity rows of the analytic Jacobian
+// (compsim/Petsc_Functions.cpp:30243-30372) with dZ/dP, dZ/dw_k from the
+// implicit derivative of the cubic (compsim/Do_Cycle.cpp:517-552):
+//   dlnphi_dx[ph][i][k][c] = d ln phi_i / d w_k,  dlnphi_dP[ph][i][c].
+template <int N>
+struct DerivArgs {
+    FluidTable<N> f;
+    const double *P, *T, *x, *y, *Zl, *Zg;
+    long n;
+    double *dlnphi_dx, *dlnphi_dP;
+};
+
+template <int N>
+__device__ __forceinline__ void phase_derivs(const FluidTable<N> &f, const double *sa, double P, double T,
+                                             const double *w, double Z, double *out_dx, double *out_dp, long n,
+                                             long c) {
+    double u[N], v[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) u[i] = w[i] * sa[i];
+    double Ca = 0, Cb = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < N; j++) s += f.bic[i * N + j] * u[j];
+        v[i] = s;  // sum_j w_j sqrt(a_i a_j)(1-k_ij) = sa[i] * v[i]
+        Ca += u[i] * s;
+        Cb += w[i] * f.b[i];
+    }
+    const bool srk = f.srk != 0;
+    const double rt = kR * T;
+    const double pa = P / (rt * rt), pb = P / rt;
+    double A = Ca * pa, B = Cb * pb;
+    double dAdp = Ca / (rt * rt), dBdp = Cb / rt;
+    double U = srk ? B : 2 * B, W = srk ? 0.0 : B;
+    double dUdp = srk ? dBdp : 2 * dBdp, dWdp = srk ? 0.0 : dBdp;
+    const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
+    double rden = 1 / (3 * Z * Z - 2 * Z * (1 + B - U) + A - B * U - U - W * W);
+    // coefficients of the implicit derivative dZ = -(cA dA + cB dB + cU dU + cW dW)/den
+    double cA = Z - B, cB = -Z * Z - U * Z - A + W * W, cU = Z * Z - B * Z - Z, cW = -2 * W * Z + 2 * B * W + 2 * W;
+    double dZdp = -(dAdp * cA + dBdp * cB + dUdp * cU + dWdp * cW) * rden;
+    double DD = A / (B * (d1 - d2));
+    double FF = log((Z + d2 * B) / (Z + d1 * B));
+    double rZB = 1 / (Z - B), rZ1 = 1 / (Z + d1 * B), rZ2 = 1 / (Z + d2 * B);
+    double rCa = 1 / Ca, rCb = 1 / Cb;
+    double dDDdp = (B * dAdp - A * dBdp) / (B * B * (d1 - d2));
+    double dFFdp = (dZdp + d2 * dBdp) * rZ2 - (dZdp + d1 * dBdp) * rZ1;
+    double dBBdp = (dBdp - dZdp) * rZB;
+    // Per-k factors of d ln(phi_i)/d w_k.  Expanding the reference's
+    //   dAA + dBB + dDD EE FF + DD dEE FF + DD EE dFF
+    // with dAA = -b_k t1 (Z-1)/Cb + t1 dZ_k, dBB = (dB_k - dZ_k)/(Z-B),
+    // dEE = 2 a_ik/Ca - 2 t_i dA_k/(pa Ca^2) + t1 b_k/Cb  (t1 = b_i/Cb) gives
+    //   t1 P1_k + P2_k + EE P3_k + (2 DD FF/Ca) a_ik - g_i P4_k.
+    double P1[N], P2[N], P3[N], P4[N];
+    const double twopa = 2 * pa;
+    const double rBB = 1 / (B * B * (d1 - d2));
+    const double DF = DD * FF;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        double dA = sa[k] * v[k] * twopa;
+        double dB = f.b[k] * pb;
+        double dU = srk ? dB : 2 * dB, dW = srk ? 0.0 : dB;
+        double dZ = -(dA * cA + dB * cB + dU * cU + dW * cW) * rden;
+        double dDD = (dA * B - dB * A) * rBB;
+        double dFF = (dZ + d2 * dB) * rZ2 - (dZ + d1 * dB) * rZ1;
+        P1[k] = dZ - f.b[k] * (Z - 1) * rCb + DF * f.b[k] * rCb;
+        P2[k] = (dB - dZ) * rZB;
+        P3[k] = dDD * FF + DD * dFF;
+        P4[k] = DF * dA;
+    }
+    const double rpa = 1 / pa;
+    const double h = 2 * DF * rCa;
+#pragma unroll 1
+    for (int i = 0; i < N; i++) {
+        double sai = 0, vi = 0, bi = 0;
+        // select sa[i], v[i], b[i] without dynamic register indexing
+#pragma unroll
+        for (int q = 0; q < N; q++)
+            if (q == i) { sai = sa[q]; vi = v[q]; bi = f.b[q]; }
+        double ti = sai * vi;
+        double t1 = bi * rCb;
+        double EE = 2 * ti * rCa - t1;
+        out_dp[(long)i * n + c] = t1 * dZdp + dBBdp + EE * (dDDdp * FF + DD * dFFdp);
+        double g = 2 * ti * rCa * rCa * rpa;
+        double hs = h * sai;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            out_dx[((long)i * N + k) * n + c] =
+                t1 * P1[k] + P2[k] + EE * P3[k] + hs * sa[k] * f.bic[i * N + k] - g * P4[k];
+        }
+    }
+}
+
+// One thread per (cell, phase); blockIdx.y selects the phase.
+template <int N>
+__global__ void __launch_bounds__(128) flash_deriv_kernel(const __grid_constant__ DerivArgs<N> a) {
+    const int ph = blockIdx.y;
+    const double *comp = ph ? a.y : a.x;
+    const double *Zp = ph ? a.Zg : a.Zl;
+    double *odx = a.dlnphi_dx + (long)ph * N * N * a.n;
+    double *odp = a.dlnphi_dP + (long)ph * N * a.n;
+    long stride = (long)gridDim.x * blockDim.x;
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += stride) {
+        double sa[N], w[N];
+        double T = a.T[c];
+        sqrt_a<N>(a.f, T, sa);
+#pragma unroll
+        for (int i = 0; i < N; i++) w[i] = comp[(long)i * a.n + c];
+        phase_derivs<N>(a.f, sa, a.P[c], T, w, Zp[c], odx, odp, a.n, c);
+    }
+}
+
+}  // namespace osr
