@@ -133,14 +133,18 @@ def test_full_size_properties(cuda_device):
     fl = oracle.Fluid(tc, pc, acf, kij, eos)
     g = _run_gpu(fl, P, T, z, derivs=False)
     two = g["label"] == 0
-    # converged two-phase cells: compositions sum to one, material balance z = L x + (1-L) y
+    # converged two-phase cells: material balance z = L x + (1-L) y holds to
+    # rounding; compositions sum to one up to the truncation of the reference's
+    # Rachford-Rice Newton (stops once step^2 <= 1e-8; the oracle's own
+    # |sum x - 1| reaches 4e-7 on 1e5 of these cells)
     conv = two & (g["iters"] < 500)
     sx = g["x"][:, conv].sum(axis=0)
     sy = g["y"][:, conv].sum(axis=0)
-    assert np.abs(sx - 1).max() < 1e-8 and np.abs(sy - 1).max() < 1e-8
+    assert np.abs(sx - 1).max() < 1e-5 and np.abs(sy - 1).max() < 1e-5
+    assert np.median(np.abs(sx - 1)) < 1e-11
     L = g["L"][conv]
     bal = L * g["x"][:, conv] + (1 - L) * g["y"][:, conv] - z[:, conv]
-    assert np.abs(bal).max() < 1e-8
+    assert np.abs(bal).max() < 1e-12
     # single-phase cells: L clamped exactly, feed carried by the present phase
     assert np.all(g["L"][g["label"] == 1] == 1.0) and np.all(g["L"][g["label"] == -1] == 0.0)
     assert np.array_equal(g["x"][:, g["label"] == 1], z[:, g["label"] == 1])
