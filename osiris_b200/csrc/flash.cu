@@ -170,8 +170,10 @@ static osr_status flash_device(const osr_fluid *fluid, const double *P, const do
                                const osr_flash_out *out, void *stream, Form form) {
     osr_status st = check_fluid(fluid);
     if (st) return st;
+    if (!out || n < 0) return OSR_ERR_ARG;
+    if (n == 0) return OSR_OK;  // nothing to do; output pointers may be null
     if ((st = check_out(out))) return st;
-    if (n < 0 || (n > 0 && (!P || !T || !z))) return OSR_ERR_ARG;
+    if (!P || !T || !z) return OSR_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     unsigned long long *counter = nullptr;
     if (form == Form::kQueue && n > 0) {
@@ -210,9 +212,10 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
                                 const osr_flash_out *out, void *stream) {
     osr_status st = check_fluid(fluid);
     if (st) return st;
-    if ((st = check_out(out))) return st;
-    if (n < 0 || (n > 0 && (!P || !T || !z))) return OSR_ERR_ARG;
+    if (!out || n < 0) return OSR_ERR_ARG;
     if (n == 0) return OSR_OK;
+    if ((st = check_out(out))) return st;
+    if (!P || !T || !z) return OSR_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int nc = fluid->nc;
     const bool derivs = out->dlnphi_dx != nullptr;
