@@ -70,8 +70,9 @@ typedef struct osr_flash_out {
  * derivative outputs restate the fugacity rows of IteratorJacobian
  * (compsim/Petsc_Functions.cpp:30243-30372).  d_P [n] Pa, d_T [n] K, d_z
  * [nc][n] feed mole fractions.  Asynchronous on `stream` (a cudaStream_t,
- * NULL = legacy default stream).  Allocates a few bytes of stream-ordered
- * scratch (the work-queue counter) per call. */
+ * NULL = legacy default stream).  Takes stream-ordered scratch from a
+ * library-private pool per call: work-queue heads and a parked-cell list
+ * of (32 + 8 nc) bytes per cell. */
 osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
                            long n, const osr_flash_out *out, void *stream);
 
@@ -87,12 +88,17 @@ osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, cons
 osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const double *T, const double *z,
                                 long n, const osr_flash_out *out, void *stream);
 
-/* Launch-shape knobs of the batched flash (the autotuner sets them):
- * ss_batch = ready lanes of a warp needed before the substitution step runs
- * (1..32), ctas_per_sm = persistent CTAs of 128 threads per SM (1..16).
- * Values outside the ranges are rejected.  Process-wide. */
-osr_status osr_flash_set_shape(int ss_batch, int ctas_per_sm);
-osr_status osr_flash_get_shape(int *ss_batch, int *ctas_per_sm);
+/* Launch-shape knobs of the batched flash (the autotuner sets them).
+ * The batched form runs two passes of a persistent kernel: the first takes
+ * every cell and parks those still running after park_after substitution
+ * steps (0 = never park); the second resumes the parked cells, heaviest
+ * predicted first.  ss_batch / tail_batch = ready lanes of a warp needed
+ * before the substitution step runs in the first / second pass (1..32);
+ * ctas_per_sm = persistent CTAs of 128 threads per SM (1..16, capped by
+ * occupancy); park_after in 0..500.  Values outside the ranges are
+ * rejected.  Process-wide. */
+osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, int park_after);
+osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm, int *park_after);
 
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The

@@ -166,11 +166,12 @@ def flash_host(fluid: Fluid, P, T, z, derivs: bool = True, out: dict | None = No
     return out
 
 
-def set_shape(ss_batch: int, ctas_per_sm: int):
-    _check(lib().osr_flash_set_shape(int(ss_batch), int(ctas_per_sm)), "osr_flash_set_shape")
+def set_shape(ss_batch: int, tail_batch: int, ctas_per_sm: int, park_after: int):
+    _check(lib().osr_flash_set_shape(int(ss_batch), int(tail_batch), int(ctas_per_sm), int(park_after)),
+           "osr_flash_set_shape")
 
 
 def get_shape():
-    a, b = ctypes.c_int(), ctypes.c_int()
-    _check(lib().osr_flash_get_shape(ctypes.byref(a), ctypes.byref(b)), "osr_flash_get_shape")
-    return a.value, b.value
+    v = [ctypes.c_int() for _ in range(4)]
+    _check(lib().osr_flash_get_shape(*[ctypes.byref(x) for x in v]), "osr_flash_get_shape")
+    return tuple(x.value for x in v)

@@ -14,7 +14,9 @@ namespace osr {
 
 static std::atomic<int> g_last_cuda{0};
 static std::atomic<int> g_ss_batch{20};
+static std::atomic<int> g_tail_batch{32};
 static std::atomic<int> g_ctas_per_sm{4};
+static std::atomic<int> g_park_after{8};
 
 static osr_status cuda_fail(cudaError_t e) {
     g_last_cuda.store((int)e);
@@ -105,59 +107,125 @@ static int sm_count() {
 
 enum class Form { kQueue, kPlain };
 
+// Scratch of the batched form, carved from one device block:
+//   header (1 KiB): first-pass head, second-pass head, parked count,
+//                   key histogram, scatter cursors -- zeroed per call;
+//   parked-cell list with room for every cell (cell, k, rr, key, order, Lb, K).
+struct ScratchLayout {
+    size_t head1 = 0, head2 = 8, count = 16, hist = 256, cursor = 512, header = 1024;
+    size_t cell, k, rr, key, order, Lb, K, total;
+    ScratchLayout(long cap, int nc) {
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        size_t c = (size_t)cap;
+        cell = header;
+        k = cell + al(c * 8);
+        rr = k + al(c * 4);
+        key = rr + al(c * 4);
+        order = key + al(c * 4);
+        Lb = order + al(c * 4);
+        K = Lb + al(c * 8);
+        total = K + al(c * 8 * (size_t)nc);
+    }
+};
+
+static size_t queue_scratch_bytes(long n, int nc) { return ScratchLayout(n, nc).total; }
+
+static ParkList park_view(char *base, long cap, int nc) {
+    ScratchLayout L(cap, nc);
+    ParkList p;
+    p.cell = (long *)(base + L.cell);
+    p.k = (int *)(base + L.k);
+    p.rr = (int *)(base + L.rr);
+    p.key = (int *)(base + L.key);
+    p.order = (int *)(base + L.order);
+    p.Lb = (double *)(base + L.Lb);
+    p.K = (double *)(base + L.K);
+    p.cap = cap;
+    p.count = (unsigned *)(base + L.count);
+    p.hist = (unsigned *)(base + L.hist);
+    p.cursor = (unsigned *)(base + L.cursor);
+    return p;
+}
+
+template <int N>
+static int queue_blocks(long n) {
+    long warps_needed = (n + 31) / 32;
+    int per_sm = g_ctas_per_sm.load(), fit = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N>, 128, 0) == cudaSuccess &&
+        fit > 0 && per_sm > fit)
+        per_sm = fit;
+    long blocks = (long)sm_count() * per_sm;
+    long max_blocks = (warps_needed + 3) / 4;
+    if (blocks > max_blocks) blocks = max_blocks;
+    if (blocks < 1) blocks = 1;
+    return (int)blocks;
+}
+
 template <int N>
 static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double *T, const double *z, long n,
-                              const osr_flash_out &o, cudaStream_t s, Form form,
-                              unsigned long long *counter) {
-    FlashArgs<N> a;
-    make_table<N>(fl, a.f);
-    a.io = FlashIO{P, T, z, n, o.label, o.L, o.x, o.y, o.Zl, o.Zg, o.iters, o.rr_iters};
-    a.counter = counter;
-    a.ss_batch = g_ss_batch.load();
-    if (n > 0) {
-        if (form == Form::kPlain) {
-            unsigned blocks = (unsigned)((n + 127) / 128);
-            flash_plain_kernel<N><<<blocks, 128, 0, s>>>(a);
-        } else {
-            long warps_needed = (n + 31) / 32;
-            int per_sm = g_ctas_per_sm.load(), fit = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N>, 128, 0) ==
-                    cudaSuccess && fit > 0 && per_sm > fit)
-                per_sm = fit;
-            long blocks = (long)sm_count() * per_sm;
-            long max_blocks = (warps_needed + 3) / 4;
-            if (blocks > max_blocks) blocks = max_blocks;
-            if (blocks < 1) blocks = 1;
-            flash_queue_kernel<N><<<(unsigned)blocks, 128, 0, s>>>(a);
-        }
+                              const osr_flash_out &o, cudaStream_t s, Form form, char *scratch) {
+    FluidTable<N> table;
+    make_table<N>(fl, table);
+    FlashIO io{P, T, z, n, o.label, o.L, o.x, o.y, o.Zl, o.Zg, o.iters, o.rr_iters};
+    if (form == Form::kPlain) {
+        FlashArgs<N> a;
+        a.f = table;
+        a.io = io;
+        unsigned blocks = (unsigned)((n + 127) / 128);
+        flash_plain_kernel<N><<<blocks, 128, 0, s>>>(a);
         OSR_CUDA(cudaGetLastError());
-        if (o.dlnphi_dx) {
-            DerivArgs<N> d;
-            d.f = a.f;
-            d.P = P;
-            d.T = T;
-            d.x = o.x;
-            d.y = o.y;
-            d.Zl = o.Zl;
-            d.Zg = o.Zg;
-            d.n = n;
-            d.dlnphi_dx = o.dlnphi_dx;
-            d.dlnphi_dP = o.dlnphi_dP;
-            long blocks = (n + 127) / 128;
-            long cap = (long)sm_count() * 8;
-            if (blocks > cap) blocks = cap;
-            flash_deriv_kernel<N><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+    } else {
+        ScratchLayout lay(n, N);
+        OSR_CUDA(cudaMemsetAsync(scratch, 0, lay.header, s));
+        QueueArgs<N> q;
+        q.f = table;
+        q.io = io;
+        q.park = park_view(scratch, n, N);
+        q.head = (unsigned long long *)(scratch + lay.head1);
+        q.ss_batch = g_ss_batch.load();
+        q.park_after = g_park_after.load();
+        q.resume = 0;
+        const int blocks = queue_blocks<N>(n);
+        flash_queue_kernel<N><<<blocks, 128, 0, s>>>(q);
+        OSR_CUDA(cudaGetLastError());
+        if (q.park_after > 0) {
+            const int sb = sm_count() * 2;
+            park_hist_kernel<<<sb, 256, 0, s>>>(q.park);
+            park_scatter_kernel<<<sb, 256, 0, s>>>(q.park);
+            q.head = (unsigned long long *)(scratch + lay.head2);
+            q.ss_batch = g_tail_batch.load();
+            q.park_after = 0;
+            q.resume = 1;
+            flash_queue_kernel<N><<<blocks, 128, 0, s>>>(q);
             OSR_CUDA(cudaGetLastError());
         }
+    }
+    if (o.dlnphi_dx) {
+        DerivArgs<N> d;
+        d.f = table;
+        d.P = P;
+        d.T = T;
+        d.x = o.x;
+        d.y = o.y;
+        d.Zl = o.Zl;
+        d.Zg = o.Zg;
+        d.n = n;
+        d.dlnphi_dx = o.dlnphi_dx;
+        d.dlnphi_dP = o.dlnphi_dP;
+        long blocks = (n + 127) / 128;
+        long cap = (long)sm_count() * 8;
+        if (blocks > cap) blocks = cap;
+        flash_deriv_kernel<N><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+        OSR_CUDA(cudaGetLastError());
     }
     return OSR_OK;
 }
 
 static osr_status run_flash(const osr_fluid &fl, const double *P, const double *T, const double *z, long n,
-                            const osr_flash_out &o, cudaStream_t s, Form form, unsigned long long *counter) {
+                            const osr_flash_out &o, cudaStream_t s, Form form, char *scratch) {
     switch (fl.nc) {
 #define OSR_NC_CASE(K) \
-    case K: return run_flash_n<K>(fl, P, T, z, n, o, s, form, counter);
+    case K: return run_flash_n<K>(fl, P, T, z, n, o, s, form, scratch);
         OSR_NC_CASE(1) OSR_NC_CASE(2) OSR_NC_CASE(3) OSR_NC_CASE(4) OSR_NC_CASE(5) OSR_NC_CASE(6)
         OSR_NC_CASE(7) OSR_NC_CASE(8) OSR_NC_CASE(9) OSR_NC_CASE(10) OSR_NC_CASE(11) OSR_NC_CASE(12)
         OSR_NC_CASE(13) OSR_NC_CASE(14) OSR_NC_CASE(15) OSR_NC_CASE(16)
@@ -175,18 +243,11 @@ static osr_status flash_device(const osr_fluid *fluid, const double *P, const do
     if ((st = check_out(out))) return st;
     if (!P || !T || !z) return OSR_ERR_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    unsigned long long *counter = nullptr;
-    if (form == Form::kQueue && n > 0) {
-        OSR_CUDA(pool_alloc((void **)&counter, sizeof(unsigned long long), s));
-        cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
-        if (e != cudaSuccess) {
-            cudaFreeAsync(counter, s);
-            return cuda_fail(e);
-        }
-    }
-    st = run_flash(*fluid, P, T, z, n, *out, s, form, counter);
-    if (counter) {
-        cudaError_t e = cudaFreeAsync(counter, s);
+    char *scratch = nullptr;
+    if (form == Form::kQueue) OSR_CUDA(pool_alloc((void **)&scratch, queue_scratch_bytes(n, fluid->nc), s));
+    st = run_flash(*fluid, P, T, z, n, *out, s, form, scratch);
+    if (scratch) {
+        cudaError_t e = cudaFreeAsync(scratch, s);
         if (st == OSR_OK && e != cudaSuccess) return cuda_fail(e);
     }
     return st;
@@ -276,17 +337,23 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
     return OSR_OK;
 }
 
-osr_status osr_flash_set_shape(int ss_batch, int ctas_per_sm) {
-    if (ss_batch < 1 || ss_batch > 32 || ctas_per_sm < 1 || ctas_per_sm > 16) return OSR_ERR_ARG;
+osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, int park_after) {
+    if (ss_batch < 1 || ss_batch > 32 || tail_batch < 1 || tail_batch > 32 || ctas_per_sm < 1 ||
+        ctas_per_sm > 16 || park_after < 0 || park_after > 500)
+        return OSR_ERR_ARG;
     g_ss_batch.store(ss_batch);
+    g_tail_batch.store(tail_batch);
     g_ctas_per_sm.store(ctas_per_sm);
+    g_park_after.store(park_after);
     return OSR_OK;
 }
 
-osr_status osr_flash_get_shape(int *ss_batch, int *ctas_per_sm) {
-    if (!ss_batch || !ctas_per_sm) return OSR_ERR_ARG;
+osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm, int *park_after) {
+    if (!ss_batch || !tail_batch || !ctas_per_sm || !park_after) return OSR_ERR_ARG;
     *ss_batch = g_ss_batch.load();
+    *tail_batch = g_tail_batch.load();
     *ctas_per_sm = g_ctas_per_sm.load();
+    *park_after = g_park_after.load();
     return OSR_OK;
 }
 

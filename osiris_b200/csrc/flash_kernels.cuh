@@ -40,18 +40,37 @@ template <int N>
 struct FlashArgs {
     FluidTable<N> f;
     FlashIO io;
-    unsigned long long *counter;  // work-queue head; must be zero at launch
-    int ss_batch;                 // ready lanes needed before a substitution step runs
 };
 
-// One Rachford-Rice Newton step (compsim/Init_Calcs.cpp:595-605).  Returns
-// the step t; L is updated in place.
+// Bound beyond which a Rachford-Rice Newton run provably ends outside [0,1].
+// Every term of F(L) = sum_i z_i (1-K_i)/(L + (1-L) K_i) is z_i/(L + c_i) with
+// c_i = K_i/(1-K_i) (c_i = -1 for a flagged K_i < 0; K_i = 1 contributes 0).
+// For |L| > 2 max|c_i| + 2 every denominator has the sign of L, so the Newton
+// step L - F/F' = L + (weighted mean of L + c_i) moves L further out by more
+// than 1e-4 each time: the loop runs to its 100-step cap and the clamp that
+// follows (compsim/Init_Calcs.cpp:608-615) gives 1 for L > 0 and 0 for L < 0
+// whatever the remaining steps do.  Stopping there returns the same clamped L.
+template <int N>
+__device__ __forceinline__ double rr_bound(const double *K) {
+    double M = 1;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+        if (K[i] >= 0 && K[i] != 1) M = fmax(M, fabs(K[i] / (1 - K[i])));
+    return 2 * M + 2;
+}
+
+// One Rachford-Rice Newton step (compsim/Init_Calcs.cpp:595-605), one
+// division per component.  Returns the step t; L is updated in place.
 template <int N>
 __device__ __forceinline__ double rr_step(const double *K, const double *z, double &L) {
     double F = 0, dF = 0;
+    const double omL = 1 - L;
 #pragma unroll
     for (int i = 0; i < N; i++) {
-        double td = (K[i] >= 0) ? (1 - K[i]) / (L + (1 - L) * K[i]) : 1 / (L - 1);
+        const bool pos = K[i] >= 0;
+        double num = pos ? 1 - K[i] : 1.0;
+        double den = pos ? L + omL * K[i] : L - 1;
+        double td = num / den;
         double zt = z[i] * td;
         F += zt;
         dF -= zt * td;
@@ -59,6 +78,22 @@ __device__ __forceinline__ double rr_step(const double *K, const double *z, doub
     double t = F / dF;
     L -= t;
     return t;
+}
+
+// The whole Newton run of one substitution step; returns the step count the
+// reference would take (the provably divergent tail is cut, see rr_bound).
+template <int N>
+__device__ __forceinline__ int rr_solve(const double *K, const double *z, double &L) {
+    const double big = rr_bound<N>(K);
+    L = 0.6;
+    int j = 0;
+    double t;
+    do {
+        t = rr_step<N>(K, z, L);
+        j++;
+        if (fabs(L) > big) return kRRMaxIt;
+    } while ((t * t > kRRTol) && (j < kRRMaxIt));
+    return j;
 }
 
 // One substitution step after the Newton loop: clamp L, form x, y, solve both
@@ -179,14 +214,7 @@ __global__ void __launch_bounds__(128) flash_plain_kernel(const __grid_constant_
     double L = 0, Lb = 10, Zl = 0, Zg = 0, es;
     int k = 0, rr = 0;
     do {
-        L = 0.6;
-        int j = 0;
-        double t;
-        do {
-            t = rr_step<N>(K, z, L);
-            j++;
-        } while ((t * t > kRRTol) && (j < kRRMaxIt));
-        rr += j;
+        rr += rr_solve<N>(K, z, L);
         es = ss_update<N>(a.f, sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
         k++;
     } while ((es > kSSTol) && (k < kSSMaxIt));
@@ -195,17 +223,67 @@ __global__ void __launch_bounds__(128) flash_plain_kernel(const __grid_constant_
 
 enum : int { kFetch = 0, kNewton = 1, kReady = 2, kDone = 3 };
 
-// Batched form: persistent warps, per-lane state machine, global work queue.
+// Cells parked by the first pass: their substitution state, so that the
+// second pass resumes them exactly where they stopped (K, iteration counts,
+// the previous L), and a sort key predicting their remaining work.
+struct ParkList {
+    long *cell;          // [cap] cell index
+    int *k, *rr, *key;   // [cap] SS steps so far, Newton steps so far, work key
+    int *order;          // [cap] slots sorted by descending key (second pass)
+    double *Lb;          // [cap] L of the last substitution step
+    double *K;           // [nc][cap] K-values
+    long cap;
+    unsigned *count;     // cells parked
+    unsigned *hist;      // [kParkKeys] cells per key
+    unsigned *cursor;    // [kParkKeys] scatter cursors
+};
+
+constexpr int kParkKeys = 64;
+
 template <int N>
-__global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant__ FlashArgs<N> a) {
+struct QueueArgs {
+    FluidTable<N> f;
+    FlashIO io;
+    ParkList park;
+    unsigned long long *head;  // work-queue head; zero at launch
+    int ss_batch;              // ready lanes needed before a substitution step runs
+    int park_after;            // park a cell still running after this many SS steps (0 = never)
+    int resume;                // 0: cells [0, n); 1: the parked cells in key order
+};
+
+// Predicted remaining work of a parked cell: substitution steps left from the
+// last two |dL| (linear convergence), times the cost of one step with the
+// cell's mean Newton count; bucketed by log2.
+__device__ __forceinline__ int park_key(int k, int rr, double es_last, double es_prev) {
+    double left = (double)(kSSMaxIt - k);
+    if (es_prev > 0 && es_last > 0 && es_last < es_prev) {
+        double r = es_last / es_prev;
+        double need = log(kSSTol / es_last) / log(r);
+        if (need >= 0 && need < left) left = need;
+    }
+    double per = 8.0 + (double)rr / (double)(k > 0 ? k : 1);  // a substitution step ~ 8 Newton steps
+    double w = left * per;
+    int key = (int)log2(w + 1.0);
+    return key < 0 ? 0 : (key >= kParkKeys ? kParkKeys - 1 : key);
+}
+
+// Batched form: persistent warps, per-lane state machine, global work queue.
+// First pass (resume = 0): cells [0, n); a cell still running after
+// park_after substitution steps is parked.  Second pass (resume = 1): the
+// parked cells, heaviest predicted first, run to completion.
+template <int N>
+__global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant__ QueueArgs<N> a) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const FlashIO &io = a.io;
+    const ParkList &pk = a.park;
+    const long total = a.resume ? (long)*pk.count : io.n;
     int mode = kFetch;
     long c = -1;
-    double P = 0, T = 0, L = 0, Lb = 10;
+    double P = 0, T = 0, L = 0, Lb = 10, es_prev = 0, es_last = 0;
     double z[N], K[N], sa[N];
     int j = 0, k = 0, rr = 0;
+    double big = 0;
 #pragma unroll
     for (int i = 0; i < N; i++) z[i] = K[i] = sa[i] = 0;
     for (;;) {
@@ -213,22 +291,35 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
         if (need) {
             int leader = __ffs(need) - 1;
             unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(a.counter, (unsigned long long)__popc(need));
+            if (lane == leader) base = atomicAdd(a.head, (unsigned long long)__popc(need));
             base = __shfl_sync(kFull, base, leader);
             if (mode == kFetch) {
-                long cc = (long)base + __popc(need & ((1u << lane) - 1));
-                if (cc < io.n) {
-                    c = cc;
+                long q = (long)base + __popc(need & ((1u << lane) - 1));
+                if (q < total) {
+                    if (a.resume) {
+                        long slot = pk.order[q];
+                        c = pk.cell[slot];
+                        k = pk.k[slot];
+                        rr = pk.rr[slot];
+                        Lb = pk.Lb[slot];
+#pragma unroll
+                        for (int i = 0; i < N; i++) K[i] = pk.K[(long)i * pk.cap + slot];
+                    } else {
+                        c = q;
+                        k = 0;
+                        rr = 0;
+                        Lb = 10;
+                    }
                     P = io.P[c];
                     T = io.T[c];
 #pragma unroll
                     for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
-                    flash_init<N>(a.f, P, T, K, sa);
+                    if (a.resume) sqrt_a<N>(a.f, T, sa);
+                    else flash_init<N>(a.f, P, T, K, sa);
+                    es_prev = es_last = 0;
                     L = 0.6;
-                    Lb = 10;
                     j = 0;
-                    k = 0;
-                    rr = 0;
+                    big = rr_bound<N>(K);
                     mode = kNewton;
                 } else {
                     mode = kDone;
@@ -239,7 +330,12 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
         if (mode == kNewton) {
             double t = rr_step<N>(K, z, L);
             j++;
-            if (!((t * t > kRRTol) && (j < kRRMaxIt))) mode = kReady;
+            if (fabs(L) > big) {
+                j = kRRMaxIt;  // provably divergent: the reference runs to its cap
+                mode = kReady;
+            } else if (!((t * t > kRRTol) && (j < kRRMaxIt))) {
+                mode = kReady;
+            }
         }
         unsigned ready = __ballot_sync(kFull, mode == kReady);
         unsigned newton = __ballot_sync(kFull, mode == kNewton);
@@ -249,16 +345,58 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
                 double es = ss_update<N>(a.f, sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
                 rr += j;
                 k++;
+                es_prev = es_last;
+                es_last = es;
                 if ((es > kSSTol) && (k < kSSMaxIt)) {
-                    L = 0.6;
-                    j = 0;
-                    mode = kNewton;
+                    if (a.park_after > 0 && k >= a.park_after) {
+                        unsigned slot = atomicAdd(pk.count, 1u);
+                        pk.cell[slot] = c;
+                        pk.k[slot] = k;
+                        pk.rr[slot] = rr;
+                        pk.Lb[slot] = Lb;
+                        pk.key[slot] = park_key(k, rr, es_last, es_prev);
+#pragma unroll
+                        for (int i = 0; i < N; i++) pk.K[(long)i * pk.cap + slot] = K[i];
+                        mode = kFetch;
+                    } else {
+                        L = 0.6;
+                        j = 0;
+                        big = rr_bound<N>(K);
+                        mode = kNewton;
+                    }
                 } else {
                     flash_store<N>(io, c, L, x, y, Zl, Zg, k, rr);
                     mode = kFetch;
                 }
             }
         }
+    }
+}
+
+// Counting sort of the parked cells by descending key: histogram ...
+__global__ void park_hist_kernel(ParkList pk) {
+    long n = *pk.count;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        atomicAdd(&pk.hist[pk.key[q]], 1u);
+}
+
+// ... then scatter: a slot's position is the number of cells with a larger
+// key plus its rank within its key (order within a key is immaterial).
+__global__ void park_scatter_kernel(ParkList pk) {
+    __shared__ unsigned start[kParkKeys];
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int key = kParkKeys - 1; key >= 0; key--) {
+            start[key] = acc;
+            acc += pk.hist[key];
+        }
+    }
+    __syncthreads();
+    long n = *pk.count;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+        int key = pk.key[q];
+        unsigned pos = start[key] + atomicAdd(&pk.cursor[key], 1u);
+        pk.order[pos] = (int)q;
     }
 }
 

@@ -45,16 +45,18 @@ def test_argument_validation_without_device():
     assert _bad_call(eos=7) == 1                # OSR_ERR_ARG
     assert _bad_call(n=-1) == 1
     L = osr.lib()
-    assert L.osr_flash_set_shape(0, 4) == 1
-    assert L.osr_flash_set_shape(8, 0) == 1
-    a, b = osr.get_shape()
-    assert 1 <= a <= 32 and 1 <= b <= 16
+    assert L.osr_flash_set_shape(0, 32, 4, 8) == 1
+    assert L.osr_flash_set_shape(8, 32, 0, 8) == 1
+    assert L.osr_flash_set_shape(8, 0, 4, 8) == 1
+    assert L.osr_flash_set_shape(8, 32, 4, -1) == 1
+    a, b, c, d = osr.get_shape()
+    assert 1 <= a <= 32 and 1 <= b <= 32 and 1 <= c <= 16 and 0 <= d <= 500
 
 
 def test_shape_roundtrip():
-    a, b = osr.get_shape()
-    osr.set_shape(12, 3)
-    assert osr.get_shape() == (12, 3)
-    osr.set_shape(a, b)
+    old = osr.get_shape()
+    osr.set_shape(12, 30, 3, 6)
+    assert osr.get_shape() == (12, 30, 3, 6)
+    osr.set_shape(*old)
     with pytest.raises(osr.OsrError):
-        osr.set_shape(33, 1)
+        osr.set_shape(33, 1, 1, 1)
