@@ -100,6 +100,11 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
 osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, int park_after);
 osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm, int *park_after);
 
+/* Age limit of the substitution-step batching: a warp runs the step for its
+ * ready lanes once they have waited more than max_wait Newton trips, even if
+ * fewer than ss_batch/tail_batch lanes are ready (0..1000).  Process-wide. */
+osr_status osr_flash_set_max_wait(int max_wait);
+
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The
  * denominator of the flash kernel's roofline.  No reference counterpart. */

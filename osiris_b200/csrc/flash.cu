@@ -17,6 +17,7 @@ static std::atomic<int> g_ss_batch{20};
 static std::atomic<int> g_tail_batch{32};
 static std::atomic<int> g_ctas_per_sm{4};
 static std::atomic<int> g_park_after{8};
+static std::atomic<int> g_max_wait{1000};
 
 static osr_status cuda_fail(cudaError_t e) {
     g_last_cuda.store((int)e);
@@ -108,43 +109,59 @@ static int sm_count() {
 enum class Form { kQueue, kPlain };
 
 // Scratch of the batched form, carved from one device block:
-//   header (1 KiB): first-pass head, second-pass head, parked count,
-//                   key histogram, scatter cursors -- zeroed per call;
-//   parked-cell list with room for every cell (cell, k, rr, key, order, Lb, K).
+//   header (256 B): per-pass queue heads [kMaxPasses] and parked counts
+//                   [kMaxPasses] -- zeroed per call;
+//   two parked-cell lists (ping-pong between passes), each with room for
+//   every cell: cell, k, rr, Lb, K[nc].
+constexpr int kMaxPasses = 12;
 struct ScratchLayout {
-    size_t head1 = 0, head2 = 8, count = 16, hist = 256, cursor = 512, header = 1024;
-    size_t cell, k, rr, key, order, Lb, K, total;
+    size_t heads = 0, counts = 8 * kMaxPasses, header = 256;
+    size_t list[2], cell, k, rr, Lb, K, list_bytes, total;
     ScratchLayout(long cap, int nc) {
         auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
         size_t c = (size_t)cap;
-        cell = header;
+        cell = 0;
         k = cell + al(c * 8);
         rr = k + al(c * 4);
-        key = rr + al(c * 4);
-        order = key + al(c * 4);
-        Lb = order + al(c * 4);
+        Lb = rr + al(c * 4);
         K = Lb + al(c * 8);
-        total = K + al(c * 8 * (size_t)nc);
+        list_bytes = K + al(c * 8 * (size_t)nc);
+        list[0] = header;
+        list[1] = header + list_bytes;
+        total = header + 2 * list_bytes;
     }
 };
 
 static size_t queue_scratch_bytes(long n, int nc) { return ScratchLayout(n, nc).total; }
 
-static ParkList park_view(char *base, long cap, int nc) {
+static ParkList park_view(char *base, long cap, int nc, int which) {
     ScratchLayout L(cap, nc);
+    char *b = base + L.list[which];
     ParkList p;
-    p.cell = (long *)(base + L.cell);
-    p.k = (int *)(base + L.k);
-    p.rr = (int *)(base + L.rr);
-    p.key = (int *)(base + L.key);
-    p.order = (int *)(base + L.order);
-    p.Lb = (double *)(base + L.Lb);
-    p.K = (double *)(base + L.K);
+    p.cell = (long *)(b + L.cell);
+    p.k = (int *)(b + L.k);
+    p.rr = (int *)(b + L.rr);
+    p.Lb = (double *)(b + L.Lb);
+    p.K = (double *)(b + L.K);
     p.cap = cap;
-    p.count = (unsigned *)(base + L.count);
-    p.hist = (unsigned *)(base + L.hist);
-    p.cursor = (unsigned *)(base + L.cursor);
     return p;
+}
+
+// Substitution-step limits of the successive passes: park_after, doubling,
+// ending at the reference's cap of 500 (the last pass parks nothing).
+static int pass_limits(int park_after, int *lim) {
+    int np = 0;
+    if (park_after <= 0) {
+        lim[np++] = kSSMaxIt;
+        return np;
+    }
+    int s = park_after;
+    while (s < kSSMaxIt && np < kMaxPasses - 1) {
+        lim[np++] = s;
+        s *= 2;
+    }
+    lim[np++] = kSSMaxIt;
+    return np;
 }
 
 template <int N>
@@ -177,25 +194,24 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
     } else {
         ScratchLayout lay(n, N);
         OSR_CUDA(cudaMemsetAsync(scratch, 0, lay.header, s));
+        int lim[kMaxPasses];
+        const int np = pass_limits(g_park_after.load(), lim);
+        unsigned long long *heads = (unsigned long long *)(scratch + lay.heads);
+        unsigned *counts = (unsigned *)(scratch + lay.counts);
         QueueArgs<N> q;
         q.f = table;
         q.io = io;
-        q.park = park_view(scratch, n, N);
-        q.head = (unsigned long long *)(scratch + lay.head1);
-        q.ss_batch = g_ss_batch.load();
-        q.park_after = g_park_after.load();
-        q.resume = 0;
+        q.max_wait = g_max_wait.load();
         const int blocks = queue_blocks<N>(n);
-        flash_queue_kernel<N><<<blocks, 128, 0, s>>>(q);
-        OSR_CUDA(cudaGetLastError());
-        if (q.park_after > 0) {
-            const int sb = sm_count() * 2;
-            park_hist_kernel<<<sb, 256, 0, s>>>(q.park);
-            park_scatter_kernel<<<sb, 256, 0, s>>>(q.park);
-            q.head = (unsigned long long *)(scratch + lay.head2);
-            q.ss_batch = g_tail_batch.load();
-            q.park_after = 0;
-            q.resume = 1;
+        for (int p = 0; p < np; p++) {
+            q.first = p == 0;
+            q.src = park_view(scratch, n, N, (p + 1) & 1);
+            q.dst = park_view(scratch, n, N, p & 1);
+            q.src_count = p > 0 ? counts + (p - 1) : nullptr;
+            q.dst_count = counts + p;
+            q.head = heads + p;
+            q.park_at = lim[p];
+            q.ss_batch = p == 0 ? g_ss_batch.load() : g_tail_batch.load();
             flash_queue_kernel<N><<<blocks, 128, 0, s>>>(q);
             OSR_CUDA(cudaGetLastError());
         }
@@ -345,6 +361,12 @@ osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, in
     g_tail_batch.store(tail_batch);
     g_ctas_per_sm.store(ctas_per_sm);
     g_park_after.store(park_after);
+    return OSR_OK;
+}
+
+osr_status osr_flash_set_max_wait(int max_wait) {
+    if (max_wait < 0 || max_wait > 1000) return OSR_ERR_ARG;
+    g_max_wait.store(max_wait);
     return OSR_OK;
 }
 

@@ -60,22 +60,50 @@ __device__ __forceinline__ double rr_bound(const double *K) {
 }
 
 // One Rachford-Rice Newton step (compsim/Init_Calcs.cpp:595-605), one
-// division per component.  Returns the step t; L is updated in place.
-template <int N>
-__device__ __forceinline__ double rr_step(const double *K, const double *z, double &L) {
-    double F = 0, dF = 0;
+// division per component, the sums as a pairwise tree.  Returns the step t;
+// L is updated in place.
+template <int N, bool Fast>
+__device__ __forceinline__ double rr_step_impl(const double *K, const double *z, double &L, bool &ok) {
+    double zt[N], zq[N];
     const double omL = 1 - L;
 #pragma unroll
     for (int i = 0; i < N; i++) {
         const bool pos = K[i] >= 0;
         double num = pos ? 1 - K[i] : 1.0;
         double den = pos ? L + omL * K[i] : L - 1;
-        double td = num / den;
-        double zt = z[i] * td;
-        F += zt;
-        dF -= zt * td;
+        double td;
+        if (Fast) {
+            ok &= qdiv_ok(num, den);
+            td = qdiv(num, den);
+        } else {
+            td = num / den;
+        }
+        zt[i] = z[i] * td;
+        zq[i] = zt[i] * td;
     }
-    double t = F / dF;
+#pragma unroll
+    for (int w = 1; w < N; w *= 2)
+#pragma unroll
+        for (int i = 0; i + w < N; i += 2 * w) {
+            zt[i] += zt[i + w];
+            zq[i] += zq[i + w];
+        }
+    double F = zt[0], dF = -zq[0];
+    double t;
+    if (Fast) {
+        ok &= qdiv_ok(F, dF);
+        t = qdiv(F, dF);
+    } else {
+        t = F / dF;
+    }
+    return t;
+}
+
+template <int N>
+__device__ __forceinline__ double rr_step(const double *K, const double *z, double &L) {
+    bool ok = true;
+    double t = rr_step_impl<N, true>(K, z, L, ok);
+    if (!ok) t = rr_step_impl<N, false>(K, z, L, ok);
     L -= t;
     return t;
 }
@@ -98,22 +126,32 @@ __device__ __forceinline__ int rr_solve(const double *K, const double *z, double
 
 // One substitution step after the Newton loop: clamp L, form x, y, solve both
 // cubics and update K (compsim/Init_Calcs.cpp:608-712).  Returns |Lb - L|.
-template <int N>
-__device__ __forceinline__ double ss_update(const FluidTable<N> &f, const double *sa, double P, double T,
-                                            const double *z, double *K, double &L, double &Lb, double *x,
-                                            double *y, double &Zl, double &Zg) {
+// The Fast instantiation uses the branch-free quotients and reports through
+// ok whether every operand was in range; K is written only by the caller.
+template <int N, bool Fast>
+__device__ __forceinline__ double ss_update_impl(const FluidTable<N> &f, const double *sa, double P, double T,
+                                                 const double *z, const double *K, double *Kn, double L0,
+                                                 double &L, double Lb, double *x, double *y, double &Zl,
+                                                 double &Zg, bool &ok) {
+    auto DIV = [&](double a, double b) -> double {
+        if (Fast) {
+            ok &= qdiv_ok(a, b);
+            return qdiv(a, b);
+        }
+        return a / b;
+    };
+    L = L0;
     if (L > 1) L = 1;
     else if (L < 0) L = 0;
     double es = fabs(Lb - L);
-    Lb = L;
 #pragma unroll
     for (int i = 0; i < N; i++) {
         if (K[i] >= 0) {
-            x[i] = z[i] / (L + K[i] * (1 - L));
+            x[i] = DIV(z[i], L + K[i] * (1 - L));
             y[i] = K[i] * x[i];
         } else {
             x[i] = 0;
-            y[i] = z[i] / (1 - L);
+            y[i] = DIV(z[i], 1 - L);
         }
     }
     // Mixing rule: with u_i = w_i sqrt(a_i) and v_i = sum_j (1-k_ij) u_j,
@@ -148,26 +186,51 @@ __device__ __forceinline__ double ss_update(const FluidTable<N> &f, const double
     Zg = phase_z(Ag, Bg, srk, true);
     const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
     // i-independent parts of ln(phi_i) (the reference re-evaluates them per i)
-    double DDl = Al / (Bl * (d1 - d2)), DDg = Ag / (Bg * (d1 - d2));
-    double FFl = log((Zl + d2 * Bl) / (Zl + d1 * Bl)), FFg = log((Zg + d2 * Bg) / (Zg + d1 * Bg));
+    double DDl = DIV(Al, Bl * (d1 - d2)), DDg = DIV(Ag, Bg * (d1 - d2));
+    double FFl = log(DIV(Zl + d2 * Bl, Zl + d1 * Bl)), FFg = log(DIV(Zg + d2 * Bg, Zg + d1 * Bg));
     double cl = log(Zl - Bl), cg = log(Zg - Bg);
-    double rCal = 2 / Cal, rCag = 2 / Cag, rCbl = 1 / Cbl, rCbg = 1 / Cbg;
+    double rCal = DIV(2.0, Cal), rCag = DIV(2.0, Cag), rCbl = DIV(1.0, Cbl), rCbg = DIV(1.0, Cbg);
     double DFl = DDl * FFl, DFg = DDg * FFg;
 #pragma unroll
     for (int i = 0; i < N; i++) {
         double t1l = f.b[i] * rCbl, t1g = f.b[i] * rCbg;
         double EEl = sa[i] * vl[i] * rCal - t1l;
         double EEg = sa[i] * vg[i] * rCag - t1g;
-        double phiL = exp(t1l * (Zl - 1) - cl + DFl * EEl);
-        double phiG = exp(t1g * (Zg - 1) - cg + DFg * EEg);
-        double fL = x[i] * phiL, fG = y[i] * phiG;
+        double lnL = t1l * (Zl - 1) - cl + DFl * EEl;
+        double lnG = t1g * (Zg - 1) - cg + DFg * EEg;
+        Kn[i] = K[i];
         if (z[i] != 0) {
-            if (fG != 0) K[i] *= fL / fG;
-            else K[i] = -1;
-            if (fL != fL) K[i] = -1;
-            if (fG != fG) K[i] = 1;
+            // K_i x_i phi_i^L / (y_i phi_i^V) with y_i = K_i x_i is phi_i^L / phi_i^V:
+            // one exponential when every factor is finite and non-zero; the
+            // reference's own form (and its zero/NaN rules) otherwise.
+            double d = lnL - lnG;
+            if (K[i] > 0 && x[i] > 0 && y[i] > 0 && x[i] < 1e300 && y[i] < 1e300 && fabs(lnL) < 700 &&
+                fabs(lnG) < 700 && fabs(d) < 700) {
+                Kn[i] = exp(d);
+            } else {
+                double fL = x[i] * exp(lnL), fG = y[i] * exp(lnG);
+                if (fG != 0) Kn[i] = K[i] * (fL / fG);
+                else Kn[i] = -1;
+                if (fL != fL) Kn[i] = -1;
+                if (fG != fG) Kn[i] = 1;
+            }
         }
     }
+    return es;
+}
+
+template <int N>
+__device__ __forceinline__ double ss_update(const FluidTable<N> &f, const double *sa, double P, double T,
+                                            const double *z, double *K, double &L, double &Lb, double *x,
+                                            double *y, double &Zl, double &Zg) {
+    bool ok = true;
+    double Kn[N];
+    const double L0 = L;
+    double es = ss_update_impl<N, true>(f, sa, P, T, z, K, Kn, L0, L, Lb, x, y, Zl, Zg, ok);
+    if (!ok) es = ss_update_impl<N, false>(f, sa, P, T, z, K, Kn, L0, L, Lb, x, y, Zl, Zg, ok);
+#pragma unroll
+    for (int i = 0; i < N; i++) K[i] = Kn[i];
+    Lb = L;
     return es;
 }
 
@@ -223,66 +286,49 @@ __global__ void __launch_bounds__(128) flash_plain_kernel(const __grid_constant_
 
 enum : int { kFetch = 0, kNewton = 1, kReady = 2, kDone = 3 };
 
-// Cells parked by the first pass: their substitution state, so that the
-// second pass resumes them exactly where they stopped (K, iteration counts,
-// the previous L), and a sort key predicting their remaining work.
+// A list of cells in flight: their substitution state, so that a later pass
+// resumes each exactly where it stopped (K, iteration counts, previous L).
 struct ParkList {
     long *cell;          // [cap] cell index
-    int *k, *rr, *key;   // [cap] SS steps so far, Newton steps so far, work key
-    int *order;          // [cap] slots sorted by descending key (second pass)
+    int *k, *rr;         // [cap] SS steps so far, Newton steps so far
     double *Lb;          // [cap] L of the last substitution step
     double *K;           // [nc][cap] K-values
     long cap;
-    unsigned *count;     // cells parked
-    unsigned *hist;      // [kParkKeys] cells per key
-    unsigned *cursor;    // [kParkKeys] scatter cursors
 };
-
-constexpr int kParkKeys = 64;
 
 template <int N>
 struct QueueArgs {
     FluidTable<N> f;
     FlashIO io;
-    ParkList park;
-    unsigned long long *head;  // work-queue head; zero at launch
-    int ss_batch;              // ready lanes needed before a substitution step runs
-    int park_after;            // park a cell still running after this many SS steps (0 = never)
-    int resume;                // 0: cells [0, n); 1: the parked cells in key order
+    ParkList src, dst;           // resume from src (pass > 0); park into dst
+    const unsigned *src_count;   // cells in src (pass > 0)
+    unsigned *dst_count;         // cells parked into dst
+    unsigned long long *head;    // work-queue head of this pass; zero at launch
+    int ss_batch;                // ready lanes needed before a substitution step runs ...
+    int max_wait;                // ... or Newton trips the ready lanes have waited
+    int park_at;                 // park a cell still running once it reaches this many SS steps
+    int first;                   // 1: take cells [0, n) fresh; 0: resume src
 };
 
-// Predicted remaining work of a parked cell: substitution steps left from the
-// last two |dL| (linear convergence), times the cost of one step with the
-// cell's mean Newton count; bucketed by log2.
-__device__ __forceinline__ int park_key(int k, int rr, double es_last, double es_prev) {
-    double left = (double)(kSSMaxIt - k);
-    if (es_prev > 0 && es_last > 0 && es_last < es_prev) {
-        double r = es_last / es_prev;
-        double need = log(kSSTol / es_last) / log(r);
-        if (need >= 0 && need < left) left = need;
-    }
-    double per = 8.0 + (double)rr / (double)(k > 0 ? k : 1);  // a substitution step ~ 8 Newton steps
-    double w = left * per;
-    int key = (int)log2(w + 1.0);
-    return key < 0 ? 0 : (key >= kParkKeys ? kParkKeys - 1 : key);
-}
-
-// Batched form: persistent warps, per-lane state machine, global work queue.
-// First pass (resume = 0): cells [0, n); a cell still running after
-// park_after substitution steps is parked.  Second pass (resume = 1): the
-// parked cells, heaviest predicted first, run to completion.
+// Batched form: persistent warps, a per-lane state machine and a global work
+// queue, run as a sequence of passes.  The first pass takes every cell; a
+// cell still running when it reaches park_at substitution steps is parked
+// (its state written to dst) and its lane takes the next cell.  Each later
+// pass resumes the parked cells of the previous one with a doubled limit, so
+// every pass starts with fully populated warps instead of draining a few
+// long cells through mostly idle warps.
 template <int N>
 __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant__ QueueArgs<N> a) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const FlashIO &io = a.io;
-    const ParkList &pk = a.park;
-    const long total = a.resume ? (long)*pk.count : io.n;
+    const long total = a.first ? io.n : (long)*a.src_count;
     int mode = kFetch;
     long c = -1;
-    double P = 0, T = 0, L = 0, Lb = 10, es_prev = 0, es_last = 0;
+    double P = 0, T = 0, L = 0, Lb = 10;
     double z[N], K[N], sa[N];
     int j = 0, k = 0, rr = 0;
+    int waited = 0;  // warp-uniform: Newton trips since ready lanes appeared
     double big = 0;
 #pragma unroll
     for (int i = 0; i < N; i++) z[i] = K[i] = sa[i] = 0;
@@ -296,27 +342,25 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
             if (mode == kFetch) {
                 long q = (long)base + __popc(need & ((1u << lane) - 1));
                 if (q < total) {
-                    if (a.resume) {
-                        long slot = pk.order[q];
-                        c = pk.cell[slot];
-                        k = pk.k[slot];
-                        rr = pk.rr[slot];
-                        Lb = pk.Lb[slot];
-#pragma unroll
-                        for (int i = 0; i < N; i++) K[i] = pk.K[(long)i * pk.cap + slot];
-                    } else {
+                    if (a.first) {
                         c = q;
                         k = 0;
                         rr = 0;
                         Lb = 10;
+                    } else {
+                        c = a.src.cell[q];
+                        k = a.src.k[q];
+                        rr = a.src.rr[q];
+                        Lb = a.src.Lb[q];
+#pragma unroll
+                        for (int i = 0; i < N; i++) K[i] = a.src.K[(long)i * a.src.cap + q];
                     }
                     P = io.P[c];
                     T = io.T[c];
 #pragma unroll
                     for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
-                    if (a.resume) sqrt_a<N>(a.f, T, sa);
-                    else flash_init<N>(a.f, P, T, K, sa);
-                    es_prev = es_last = 0;
+                    if (a.first) flash_init<N>(a.f, P, T, K, sa);
+                    else sqrt_a<N>(a.f, T, sa);
                     L = 0.6;
                     j = 0;
                     big = rr_bound<N>(K);
@@ -339,24 +383,23 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
         }
         unsigned ready = __ballot_sync(kFull, mode == kReady);
         unsigned newton = __ballot_sync(kFull, mode == kNewton);
-        if (ready != 0 && (__popc(ready) >= a.ss_batch || newton == 0)) {
+        if (ready != 0) waited++;
+        if (ready != 0 && (__popc(ready) >= a.ss_batch || newton == 0 || waited > a.max_wait)) {
+            waited = 0;
             if (mode == kReady) {
                 double x[N], y[N], Zl, Zg;
                 double es = ss_update<N>(a.f, sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
                 rr += j;
                 k++;
-                es_prev = es_last;
-                es_last = es;
                 if ((es > kSSTol) && (k < kSSMaxIt)) {
-                    if (a.park_after > 0 && k >= a.park_after) {
-                        unsigned slot = atomicAdd(pk.count, 1u);
-                        pk.cell[slot] = c;
-                        pk.k[slot] = k;
-                        pk.rr[slot] = rr;
-                        pk.Lb[slot] = Lb;
-                        pk.key[slot] = park_key(k, rr, es_last, es_prev);
+                    if (k >= a.park_at) {
+                        unsigned slot = atomicAdd(a.dst_count, 1u);
+                        a.dst.cell[slot] = c;
+                        a.dst.k[slot] = k;
+                        a.dst.rr[slot] = rr;
+                        a.dst.Lb[slot] = Lb;
 #pragma unroll
-                        for (int i = 0; i < N; i++) pk.K[(long)i * pk.cap + slot] = K[i];
+                        for (int i = 0; i < N; i++) a.dst.K[(long)i * a.dst.cap + slot] = K[i];
                         mode = kFetch;
                     } else {
                         L = 0.6;
@@ -370,33 +413,6 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
                 }
             }
         }
-    }
-}
-
-// Counting sort of the parked cells by descending key: histogram ...
-__global__ void park_hist_kernel(ParkList pk) {
-    long n = *pk.count;
-    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
-        atomicAdd(&pk.hist[pk.key[q]], 1u);
-}
-
-// ... then scatter: a slot's position is the number of cells with a larger
-// key plus its rank within its key (order within a key is immaterial).
-__global__ void park_scatter_kernel(ParkList pk) {
-    __shared__ unsigned start[kParkKeys];
-    if (threadIdx.x == 0) {
-        unsigned acc = 0;
-        for (int key = kParkKeys - 1; key >= 0; key--) {
-            start[key] = acc;
-            acc += pk.hist[key];
-        }
-    }
-    __syncthreads();
-    long n = *pk.count;
-    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-        int key = pk.key[q];
-        unsigned pos = start[key] + atomicAdd(&pk.cursor[key], 1u);
-        pk.order[pos] = (int)q;
     }
 }
 
