@@ -13,10 +13,10 @@
 namespace osr {
 
 static std::atomic<int> g_last_cuda{0};
-static std::atomic<int> g_ss_batch{20};
+static std::atomic<int> g_ss_batch{28};
 static std::atomic<int> g_tail_batch{32};
-static std::atomic<int> g_ctas_per_sm{4};
-static std::atomic<int> g_park_after{8};
+static std::atomic<int> g_ctas_per_sm{3};
+static std::atomic<int> g_park_after{2};
 static std::atomic<int> g_max_wait{1000};
 
 static osr_status cuda_fail(cudaError_t e) {

@@ -191,24 +191,37 @@ __device__ __forceinline__ double ss_update_impl(const FluidTable<N> &f, const d
     double cl = log(Zl - Bl), cg = log(Zg - Bg);
     double rCal = DIV(2.0, Cal), rCag = DIV(2.0, Cag), rCbl = DIV(1.0, Cbl), rCbg = DIV(1.0, Cbg);
     double DFl = DDl * FFl, DFg = DDg * FFg;
+    double lnl[N], lng[N];
 #pragma unroll
     for (int i = 0; i < N; i++) {
         double t1l = f.b[i] * rCbl, t1g = f.b[i] * rCbg;
         double EEl = sa[i] * vl[i] * rCal - t1l;
         double EEg = sa[i] * vg[i] * rCag - t1g;
-        double lnL = t1l * (Zl - 1) - cl + DFl * EEl;
-        double lnG = t1g * (Zg - 1) - cg + DFg * EEg;
-        Kn[i] = K[i];
-        if (z[i] != 0) {
-            // K_i x_i phi_i^L / (y_i phi_i^V) with y_i = K_i x_i is phi_i^L / phi_i^V:
-            // one exponential when every factor is finite and non-zero; the
-            // reference's own form (and its zero/NaN rules) otherwise.
-            double d = lnL - lnG;
-            if (K[i] > 0 && x[i] > 0 && y[i] > 0 && x[i] < 1e300 && y[i] < 1e300 && fabs(lnL) < 700 &&
-                fabs(lnG) < 700 && fabs(d) < 700) {
-                Kn[i] = exp(d);
-            } else {
-                double fL = x[i] * exp(lnL), fG = y[i] * exp(lnG);
+        lnl[i] = t1l * (Zl - 1) - cl + DFl * EEl;
+        lng[i] = t1g * (Zg - 1) - cg + DFg * EEg;
+    }
+    // K_i x_i phi_i^L / (y_i phi_i^V) with y_i = K_i x_i is phi_i^L / phi_i^V:
+    // one exponential per component, evaluated for all components without
+    // branching; components with a zero, infinite or extreme factor take the
+    // reference's own form (and its zero/NaN rules) in one separate pass.
+    bool plain = true;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        double d = lnl[i] - lng[i];
+        bool fast = K[i] > 0 && x[i] > 0 && y[i] > 0 && x[i] < 1e300 && y[i] < 1e300 && fabs(lnl[i]) < 700 &&
+                    fabs(lng[i]) < 700 && fabs(d) < 700;
+        plain &= fast || z[i] == 0;
+        double e = exp(fast ? d : 0.0);
+        Kn[i] = (z[i] != 0 && fast) ? e : K[i];
+    }
+    if (!plain) {
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            double d = lnl[i] - lng[i];
+            bool fast = K[i] > 0 && x[i] > 0 && y[i] > 0 && x[i] < 1e300 && y[i] < 1e300 &&
+                        fabs(lnl[i]) < 700 && fabs(lng[i]) < 700 && fabs(d) < 700;
+            if (z[i] != 0 && !fast) {
+                double fL = x[i] * exp(lnl[i]), fG = y[i] * exp(lng[i]);
                 if (fG != 0) Kn[i] = K[i] * (fL / fG);
                 else Kn[i] = -1;
                 if (fL != fL) Kn[i] = -1;
