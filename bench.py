@@ -342,14 +342,15 @@ def run_ours(args):
                    "two_phase_fraction": two_phase, "mean_ss_iters": float(iters.mean()),
                    "mean_rr_iters": float(rr.mean()), "max_ss_iters": int(iters.max()),
                    "max_rr_iters": int(rr.max())},
-        "roofline": {"bound": "fp64", "kernel": "flash_queue_kernel<6>", "achieved": achieved,
+        "roofline": {"bound": "fp64", "kernel": f"flash_queue_kernel<6>, all {osr.flash_passes()} passes of one call",
+                     "achieved": achieved,
                      "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "peak_source": "measured: osr_probe_fp64_peak (dependent-FMA microbenchmark, this run)",
                      "traffic": traffic, "flops_per_launch": kflops, "ms_per_launch": kms},
         "deriv_kernel": {"bound": "hbm", "ms_per_launch": deriv_ms,
                          "achieved_gbs": deriv_bytes / (deriv_ms * 1e-3) / 1e9, "bytes_per_launch": deriv_bytes,
                          "flops_per_launch": dflops},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": (osr.flash_passes() + 1) * args.steps,
         "clocks": clk,
         "timed_wall_s": t_wall,
     }

@@ -166,6 +166,19 @@ def flash_host(fluid: Fluid, P, T, z, derivs: bool = True, out: dict | None = No
     return out
 
 
+def flash_passes() -> int:
+    """Launches of the batched flash kernel per call with the current shape:
+    park_after, doubling, ending at 500 substitution steps."""
+    park = get_shape()[3]
+    if park <= 0:
+        return 1
+    n, s = 0, park
+    while s < 500 and n < 11:
+        n += 1
+        s *= 2
+    return n + 1
+
+
 def set_shape(ss_batch: int, tail_batch: int, ctas_per_sm: int, park_after: int):
     _check(lib().osr_flash_set_shape(int(ss_batch), int(tail_batch), int(ctas_per_sm), int(park_after)),
            "osr_flash_set_shape")
