@@ -76,6 +76,27 @@ typedef struct osr_flash_out {
 osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
                            long n, const osr_flash_out *out, void *stream);
 
+/* Same results as osr_flash_batch, for callers that cannot allocate device
+ * memory: a host program embedding the simulator whose device memory is
+ * owned by another runtime or allocator (a solver library's pool, a graph
+ * being captured by someone else), or that runs under a no-allocation policy
+ * in its time-step loop.  The caller passes inputs and outputs as for
+ * osr_flash_batch; the work-queue heads and parked-cell lists live in one
+ * library-wide static device array of 64 MiB, which every GPU that loads the
+ * library holds until the process exits.  No reference counterpart.
+ *   - Size limit: n * (48 + 16 * nc) + 4096 bytes must fit in 64 MiB
+ *     (about 466,000 cells at nc = 6, 220,000 at nc = 16); larger n returns
+ *     OSR_ERR_SIZE before any device work.  Split larger batches.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress, that device current) and caches it; make that
+ *     first call before any stream capture.
+ *   - Every call shares the array: the call clears its header on `stream`,
+ *     and calls that overlap on the GPU (other streams, other threads) race.
+ *     Serialise them.
+ *   - Calls no cudaMalloc/cudaFree or pool allocation. */
+osr_status osr_flash_batch_noalloc(const osr_fluid *fluid, const double *d_P, const double *d_T,
+                                   const double *d_z, long n, const osr_flash_out *out, void *stream);
+
 /* Same results, plain form: one thread per cell, no work queue.  Kept as the
  * baseline the batched form is measured against. */
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T,

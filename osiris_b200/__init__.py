@@ -134,7 +134,8 @@ def flash(fluid: Fluid, P, T, z, derivs: bool = True, form: str = "batched", out
     if stream is None:
         stream = torch.cuda.current_stream(P.device)
     co = _out_struct(out, lambda t: t.data_ptr())
-    fn = {"batched": lib().osr_flash_batch, "plain": lib().osr_flash_batch_plain}[form]
+    fn = {"batched": lib().osr_flash_batch, "plain": lib().osr_flash_batch_plain,
+          "noalloc": lib().osr_flash_batch_noalloc}[form]
     rc = fn(fluid.cref, _vp(P.data_ptr()), _vp(T.data_ptr()), _vp(z.data_ptr()), ctypes.c_long(n),
             ctypes.byref(co), _vp(stream.cuda_stream))
     _check(rc, f"osr_flash_batch ({form})")

@@ -269,6 +269,35 @@ static osr_status flash_device(const osr_fluid *fluid, const double *P, const do
     return st;
 }
 
+// ---------------------------------------------------------------------------
+// No-allocation variant of the batched flash.
+//
+// Its scratch (queue heads, parked counts, the two parked-cell lists) lives in
+// this file-scope device array instead of memory taken per call.  Every GPU
+// that loads the library holds the array until the process exits.  Host code
+// cannot use the array's name as a device address; the address is looked up
+// once per device with cudaGetSymbolAddress (that device current) and cached.
+constexpr size_t kNoAllocScratchBytes = (size_t)64 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static cudaError_t noalloc_scratch(char **out) {
+    static std::mutex mu;
+    static char *addr[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *a = nullptr;
+        e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = (char *)a;
+    }
+    *out = addr[dev];
+    return cudaSuccess;
+}
+
 }  // namespace osr
 
 using namespace osr;
@@ -278,6 +307,22 @@ extern "C" {
 osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z, long n,
                            const osr_flash_out *out, void *stream) {
     return flash_device(fluid, d_P, d_T, d_z, n, out, stream, Form::kQueue);
+}
+
+osr_status osr_flash_batch_noalloc(const osr_fluid *fluid, const double *d_P, const double *d_T,
+                                   const double *d_z, long n, const osr_flash_out *out, void *stream) {
+    osr_status st = check_fluid(fluid);
+    if (st) return st;
+    if (!out || n < 0) return OSR_ERR_ARG;
+    if (n == 0) return OSR_OK;
+    if ((st = check_out(out))) return st;
+    if (!d_P || !d_T || !d_z) return OSR_ERR_ARG;
+    if (queue_scratch_bytes(n, fluid->nc) > kNoAllocScratchBytes) return OSR_ERR_SIZE;
+    char *scratch = nullptr;
+    OSR_CUDA(noalloc_scratch(&scratch));
+    // run_flash clears the scratch header (queue heads, parked counts) on
+    // `stream` before the first pass; the parked lists are written before read.
+    return run_flash(*fluid, d_P, d_T, d_z, n, *out, (cudaStream_t)stream, Form::kQueue, scratch);
 }
 
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
