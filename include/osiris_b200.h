@@ -71,8 +71,8 @@ typedef struct osr_flash_out {
  * (compsim/Petsc_Functions.cpp:30243-30372).  d_P [n] Pa, d_T [n] K, d_z
  * [nc][n] feed mole fractions.  Asynchronous on `stream` (a cudaStream_t,
  * NULL = legacy default stream).  Takes stream-ordered scratch from a
- * library-private pool per call: work-queue heads and a parked-cell list
- * of (32 + 8 nc) bytes per cell. */
+ * library-private pool per call: work-queue heads and two parked-cell lists,
+ * 48 + 16 nc bytes per cell in all. */
 osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
                            long n, const osr_flash_out *out, void *stream);
 
@@ -110,11 +110,12 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
                                 long n, const osr_flash_out *out, void *stream);
 
 /* Launch-shape knobs of the batched flash (the autotuner sets them).
- * The batched form runs two passes of a persistent kernel: the first takes
- * every cell and parks those still running after park_after substitution
- * steps (0 = never park); the second resumes the parked cells, heaviest
- * predicted first.  ss_batch / tail_batch = ready lanes of a warp needed
- * before the substitution step runs in the first / second pass (1..32);
+ * The batched form runs a sequence of passes of a persistent kernel: the
+ * first takes every cell and parks those still running after park_after
+ * substitution steps (0 = never park, one pass); each later pass resumes the
+ * parked cells with a doubled limit, up to the reference's 500 steps.
+ * ss_batch / tail_batch = ready lanes of a warp needed before the
+ * substitution step runs in the first / later passes (1..32);
  * ctas_per_sm = persistent CTAs of 128 threads per SM (1..16, capped by
  * occupancy); park_after in 0..500.  Values outside the ranges are
  * rejected.  Process-wide. */
@@ -125,6 +126,65 @@ osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm,
  * ready lanes once they have waited more than max_wait Newton trips, even if
  * fewer than ss_batch/tail_batch lanes are ready (0..1000).  Process-wide. */
 osr_status osr_flash_set_max_wait(int max_wait);
+
+/* ---------------------------------------------------------------------------
+ * Grid path: a dual-porosity (matrix + fracture) model on the device.
+ * ------------------------------------------------------------------------- */
+
+/* The content of a Data_Input deck (compsim/Data_Input.cpp:13-1349), HOST
+ * pointers read during osr_grid_create only.  Cell index c = i + nx*(j +
+ * ny*k); per-direction fields are [3][cells] (x, y, z). */
+typedef struct osr_model {
+    int nx, ny, nz;       /* GRID */
+    int nc;               /* NC (pure + pseudo components) */
+    int eos;              /* MODEL: osr_eos */
+    double restemp;       /* RESTEMP in K (deck value + 273.15) */
+    double wat_ro, wat_mu;   /* WATERPROPS */
+    double refp, cpor, dcpor;   /* REFP, CPOR, DCPOR */
+    double lf, re_f, sigma;     /* Lf, Re_f, SIGMA (1 when absent) */
+    int has_cdif;         /* CDIF keyword present */
+    double cdif;          /* its value */
+    const double *di, *dj, *dk;   /* [nx], [ny], [nz] block sizes, m */
+    const double *por, *fpor;     /* [cells] matrix / fracture porosity */
+    const double *perm, *fperm;   /* [3][cells] permeability, mD */
+    const double *mw, *tc, *pc, *vc, *acf, *parachor, *zc;  /* [nc]; vc in cm3/mol as in the deck */
+    const double *kij;            /* [nc*nc] BIC values as listed in the deck (the reference stores 1 - kij) */
+    int nswt, nsgt;
+    const double *swt, *sgt;      /* [n][4]: S, kr, kro, Pc (SWT: water, SGT: gas) */
+    int nwells;
+    const int *wells_i;           /* [nwells][5] type, i, j, k0, k1 (0-based, as the reference stores them) */
+    const double *wells_f;        /* [nwells][nc+6] the well's values (times in s) */
+} osr_model;
+
+typedef struct osr_grid osr_grid;
+
+/* Upload a model; geometric transmissibilities (IFK_Calc,
+ * compsim/Init_Calcs.cpp:21-46) and block heights are formed here. */
+osr_status osr_grid_create(const osr_model *model, osr_grid **out);
+osr_status osr_grid_destroy(osr_grid *grid);
+osr_status osr_grid_dims(osr_grid *grid, int *dims /* [4]: nx, ny, nz, nc */);
+
+/* Set the state of one medium (0 = matrix, 1 = fracture) from HOST arrays:
+ * oil pressure [cells], saturations [3][cells] (water, oil, gas), liquid,
+ * vapour and feed compositions [nc][cells], phase labels [cells], and
+ * optionally the densities of the previous property update [2][cells]
+ * (the interfacial tension is formed from them, as the reference does). */
+osr_status osr_grid_set_state(osr_grid *grid, int medium, const double *P_oil, const double *sat, const double *x,
+                              const double *y, const double *z, const signed char *label, const double *rho);
+
+/* The property sweeps of UpdateDependencies (compsim/PetscAUX.cpp:530-548)
+ * for both media: IFT, relative permeability and capillary pressure, phase
+ * pressures, densities with d rho/dx and d rho/dP, LBC viscosities,
+ * accumulation at the linearisation point, diffusion coefficients, phase
+ * gravity, and the upstream-weighted face transmissibilities. */
+osr_status osr_grid_update_dependencies(osr_grid *grid, void *stream);
+
+/* Copy a device field to HOST memory as doubles: "m.<name>" (matrix) or
+ * "f.<name>" (fracture), names P sat x y z label rho pc mu gam kr dkr dE pre
+ * diff ift trans transS wtran dwtran por perm iftran, laid out [planes][cells].
+ * osr_grid_field_size returns planes*cells (or -1 for an unknown name). */
+long osr_grid_field_size(osr_grid *grid, const char *field);
+osr_status osr_grid_get(osr_grid *grid, const char *field, double *out);
 
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The

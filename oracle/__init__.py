@@ -282,3 +282,88 @@ def flash_parity(got, ref, fields=FLASH_FIELDS):
     return dict(ok=ok, labels_equal=labels_equal, wide_ok=wide_ok, frac_tight=frac_tight,
                 frac_tight_incipient=frac_tight_abs, margin=margin, margin_incipient=margin_abs,
                 max_scaled_err=max_scaled)
+
+
+# ----------------------------------------------------------------------------- deck-driven reference
+
+_FIELD_SHAPES = {"P": (3,), "sat": (3,), "x": ("nc",), "y": ("nc",), "z": ("nc",), "label": (), "rho": (2,),
+                 "pc": (2,), "mu": (2,), "gam": (2,), "kr": (3,), "dkr": (5,), "dE": ("nc1", 2),
+                 "pre": ("nc1",), "diff": ("nc", 2), "ift": (), "trans": (12, 3), "transS": (3, 3),
+                 "wtran": (3,), "dwtran": (3,), "iftran": (3,), "por": (), "perm": (3,), "blockH": ()}
+
+
+class RefDeck:
+    """The reference simulator loaded from a deck (compsim/PrimeSim.cpp:35-85).
+    One instance at a time: the reference keeps its state in globals."""
+
+    def __init__(self, path: str):
+        lib = ref_lib()
+        lib.ref_deck_open.restype = ctypes.c_int
+        lib.ref_get.restype = ctypes.c_long
+        lib.ref_scalar.restype = ctypes.c_double
+        lib.ref_form_jacobian.restype = ctypes.c_long
+        rc = lib.ref_deck_open(path.encode())
+        if rc:
+            raise RuntimeError(f"reference could not open {path}")
+        info = np.zeros(10, np.int32)
+        lib.ref_deck_info(_p(info))
+        self.nx, self.ny, self.nz, self.nc, self.pr, self.rows, self.nwells, self.nswt, self.nsgt, self.cdif = \
+            (int(v) for v in info)
+        self.cells = self.nx * self.ny * self.nz
+        self.lib = lib
+
+    def scalar(self, name: str) -> float:
+        return float(self.lib.ref_scalar(name.encode()))
+
+    def get(self, name: str) -> np.ndarray:
+        key = name.split(".", 1)[-1]
+        if name in ("gridDim",):
+            n = self.nx + self.ny + self.nz
+            shape = (n,)
+        elif name == "fluid":
+            shape = (self.nc, 15)
+        elif name == "bic":
+            shape = (self.nc, self.nc)
+        elif name == "rowoff":
+            shape = (2 * self.cells + 1,)
+        else:
+            dims = tuple(self.nc if d == "nc" else self.nc + 1 if d == "nc1" else d for d in _FIELD_SHAPES[key])
+            shape = dims + (self.cells,)
+        out = np.zeros(int(np.prod(shape)))
+        w = self.lib.ref_get(name.encode(), _p(out))
+        if w < 0:
+            raise KeyError(name)
+        return out.reshape(shape)
+
+    def init_guess(self) -> np.ndarray:
+        self.rows = int(self.lib_info()[5])
+        x = np.zeros(self.rows)
+        self.lib.ref_init_guess(_p(x))
+        return x
+
+    def lib_info(self):
+        info = np.zeros(10, np.int32)
+        self.lib.ref_deck_info(_p(info))
+        return info
+
+    def update_all(self, x, full: bool):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        self.lib.ref_update_all(_p(x), int(full))
+        self.rows = int(self.lib_info()[5])
+
+    def form_function(self, x, t: float = 0.0) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64).copy()
+        f = np.zeros(self.rows)
+        self.lib.ref_form_function(_p(x), _p(f), ctypes.c_double(t))
+        return f
+
+    def form_jacobian(self, x, t: float = 0.0):
+        x = np.ascontiguousarray(x, np.float64).copy()
+        cap = self.rows * 10 * (2 * self.nc + 4)
+        r = np.zeros(cap, np.int32)
+        c = np.zeros(cap, np.int32)
+        v = np.zeros(cap)
+        n = self.lib.ref_form_jacobian(_p(x), ctypes.c_double(t), ctypes.c_long(cap), _p(r), _p(c), _p(v))
+        if n < 0:
+            raise RuntimeError("jacobian triplet buffer too small")
+        return r[:n], c[:n], v[:n]

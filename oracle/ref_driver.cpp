@@ -125,3 +125,226 @@ int ref_eos_params(int nc, int eos, const double *tc, const double *pc, const do
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------------
+ * Deck-driven entry points: the reference reads a Data_Input deck and runs
+ * the initialisation of its main program (compsim/PrimeSim.cpp:35-85); the
+ * driver then exposes its state and property arrays, and evaluates the
+ * PETSc callbacks (FormFunction, FormJacobian, InitGuess2, UpdateAll) on
+ * caller-owned vectors through the PETSc-lite shim.
+ *
+ * Field layout of every dump: cell index c = Ix + Nx*(Iy + Ny*Iz) fastest,
+ * then the array's trailing index (component, phase, direction), e.g.
+ * "m.x" -> [nc][cells], "m.dE" -> [nc+1][2][cells], "m.trans" ->
+ * [12][3][cells].  Prefix "m." = matrix, "f." = fracture.
+ * ------------------------------------------------------------------------ */
+#include "shim_types.h"
+#include "MIfstream.h"
+
+namespace {
+
+long ncell() { return (long)Nx * Ny * Nz; }
+
+template <class F>
+void each_cell(F f) {
+    for (int Iz = 0; Iz < Nz; Iz++)
+        for (int Iy = 0; Iy < Ny; Iy++)
+            for (int Ix = 0; Ix < Nx; Ix++) f(Ix, Iy, Iz, (long)Ix + (long)Nx * (Iy + (long)Ny * Iz));
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Read a deck and initialise as main() does before its time loop. */
+int ref_deck_open(const char *path) {
+    MIfstream fin;
+    fin.open(path, std::ios::in);
+    if (!fin.is_open()) return -1;
+    g_alloc_nc = -1;
+    MPIsize = 1;
+    MPIRank = 0;
+    Data_Input(fin);
+    fin.close();
+    ManageTSMarker();
+    IFK_Calc();
+    Tr_Mu();
+    QInitValue();
+    Edge_Trans();
+    Edge_fTrans();
+    InitWells();
+    WellCompSadeq_cum[0] = WellCompSadeq_cum[1] = WellCompSadeq_cum[2] = 0;
+    SMethQ = 0;
+    UpdateDependencies(true);
+    return 0;
+}
+
+/* Nx, Ny, Nz, Nc, PR, MatrixSize, wellNO, Nswt, Nsgt, IsConstDif */
+void ref_deck_info(int *info) {
+    info[0] = Nx; info[1] = Ny; info[2] = Nz; info[3] = Nc; info[4] = PR;
+    info[5] = MatrixSize; info[6] = wellNO; info[7] = Nswt; info[8] = Nsgt; info[9] = IsConstDif ? 1 : 0;
+}
+
+double ref_scalar(const char *name) {
+    std::string s(name);
+    if (s == "PCoeff") return PCoeff;
+    if (s == "resTemp") return resTemp;
+    if (s == "watRo") return watRo;
+    if (s == "watMu") return watMu;
+    if (s == "refP") return refP;
+    if (s == "cpor") return cpor;
+    if (s == "dcpor") return dcpor;
+    if (s == "Lf") return Lf;
+    if (s == "Re_f") return Re_f;
+    if (s == "SigmaMF") return SigmaMF;
+    if (s == "CDiffCoef") return CDiffCoef;
+    if (s == "Dt") return Dt;
+    return 0.0 / 0.0;
+}
+
+/* Copy a named array into out (layout above); returns values written or -1. */
+long ref_get(const char *name, double *out) {
+    std::string s(name);
+    const long n = ncell();
+    bool fr = s.size() > 2 && s[0] == 'f' && s[1] == '.';
+    std::string k = s.size() > 2 ? s.substr(2) : s;
+    FType *****cp = fr ? fcomp : comp;
+    FType ****pp = fr ? fP : P;
+    FType ****st = fr ? fsat : sat;
+    signed char ***ps = fr ? fphaseStat : phaseStat;
+    FType *****bp = fr ? fblockFProps : blockFProps;
+    FType ****kr = fr ? frelPerm : relPerm;
+    FType ****dkr = fr ? fdRelPerm : dRelPerm;
+    FType *****de = fr ? fdE : dE;
+    FType ****pre = fr ? fpreProp : preProp;
+    FType *****dif = fr ? fdiffusion : diffusion;
+    FType ***ift = fr ? fBift : Bift;
+    FType *****tr = fr ? ftrans : trans;
+    char *****trs = fr ? ftransS : transS;
+    FType ****wt = fr ? fWtran : Wtran;
+    FType ****dwt = fr ? fdWtran : dWtran;
+    FType ****ift3 = fr ? fIFTran : IFTran;
+    FType ***por = fr ? fporosity : porosity;
+    FType ****perm4 = fr ? fperm : perm;
+    long w = 0;
+    if (k == "P") {
+        for (int p = 0; p < 3; p++) each_cell([&](int i, int j, int l, long c) { out[p * n + c] = pp[i + 1][j + 1][l + 1][p]; });
+        w = 3 * n;
+    } else if (k == "sat") {
+        for (int p = 0; p < 3; p++) each_cell([&](int i, int j, int l, long c) { out[p * n + c] = st[i][j][l][p]; });
+        w = 3 * n;
+    } else if (k == "x" || k == "y" || k == "z") {
+        int ph = k == "x" ? 0 : (k == "y" ? 1 : 2);
+        for (int q = 0; q < Nc; q++) each_cell([&](int i, int j, int l, long c) { out[q * n + c] = cp[i][j][l][q][ph]; });
+        w = (long)Nc * n;
+    } else if (k == "label") {
+        each_cell([&](int i, int j, int l, long c) { out[c] = ps[i][j][l]; });
+        w = n;
+    } else if (k == "rho" || k == "pc" || k == "mu" || k == "gam") {
+        int f = k == "rho" ? RO : (k == "pc" ? BLOCK_PC : (k == "mu" ? BMU : BGAM));
+        for (int p = 0; p < 2; p++) each_cell([&](int i, int j, int l, long c) { out[p * n + c] = bp[i][j][l][f][p]; });
+        w = 2 * n;
+    } else if (k == "kr") {
+        for (int p = 0; p < 3; p++) each_cell([&](int i, int j, int l, long c) { out[p * n + c] = kr[i][j][l][p]; });
+        w = 3 * n;
+    } else if (k == "dkr") {
+        for (int p = 0; p < 5; p++) each_cell([&](int i, int j, int l, long c) { out[p * n + c] = dkr[i][j][l][p]; });
+        w = 5 * n;
+    } else if (k == "dE") {
+        for (int q = 0; q <= Nc; q++)
+            for (int p = 0; p < 2; p++) each_cell([&](int i, int j, int l, long c) { out[(q * 2 + p) * n + c] = de[i][j][l][q][p]; });
+        w = (long)(Nc + 1) * 2 * n;
+    } else if (k == "pre") {
+        for (int q = 0; q <= Nc; q++) each_cell([&](int i, int j, int l, long c) { out[q * n + c] = pre[i][j][l][q]; });
+        w = (long)(Nc + 1) * n;
+    } else if (k == "diff") {
+        for (int q = 0; q < Nc; q++)
+            for (int p = 0; p < 2; p++) each_cell([&](int i, int j, int l, long c) { out[(q * 2 + p) * n + c] = dif[i][j][l][q][p]; });
+        w = (long)Nc * 2 * n;
+    } else if (k == "ift") {
+        each_cell([&](int i, int j, int l, long c) { out[c] = ift[i][j][l]; });
+        w = n;
+    } else if (k == "trans") {
+        for (int t = 0; t < 12; t++)
+            for (int d = 0; d < 3; d++) each_cell([&](int i, int j, int l, long c) { out[(t * 3 + d) * n + c] = tr[i + 1][j + 1][l + 1][t][d]; });
+        w = 36 * n;
+    } else if (k == "transS") {
+        for (int t = 0; t < 3; t++)
+            for (int d = 0; d < 3; d++) each_cell([&](int i, int j, int l, long c) { out[(t * 3 + d) * n + c] = trs[i + 1][j + 1][l + 1][t][d]; });
+        w = 9 * n;
+    } else if (k == "wtran" || k == "dwtran") {
+        FType ****a = k == "wtran" ? wt : dwt;
+        for (int d = 0; d < 3; d++) each_cell([&](int i, int j, int l, long c) { out[d * n + c] = a[i + 1][j + 1][l + 1][d]; });
+        w = 3 * n;
+    } else if (k == "iftran") {
+        for (int d = 0; d < 3; d++) each_cell([&](int i, int j, int l, long c) { out[d * n + c] = ift3[i][j][l][d]; });
+        w = 3 * n;
+    } else if (k == "por") {
+        each_cell([&](int i, int j, int l, long c) { out[c] = por[i][j][l]; });
+        w = n;
+    } else if (k == "perm") {
+        for (int d = 0; d < 3; d++) each_cell([&](int i, int j, int l, long c) { out[d * n + c] = perm4[i][j][l][d]; });
+        w = 3 * n;
+    } else if (k == "blockH") {
+        each_cell([&](int i, int j, int l, long c) { out[c] = blockH[i + 1][j + 1][l + 1]; });
+        w = n;
+    } else if (s == "gridDim") {
+        for (int q = 0; q < Nx + Ny + Nz; q++) out[q] = gridDim[q];
+        w = Nx + Ny + Nz;
+    } else if (s == "fluid") {  /* [nc][15] fluidProp */
+        for (int q = 0; q < Nc; q++)
+            for (int f = 0; f < COMP_PROPS; f++) out[q * COMP_PROPS + f] = fluidProp[q][f];
+        w = (long)Nc * COMP_PROPS;
+    } else if (s == "bic") {
+        for (int q = 0; q < Nc; q++)
+            for (int r = 0; r < Nc; r++) out[q * Nc + r] = bic[q][r];
+        w = (long)Nc * Nc;
+    } else if (s == "rowoff") {  /* preConRow[0..2*cells] */
+        for (long q = 0; q <= 2 * n; q++) out[q] = preConRow[q];
+        w = 2 * n + 1;
+    } else {
+        return -1;
+    }
+    return w;
+}
+
+/* UpdateAll(x, full) (compsim/PetscAUX.cpp:176-498). */
+int ref_update_all(double *x, int full) {
+    _p_Vec v{x, MatrixSize};
+    UpdateAll(&v, full != 0);
+    return 0;
+}
+
+/* InitGuess2: state -> x (compsim/PetscAUX.cpp:878-964). */
+int ref_init_guess(double *x) {
+    _p_Vec v{x, MatrixSize};
+    InitGuess2(nullptr, &v, nullptr);
+    return 0;
+}
+
+/* FormFunction(x) -> f (compsim/PetscAUX.cpp:59-104) at simulation time t. */
+int ref_form_function(double *x, double *f, double t) {
+    _p_Vec vx{x, MatrixSize}, vf{f, MatrixSize};
+    SSimTime = t;
+    return FormFunction(nullptr, &vx, &vf, &userData);
+}
+
+/* FormJacobian(x) (compsim/PetscAUX.cpp:106-173): the (row, col, value)
+ * triplets MatSetValues received, in call order.  Returns their count, or
+ * -(count) when cap was too small. */
+long ref_form_jacobian(double *x, double t, long cap, int *rows, int *cols, double *vals) {
+    _p_Vec vx{x, MatrixSize};
+    _p_Mat m;
+    SSimTime = t;
+    FormJacobian(nullptr, &vx, &m, &m, &userData);
+    long cnt = (long)m.v.size();
+    if (cnt > cap) return -cnt;
+    for (long q = 0; q < cnt; q++) {
+        rows[q] = m.r[q];
+        cols[q] = m.c[q];
+        vals[q] = m.v[q];
+    }
+    return cnt;
+}
+
+}  // extern "C"

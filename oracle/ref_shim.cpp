@@ -22,15 +22,7 @@
 #include "mpi.h"
 #include "lapacke.h"
 
-struct _p_Vec {
-    double *a;
-    int n;
-};
-
-struct _p_Mat {
-    std::vector<int> r, c;
-    std::vector<double> v;
-};
+#include "shim_types.h"
 
 /* The stub headers declare these with C++ linkage (the reference includes
  * them from C++ translation units), so they are defined with C++ linkage. */

@@ -189,3 +189,86 @@ def get_shape():
     v = [ctypes.c_int() for _ in range(4)]
     _check(lib().osr_flash_get_shape(*[ctypes.byref(x) for x in v]), "osr_flash_get_shape")
     return tuple(x.value for x in v)
+
+
+# ----------------------------------------------------------------------------- grid path
+
+class _CModel(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nc", ctypes.c_int),
+                ("eos", ctypes.c_int), ("restemp", ctypes.c_double), ("wat_ro", ctypes.c_double),
+                ("wat_mu", ctypes.c_double), ("refp", ctypes.c_double), ("cpor", ctypes.c_double),
+                ("dcpor", ctypes.c_double), ("lf", ctypes.c_double), ("re_f", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("has_cdif", ctypes.c_int), ("cdif", ctypes.c_double),
+                ("di", _vp), ("dj", _vp), ("dk", _vp), ("por", _vp), ("fpor", _vp), ("perm", _vp), ("fperm", _vp),
+                ("mw", _vp), ("tc", _vp), ("pc", _vp), ("vc", _vp), ("acf", _vp), ("parachor", _vp), ("zc", _vp),
+                ("kij", _vp), ("nswt", ctypes.c_int), ("nsgt", ctypes.c_int), ("swt", _vp), ("sgt", _vp),
+                ("nwells", ctypes.c_int), ("wells_i", _vp), ("wells_f", _vp)]
+
+
+class Grid:
+    """A dual-porosity model on the device, built from a parsed deck
+    (``osiris_b200.deck.parse_deck``)."""
+
+    FIELD_PLANES = {"P": 3, "sat": 3, "x": "nc", "y": "nc", "z": "nc", "label": 1, "rho": 2, "pc": 2, "mu": 2,
+                    "gam": 2, "kr": 3, "dkr": 5, "dE": "2nc1", "pre": "nc1", "diff": "2nc", "ift": 1, "trans": 36,
+                    "transS": 9, "wtran": 3, "dwtran": 3, "por": 1, "perm": 3, "iftran": 3}
+
+    def __init__(self, d):
+        self.deck = d
+        self.nc = d.nc
+        self.cells = d.cells
+        keep = dict(di=d.di, dj=d.dj, dk=d.dk, por=d.por, fpor=d.fpor, perm=d.perm, fperm=d.fperm, mw=d.mw, tc=d.tc,
+                    pc=d.pc, vc=d.vc, acf=d.acf, parachor=d.parachor, zc=d.zc, kij=d.kij, swt=d.swt, sgt=d.sgt,
+                    wells_f=d.wells_f)
+        self._keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in keep.items()}
+        self._keep["wells_i"] = np.ascontiguousarray(d.wells_i, dtype=np.int32)
+        k = self._keep
+        m = _CModel(d.nx, d.ny, d.nz, d.nc, d.eos, d.restemp, d.wat_ro, d.wat_mu, d.refp, d.cpor, d.dcpor, d.lf,
+                    d.re_f, d.sigma, 0 if d.cdif is None else 1, 0.0 if d.cdif is None else d.cdif,
+                    *[k[n].ctypes.data for n in ("di", "dj", "dk", "por", "fpor", "perm", "fperm", "mw", "tc", "pc",
+                                                  "vc", "acf", "parachor", "zc", "kij")],
+                    d.swt.shape[0], d.sgt.shape[0], k["swt"].ctypes.data, k["sgt"].ctypes.data,
+                    d.wells_i.shape[0], k["wells_i"].ctypes.data, k["wells_f"].ctypes.data)
+        self._model = m
+        h = ctypes.c_void_p()
+        L = lib()
+        L.osr_grid_field_size.restype = ctypes.c_long
+        _check(L.osr_grid_create(ctypes.byref(m), ctypes.byref(h)), "osr_grid_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().osr_grid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, medium: int, P_oil, sat, x, y, z, label, rho=None):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (P_oil, sat, x, y, z)]
+        lab = np.ascontiguousarray(label, np.int8)
+        r = None if rho is None else np.ascontiguousarray(rho, np.float64)
+        _check(lib().osr_grid_set_state(self._h, int(medium), *[a.ctypes.data for a in arrs], lab.ctypes.data,
+                                        None if r is None else r.ctypes.data), "osr_grid_set_state")
+
+    def update_dependencies(self, stream=None):
+        _check(lib().osr_grid_update_dependencies(self._h, None if stream is None else _vp(stream)),
+               "osr_grid_update_dependencies")
+
+    def get(self, name: str) -> np.ndarray:
+        L = lib()
+        n = L.osr_grid_field_size(self._h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        _check(L.osr_grid_get(self._h, name.encode(), out.ctypes.data), "osr_grid_get")
+        key = name.split(".", 1)[1]
+        planes = self.FIELD_PLANES[key]
+        nc = self.nc
+        shape = {"nc": (nc,), "2nc1": (nc + 1, 2), "nc1": (nc + 1,), "2nc": (nc, 2)}.get(planes)
+        if shape is None:
+            shape = () if planes == 1 else ((12, 3) if key == "trans" else (3, 3) if key == "transS" else (planes,))
+        return out.reshape(shape + (self.cells,))
