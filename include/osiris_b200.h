@@ -154,6 +154,8 @@ typedef struct osr_model {
     int nwells;
     const int *wells_i;           /* [nwells][5] type, i, j, k0, k1 (0-based, as the reference stores them) */
     const double *wells_f;        /* [nwells][nc+6] the well's values (times in s) */
+    const double *tor;            /* [cells] TOR tortuosity, NULL = 1 */
+    double dt;                    /* time-step length in s (DT x 3600) */
 } osr_model;
 
 typedef struct osr_grid osr_grid;
@@ -185,6 +187,55 @@ osr_status osr_grid_update_dependencies(osr_grid *grid, void *stream);
  * osr_grid_field_size returns planes*cells (or -1 for an unknown name). */
 long osr_grid_field_size(osr_grid *grid, const char *field);
 osr_status osr_grid_get(osr_grid *grid, const char *field, double *out);
+
+/* ---------------------------------------------------------------------------
+ * Residual path: the PETSc FormFunction callback on the device.
+ *
+ * Row layout (PJac, compsim/Init_Calcs.cpp:1013-1116): blocks of all matrix
+ * cells in cell order, then all fracture cells.  A two-phase cell owns 2N+4
+ * rows and unknowns [x (N) | y (N), P/PCoeff, Sw, So, Sg]; a one-phase cell N+3
+ * [w (N), P/PCoeff, Sw, S of its phase].  Residual rows of a two-phase cell:
+ * N fugacity equalities, N-1 component balances, total hydrocarbon, water,
+ * sum x - 1, sum y - 1, sum S - 1; of a one-phase cell: N-1 component
+ * balances, total, water, sum w - 1, sum S - 1.
+ * ------------------------------------------------------------------------- */
+
+/* Row offsets of the current phase labels and the pressure scale PCoeff
+ * (the FullTimeStep part of UpdateDependencies: CalcPCoeff and PJac,
+ * compsim/PetscAUX.cpp:502-507).  Synchronises `stream`. */
+osr_status osr_grid_refresh_layout(osr_grid *grid, void *stream);
+osr_status osr_grid_layout(osr_grid *grid, long *n_rows, double *pcoeff);
+osr_status osr_grid_row_offsets(osr_grid *grid, long *out /* HOST [2 cells + 1] */);
+
+/* Time-step length (the reference's Dt, seconds) and, when pcoeff > 0, an
+ * explicit pressure scale. */
+osr_status osr_grid_set_controls(osr_grid *grid, double dt, double pcoeff);
+
+/* The WellCondition latch of a rate-controlled well (switches it to its
+ * bottom-hole-pressure limit; compsim/Do_Cycle.cpp:1745). */
+osr_status osr_grid_set_well_condition(osr_grid *grid, int well, int latched);
+
+/* Effective radius of the well's matrix completions (Calc_Re,
+ * compsim/Minor_NR.cpp:2700-3249), formed once per well at create. */
+osr_status osr_grid_well_radius(osr_grid *grid, int well, double *re);
+
+/* State -> unknowns (InitGuess2, compsim/PetscAUX.cpp:878-964); d_x DEVICE
+ * [n_rows]. */
+osr_status osr_grid_init_guess(osr_grid *grid, double *d_x, void *stream);
+
+/* Unknowns -> state plus the property sweeps (UpdateAll(x, false),
+ * compsim/PetscAUX.cpp:176-498). */
+osr_status osr_grid_update_all(osr_grid *grid, const double *d_x, void *stream);
+
+/* Residual rows at the current state (IteratorFunction,
+ * compsim/Petsc_Functions.cpp:10-6895) into d_f [n_rows]; d_scale (optional,
+ * DEVICE [n_rows]) receives the sum of the absolute values of each row's
+ * terms.  sim_time (s) selects the active wells. */
+osr_status osr_grid_residual(osr_grid *grid, double *d_f, double *d_scale, double sim_time, void *stream);
+
+/* FormFunction (compsim/PetscAUX.cpp:59-104): osr_grid_update_all then
+ * osr_grid_residual. */
+osr_status osr_grid_form_function(osr_grid *grid, const double *d_x, double *d_f, double sim_time, void *stream);
 
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The

@@ -335,6 +335,14 @@ class RefDeck:
             raise KeyError(name)
         return out.reshape(shape)
 
+    def calc_re(self, well: int) -> float:
+        self.lib.ref_calc_re.restype = ctypes.c_double
+        return float(self.lib.ref_calc_re(int(well)))
+
+    def set_well_condition(self, well: int, latched: bool):
+        if self.lib.ref_set_well_condition(int(well), int(bool(latched))):
+            raise IndexError(well)
+
     def init_guess(self) -> np.ndarray:
         self.rows = int(self.lib_info()[5])
         x = np.zeros(self.rows)

@@ -315,6 +315,19 @@ int ref_update_all(double *x, int full) {
     return 0;
 }
 
+/* Calc_Re of well i at its first completion (compsim/Minor_NR.cpp:2700). */
+double ref_calc_re(int i) {
+    if (i < 0 || i >= wellNO) return -1;
+    return Calc_Re(welli[i][1], welli[i][2], welli[i][3], i);
+}
+
+/* The WellCondition latch of well i (compsim/Do_Cycle.cpp:1745). */
+int ref_set_well_condition(int i, int v) {
+    if (i < 0 || i >= wellNO) return -1;
+    WellCondition[i] = v != 0;
+    return 0;
+}
+
 /* InitGuess2: state -> x (compsim/PetscAUX.cpp:878-964). */
 int ref_init_guess(double *x) {
     _p_Vec v{x, MatrixSize};

@@ -202,7 +202,7 @@ class _CModel(ctypes.Structure):
                 ("di", _vp), ("dj", _vp), ("dk", _vp), ("por", _vp), ("fpor", _vp), ("perm", _vp), ("fperm", _vp),
                 ("mw", _vp), ("tc", _vp), ("pc", _vp), ("vc", _vp), ("acf", _vp), ("parachor", _vp), ("zc", _vp),
                 ("kij", _vp), ("nswt", ctypes.c_int), ("nsgt", ctypes.c_int), ("swt", _vp), ("sgt", _vp),
-                ("nwells", ctypes.c_int), ("wells_i", _vp), ("wells_f", _vp)]
+                ("nwells", ctypes.c_int), ("wells_i", _vp), ("wells_f", _vp), ("tor", _vp), ("dt", ctypes.c_double)]
 
 
 class Grid:
@@ -219,7 +219,7 @@ class Grid:
         self.cells = d.cells
         keep = dict(di=d.di, dj=d.dj, dk=d.dk, por=d.por, fpor=d.fpor, perm=d.perm, fperm=d.fperm, mw=d.mw, tc=d.tc,
                     pc=d.pc, vc=d.vc, acf=d.acf, parachor=d.parachor, zc=d.zc, kij=d.kij, swt=d.swt, sgt=d.sgt,
-                    wells_f=d.wells_f)
+                    wells_f=d.wells_f, tor=d.tor)
         self._keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in keep.items()}
         self._keep["wells_i"] = np.ascontiguousarray(d.wells_i, dtype=np.int32)
         k = self._keep
@@ -228,7 +228,8 @@ class Grid:
                     *[k[n].ctypes.data for n in ("di", "dj", "dk", "por", "fpor", "perm", "fperm", "mw", "tc", "pc",
                                                   "vc", "acf", "parachor", "zc", "kij")],
                     d.swt.shape[0], d.sgt.shape[0], k["swt"].ctypes.data, k["sgt"].ctypes.data,
-                    d.wells_i.shape[0], k["wells_i"].ctypes.data, k["wells_f"].ctypes.data)
+                    d.wells_i.shape[0], k["wells_i"].ctypes.data, k["wells_f"].ctypes.data, k["tor"].ctypes.data,
+                    d.dt)
         self._model = m
         h = ctypes.c_void_p()
         L = lib()
@@ -257,6 +258,56 @@ class Grid:
     def update_dependencies(self, stream=None):
         _check(lib().osr_grid_update_dependencies(self._h, None if stream is None else _vp(stream)),
                "osr_grid_update_dependencies")
+
+    # -- residual path -------------------------------------------------------
+    def refresh_layout(self, stream=None):
+        """Row offsets of the current phase labels and PCoeff (PJac, CalcPCoeff)."""
+        _check(lib().osr_grid_refresh_layout(self._h, None if stream is None else _vp(stream)),
+               "osr_grid_refresh_layout")
+        return self.layout()
+
+    def layout(self):
+        rows = ctypes.c_long()
+        pc = ctypes.c_double()
+        _check(lib().osr_grid_layout(self._h, ctypes.byref(rows), ctypes.byref(pc)), "osr_grid_layout")
+        return rows.value, pc.value
+
+    def row_offsets(self) -> np.ndarray:
+        out = np.zeros(2 * self.cells + 1, np.int64)
+        _check(lib().osr_grid_row_offsets(self._h, out.ctypes.data), "osr_grid_row_offsets")
+        return out
+
+    def set_controls(self, dt: float, pcoeff: float = 0.0):
+        _check(lib().osr_grid_set_controls(self._h, ctypes.c_double(dt), ctypes.c_double(pcoeff)),
+               "osr_grid_set_controls")
+
+    def set_well_condition(self, well: int, latched: bool):
+        _check(lib().osr_grid_set_well_condition(self._h, int(well), int(bool(latched))), "osr_grid_set_well_condition")
+
+    def well_radius(self, well: int) -> float:
+        v = ctypes.c_double()
+        _check(lib().osr_grid_well_radius(self._h, int(well), ctypes.byref(v)), "osr_grid_well_radius")
+        return v.value
+
+    def init_guess(self, d_x, stream=None):
+        """Write the unknown vector of the current state into device memory d_x (a CUDA tensor)."""
+        _check(lib().osr_grid_init_guess(self._h, _vp(d_x.data_ptr()), None if stream is None else _vp(stream)),
+               "osr_grid_init_guess")
+
+    def update_all(self, d_x, stream=None):
+        _check(lib().osr_grid_update_all(self._h, _vp(d_x.data_ptr()), None if stream is None else _vp(stream)),
+               "osr_grid_update_all")
+
+    def residual(self, d_f, d_scale=None, sim_time: float = 0.0, stream=None):
+        _check(lib().osr_grid_residual(self._h, _vp(d_f.data_ptr()),
+                                       None if d_scale is None else _vp(d_scale.data_ptr()),
+                                       ctypes.c_double(sim_time), None if stream is None else _vp(stream)),
+               "osr_grid_residual")
+
+    def form_function(self, d_x, d_f, sim_time: float = 0.0, stream=None):
+        _check(lib().osr_grid_form_function(self._h, _vp(d_x.data_ptr()), _vp(d_f.data_ptr()),
+                                            ctypes.c_double(sim_time), None if stream is None else _vp(stream)),
+               "osr_grid_form_function")
 
     def get(self, name: str) -> np.ndarray:
         L = lib()

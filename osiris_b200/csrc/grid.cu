@@ -6,25 +6,8 @@
 #include <string>
 #include <vector>
 #include "osiris_b200.h"
-#include "grid_kernels.cuh"
 
-struct osr_grid {
-    int nx, ny, nz, nc, eos;
-    long cells;
-    double T, wat_ro, wat_mu, refp, cpor, dcpor, lf, re_f, sigma, cdif;
-    int const_dif;
-    std::vector<double> mw, tc, pc, vc, acf, parachor, zc, kij;
-    std::vector<double> swt, sgt;
-    std::vector<int> wells_i;
-    std::vector<double> wells_f;
-    int nwells;
-    // device
-    char *block = nullptr;
-    size_t block_bytes = 0;
-    double *di = nullptr, *dj = nullptr, *dk = nullptr, *blockH = nullptr, *d_swt = nullptr, *d_sgt = nullptr;
-    osr::MediumFields m[2];
-    cudaStream_t stream = nullptr;
-};
+#include "grid_internal.h"
 
 namespace osr {
 
@@ -36,64 +19,7 @@ static osr_status gfail(cudaError_t) { return OSR_ERR_CUDA; }
         if (e_ != cudaSuccess) return gfail(e_);    \
     } while (0)
 
-// Per-component constants at the reservoir temperature, formed with the
-// reference's expressions: EOS_Init (compsim/Init_Calcs.cpp:66-97), Tr_Mu
-// (:48-64) and the pair factors of CalcDiffusion (compsim/Mass_Tran.cpp:43-46).
-template <int N>
-static void make_grid_fluid(const osr_grid &g, GridFluid<N> &G) {
-    std::memset(&G, 0, sizeof(G));
-    FluidTable<N> &t = G.f;
-    t.srk = g.eos == OSR_EOS_SRK;
-    double coldia[N], epdia[N];
-    for (int i = 0; i < N; i++) {
-        double tc = g.tc[i], pc = g.pc[i], w = g.acf[i];
-        coldia[i] = 0.1866 * pow(g.vc[i], 1.0 / 3.0) * pow(g.zc[i], -1.2);
-        epdia[i] = 65.3 * tc * pow(g.zc[i], 3.6);
-        double tr = g.T / tc;
-        t.pc[i] = pc;
-        t.tc[i] = tc;
-        t.wil[i] = 5.37 * (1 + w);
-        double ac, m, b;
-        if (t.srk) {
-            ac = 0.42747 * kR * kR * tc * tc / pc;
-            m = 0.48508 + 1.55171 * w - 0.15613 * w * w;
-            b = 0.08664 * kR * tc / pc;
-        } else {
-            ac = 0.457235 * kR * kR * tc * tc / pc;
-            m = 0.3796 + 1.485 * w - 0.1644 * w * w + 0.01667 * w * w * w;
-            b = 0.077796 * kR * tc / pc;
-        }
-        t.ac[i] = ac;
-        t.m[i] = m;
-        t.b[i] = b;
-        double a = ac * (1 + m * (1 - sqrt(tr))) * (1 + m * (1 - sqrt(tr)));
-        G.sa[i] = sqrt(a);
-        for (int j = 0; j < N; j++) t.bic[i * N + j] = 1 - g.kij[i * N + j];
-        G.mw[i] = g.mw[i];
-        G.smw[i] = sqrt(g.mw[i]);
-        double gamma = pow(tc, (1.0 / 6)) / (sqrt(g.mw[i]) * pow((pc / 101325), (2.0 / 3)));
-        G.mui[i] = (4.61 * pow(tr, 0.618) - 2.04 * exp(-0.449 * tr) + 1.94 * exp(-4.058 * tr) + 0.1) * 1e-4 / gamma;
-        G.vcm[i] = g.vc[i] / 1000000.0;
-        G.pcr_atm[i] = pc / 101325;
-        G.vc53[i] = pow(G.vcm[i], (5.0 / 3.0));
-        G.vc23[i] = pow(G.vcm[i], (2.0 / 3.0));
-        G.parachor[i] = g.parachor[i];
-    }
-    for (int j = 0; j < N; j++) {
-        for (int k = 0; k < N; k++) {
-            if (j == k) continue;
-            double Sij = (coldia[j] + coldia[k]) / 2;
-            double Tij = g.T / sqrt(epdia[j] * epdia[k]);
-            double Oij = 1.06306 * pow(Tij, -0.1561) + 0.193 * exp(-0.47635 * Tij) + 1.03587 * exp(-1.52996 * Tij) +
-                         1.76474 * exp(-3.89411 * Tij);
-            G.pD[j * N + k] = 188.2922475 * sqrt(g.T * (1.0 / g.mw[j] + 1.0 / g.mw[k])) / (kR * Oij * Sij * Sij);
-            G.pDlast[j] = G.pD[j * N + k];
-        }
-    }
-    G.T = g.T;
-}
-
-static GridScalars scalars(const osr_grid &g) {
+GridScalars grid_scalars(const osr_grid &g) {
     GridScalars s;
     s.nx = g.nx;
     s.ny = g.ny;
@@ -117,7 +43,7 @@ template <int N>
 static osr_status update_n(osr_grid &g, cudaStream_t st) {
     GridArgs<N> a;
     make_grid_fluid<N>(g, a.g);
-    a.s = scalars(g);
+    a.s = grid_scalars(g);
     a.geo = GridGeom{g.di, g.dj, g.dk, g.blockH};
     a.m[0] = g.m[0];
     a.m[1] = g.m[1];
@@ -128,6 +54,17 @@ static osr_status update_n(osr_grid &g, cudaStream_t st) {
     face_trans_kernel<N><<<dim3((unsigned)blocks, 2), 128, 0, st>>>(a);
     GRID_CUDA(cudaGetLastError());
     return OSR_OK;
+}
+
+osr_status grid_update(osr_grid &g, cudaStream_t s) {
+    switch (g.nc) {
+#define GRID_NC(K) \
+    case K: return update_n<K>(g, s);
+        GRID_NC(1) GRID_NC(2) GRID_NC(3) GRID_NC(4) GRID_NC(5) GRID_NC(6) GRID_NC(7) GRID_NC(8) GRID_NC(9)
+        GRID_NC(10) GRID_NC(11) GRID_NC(12) GRID_NC(13) GRID_NC(14) GRID_NC(15) GRID_NC(16)
+#undef GRID_NC
+        default: return OSR_ERR_NC;
+    }
 }
 
 // Geometry of IFK_Calc (compsim/Init_Calcs.cpp:21-46) and CalcBlockHeight
@@ -331,12 +268,20 @@ osr_status osr_grid_create(const osr_model *md, osr_grid **out) {
         delete g;
         return osr::gfail(e);
     }
+    osr_status st = osr::grid_assembly_init(*g, md);
+    if (st != OSR_OK) {
+        osr::grid_assembly_free(*g);
+        cudaFree(g->block);
+        delete g;
+        return st;
+    }
     *out = g;
     return OSR_OK;
 }
 
 osr_status osr_grid_destroy(osr_grid *g) {
     if (!g) return OSR_ERR_ARG;
+    osr::grid_assembly_free(*g);
     if (g->block) cudaFree(g->block);
     delete g;
     return OSR_OK;
@@ -364,15 +309,7 @@ osr_status osr_grid_set_state(osr_grid *g, int medium, const double *P_oil, cons
 
 osr_status osr_grid_update_dependencies(osr_grid *g, void *stream) {
     if (!g) return OSR_ERR_ARG;
-    cudaStream_t s = (cudaStream_t)stream;
-    switch (g->nc) {
-#define GRID_NC(K) \
-    case K: return osr::update_n<K>(*g, s);
-        GRID_NC(1) GRID_NC(2) GRID_NC(3) GRID_NC(4) GRID_NC(5) GRID_NC(6) GRID_NC(7) GRID_NC(8) GRID_NC(9)
-        GRID_NC(10) GRID_NC(11) GRID_NC(12) GRID_NC(13) GRID_NC(14) GRID_NC(15) GRID_NC(16)
-#undef GRID_NC
-        default: return OSR_ERR_NC;
-    }
+    return osr::grid_update(*g, (cudaStream_t)stream);
 }
 
 long osr_grid_field_size(osr_grid *g, const char *field) {

@@ -461,6 +461,26 @@ def config_deck(nx=10, ny=10, nz=3, seed=1, cdif=0.0, ipress=2e7, iws=0.2, reste
                 figc=list(igc))
 
 
+def all_wells_deck(ipress=9e6, cdif=None) -> dict:
+    """A 6 x 5 x 3 plain-case grid carrying one well of every type 0..8, at
+    interior, edge and corner blocks (so every branch of the completion
+    radius is used), two-phase at 9 MPa."""
+    spec = config_deck(nx=6, ny=5, nz=3, cdif=cdif, ipress=ipress, seed=9)
+    t = [1, 17520]
+    spec["wells"] = [
+        [0, 3, 3, 1, 2, 9.5e6, 1e-6, 0.5, 0.1] + t,       # constant Pwf production, interior, rate cap
+        [1, 1, 3, 1, 3, 9.5e6, 1e-6, 0, 0.1] + t,         # constant Pwf gas production, edge x = 0
+        [2, 6, 3, 2, 3, 9.5e6, 1e-6, 0, 0.1] + t,         # constant Pwf water injection, edge x = nx
+        [3, 3, 1, 1, 3, 9.5e6, 1e-6, 0, 0.1, 0.9, 0.1, 0.0] + t,  # constant Pwf gas injection, edge y = 0
+        [4, 3, 5, 1, 3, 0.5, 8e6, 0, 0.1] + t,            # constant oil rate, edge y = ny
+        [5, 1, 5, 1, 3, 8e6, 0.5, 0, 0.1] + t,            # constant gas rate, corner (0, ny)
+        [6, 6, 1, 1, 3, 0.5, 8e6, 0, 0.1] + t,            # constant total rate, corner (nx, 0)
+        [7, 2, 2, 1, 3, 0.5, 9.5e6, 0, 0.1] + t,          # constant water injection rate, interior
+        [8, 5, 4, 1, 3, 0.5, 9.5e6, 0, 0.1, 1, 0, 0] + t,  # constant gas injection rate, interior
+    ]
+    return spec
+
+
 def sample_deck(ipress=12000000.0, iws=0.2, cdif=0.0) -> dict:
     """The reference's own sample deck (compsim/test.dat): 10 x 10 x 5,
     PR with C1 C2 nC5 nC10 nC15, initial pressure 12 MPa, feed
