@@ -32,7 +32,8 @@ typedef enum {
     OSR_ERR_NC = 2,        /* component count outside 1..OSR_MAX_NC */
     OSR_ERR_CUDA = 3,      /* a CUDA runtime call failed (see osr_last_cuda_error) */
     OSR_ERR_NODEVICE = 4,  /* no sm_100 device is current */
-    OSR_ERR_SIZE = 5       /* request larger than the entry point supports */
+    OSR_ERR_SIZE = 5,      /* request larger than the entry point supports */
+    OSR_ERR_UNSUPPORTED = 6  /* a cell state the entry point does not cover (see its description) */
 } osr_status;
 
 typedef enum { OSR_EOS_PR = 0, OSR_EOS_SRK = 1 } osr_eos;
@@ -236,6 +237,45 @@ osr_status osr_grid_residual(osr_grid *grid, double *d_f, double *d_scale, doubl
 /* FormFunction (compsim/PetscAUX.cpp:59-104): osr_grid_update_all then
  * osr_grid_residual. */
 osr_status osr_grid_form_function(osr_grid *grid, const double *d_x, double *d_f, double sim_time, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Jacobian path: the PETSc FormJacobian callback on the device.
+ *
+ * Output: a uniform block-sparse matrix with block size bs = 2N+4 and eight
+ * block slots per block row (this cell-medium, -x, +x, -y, +y, -z, +z
+ * neighbours, the same cell of the other continuum; osr_grid_block_columns
+ * gives each slot's block column, -1 when absent).  Block rows/columns follow
+ * the row layout of osr_grid_refresh_layout; a one-phase cell uses the first
+ * N+3 rows and columns of its blocks.  vals [2 cells][8][bs][bs] row-major.
+ * The reference adds a few entries outside this pattern (some total-row
+ * neighbour columns counted from the following block's offset); they are
+ * returned per block row as (local row, global column, value) triples,
+ * ovf_* [2 cells][overflow], counts ovf_n [2 cells].  All DEVICE pointers.
+ * The matrix is the reference's IteratorJacobian (compsim/Petsc_Functions.cpp:
+ * 6898-42073) entry for entry, including its approximate derivatives; the
+ * PETSc adapter adds these values with MatSetValues(ADD_VALUES).
+ * ------------------------------------------------------------------------- */
+typedef struct osr_jacobian_out {
+    double *vals;
+    int *ovf_row;
+    long *ovf_col;
+    double *ovf_val;
+    int *ovf_n;
+} osr_jacobian_out;
+
+osr_status osr_grid_jacobian_shape(osr_grid *grid, int *bs, int *slots, int *overflow);
+osr_status osr_grid_block_columns(osr_grid *grid, long *out /* HOST [2 cells][8] */);
+
+/* The Jacobian at the current state (after osr_grid_update_all or
+ * osr_grid_form_function).  Cells of both continua in the two-phase state
+ * are covered; a one-phase cell-medium leaves its block row zero and the
+ * call returns OSR_ERR_UNSUPPORTED.  Synchronises `stream`. */
+osr_status osr_grid_jacobian(osr_grid *grid, double sim_time, const osr_jacobian_out *out, void *stream);
+
+/* FormJacobian (compsim/PetscAUX.cpp:106-173): osr_grid_update_all then
+ * osr_grid_jacobian. */
+osr_status osr_grid_form_jacobian(osr_grid *grid, const double *d_x, double sim_time, const osr_jacobian_out *out,
+                                  void *stream);
 
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The

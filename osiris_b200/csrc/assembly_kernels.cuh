@@ -568,6 +568,29 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
     }
 }
 
+// Well rates and productivity indices of every cell-medium at the current
+// state ([2 cells][3] water, oil, gas) and the injection well setting each
+// completion's component split (-1 when none).
+template <int N>
+__global__ void well_terms_kernel(const __grid_constant__ AsmArgs<N> A, double *q, double *pi, int *iw) {
+    const GridScalars &s = A.a.s;
+    const long n = s.cells;
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < 2 * n; b += (long)gridDim.x * blockDim.x) {
+        const int med = b >= n;
+        const long c = med ? b - n : b;
+        const int ix = (int)(c % s.nx), iy = (int)((c / s.nx) % s.ny), iz = (int)(c / ((long)s.nx * s.ny));
+        WellRates r;
+        well_rates<N>(A, med, c, ix, iy, iz, r);
+        q[3 * b] = r.Qw;
+        q[3 * b + 1] = r.Qo;
+        q[3 * b + 2] = r.Qg;
+        pi[3 * b] = r.PIw;
+        pi[3 * b + 1] = r.PIo;
+        pi[3 * b + 2] = r.PIg;
+        iw[b] = r.iwell;
+    }
+}
+
 // Fugacity of component i in one phase at the phase's own pressure with Z
 // taken from the stored density, as the two-phase rows evaluate it
 // (compsim/Petsc_Functions.cpp:4559-4621).

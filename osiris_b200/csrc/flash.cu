@@ -432,6 +432,7 @@ const char *osr_status_string(osr_status s) {
         case OSR_ERR_CUDA: return "CUDA runtime error";
         case OSR_ERR_NODEVICE: return "no suitable CUDA device";
         case OSR_ERR_SIZE: return "request exceeds the entry point's size limit";
+        case OSR_ERR_UNSUPPORTED: return "a cell state the entry point does not cover";
     }
     return "unknown status";
 }

@@ -38,6 +38,10 @@ struct osr_grid {
     osr::WellStream *d_ws = nullptr;
     std::vector<double> re_host;
     std::vector<unsigned char> cond_host;
+    // Jacobian scratch: per cell-medium well rates / productivity indices,
+    // injection-well index, injected gas compositions, unsupported-cell count
+    double *jw_q = nullptr, *jw_pi = nullptr, *j_stream_y = nullptr;
+    int *jw_iw = nullptr, *j_unsup = nullptr;
 };
 
 namespace osr {
