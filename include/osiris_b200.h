@@ -267,9 +267,10 @@ osr_status osr_grid_jacobian_shape(osr_grid *grid, int *bs, int *slots, int *ove
 osr_status osr_grid_block_columns(osr_grid *grid, long *out /* HOST [2 cells][8] */);
 
 /* The Jacobian at the current state (after osr_grid_update_all or
- * osr_grid_form_function).  Cells of both continua in the two-phase state
- * are covered; a one-phase cell-medium leaves its block row zero and the
- * call returns OSR_ERR_UNSUPPORTED.  Synchronises `stream`. */
+ * osr_grid_form_function): every cell-medium in any phase state; inactive
+ * cell-media (porosity < 1e-10) get a unit diagonal as in the reference.
+ * Returns OSR_ERR_UNSUPPORTED if a cell-medium falls outside the covered
+ * cases (none do in this version).  Synchronises `stream`. */
 osr_status osr_grid_jacobian(osr_grid *grid, double sim_time, const osr_jacobian_out *out, void *stream);
 
 /* FormJacobian (compsim/PetscAUX.cpp:106-173): osr_grid_update_all then

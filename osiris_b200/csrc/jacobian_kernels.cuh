@@ -247,6 +247,21 @@ OSR_HD inline long upstream(const JFace &e, const FaceData &fd, long c, int p) {
     return fd.ts[p] ? c : e.nb;
 }
 
+// Columns of a cell's own unknowns by phase state (the reference's reCol /
+// reCol3 offsets): a one-phase cell has no column for the absent phase's
+// composition and saturation, and an oil-only or gas-only cell emits its own
+// saturation derivatives only for the phases it carries.
+struct OwnLayout {
+    int P, Sw, So, Sg, X, Y;
+    bool swso, sg, x, y;
+};
+
+OSR_HD inline OwnLayout own_layout(int N, int lab) {
+    if (lab == 0) return OwnLayout{2 * N, 2 * N + 1, 2 * N + 2, 2 * N + 3, 0, N, true, true, true, true};
+    if (lab == 1) return OwnLayout{N, N + 1, N + 2, -1, 0, -1, true, false, true, false};
+    return OwnLayout{N, N + 1, -1, N + 2, -1, 0, false, true, false, true};
+}
+
 // Mobility-ratio derivative factors of one phase across a face: the
 // derivatives of (rho_c dl + rho_n dn C) / (mu_c dl + mu_n dn C) and of the
 // face-averaged gravity with respect to a variable of this cell (M, MG) and
@@ -682,10 +697,13 @@ OSR_HD inline void matrix_comp_row_2ph(const JacView &v, long c, int i, const Bl
     for (int q = 0; q < nf; q++) comp_face_ps(v, M, i, fc[q], matrix_comp_quirks(fc[q]), out, row, a, false);
     // this cell's pressure and saturations (with the completion's productivity terms)
     const WellAt W = well_at(v, 0, c, i, yi);
-    out.add(0, row, 2 * N, v.pcoeff * (dLdp + a.dp + xi * W.PIo + W.gcomp * W.PIg));
-    out.add(0, row, 2 * N + 1, -a.dSw);
-    out.add(0, row, 2 * N + 2, dLdSo - a.dSo);
-    out.add(0, row, 2 * N + 3, dLdSg - a.dSg);
+    const OwnLayout L = own_layout(N, lm);
+    out.add(0, row, L.P, v.pcoeff * (dLdp + a.dp + xi * W.PIo + W.gcomp * W.PIg));
+    if (L.swso) {
+        out.add(0, row, L.Sw, -a.dSw);
+        out.add(0, row, L.So, dLdSo - a.dSo);
+    }
+    if (L.sg) out.add(0, row, L.Sg, dLdSg - a.dSg);
     // the fracture's pressure and saturations
     const int rf = lf ? N : 0;
     if (lf == 1) out.add(7, row, 2 * N + 2 - rf, dRfdSo);
@@ -736,8 +754,8 @@ OSR_HD inline void matrix_comp_row_2ph(const JacView &v, long c, int i, const Bl
             out.add(7, row, k, dRfxl);
             out.add(7, row, N + k, dRfxg);
         }
-        out.add(0, row, k, (Vb / v.dt) * pm * M.S(1) * dLxl - dQxl - dRxl);
-        out.add(0, row, N + k, (Vb / v.dt) * pm * M.S(2) * dLxg - dQxg - dRxg);
+        if (L.x) out.add(0, row, L.X + k, (Vb / v.dt) * pm * M.S(1) * dLxl - dQxl - dRxl);
+        if (L.y) out.add(0, row, L.Y + k, (Vb / v.dt) * pm * M.S(2) * dLxg - dQxg - dRxg);
     }
 }
 
@@ -883,10 +901,13 @@ OSR_HD inline void total_row_2ph(const JacView &v, int med, long c, const BlockR
     const double dROSo = sg * (med ? smSo : sfSo), dROSg = sg * (med ? smSg : sfSg), dROSw = sg * (med ? smSw : sfSw);
     for (int q = 0; q < nf; q++) comp_face_ps(v, O, 0, fc[q], matrix_total_quirks(fc[q]), out, row, a, med == 1, true);
     const WellAt W = well_at(v, med, c, 0, 0.0);
-    out.add(0, row, 2 * N, v.pcoeff * (dLdp + a.dp + W.PIo + W.PIg));
-    out.add(0, row, 2 * N + 1, -a.dSw);
-    out.add(0, row, 2 * N + 2, dLdSo - a.dSo);
-    out.add(0, row, 2 * N + 3, dLdSg - a.dSg);
+    const OwnLayout L = own_layout(N, O.label());
+    out.add(0, row, L.P, v.pcoeff * (dLdp + a.dp + W.PIo + W.PIg));
+    if (L.swso) {
+        out.add(0, row, L.Sw, -a.dSw);
+        out.add(0, row, L.So, dLdSo - a.dSo);
+    }
+    if (L.sg) out.add(0, row, L.Sg, dLdSg - a.dSg);
     const int rf = lo ? N : 0;
     if (lo == 1) out.add(7, row, 2 * N + 2 - rf, dROSo);
     else if (lo == -1) out.add(7, row, 2 * N + 2 - rf, dROSg);
@@ -906,9 +927,10 @@ OSR_HD inline void total_row_2ph(const JacView &v, int med, long c, const BlockR
         const double yf = -kSIC * visc_deriv(Fr, k, 1) * rg * SF2 * Vb * t.krg * pf / (t.Dg * t.Dg) * t.dPg * (pm + pf);
         double dRxl = sg * (med ? xf : xm), dRxg = sg * (med ? yf : ym);
         const double dROxl = sg * (med ? xm : xf), dROxg = sg * (med ? ym : yf);
-        for (int q = 0; q < nf; q++) comp_face_x(v, O, 0, k, fc[q], matrix_comp_quirks(fc[q]), out, row, dRxl, dRxg, med == 1, true);
-        out.add(0, row, k, (Vb / v.dt) * po_ * O.S(1) * O.dE(k, 0) - dRxl);
-        out.add(0, row, N + k, (Vb / v.dt) * po_ * O.S(2) * O.dE(k, 1) - dRxg);
+        const FaceQuirks none{false, false, false, false, false, false, false};
+        for (int q = 0; q < nf; q++) comp_face_x(v, O, 0, k, fc[q], none, out, row, dRxl, dRxg, med == 1, true);
+        if (L.x) out.add(0, row, L.X + k, (Vb / v.dt) * po_ * O.S(1) * O.dE(k, 0) - dRxl);
+        if (L.y) out.add(0, row, L.Y + k, (Vb / v.dt) * po_ * O.S(2) * O.dE(k, 1) - dRxg);
         if (lo == 1) out.add(7, row, k, dROxl);
         else if (lo == -1) out.add(7, row, k, dROxg);
         else {
@@ -931,14 +953,16 @@ OSR_HD inline void water_row_2ph(const JacView &v, int med, long c, const BlockR
     const double dLdp = (t.Vb / v.dt) * wr * O.S(0) * dpo_;
     const double dLdSw = (t.Vb / v.dt) * (po_ * wr);
     const double tr = kSIC * v.wat_ro * kWatMRo * t.SF2 * t.krw / v.wat_mu * t.Vb;
-    double dRdp = -sg * tr;
-    const double dROdp = sg * tr;
+    // both continua's water rows take -tr for their own pressure, +tr for the other's
+    double dRdp = -tr;
+    const double dROdp = tr;
     JFace fc[6];
     const int nf = jac_faces(v, c, fc);
     const long n = v.n;
     for (int q = 0; q < nf; q++) dRdp += F.wtran[(long)fc[q].d * n + fc[q].tc];
     const WellAt W = well_at(v, med, c, 0, 0.0);
-    out.add(0, row, 2 * N, v.pcoeff * (dLdp + dRdp + W.PIw));
+    const OwnLayout L = own_layout(N, O.label());
+    out.add(0, row, L.P, v.pcoeff * (dLdp + dRdp + W.PIw));
     const double smw = kSIC * kWatMRo * t.dkm[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
     const double sfw = kSIC * kWatMRo * t.dkf[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
     double dRdSw = sg * (med ? sfw : smw);
@@ -954,7 +978,7 @@ OSR_HD inline void water_row_2ph(const JacView &v, int med, long c, const BlockR
         if (upstream(e, fd, c, 2) == e.nb) out.add(e.slot, row, nbase + 2 * N + 1, dsw);
         else dRdSw += dsw;
     }
-    out.add(0, row, 2 * N + 1, dLdSw - dRdSw);
+    out.add(0, row, L.P + 1, dLdSw - dRdSw);
     const int rf = (med ? M : Fr).label() ? N : 0;
     out.add(7, row, 2 * N - rf, v.pcoeff * dROdp);
     out.add(7, row, 2 * N + 1 - rf, dROSw);
@@ -1046,10 +1070,13 @@ OSR_HD inline void fracture_comp_row_2ph(const JacView &v, long c, int i, const 
     a.dSw -= kSIC * t.dkf[1] * po;
     for (int q = 0; q < nf; q++) comp_face_ps(v, Fr, i, fc[q], fracture_comp_quirks(fc[q]), out, row, a, true);
     const WellAt W = well_at(v, 1, c, i, fyi);
-    out.add(0, row, 2 * N, v.pcoeff * (dLdp + a.dp + fxi * W.PIo + W.gcomp * W.PIg));
-    out.add(0, row, 2 * N + 1, -a.dSw);
-    out.add(0, row, 2 * N + 2, dLdSo - a.dSo);
-    out.add(0, row, 2 * N + 3, dLdSg - a.dSg);
+    const OwnLayout L = own_layout(N, lf);
+    out.add(0, row, L.P, v.pcoeff * (dLdp + a.dp + fxi * W.PIo + W.gcomp * W.PIg));
+    if (L.swso) {
+        out.add(0, row, L.Sw, -a.dSw);
+        out.add(0, row, L.So, dLdSo - a.dSo);
+    }
+    if (L.sg) out.add(0, row, L.Sg, dLdSg - a.dSg);
     const int rm = lm ? N : 0;
     if (lm == 1) out.add(7, row, 2 * N + 2 - rm, dRMdSo);
     else if (lm == -1) out.add(7, row, 2 * N + 2 - rm, dRMdSg);
@@ -1107,8 +1134,8 @@ OSR_HD inline void fracture_comp_row_2ph(const JacView &v, long c, int i, const 
             out.add(7, row, k, dRMxl);
             out.add(7, row, N + k, dRMxg);
         }
-        out.add(0, row, k, (Vb / v.dt) * pf * Fr.S(1) * dLxl - dQxl - dRxl);
-        out.add(0, row, N + k, (Vb / v.dt) * pf * Fr.S(2) * dLxg - dQxg - dRxg);
+        if (L.x) out.add(0, row, L.X + k, (Vb / v.dt) * pf * Fr.S(1) * dLxl - dQxl - dRxl);
+        if (L.y) out.add(0, row, L.Y + k, (Vb / v.dt) * pf * Fr.S(2) * dLxg - dQxg - dRxg);
     }
 }
 
@@ -1120,16 +1147,29 @@ OSR_HD inline bool jacobian_block(const JacView &v, long b) {
     const long c = med ? b - v.n : b;
     const BlockRow out{&v, b};
     const Cell q{&v, &v.m[med], c};
-    if (q.label() != 0) return false;
-    fugacity_rows(v, q, out);
-    if (med == 0) {
-        for (int i = 0; i < N - 1; i++) matrix_comp_row_2ph(v, c, i, out, N + i);
-    } else {
-        for (int i = 0; i < N - 1; i++) fracture_comp_row_2ph(v, c, i, out, N + i);
+    const int lab = q.label();
+    const int rows = lab == 0 ? 2 * N + 4 : N + 3;
+    if (q.por() < 1e-10) {
+        // an inactive cell-medium: unit diagonal
+        for (int r = 0; r < rows; r++) out.add(0, r, r, 1.0);
+        return true;
     }
-    total_row_2ph(v, med, c, out, 2 * N - 1);
-    water_row_2ph(v, med, c, out, 2 * N);
-    constraint_rows_2ph(v, out);
+    const int r0 = lab == 0 ? N : 0;
+    if (lab == 0) fugacity_rows(v, q, out);
+    if (med == 0)
+        for (int i = 0; i < N - 1; i++) matrix_comp_row_2ph(v, c, i, out, r0 + i);
+    else
+        for (int i = 0; i < N - 1; i++) fracture_comp_row_2ph(v, c, i, out, r0 + i);
+    total_row_2ph(v, med, c, out, r0 + N - 1);
+    water_row_2ph(v, med, c, out, r0 + N);
+    if (lab == 0) {
+        constraint_rows_2ph(v, out);
+    } else {
+        const OwnLayout L = own_layout(N, lab);
+        for (int k = 0; k < N; k++) out.add(0, N + 1, (lab == 1 ? L.X : L.Y) + k, 1.0);
+        out.add(0, N + 2, L.Sw, 1.0);
+        out.add(0, N + 2, lab == 1 ? L.So : L.Sg, 1.0);
+    }
     return true;
 }
 

@@ -407,13 +407,27 @@ def write_deck(path: str, spec: dict) -> str:
     L.append(f"DTMAX {_fmt(spec.get('dtmax', 100))}")
     if spec.get("cdif") is not None:
         L.append(f"CDIF {_fmt(spec['cdif'])}")
-    L.append("INITCOND 3")
-    L.append(f"IPRESS {_fmt(spec['ipress'])}")
-    L.append(f"IWS {_fmt(spec['iws'])}")
-    L.append("IGC " + " ".join(_fmt(x) for x in spec["igc"]))
-    L.append(f"FIPRESS {_fmt(spec['fipress'])}")
-    L.append(f"FIWS {_fmt(spec['fiws'])}")
-    L.append("FIGC " + " ".join(_fmt(x) for x in spec["figc"]))
+    if np.ndim(spec["ipress"]) == 0:
+        L.append("INITCOND 3")
+        L.append(f"IPRESS {_fmt(spec['ipress'])}")
+        L.append(f"IWS {_fmt(spec['iws'])}")
+        L.append("IGC " + " ".join(_fmt(x) for x in spec["igc"]))
+        L.append(f"FIPRESS {_fmt(spec['fipress'])}")
+        L.append(f"FIWS {_fmt(spec['fiws'])}")
+        L.append("FIGC " + " ".join(_fmt(x) for x in spec["figc"]))
+    else:
+        # one value (or composition row) per layer
+        nz = spec["grid"][2]
+        def lay(v, per):
+            a = np.asarray(v, dtype=float).reshape(-1)
+            return a if a.size == nz * per else np.tile(a, nz)
+        L.append("INITCOND 1")
+        L.append("IPRESS " + " ".join(_fmt(x) for x in lay(spec["ipress"], 1)))
+        L.append("IWS " + " ".join(_fmt(x) for x in lay(spec["iws"], 1)))
+        L.append("IGC " + " ".join(_fmt(x) for x in lay(spec["igc"], len(spec["comps"]))))
+        L.append("FIPRESS " + " ".join(_fmt(x) for x in lay(spec["fipress"], 1)))
+        L.append("FIWS " + " ".join(_fmt(x) for x in lay(spec["fiws"], 1)))
+        L.append("FIGC " + " ".join(_fmt(x) for x in lay(spec["figc"], len(spec["comps"]))))
     text = "\n".join(L) + "\n"
     with open(path, "w") as fh:
         fh.write(text)
@@ -435,7 +449,8 @@ SAMPLE_SWT = [
 
 
 def config_deck(nx=10, ny=10, nz=3, seed=1, cdif=0.0, ipress=2e7, iws=0.2, restemp_c=86.85,
-                comps=("C1", "nC4", "nC10"), igc=(0.5, 0.2, 0.3), bic=None, wells=True) -> dict:
+                comps=("C1", "nC4", "nC10"), igc=(0.5, 0.2, 0.3), bic=None, wells=True, fipress=None,
+                figc=None) -> dict:
     """The small plain case: nx x ny x nz dual-porosity grid, matrix porosity
     0.20, fracture porosity 0.01, log-normal matrix permeability (median 10 mD,
     sigma_ln 0.5, seeded; the median is exp(mean of ln k)), fracture
@@ -457,8 +472,9 @@ def config_deck(nx=10, ny=10, nz=3, seed=1, cdif=0.0, ipress=2e7, iws=0.2, reste
                 fpermi=1000, fpermj=1000, fpermk=1000, lf=0.01, re_f=1000000, model="PR", comps=list(comps), bic=bic,
                 sgt=SAMPLE_SGT, swt=SAMPLE_SWT, refp=101325, cpor=0, dcpor=0,
                 wells=[inj, prod] if wells else [], restemp_c=restemp_c, wat_ro=1000, wat_mu=1, dt=0.01,
-                totalt=17520, dtmax=100, cdif=cdif, ipress=ipress, iws=iws, igc=list(igc), fipress=ipress, fiws=0,
-                figc=list(igc))
+                totalt=17520, dtmax=100, cdif=cdif, ipress=ipress, iws=iws, igc=np.asarray(igc).tolist(),
+                fipress=ipress if fipress is None else fipress, fiws=0,
+                figc=np.asarray(igc if figc is None else figc).tolist())
 
 
 def all_wells_deck(ipress=9e6, cdif=None) -> dict:

@@ -1,5 +1,9 @@
 """GPU parity of the Jacobian path (FormJacobian) against the reference.
 
+Decks cover two-phase, oil-only and gas-only cells of both continua, every
+pairing of matrix and fracture states, diffusion on and off, and all nine
+well types with and without the rate-limit latch.
+
 Both sides start from the same deck state and assemble the Jacobian at the
 same perturbed unknown vector; the reference's MatSetValues triplets and the
 device block-sparse output (plus its overflow entries) are summed into dense
@@ -18,7 +22,26 @@ from osiris_b200 import deck
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle.ref_available(), reason="reference library missing")]
 
+G_, O_ = (0.9, 0.07, 0.03), (0.5, 0.2, 0.3)
+_ST = {-1: (8e6, G_), 1: (2e7, O_), 0: (8e6, O_)}
+_PAIRS = [(a, b) for a in (-1, 0, 1) for b in (-1, 0, 1)]
+
+
+def _pairs_deck(cdif, wells):
+    """Nine layers: every (matrix, fracture) pairing of gas-only, two-phase and
+    oil-only states."""
+    return deck.config_deck(nx=2, ny=3, nz=9, ipress=[_ST[a][0] for a, _ in _PAIRS], igc=[_ST[a][1] for a, _ in _PAIRS],
+                            fipress=[_ST[b][0] for _, b in _PAIRS], figc=[_ST[b][1] for _, b in _PAIRS],
+                            wells=wells, cdif=cdif)
+
+
 CASES = {
+    "state_pairs_diffusion": (lambda: _pairs_deck(None, False), 3600.0),
+    "state_pairs_cdif0_wells": (lambda: _pairs_deck(0.0, True), 3600.0),
+    "oil_twophase_layers_wells": (lambda: deck.config_deck(nx=4, ny=3, nz=3, ipress=[8e6, 2e7, 8e6],
+                                                           fipress=[2e7, 8e6, 8e6], cdif=None), 3600.0),
+    "sample_12MPa": (lambda: deck.sample_deck(), 3600.0),
+    "all_well_types_20MPa_oil": (lambda: deck.all_wells_deck(ipress=20e6), 3600.0),
     "twophase_cdif0_no_wells": (lambda: deck.config_deck(nx=4, ny=3, nz=3, cdif=0.0, ipress=8e6, wells=False), 3600.0),
     "twophase_diffusion_no_wells": (lambda: deck.config_deck(nx=4, ny=4, nz=3, cdif=None, ipress=8e6, wells=False,
                                                              seed=8), 3600.0),
@@ -68,19 +91,3 @@ def test_form_jacobian_matches_reference(name, tmp_path, cuda_device):
     bad = np.argwhere(err > 1e-9)
     assert len(bad) == 0, (len(bad), [(int(r), int(c), Jg[r, c], Jr[r, c]) for r, c in bad[:8]])
 
-
-def test_one_phase_cells_are_reported(tmp_path, cuda_device):
-    import torch
-    path = os.path.join(str(tmp_path), "oil.dat")
-    deck.write_deck(path, deck.config_deck(nx=3, ny=3, nz=2, cdif=0.0, ipress=2e7))
-    d = deck.parse_deck(path)
-    R = oracle.RefDeck(path)
-    G = osr.Grid(d)
-    for mi, m in enumerate("mf"):
-        G.set_state(mi, R.get(f"{m}.P")[1], R.get(f"{m}.sat"), R.get(f"{m}.x"), R.get(f"{m}.y"), R.get(f"{m}.z"),
-                    R.get(f"{m}.label"), R.get(f"{m}.rho"))
-    n, _ = G.refresh_layout()
-    d_x = torch.zeros(n, dtype=torch.float64, device=cuda_device)
-    G.init_guess(d_x)
-    Jb = G.alloc_jacobian(cuda_device)
-    assert G.form_jacobian(d_x, Jb, 3600.0) == 6   # OSR_ERR_UNSUPPORTED
