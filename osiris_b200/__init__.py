@@ -45,15 +45,40 @@ class _CFlashOut(ctypes.Structure):
 FLASH_OUTPUTS = ("label", "L", "x", "y", "Zl", "Zg", "iters", "rr_iters", "dlnphi_dx", "dlnphi_dP")
 
 
-def header_symbols():
-    """Every function the public header declares."""
-    names = []
+def header_signatures():
+    """(return type, name, [parameter declarations]) of every function the
+    public header declares."""
+    out = []
     for h in sorted(os.listdir(INCLUDE)):
         if h.endswith(".h"):
             text = open(os.path.join(INCLUDE, h)).read()
-            names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z_0-9]*\s*\**\s*(osr_[a-z0-9_]+)\s*\(", text,
-                                flags=re.M)
-    return sorted(set(names))
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            text = re.sub(r"//[^\n]*", "", text)
+            for ret, name, params in re.findall(
+                    r"^\s*((?:const\s+)?[A-Za-z_]\w*\s*\**)\s*(osr_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.M):
+                ps = [p.strip() for p in params.split(",")]
+                out.append((ret.strip(), name, [] if ps == ["void"] else ps))
+    return out
+
+
+def header_symbols():
+    """Every function the public header declares."""
+    return sorted({name for _, name, _ in header_signatures()})
+
+
+_SCALARS = {"int": ctypes.c_int, "osr_status": ctypes.c_int, "long": ctypes.c_long, "double": ctypes.c_double}
+
+
+def _ctype(decl: str):
+    """ctypes type of one C declaration (a parameter or a return type).
+    Every pointer is a full-width address; passing an address as a bare
+    Python int without this would truncate it to a C int."""
+    if "*" in decl:
+        return ctypes.c_char_p if re.match(r"(const\s+)?char\s*\*\s*\w*$", decl) else ctypes.c_void_p
+    base = re.sub(r"\s+\w+$", "", decl.strip()) if len(decl.split()) > 1 else decl.strip()
+    if base not in _SCALARS:
+        raise OsrError(f"unmapped C type in header: {decl!r}")
+    return _SCALARS[base]
 
 
 def lib():
@@ -63,9 +88,10 @@ def lib():
         if not os.path.exists(LIB):
             raise OsrError(f"{LIB} is missing: run `python -m osiris_b200.build` (no CPU fallback exists)")
         L = ctypes.CDLL(LIB)
-        for name in header_symbols():
-            getattr(L, name)  # every declared entry point must resolve
-        L.osr_status_string.restype = ctypes.c_char_p
+        for ret, name, params in header_signatures():
+            fn = getattr(L, name)  # every declared entry point must resolve
+            fn.restype = _ctype(ret)
+            fn.argtypes = [_ctype(p) for p in params]
         _lib = L
     return _lib
 
@@ -237,7 +263,6 @@ class Grid:
         self._model = m
         h = ctypes.c_void_p()
         L = lib()
-        L.osr_grid_field_size.restype = ctypes.c_long
         _check(L.osr_grid_create(ctypes.byref(m), ctypes.byref(h)), "osr_grid_create")
         self._h = h
 

@@ -69,3 +69,83 @@ def flash_bytes_per_cell(nc: int, derivs: bool = True, iters: bool = True) -> in
     if derivs:
         b_out += (2 * nc * nc + 2 * nc) * 8
     return b_in + b_out
+
+
+# ----------------------------------------------------------------------------
+# Full Newton-step assembly: 128 x 128 x 32 dual-porosity grid, PR, 8
+# components with the seeded table of the batched flash (seed 2), all cells
+# two-phase.
+# ----------------------------------------------------------------------------
+ASSEMBLY_GRID = (128, 128, 32)
+
+
+def assembly_deck(nx: int = 128, ny: int = 128, nz: int = 32, nc: int = 8, seed: int = 2, cdif=0.0):
+    """A ``deck.Deck`` for the assembly workload.  Component criticals as the
+    batched flash's table; molecular weight ~ U(16, 250), Z_c 0.27 (so V_c =
+    Z_c R T_c / P_c), parachor ~ U(70, 700); matrix porosity 0.2, fracture 0.01,
+    log-normal matrix permeability (median 10 mD, sigma_ln 0.5), fracture
+    permeability 1000 mD, 50 m x 50 m x 5 m blocks, the sample deck's
+    saturation tables, no wells.  Initial state is set by ``assembly_state``."""
+    from .deck import Deck, SAMPLE_SGT, SAMPLE_SWT
+    rng = np.random.default_rng(seed)
+    tc, pc, acf, kij = flash_table(nc, seed)
+    n = nx * ny * nz
+    d = Deck()
+    d.nx, d.ny, d.nz, d.pnc, d.unc, d.eos = nx, ny, nz, nc, 0, 0
+    d.restemp, d.wat_ro, d.wat_mu = 360.0, 1000.0, 1.0
+    d.di, d.dj, d.dk = np.full(nx, 50.0), np.full(ny, 50.0), np.full(nz, 5.0)
+    d.tor = np.ones(n)
+    d.por, d.fpor = np.full(n, 0.2), np.full(n, 0.01)
+    d.perm = np.exp(np.log(10.0) + 0.5 * rng.standard_normal((3, n)))
+    d.fperm = np.full((3, n), 1000.0)
+    d.cdif = cdif
+    d.sigma, d.lf, d.re_f = 1.0, 0.01, 1e6
+    d.refp, d.cpor, d.dcpor = 101325.0, 0.0, 0.0
+    d.tc, d.pc, d.acf = tc, pc, acf
+    d.mw = rng.uniform(16.0, 250.0, nc)
+    d.zc = np.full(nc, 0.27)
+    d.vc = d.zc * 8.3144621 * tc / pc * 1e6
+    d.parachor = rng.uniform(70.0, 700.0, nc)
+    d.kij = kij
+    d.swt = np.array(SAMPLE_SWT, dtype=float)
+    d.sgt = np.array(SAMPLE_SGT, dtype=float)
+    d.wells_i = np.zeros((0, 5), dtype=np.int32)
+    d.wells_f = np.zeros((0, nc + 6))
+    d.dt = 3600.0
+    return d
+
+
+def assembly_state(grid, d, device, seed: int = 4):
+    """Initial two-phase state of the assembly workload on the device: one
+    feed composition and the middle of its two-phase pressure range (found by
+    a flash sweep), +-0.5 % seeded pressure noise, water saturation 0.2 in the
+    matrix and 0 in the fracture; phase split, compositions and densities from
+    the device flash.  Returns the pressure the sweep chose."""
+    import torch
+    from . import Fluid, flash
+    rng = np.random.default_rng(seed)
+    nc, n = d.nc, d.cells
+    z0 = rng.dirichlet(np.ones(nc))
+    fl = Fluid(d.tc, d.pc, d.acf, d.kij, d.eos)
+    sweep = np.linspace(1e6, 40e6, 256)
+    Ps = torch.tensor(sweep, device=device)
+    Ts = torch.full_like(Ps, d.restemp)
+    zs = torch.tensor(np.repeat(z0[:, None], len(sweep), axis=1), device=device)
+    lab = flash(fl, Ps, Ts, zs)["label"].cpu().numpy()
+    two = sweep[lab == 0]
+    if len(two) == 0:
+        raise RuntimeError("the seeded feed has no two-phase pressure range")
+    p0 = float(np.median(two))
+    R = 8.3144621
+    for med, sw in ((0, 0.2), (1, 0.0)):
+        P = torch.tensor(p0 * (1 + 0.005 * rng.uniform(-1, 1, n)), device=device)
+        T = torch.full_like(P, d.restemp)
+        z = torch.tensor(np.repeat(z0[:, None], n, axis=1), device=device)
+        o = flash(fl, P, T, z)
+        L, Zl, Zg = o["L"], o["Zl"], o["Zg"]
+        newD = Zl * L / (Zl * L + Zg * (1 - L))
+        sat = torch.stack([torch.full_like(P, sw), newD * (1 - sw), (1 - newD) * (1 - sw)])
+        rho = torch.stack([P / (Zl * R * T), P / (Zg * R * T)])
+        grid.set_state(med, P.cpu().numpy(), sat.cpu().numpy(), o["x"].cpu().numpy(), o["y"].cpu().numpy(),
+                       z.cpu().numpy(), o["label"].cpu().numpy(), rho.cpu().numpy())
+    return p0

@@ -23,6 +23,20 @@ def test_library_exports_every_header_symbol():
         assert getattr(L, n) is not None
 
 
+def test_every_entry_point_has_full_width_signature():
+    """Each declared function gets argtypes from the header, so host addresses
+    above 4 GiB (large numpy arrays) are never truncated to a C int."""
+    L = osr.lib()
+    for ret, name, params in osr.header_signatures():
+        fn = getattr(L, name)
+        assert fn.argtypes is not None and len(fn.argtypes) == len(params), name
+        for p, t in zip(params, fn.argtypes):
+            if "*" in p:
+                assert t in (ctypes.c_void_p, ctypes.c_char_p), (name, p)
+    assert L.osr_grid_field_size.restype is ctypes.c_long
+    assert L.osr_status_string.restype is ctypes.c_char_p
+
+
 def test_status_strings_and_version():
     L = osr.lib()
     assert L.osr_version() == 1
