@@ -241,41 +241,55 @@ osr_status osr_grid_form_function(osr_grid *grid, const double *d_x, double *d_f
 /* ---------------------------------------------------------------------------
  * Jacobian path: the PETSc FormJacobian callback on the device.
  *
- * Output: a uniform block-sparse matrix with block size bs = 2N+4 and eight
- * block slots per block row (this cell-medium, -x, +x, -y, +y, -z, +z
- * neighbours, the same cell of the other continuum; osr_grid_block_columns
- * gives each slot's block column, -1 when absent).  Block rows/columns follow
- * the row layout of osr_grid_refresh_layout; a one-phase cell uses the first
- * N+3 rows and columns of its blocks.  vals [2 cells][8][bs][bs] row-major.
- * The reference adds a few entries outside this pattern (some total-row
- * neighbour columns counted from the following block's offset); they are
- * returned per block row as (local row, global column, value) triples,
- * ovf_* [2 cells][overflow], counts ovf_n [2 cells].  All DEVICE pointers.
  * The matrix is the reference's IteratorJacobian (compsim/Petsc_Functions.cpp:
- * 6898-42073) entry for entry, including its approximate derivatives; the
- * PETSc adapter adds these values with MatSetValues(ADD_VALUES).
+ * 6898-42073) entry for entry, including its approximate derivatives.  It is
+ * returned as a fixed set of values per block row (one cell of one
+ * continuum, block rows ordered as osr_grid_refresh_layout orders them):
+ *
+ *   canonical unknowns of every block (bs = 2N+4 columns):
+ *     x_0..x_{N-1}, y_0..y_{N-1}, P, Sw, So, Sg
+ *   canonical rows: fugacity 0..N-1, component balances N..2N-2, total
+ *     2N-1, water 2N, sum x 2N+1, sum y 2N+2, sum S 2N+3
+ *   a one-phase cell's N+3 reference rows and unknowns map onto these; its
+ *   unused rows carry a unit entry in an unused column;
+ *   eight block slots: this cell, -x, +x, -y, +y, -z, +z neighbours, the
+ *     same cell of the other continuum (osr_grid_block_columns);
+ *   stored entries, in this order:
+ *     fugacity rows x own slot x columns 0..2N          N (2N+1)
+ *     rows N..2N-1 x 8 slots x all columns              8 N (2N+4)
+ *     water row x 8 slots x {P, Sw}                     16
+ *     rows 2N+1..2N+3 x own slot x all columns          3 (2N+4)
+ *     eight entries of the total row the reference places in the block after
+ *     a neighbour's (its -y / -z face columns counted from the following
+ *     block's row offset)                               8
+ *
+ * vals: DEVICE [ceil(2 cells / 32)][entries][32]: block row b's value e at
+ * ((b / 32) entries + e) 32 + b % 32 (entries from osr_grid_jacobian_shape;
+ * values of the last chunk beyond the grid are zeros).
+ * osr_grid_jacobian_pattern gives every value's
+ * reference (global row, global column), -1 for a value the reference's
+ * matrix does not hold (unit entries of unused rows, absent neighbours and
+ * unknowns); a PETSc adapter passes the pattern to MatSetPreallocationCOO
+ * once per row layout and vals to MatSetValuesCOO each call (COO sums
+ * duplicates, as the reference's ADD_VALUES does).
  * ------------------------------------------------------------------------- */
-typedef struct osr_jacobian_out {
-    double *vals;
-    int *ovf_row;
-    long *ovf_col;
-    double *ovf_val;
-    int *ovf_n;
-} osr_jacobian_out;
-
-osr_status osr_grid_jacobian_shape(osr_grid *grid, int *bs, int *slots, int *overflow);
+osr_status osr_grid_jacobian_shape(osr_grid *grid, int *bs, int *entries, int *overflow);
 osr_status osr_grid_block_columns(osr_grid *grid, long *out /* HOST [2 cells][8] */);
+
+/* Reference (row, column) of each value: DEVICE d_row, d_col, same layout
+ * as vals.  Depends on the row layout only (osr_grid_refresh_layout). */
+osr_status osr_grid_jacobian_pattern(osr_grid *grid, long *d_row, long *d_col, void *stream);
 
 /* The Jacobian at the current state (after osr_grid_update_all or
  * osr_grid_form_function): every cell-medium in any phase state; inactive
  * cell-media (porosity < 1e-10) get a unit diagonal as in the reference.
- * Returns OSR_ERR_UNSUPPORTED if a cell-medium falls outside the covered
- * cases (none do in this version).  Synchronises `stream`. */
-osr_status osr_grid_jacobian(osr_grid *grid, double sim_time, const osr_jacobian_out *out, void *stream);
+ * Every value is written (no clearing needed).  Asynchronous on `stream`
+ * (the first call on a grid allocates its scratch). */
+osr_status osr_grid_jacobian(osr_grid *grid, double sim_time, double *d_vals, void *stream);
 
 /* FormJacobian (compsim/PetscAUX.cpp:106-173): osr_grid_update_all then
  * osr_grid_jacobian. */
-osr_status osr_grid_form_jacobian(osr_grid *grid, const double *d_x, double sim_time, const osr_jacobian_out *out,
+osr_status osr_grid_form_jacobian(osr_grid *grid, const double *d_x, double sim_time, double *d_vals,
                                   void *stream);
 
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA

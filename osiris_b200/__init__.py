@@ -231,10 +231,6 @@ class _CModel(ctypes.Structure):
                 ("nwells", ctypes.c_int), ("wells_i", _vp), ("wells_f", _vp), ("tor", _vp), ("dt", ctypes.c_double)]
 
 
-class _CJacOut(ctypes.Structure):
-    _fields_ = [("vals", _vp), ("ovf_row", _vp), ("ovf_col", _vp), ("ovf_val", _vp), ("ovf_n", _vp)]
-
-
 class Grid:
     """A dual-porosity model on the device, built from a parsed deck
     (``osiris_b200.deck.parse_deck``)."""
@@ -340,10 +336,11 @@ class Grid:
 
     # -- Jacobian path -------------------------------------------------------
     def jacobian_shape(self):
-        bs, slots, ovf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        _check(lib().osr_grid_jacobian_shape(self._h, ctypes.byref(bs), ctypes.byref(slots), ctypes.byref(ovf)),
+        """(block size, values per block row, shifted entries per block row)."""
+        bs, ent, ovf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().osr_grid_jacobian_shape(self._h, ctypes.byref(bs), ctypes.byref(ent), ctypes.byref(ovf)),
                "osr_grid_jacobian_shape")
-        return bs.value, slots.value, ovf.value
+        return bs.value, ent.value, ovf.value
 
     def block_columns(self) -> np.ndarray:
         out = np.zeros((2 * self.cells, 8), np.int64)
@@ -351,57 +348,41 @@ class Grid:
         return out
 
     def alloc_jacobian(self, device):
-        """Device buffers for osr_grid_jacobian (a dict of CUDA tensors)."""
+        """Device values of osr_grid_jacobian: float64 [chunks, entries, 32]
+        (block row b at [b // 32, :, b % 32])."""
         import torch
-        bs, slots, ovf = self.jacobian_shape()
-        nb = 2 * self.cells
-        return dict(vals=torch.zeros((nb, slots, bs, bs), dtype=torch.float64, device=device),
-                    ovf_row=torch.zeros((nb, ovf), dtype=torch.int32, device=device),
-                    ovf_col=torch.zeros((nb, ovf), dtype=torch.int64, device=device),
-                    ovf_val=torch.zeros((nb, ovf), dtype=torch.float64, device=device),
-                    ovf_n=torch.zeros(nb, dtype=torch.int32, device=device))
+        _, ent, _ = self.jacobian_shape()
+        return torch.empty(((2 * self.cells + 31) // 32, ent, 32), dtype=torch.float64, device=device)
 
-    def _jac_struct(self, J):
-        return _CJacOut(*[_vp(J[k].data_ptr()) for k in ("vals", "ovf_row", "ovf_col", "ovf_val", "ovf_n")])
+    def jacobian_pattern(self, device, stream=None):
+        """Reference (row, column) of every value, int64 device tensors in the
+        values' layout, -1 where the reference's matrix holds no entry."""
+        import torch
+        _, ent, _ = self.jacobian_shape()
+        rows = torch.empty(((2 * self.cells + 31) // 32, ent, 32), dtype=torch.int64, device=device)
+        cols = torch.empty_like(rows)
+        _check(lib().osr_grid_jacobian_pattern(self._h, _vp(rows.data_ptr()), _vp(cols.data_ptr()),
+                                               None if stream is None else _vp(stream)), "osr_grid_jacobian_pattern")
+        return rows, cols
 
-    def jacobian(self, J, sim_time: float = 0.0, stream=None):
-        o = self._jac_struct(J)
-        return lib().osr_grid_jacobian(self._h, ctypes.c_double(sim_time), ctypes.byref(o),
+    def jacobian(self, vals, sim_time: float = 0.0, stream=None):
+        return lib().osr_grid_jacobian(self._h, ctypes.c_double(sim_time), _vp(vals.data_ptr()),
                                        None if stream is None else _vp(stream))
 
-    def form_jacobian(self, d_x, J, sim_time: float = 0.0, stream=None):
-        o = self._jac_struct(J)
-        return lib().osr_grid_form_jacobian(self._h, _vp(d_x.data_ptr()), ctypes.c_double(sim_time), ctypes.byref(o),
-                                            None if stream is None else _vp(stream))
+    def form_jacobian(self, d_x, vals, sim_time: float = 0.0, stream=None):
+        return lib().osr_grid_form_jacobian(self._h, _vp(d_x.data_ptr()), ctypes.c_double(sim_time),
+                                            _vp(vals.data_ptr()), None if stream is None else _vp(stream))
 
-    def jacobian_coo(self, J):
-        """(rows, cols, vals) in the reference's global numbering from the
-        device block-sparse output (host arrays; zeros dropped)."""
-        rowoff = self.row_offsets()
-        cols = self.block_columns()
-        vals = J["vals"].cpu().numpy()
-        nb, slots, bs, _ = vals.shape
-        R, C, V = [], [], []
-        for b in range(nb):
-            size = rowoff[b + 1] - rowoff[b]
-            for s in range(slots):
-                tb = cols[b, s]
-                if tb < 0:
-                    continue
-                tsize = rowoff[tb + 1] - rowoff[tb]
-                blk = vals[b, s, :size, :tsize]
-                r, c = np.nonzero(blk)
-                R.append(rowoff[b] + r)
-                C.append(rowoff[tb] + c)
-                V.append(blk[r, c])
-        on = J["ovf_n"].cpu().numpy()
-        orow, ocol, oval = (J[k].cpu().numpy() for k in ("ovf_row", "ovf_col", "ovf_val"))
-        for b in np.nonzero(on)[0]:
-            k = on[b]
-            R.append(rowoff[b] + orow[b, :k])
-            C.append(ocol[b, :k])
-            V.append(oval[b, :k])
-        return np.concatenate(R), np.concatenate(C), np.concatenate(V)
+    def jacobian_coo(self, vals):
+        """(rows, cols, vals) host arrays in the reference's global numbering
+        (the COO triplets a PETSc adapter hands to MatSetValuesCOO)."""
+        import torch
+        torch.cuda.synchronize(vals.device)
+        rows, cols = self.jacobian_pattern(vals.device)
+        torch.cuda.synchronize(vals.device)
+        r, c, v = rows.cpu().numpy().ravel(), cols.cpu().numpy().ravel(), vals.cpu().numpy().ravel()
+        keep = r >= 0
+        return r[keep], c[keep], v[keep]
 
     def get(self, name: str) -> np.ndarray:
         L = lib()

@@ -246,7 +246,7 @@ osr_status grid_assembly_init(osr_grid &g, const osr_model *md) {
 
 void grid_assembly_free(osr_grid &g) {
     void *ptrs[] = {g.tor, g.rowoff, g.sizes, g.pmax, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws,
-                    g.jw_q, g.jw_pi, g.j_stream_y, g.jw_iw, g.j_unsup};
+                    g.jw_q, g.jw_pi, g.j_stream_y, g.jw_iw, g.j_dmu, g.j_dh};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     g.tor = nullptr;
@@ -257,7 +257,8 @@ void grid_assembly_free(osr_grid &g) {
     g.d_cond = nullptr;
     g.d_ws = nullptr;
     g.jw_q = g.jw_pi = g.j_stream_y = nullptr;
-    g.jw_iw = g.j_unsup = nullptr;
+    g.jw_iw = nullptr;
+    g.j_dmu = g.j_dh = nullptr;
 }
 
 static long grid_blocks(long work) {

@@ -41,7 +41,8 @@ struct osr_grid {
     // Jacobian scratch: per cell-medium well rates / productivity indices,
     // injection-well index, injected gas compositions, unsupported-cell count
     double *jw_q = nullptr, *jw_pi = nullptr, *j_stream_y = nullptr;
-    int *jw_iw = nullptr, *j_unsup = nullptr;
+    int *jw_iw = nullptr;
+    double *j_dmu = nullptr, *j_dh = nullptr;   // Jacobian derivative tables [2][N+1][2 cells], [2][5+N][2 cells]
 };
 
 namespace osr {

@@ -1,7 +1,7 @@
-// Host side of the Jacobian path: FormJacobian on the device into a uniform
-// block-sparse matrix (block size 2N+4, eight block slots per block row) plus
-// a short per-block-row list of entries the reference places outside that
-// pattern.
+// Host side of the Jacobian path: FormJacobian on the device into the
+// compact canonical block rows of jacobian_kernels.cuh (values in chunks of
+// 32 block rows, [chunk][entry][32]), and the reference (row, column) of
+// every value for a COO consumer.
 #include <cuda_runtime.h>
 #include <cstring>
 #include <vector>
@@ -18,10 +18,65 @@ static osr_status jfail(cudaError_t) { return OSR_ERR_CUDA; }
         if (e_ != cudaSuccess) return jfail(e_);    \
     } while (0)
 
-__global__ void __launch_bounds__(128) jacobian_kernel(const __grid_constant__ osrj::JacView v, int *unsupported) {
+constexpr int kRowThreads = 128;
+
+template <int N>
+__global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_constant__ osrj::JacView v) {
     const long nb = 2 * v.n;
-    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long)gridDim.x * blockDim.x) {
-        if (!osrj::jacobian_block(v, b)) atomicAdd(unsupported, 1);
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long)gridDim.x * blockDim.x)
+        osrj::prep_cell<N>(v, b);
+}
+
+// One warp per (32 consecutive block rows, row task) of one kind (see
+// jacobian_task_kind): component rows take tasks 0..N-2, the total rows task
+// N-1, the fugacity / water / constraint rows task N.  Each thread's
+// per-component accumulators: 3N doubles of dynamic shared memory.
+template <int KIND>
+__global__ void __launch_bounds__(kRowThreads) jacobian_rows_kernel(const __grid_constant__ osrj::JacView v,
+                                                                   long chunk0, long chunks) {
+    extern __shared__ double s_acc[];
+    const int N = v.nc;
+    const int T = KIND <= 1 ? N - 1 : 1;
+    const int lane = threadIdx.x & 31;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    osrj::Acc a;
+    a.X = s_acc + threadIdx.x;
+    a.Y = s_acc + N * kRowThreads + threadIdx.x;
+    a.Z = s_acc + 2 * N * kRowThreads + threadIdx.x;
+    a.stride = kRowThreads;
+    const long items = chunks * T;
+    for (long it = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nwarps) {
+        const long cq = it / T;
+        const int tt = (int)(it - cq * T);
+        const int task = KIND <= 1 ? tt : (KIND == 2 ? N - 1 : N);
+        osrj::jacobian_task_kind<KIND>(v, (chunk0 + cq) * 32 + lane, task, a);
+    }
+}
+
+template <int KIND>
+static osr_status launch_rows(const osrj::JacView &v, long chunk0, long chunks, int tasks, cudaStream_t st) {
+    const long items = chunks * tasks;
+    if (items <= 0) return OSR_OK;
+    long rb = (items * 32 + kRowThreads - 1) / kRowThreads;
+    if (rb > 148L * 64) rb = 148L * 64;
+    jacobian_rows_kernel<KIND><<<(unsigned)rb, kRowThreads, (size_t)3 * v.nc * kRowThreads * 8, st>>>(v, chunk0, chunks);
+    JAC_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
+// Reference (row, column) of every value, in the values' chunked layout.
+__global__ void jacobian_pattern_kernel(int N, int nx, int ny, int nz, long n, const long *rowoff,
+                                        const signed char *lab_m, const signed char *lab_f, int entries, long *grow,
+                                        long *gcol) {
+    const long nb = 2 * n, total = (nb + 31) / 32 * 32 * entries;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const long chunk = idx / (32L * entries);
+        const int e = (int)((idx / 32) % entries);
+        const long b = chunk * 32 + (idx & 31);
+        long r = -1, c = -1;
+        if (b < nb) osrj::entry_position(N, nx, ny, nz, n, rowoff, lab_m, lab_f, b, e, &r, &c);
+        grow[idx] = r;
+        gcol[idx] = c;
     }
 }
 
@@ -44,13 +99,14 @@ static void fill_constants(const osr_grid &g, osrj::JacView &v) {
         for (int j = 0; j < N; j++) {
             v.bic[i * N + j] = G.f.bic[i * N + j];
             v.pD[i * N + j] = G.pD[i * N + j];
+            v.ipD[i * N + j] = 1 / G.pD[i * N + j];
         }
     }
     v.T = G.T;
     v.srk = G.f.srk;
 }
 
-static osr_status make_view(const osr_grid &g, osrj::JacView &v) {
+static void make_view(const osr_grid &g, osrj::JacView &v) {
     std::memset(&v, 0, sizeof(v));
     v.nx = g.nx;
     v.ny = g.ny;
@@ -62,14 +118,6 @@ static osr_status make_view(const osr_grid &g, osrj::JacView &v) {
     v.dk = g.dk;
     v.blockH = g.blockH;
     v.tor = g.tor;
-    switch (g.nc) {
-#define JAC_NC(K) \
-    case K: fill_constants<K>(g, v); break;
-        JAC_NC(1) JAC_NC(2) JAC_NC(3) JAC_NC(4) JAC_NC(5) JAC_NC(6) JAC_NC(7) JAC_NC(8) JAC_NC(9) JAC_NC(10)
-        JAC_NC(11) JAC_NC(12) JAC_NC(13) JAC_NC(14) JAC_NC(15) JAC_NC(16)
-#undef JAC_NC
-        default: return OSR_ERR_NC;
-    }
     v.cpor = g.cpor;
     v.dcpor = g.dcpor;
     v.refp = g.refp;
@@ -106,8 +154,12 @@ static osr_status make_view(const osr_grid &g, osrj::JacView &v) {
         J.transS = F.transS;
     }
     v.rowoff = g.rowoff;
-    v.bs = 2 * g.nc + 4;
-    return OSR_OK;
+    v.well_q = g.jw_q;
+    v.well_pi = g.jw_pi;
+    v.well_comp = g.jw_iw;
+    v.stream_y = g.j_stream_y;
+    v.dmu = g.j_dmu;
+    v.dh = g.j_dh;
 }
 
 template <int N>
@@ -139,15 +191,26 @@ static osr_status well_pass(osr_grid &g, double sim_time, cudaStream_t st) {
     return OSR_OK;
 }
 
-static osr_status dispatch_well_pass(osr_grid &g, double t, cudaStream_t st) {
-    switch (g.nc) {
-#define JAC_NC(K) \
-    case K: return well_pass<K>(g, t, st);
-        JAC_NC(1) JAC_NC(2) JAC_NC(3) JAC_NC(4) JAC_NC(5) JAC_NC(6) JAC_NC(7) JAC_NC(8) JAC_NC(9) JAC_NC(10)
-        JAC_NC(11) JAC_NC(12) JAC_NC(13) JAC_NC(14) JAC_NC(15) JAC_NC(16)
-#undef JAC_NC
-        default: return OSR_ERR_NC;
-    }
+// Well pass, derivative tables, then the row tasks, all on `st`.
+template <int N>
+static osr_status jacobian_n(osr_grid &g, double sim_time, double *vals, cudaStream_t st) {
+    osr_status s = well_pass<N>(g, sim_time, st);
+    if (s != OSR_OK) return s;
+    osrj::JacView v;
+    make_view(g, v);
+    fill_constants<N>(g, v);
+    v.vals = vals;
+    v.entries = osrj::Layout(N).ET;
+    const long nb = 2 * g.cells;
+    long blocks = (nb + kRowThreads - 1) / kRowThreads;
+    if (blocks > 148L * 16) blocks = 148L * 16;
+    jac_prep_kernel<N><<<(unsigned)blocks, kRowThreads, 0, st>>>(v);
+    JAC_CUDA(cudaGetLastError());
+    const long chunks = (nb + 31) / 32, mchunks = (g.cells + 31) / 32, fchunk0 = g.cells / 32;
+    if ((s = launch_rows<0>(v, 0, mchunks, N - 1, st)) != OSR_OK) return s;
+    if ((s = launch_rows<1>(v, fchunk0, chunks - fchunk0, N - 1, st)) != OSR_OK) return s;
+    if ((s = launch_rows<2>(v, 0, chunks, 1, st)) != OSR_OK) return s;
+    return launch_rows<3>(v, 0, chunks, 1, st);
 }
 
 static osr_status ensure_jacobian_scratch(osr_grid &g) {
@@ -156,7 +219,8 @@ static osr_status ensure_jacobian_scratch(osr_grid &g) {
     JAC_CUDA(cudaMalloc((void **)&g.jw_q, nb * 3 * 8));
     JAC_CUDA(cudaMalloc((void **)&g.jw_pi, nb * 3 * 8));
     JAC_CUDA(cudaMalloc((void **)&g.jw_iw, nb * sizeof(int)));
-    JAC_CUDA(cudaMalloc((void **)&g.j_unsup, sizeof(int)));
+    JAC_CUDA(cudaMalloc((void **)&g.j_dmu, (size_t)nb * 2 * (g.nc + 1) * 8));
+    if (!g.const_dif) JAC_CUDA(cudaMalloc((void **)&g.j_dh, (size_t)nb * 2 * (g.nc + 5) * 8));
     const int nw = g.nwells > 0 ? g.nwells : 1;
     JAC_CUDA(cudaMalloc((void **)&g.j_stream_y, (size_t)nw * osrj::kMaxNc * 8));
     JAC_CUDA(cudaMemset(g.j_stream_y, 0, (size_t)nw * osrj::kMaxNc * 8));
@@ -172,10 +236,11 @@ using namespace osr;
 
 extern "C" {
 
-osr_status osr_grid_jacobian_shape(osr_grid *g, int *bs, int *slots, int *overflow) {
+osr_status osr_grid_jacobian_shape(osr_grid *g, int *bs, int *entries, int *overflow) {
     if (!g) return OSR_ERR_ARG;
-    if (bs) *bs = 2 * g->nc + 4;
-    if (slots) *slots = 8;
+    const osrj::Layout L(g->nc);
+    if (bs) *bs = L.BS;
+    if (entries) *entries = L.ET;
     if (overflow) *overflow = osrj::kOverflow;
     return OSR_OK;
 }
@@ -199,46 +264,39 @@ osr_status osr_grid_block_columns(osr_grid *g, long *out) {
     return OSR_OK;
 }
 
-osr_status osr_grid_jacobian(osr_grid *g, double sim_time, const osr_jacobian_out *out, void *stream) {
-    if (!g || !out || !out->vals || !out->ovf_row || !out->ovf_col || !out->ovf_val || !out->ovf_n) return OSR_ERR_ARG;
+osr_status osr_grid_jacobian_pattern(osr_grid *g, long *d_row, long *d_col, void *stream) {
+    if (!g || !d_row || !d_col || !g->rowoff) return OSR_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const osrj::Layout L(g->nc);
+    const long total = (2 * g->cells + 31) / 32 * 32 * L.ET;
+    long blocks = (total + 255) / 256;
+    if (blocks > 148L * 32) blocks = 148L * 32;
+    jacobian_pattern_kernel<<<(unsigned)blocks, 256, 0, st>>>(g->nc, g->nx, g->ny, g->nz, g->cells, g->rowoff,
+                                                              g->m[0].label, g->m[1].label, L.ET, d_row, d_col);
+    JAC_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
+osr_status osr_grid_jacobian(osr_grid *g, double sim_time, double *d_vals, void *stream) {
+    if (!g || !d_vals) return OSR_ERR_ARG;
     if (!(g->pcoeff > 0) || !(g->dt > 0)) return OSR_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     osr_status s = ensure_jacobian_scratch(*g);
     if (s != OSR_OK) return s;
-    const long nb = 2 * g->cells;
-    const int bs = 2 * g->nc + 4;
-    JAC_CUDA(cudaMemsetAsync(out->vals, 0, (size_t)nb * 8 * bs * bs * 8, st));
-    JAC_CUDA(cudaMemsetAsync(out->ovf_n, 0, (size_t)nb * sizeof(int), st));
-    JAC_CUDA(cudaMemsetAsync(g->j_unsup, 0, sizeof(int), st));
-    s = dispatch_well_pass(*g, sim_time, st);
-    if (s != OSR_OK) return s;
-    osrj::JacView v;
-    s = make_view(*g, v);
-    if (s != OSR_OK) return s;
-    v.well_q = g->jw_q;
-    v.well_pi = g->jw_pi;
-    v.well_comp = g->jw_iw;
-    v.stream_y = g->j_stream_y;
-    v.vals = out->vals;
-    v.ovf_row = out->ovf_row;
-    v.ovf_col = out->ovf_col;
-    v.ovf_val = out->ovf_val;
-    v.ovf_n = out->ovf_n;
-    long blocks = (nb + 127) / 128;
-    if (blocks > 148L * 16) blocks = 148L * 16;
-    jacobian_kernel<<<(unsigned)blocks, 128, 0, st>>>(v, g->j_unsup);
-    JAC_CUDA(cudaGetLastError());
-    int unsup = 0;
-    JAC_CUDA(cudaMemcpyAsync(&unsup, g->j_unsup, sizeof(int), cudaMemcpyDeviceToHost, st));
-    JAC_CUDA(cudaStreamSynchronize(st));
-    return unsup ? OSR_ERR_UNSUPPORTED : OSR_OK;
+    switch (g->nc) {
+#define JAC_NC(K) \
+    case K: return jacobian_n<K>(*g, sim_time, d_vals, st);
+        JAC_NC(1) JAC_NC(2) JAC_NC(3) JAC_NC(4) JAC_NC(5) JAC_NC(6) JAC_NC(7) JAC_NC(8) JAC_NC(9) JAC_NC(10)
+        JAC_NC(11) JAC_NC(12) JAC_NC(13) JAC_NC(14) JAC_NC(15) JAC_NC(16)
+#undef JAC_NC
+        default: return OSR_ERR_NC;
+    }
 }
 
-osr_status osr_grid_form_jacobian(osr_grid *g, const double *d_x, double sim_time, const osr_jacobian_out *out,
-                                  void *stream) {
+osr_status osr_grid_form_jacobian(osr_grid *g, const double *d_x, double sim_time, double *d_vals, void *stream) {
     osr_status s = osr_grid_update_all(g, d_x, stream);
     if (s != OSR_OK) return s;
-    return osr_grid_jacobian(g, sim_time, out, stream);
+    return osr_grid_jacobian(g, sim_time, d_vals, stream);
 }
 
 }  // extern "C"

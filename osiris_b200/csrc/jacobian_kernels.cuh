@@ -11,14 +11,42 @@
 // of the reference's matrix), so each term here restates the reference's
 // expression; the direction-dependent deviations are kept as explicit flags.
 //
-// One thread owns one cell of one continuum and writes its whole block row
-// of a uniform block-sparse matrix: block size bs = 2N+4, eight block slots
-// per block row (this cell, -x, +x, -y, +y, -z, +z neighbours, the other
-// continuum's cell), values [block row][slot][bs][bs] row-major.  Rows and
-// columns beyond a one-phase cell's N+3 unknowns stay zero.
+// Output layout (the compact canonical block row).  Every block row (one
+// cell of one continuum) places its unknowns at fixed canonical positions
+// whatever its phase state: x_0..x_{N-1}, y_0..y_{N-1}, P, Sw, So, Sg
+// (bs = 2N+4 columns), and its rows at fixed positions: fugacity rows
+// 0..N-1, component rows N..2N-2, the total row 2N-1, the water row 2N and
+// the constraint rows 2N+1 (sum x), 2N+2 (sum y), 2N+3 (sum S).  A one-phase
+// cell's N+3 reference rows and unknowns map onto these positions; its unused
+// rows hold a unit entry in an unused column.  Eight block slots per block
+// row: this cell, the -x, +x, -y, +y, -z, +z neighbours, and the same cell of
+// the other continuum.  Only the entries that can be nonzero are stored:
+//   F  fugacity rows, own slot, columns 0..2N          N (2N+1)
+//   C  component and total rows, 8 slots, all columns  N 8 (2N+4)
+//   W  water row, 8 slots, columns P and Sw            16
+//   K  constraint rows, own slot, all columns          3 (2N+4)
+//   O  eight entries the reference places in the block after a neighbour's
+//      (its total rows' -y and -z face columns, counted from the following
+//      block's row offset)                              8
+// i.e. 1,500 values per block row at N = 8 (the reference's structural count
+// for an interior two-phase cell is 18N^2+35N+19 = 1,451).  Values are stored
+// in chunks of 32 block rows, vals[chunk][entry][32]: the 32 lanes of a warp
+// (32 consecutive block rows) store 256 contiguous bytes per entry, and a
+// chunk's values are one contiguous run (a layout with the whole grid between
+// consecutive entries puts every entry of a warp on its own page).  Each
+// entry is written exactly once per call (zeros included, and zeros for the
+// lanes of the last chunk beyond the grid): no clearing pass, no
+// read-modify-write.
 //
-// The code is plain C++ over a view of device arrays, so the same source is
-// compiled for the GPU and, for testing, for the host.
+// Work decomposition: a warp takes 32 consecutive block rows and one row task
+// -- component row i (tasks 0..N-2), the total row (task N-1), or the
+// fugacity, water and constraint rows together (task N).  Viscosity
+// derivatives and the composition sums of the diffusion-coefficient
+// derivatives are tabulated per cell-medium by a preparation kernel, so an
+// entry costs O(1).
+//
+// The code is plain C++ over a view of device arrays, so the same source also
+// compiles for the host.
 #pragma once
 #include <cmath>
 
@@ -37,6 +65,16 @@ constexpr double kWatMRo = 55.5084;              // WAT_M_RO
 constexpr double kR = 8.3144621;                 // RGAS
 constexpr double kSqrt2 = 1.4142135623730950488016887;
 constexpr int kMaxNc = 16;
+constexpr int kOverflow = 8;
+
+template <class T>
+OSR_HD inline T ld(const T *p) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
 
 // Fields of one continuum ([planes][cells], cell fastest).
 struct JMed {
@@ -51,7 +89,8 @@ struct JacView {
     const double *di, *dj, *dk, *blockH, *tor;
     // per-component constants
     double sa[kMaxNc], b[kMaxNc], bic[kMaxNc * kMaxNc], mw[kMaxNc], smw[kMaxNc], mui[kMaxNc], vcm[kMaxNc],
-        tc[kMaxNc], pc[kMaxNc], pcr_atm[kMaxNc], vc53[kMaxNc], vc23[kMaxNc], pD[kMaxNc * kMaxNc];
+        tc[kMaxNc], pc[kMaxNc], pcr_atm[kMaxNc], vc53[kMaxNc], vc23[kMaxNc], pD[kMaxNc * kMaxNc],
+        ipD[kMaxNc * kMaxNc];   // 1 / pD
     double T;
     int srk;
     // scalars
@@ -65,18 +104,83 @@ struct JacView {
     const int *well_comp;     // [2 cells] index of the injection well whose stream sets the component split, -1
     const double *well_q;     // [2 cells][3] Qw, Qo, Qg or null
     const double *stream_y;   // [wells][kMaxNc] injected gas composition
+    // derivative tables (written by the preparation kernel)
+    double *dmu;   // [2 phases][N+1][2 cells]: d mu / d w_k (k < N), d mu / d P (k = N)
+    double *dh;    // [2 phases][5+N][2 cells]: composition sums of d D / d w (see prep_cell)
     // output
-    double *vals;
-    int bs;
-    // entries the reference places outside the eight-block pattern:
-    // [block row][kOverflow] (local row, global column, value), count per block row
-    int *ovf_row;
-    long *ovf_col;
-    double *ovf_val;
-    int *ovf_n;
+    double *vals;  // [chunks of 32 block rows][entries][32]
+    int entries;   // values per block row
 };
 
-constexpr int kOverflow = 16;
+// Entry indices of the compact block row (see the file comment).
+struct Layout {
+    int N, BS, EF, EC, EW, EK, E, ET;
+    OSR_HD explicit Layout(int n)
+        : N(n), BS(2 * n + 4), EF(n * (2 * n + 1)), EC(n * 8 * (2 * n + 4)), EW(16), EK(3 * (2 * n + 4)),
+          E(n * (2 * n + 1) + n * 8 * (2 * n + 4) + 16 + 3 * (2 * n + 4)),
+          ET(n * (2 * n + 1) + n * 8 * (2 * n + 4) + 16 + 3 * (2 * n + 4) + kOverflow) {}
+    OSR_HD int f(int r, int c) const { return r * (2 * N + 1) + c; }
+    OSR_HD int cr(int r, int s, int c) const { return EF + ((r - N) * 8 + s) * BS + c; }
+    OSR_HD int w(int s, int c) const { return EF + EC + 2 * s + (c - 2 * N); }
+    OSR_HD int k(int r, int c) const { return EF + EC + EW + (r - 2 * N - 1) * BS + c; }
+    OSR_HD int o(int j) const { return E + j; }
+};
+
+// Index of value e of block row b in the chunked layout.
+OSR_HD inline long value_index(long b, int e, int entries) { return ((b >> 5) * entries + e) * 32 + (b & 31); }
+
+struct Out {
+    double *vals;
+    int entries;
+    long b;
+    OSR_HD void st(int e, double x) const {
+#if defined(__CUDA_ARCH__)
+        __stcs(vals + value_index(b, e, entries), x);
+#else
+        vals[value_index(b, e, entries)] = x;
+#endif
+    }
+};
+
+// Canonical column of the unit entry of canonical row r in a block row whose
+// rows carry no equation of their own: the reference's diagonal for an
+// inactive cell-medium, and for the rows a one-phase block does not use, a
+// column it does not use either.
+OSR_HD inline int unit_col(int N, int lab, int r) {
+    if (lab == 0) return r;
+    const bool oil = lab == 1;
+    if (r < N) return oil ? N + r : r;
+    if (r < 2 * N) return oil ? r - N : r;
+    if (r == 2 * N) return 2 * N;
+    if (r == 2 * N + 1) return oil ? 2 * N + 1 : 2 * N + 2;
+    if (r == 2 * N + 2) return oil ? 2 * N + 3 : 2 * N + 1;
+    return oil ? 2 * N + 2 : 2 * N + 3;
+}
+
+// Reference-local row of canonical row r for phase state lab (-1: unused).
+OSR_HD inline int ref_row(int N, int lab, int r) {
+    if (lab == 0) return r;
+    if (r < N) return -1;
+    if (r < 2 * N) return r - N;
+    if (r == 2 * N) return N;
+    if (r == 2 * N + 1) return lab == 1 ? N + 1 : -1;
+    if (r == 2 * N + 2) return lab == -1 ? N + 1 : -1;
+    return N + 2;
+}
+
+// Reference-local column of canonical column cc for phase state lab (-1:
+// unused).  The reference packs a one-phase cell's unknowns as
+// [w_0..w_{N-1}, P, Sw, S_h].
+OSR_HD inline int ref_col(int N, int lab, int cc) {
+    if (lab == 0) return cc;
+    const bool oil = lab == 1;
+    if (cc < N) return oil ? cc : -1;
+    if (cc < 2 * N) return oil ? -1 : cc - N;
+    if (cc == 2 * N) return N;
+    if (cc == 2 * N + 1) return N + 1;
+    if (cc == 2 * N + 2) return oil ? N + 2 : -1;
+    return oil ? -1 : N + 2;
+}
 
 // ---------------------------------------------------------------------------
 // Small accessors
@@ -85,19 +189,21 @@ struct Cell {
     const JacView *v;
     const JMed *F;
     long c;
-    OSR_HD double P(int p) const { return F->P[p * v->n + c]; }
-    OSR_HD double S(int p) const { return F->sat[p * v->n + c]; }
-    OSR_HD double w(int ph, int i) const { return (ph ? F->y : F->x)[(long)i * v->n + c]; }
-    OSR_HD double rho(int ph) const { return F->rho[ph * v->n + c]; }
-    OSR_HD double mu(int ph) const { return F->mu[ph * v->n + c]; }
-    OSR_HD double gam(int ph) const { return F->gam[ph * v->n + c]; }
-    OSR_HD double kr(int p) const { return F->kr[p * v->n + c]; }
-    OSR_HD double dkr(int p) const { return F->dkr[p * v->n + c]; }
-    OSR_HD double pc(int p) const { return F->pc[p * v->n + c]; }
-    OSR_HD double dE(int k, int ph) const { return F->dE[(long)(2 * k + ph) * v->n + c]; }
-    OSR_HD double D(int i, int ph) const { return F->diff[(long)(2 * i + ph) * v->n + c]; }
-    OSR_HD double por() const { return F->por[c]; }
-    OSR_HD int label() const { return F->label[c]; }
+    int med;
+    OSR_HD long bm() const { return med ? v->n + c : c; }
+    OSR_HD double P(int p) const { return ld(F->P + p * v->n + c); }
+    OSR_HD double S(int p) const { return ld(F->sat + p * v->n + c); }
+    OSR_HD double w(int ph, int i) const { return ld((ph ? F->y : F->x) + (long)i * v->n + c); }
+    OSR_HD double rho(int ph) const { return ld(F->rho + ph * v->n + c); }
+    OSR_HD double mu(int ph) const { return ld(F->mu + ph * v->n + c); }
+    OSR_HD double gam(int ph) const { return ld(F->gam + ph * v->n + c); }
+    OSR_HD double kr(int p) const { return ld(F->kr + p * v->n + c); }
+    OSR_HD double dkr(int p) const { return ld(F->dkr + p * v->n + c); }
+    OSR_HD double pc(int p) const { return ld(F->pc + p * v->n + c); }
+    OSR_HD double dE(int k, int ph) const { return ld(F->dE + (long)(2 * k + ph) * v->n + c); }
+    OSR_HD double D(int i, int ph) const { return ld(F->diff + (long)(2 * i + ph) * v->n + c); }
+    OSR_HD double por() const { return ld(F->por + c); }
+    OSR_HD int label() const { return ld(F->label + c); }
     OSR_HD double porpor() const {
         const double dp = P(1) - v->refp;
         return por() * (1 + v->cpor * dp + v->dcpor * dp * dp);
@@ -105,104 +211,155 @@ struct Cell {
     OSR_HD double dpordp() const { return por() * (v->cpor + 2 * v->dcpor * (P(1) - v->refp)); }
 };
 
-// d mu / d w_k (k < N) or d mu / d P (k == N) of one phase (DiffVisco /
-// fDiffVisco, compsim/Mass_Tran.cpp:307-399).
-OSR_HD inline double visc_deriv(const Cell &q, int k, int ph) {
-    const JacView &v = *q.v;
-    const int N = v.nc;
-    double s1 = 0, s2 = 0, ro = 0, tcm = 0, pcm = 0, mwm = 0;
-    for (int n = 0; n < N; n++) {
-        const double w = q.w(ph, n);
-        const double t = w * v.smw[n];
-        s1 += t * v.mui[n];
-        s2 += t;
-        ro += w * v.vcm[n];
-        tcm += w * v.tc[n];
-        pcm += w * v.pcr_atm[n];
-        mwm += w * v.mw[n];
-    }
-    const double rho = q.rho(ph);
-    const double Er = rho * ro;
-    const double eA = pow(tcm, 1.0 / 6), eB = sqrt(mwm), eC = pow(pcm, 2.0 / 3);
-    const double eta = eA / (eB * eC);
-    const double r1 = 0.10230 + 0.023364 * Er + 0.058533 * Er * Er - 0.040758 * Er * Er * Er + 0.0093324 * Er * Er * Er * Er;
-    double dMuS, dEta, dEr;
-    if (k < N) {
-        dMuS = (v.mui[k] * v.smw[k] * s2 - v.smw[k] * s1) / (s2 * s2);
-        dEta = ((1.0 / 6.0) * pow(tcm, -5.0 / 6.0) * v.tc[k] * eB * eC -
-                eA * (0.5 * v.mw[k] * eC / sqrt(mwm) + (2.0 / 3.0) * pow(pcm, -1.0 / 3.0) * v.pc[k] * eB / 101325)) /
-               (eB * eB * eC * eC);
-        dEr = q.dE(k, ph) * ro + rho * v.vcm[k];
-    } else {
-        dMuS = 0;
-        dEta = 0;
-        dEr = q.dE(N, ph) * ro;
-    }
-    const double dMM = 4 * r1 * r1 * r1 * (0.023364 * dEr + 0.117066 * dEr * Er - 0.122274 * dEr * Er * Er + 0.0373296 * dEr * Er * Er * Er);
-    return (dMM * eta - (r1 * r1 * r1 * r1 - 1e-4) * dEta) / (eta * eta) + dMuS;
-}
-
-// d D_i / d w_k (k < N) or d D_i / d P (k == N) of one phase (DifDiffusion /
-// fDifDiffusion, compsim/Mass_Tran.cpp:107-305).  Unlike the coefficient
-// itself (CalcDiffusion) it carries no 1e-4 factor.
-OSR_HD inline double diff_deriv(const Cell &q, int i, int k, int ph) {
-    const JacView &v = *q.v;
-    const int N = v.nc;
-    if (v.const_dif) return 0;
-    double s1 = 0, s2 = 0;
-    for (int j = 0; j < N; j++) {
-        s1 += q.w(ph, j) * v.vc53[j];
-        s2 += q.w(ph, j) * v.vc23[j];
-    }
-    const double rho = q.rho(ph);
-    const double Er = rho * s1 / s2;
-    const double AA = 0.99589 + 0.096016 * Er - 0.22035 * Er * Er + 0.032874 * Er * Er * Er;
-    double dEr;
-    if (k < N) dEr = q.dE(k, ph) * s1 / s2 + rho * (v.vc53[k] * s2 - v.vc23[k] * s1) / (s2 * s2);
-    else dEr = q.dE(N, ph) * s1 / s2;
-    const double dAA = 0.096016 * dEr - 0.4407 * Er * dEr + 0.098622 * Er * Er * dEr;
-    const double roRD = AA / rho;
-    const double dRho = q.dE(k < N ? k : N, ph);
-    double a1 = 0, a2 = 0;
-    for (int j = 0; j < N; j++) {
-        if (j == i) continue;
-        const double pDij = v.pD[j * N + i];
-        const double Dij = pDij * roRD;
-        if (k < N && k != i && j == k) a1 += 1.0 / (pDij * roRD);
-        const double dD = pDij * (dAA * rho - dRho * AA) / (rho * rho);
-        a1 += q.w(ph, j) * (-dD / (Dij * Dij));
-        a2 += q.w(ph, j) / Dij;
-    }
-    if (AA < 0 || a2 == 0) return 0;
-    if (k == i) return -(a2 + a1 * (1 - q.w(ph, i))) / (a2 * a2);
-    return -a1 * (1 - q.w(ph, i)) / (a2 * a2);
-}
-
 // ---------------------------------------------------------------------------
-// Output
+// Derivative tables
 // ---------------------------------------------------------------------------
-struct BlockRow {
-    const JacView *v;
-    long b;
-    OSR_HD void add(int slot, int r, int col, double val) const {
-        const int bs = v->bs;
-        v->vals[(((long)b * 8 + slot) * bs + r) * bs + col] += val;
-    }
-    // an entry at an arbitrary global column (kept in the overflow list)
-    OSR_HD void add_global(int r, long col, double val) const {
-        int k = v->ovf_n[b];
-        if (k < kOverflow) {
-            v->ovf_row[b * kOverflow + k] = r;
-            v->ovf_col[b * kOverflow + k] = col;
-            v->ovf_val[b * kOverflow + k] = val;
-            v->ovf_n[b] = k + 1;
+
+// One cell-medium's tables.  dmu: d mu / d w_k (k < N) or d mu / d P (k == N)
+// of each phase (DiffVisco / fDiffVisco, compsim/Mass_Tran.cpp:307-399).
+// dh: the composition sums of the diffusion-coefficient derivative
+// (DifDiffusion / fDifDiffusion, compsim/Mass_Tran.cpp:107-305):
+// s1 = sum w_j Vc_j^(5/3), s2 = sum w_j Vc_j^(2/3), Er = rho s1 / s2, AA(Er),
+// AA / rho and, per component i, Sm_i = sum_{j != i} w_j / pD_ji.
+template <int N>
+OSR_HD inline void prep_cell(const JacView &v, long bm) {
+    const int med = bm >= v.n;
+    const long c = med ? bm - v.n : bm;
+    const Cell q{&v, &v.m[med], c, med};
+    const long nb2 = 2 * v.n;
+    for (int ph = 0; ph < 2; ph++) {
+        double w[N];
+#pragma unroll
+        for (int n = 0; n < N; n++) w[n] = q.w(ph, n);
+        double s1 = 0, s2 = 0, ro = 0, tcm = 0, pcm = 0, mwm = 0;
+#pragma unroll
+        for (int n = 0; n < N; n++) {
+            const double t = w[n] * v.smw[n];
+            s1 += t * v.mui[n];
+            s2 += t;
+            ro += w[n] * v.vcm[n];
+            tcm += w[n] * v.tc[n];
+            pcm += w[n] * v.pcr_atm[n];
+            mwm += w[n] * v.mw[n];
+        }
+        const double rho = q.rho(ph);
+        const double Er = rho * ro;
+        const double eA = pow(tcm, 1.0 / 6), eB = sqrt(mwm), eC = pow(pcm, 2.0 / 3);
+        const double eta = eA / (eB * eC);
+        const double r1 = 0.10230 + 0.023364 * Er + 0.058533 * Er * Er - 0.040758 * Er * Er * Er + 0.0093324 * Er * Er * Er * Er;
+        const double t56 = pow(tcm, -5.0 / 6.0), p13 = pow(pcm, -1.0 / 3.0);
+        const double r4 = r1 * r1 * r1 * r1 - 1e-4;
+#pragma unroll
+        for (int k = 0; k <= N; k++) {
+            double dMuS, dEta, dEr;
+            if (k < N) {
+                dMuS = (v.mui[k] * v.smw[k] * s2 - v.smw[k] * s1) / (s2 * s2);
+                dEta = ((1.0 / 6.0) * t56 * v.tc[k] * eB * eC -
+                        eA * (0.5 * v.mw[k] * eC / eB + (2.0 / 3.0) * p13 * v.pc[k] * eB / 101325)) /
+                       (eB * eB * eC * eC);
+                dEr = q.dE(k, ph) * ro + rho * v.vcm[k];
+            } else {
+                dMuS = 0;
+                dEta = 0;
+                dEr = q.dE(N, ph) * ro;
+            }
+            const double dMM = 4 * r1 * r1 * r1 * (0.023364 * dEr + 0.117066 * dEr * Er - 0.122274 * dEr * Er * Er + 0.0373296 * dEr * Er * Er * Er);
+            v.dmu[(long)(ph * (N + 1) + k) * nb2 + bm] = (dMM * eta - r4 * dEta) / (eta * eta) + dMuS;
+        }
+        if (v.const_dif) continue;
+        double d1 = 0, d2 = 0;
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            d1 += w[j] * v.vc53[j];
+            d2 += w[j] * v.vc23[j];
+        }
+        const double Ed = rho * d1 / d2;
+        const double AA = 0.99589 + 0.096016 * Ed - 0.22035 * Ed * Ed + 0.032874 * Ed * Ed * Ed;
+        double *h = v.dh + (long)ph * (5 + N) * nb2 + bm;
+        h[0] = d1;
+        h[nb2] = d2;
+        h[2 * nb2] = Ed;
+        h[3 * nb2] = AA;
+        h[4 * nb2] = AA / rho;
+        for (int i = 0; i < N; i++) {
+            double sm = 0;
+#pragma unroll
+            for (int j = 0; j < N; j++)
+                if (j != i) sm += w[j] / v.pD[j * N + i];
+            h[(5 + i) * nb2] = sm;
         }
     }
+}
+
+OSR_HD inline double dmu(const Cell &q, int k, int ph) {
+    const int N = q.v->nc;
+    return ld(q.v->dmu + (long)(ph * (N + 1) + k) * (2 * q.v->n) + q.bm());
+}
+
+// d D_i / d w_k (k < N) or d D_i / d P (k == N) of one phase.  With
+// G = (dAA rho - dRho AA) / rho^2 the reference's sums over j != i factor as
+//   a2 = Sm_i / (AA/rho),  a1 = [k != i] / (pD_ki AA/rho) - G Sm_i / (AA/rho)^2,
+//   dD = -(a2 [k == i] + a1 (1 - w_i)) / a2^2.
+// Unlike the coefficient itself (CalcDiffusion) it carries no 1e-4 factor.
+// DDer holds the k-independent factors of one (cell-medium, phase, i).
+struct DDer {
+    double s1, s2, r12, is22, Er, cA, AA, rho, irho2, iroRD, a2, ia2sq, omw;
+    bool zero;
 };
 
-// One face of a cell for the Jacobian: neighbour, the cell holding the face's
-// transmissibilities (tc), direction and sign, the two block sizes along the
-// direction and twice the cross-section.
+OSR_HD inline DDer make_dder(const Cell &q, int i, int ph) {
+    const JacView &v = *q.v;
+    const int N = v.nc;
+    const long nb2 = 2 * v.n;
+    DDer d;
+    if (v.const_dif) {
+        d.zero = true;
+        return d;
+    }
+    const double *h = v.dh + (long)ph * (5 + N) * nb2 + q.bm();
+    d.s1 = ld(h);
+    d.s2 = ld(h + nb2);
+    d.Er = ld(h + 2 * nb2);
+    d.AA = ld(h + 3 * nb2);
+    const double roRD = ld(h + 4 * nb2), Sm = ld(h + (5 + i) * nb2);
+    d.rho = q.rho(ph);
+    d.r12 = d.s1 / d.s2;
+    d.is22 = 1 / (d.s2 * d.s2);
+    d.cA = 0.096016 - 0.4407 * d.Er + 0.098622 * d.Er * d.Er;
+    d.irho2 = 1 / (d.rho * d.rho);
+    d.iroRD = 1 / roRD;
+    d.a2 = Sm * d.iroRD;
+    d.ia2sq = 1 / (d.a2 * d.a2);
+    d.omw = 1 - q.w(ph, i);
+    d.zero = d.AA < 0 || d.a2 == 0;
+    return d;
+}
+
+// dEk: d rho / d w_k (k < N) or d rho / d P (k == N) of the same cell and phase.
+OSR_HD inline double dd_k(const JacView &v, const DDer &d, int i, int k, double dEk) {
+    if (d.zero) return 0;
+    const int N = v.nc;
+    double dEr = dEk * d.r12;
+    if (k < N) dEr += d.rho * (v.vc53[k] * d.s2 - v.vc23[k] * d.s1) * d.is22;
+    const double G = (dEr * d.cA * d.rho - dEk * d.AA) * d.irho2;
+    double a1 = -G * d.a2 * d.iroRD;
+    if (k < N && k != i) a1 += v.ipD[k * N + i] * d.iroRD;
+    if (k == i) return -(d.a2 + a1 * d.omw) * d.ia2sq;
+    return -a1 * d.omw * d.ia2sq;
+}
+
+OSR_HD inline double dD(const Cell &q, int i, int k, int ph) {
+    if (q.v->const_dif) return 0;
+    return dd_k(*q.v, make_dder(q, i, ph), i, k, q.dE(k < q.v->nc ? k : q.v->nc, ph));
+}
+
+// ---------------------------------------------------------------------------
+// Faces
+// ---------------------------------------------------------------------------
+
+// One face of a cell: neighbour, the cell holding the face's
+// transmissibilities (tc), direction and sign, block slot, the two block
+// sizes along the direction and twice the cross-section.
 struct JFace {
     long nb, tc;
     int d, sgn, slot;
@@ -212,13 +369,14 @@ struct JFace {
 OSR_HD inline int jac_faces(const JacView &v, long c, JFace *f) {
     const int ix = (int)(c % v.nx), iy = (int)((c / v.nx) % v.ny), iz = (int)(c / ((long)v.nx * v.ny));
     const long sx = 1, sy = v.nx, sz = (long)v.nx * v.ny;
+    const double di = ld(v.di + ix), dj = ld(v.dj + iy), dk = ld(v.dk + iz);
     int k = 0;
-    if (ix < v.nx - 1) f[k++] = JFace{c + sx, c, 0, 1, 2, v.di[ix], v.di[ix + 1], 2 * v.dj[iy] * v.dk[iz]};
-    if (ix > 0) f[k++] = JFace{c - sx, c - sx, 0, -1, 1, v.di[ix], v.di[ix - 1], 2 * v.dj[iy] * v.dk[iz]};
-    if (iy < v.ny - 1) f[k++] = JFace{c + sy, c, 1, 1, 4, v.dj[iy], v.dj[iy + 1], 2 * v.di[ix] * v.dk[iz]};
-    if (iy > 0) f[k++] = JFace{c - sy, c - sy, 1, -1, 3, v.dj[iy], v.dj[iy - 1], 2 * v.di[ix] * v.dk[iz]};
-    if (iz < v.nz - 1) f[k++] = JFace{c + sz, c, 2, 1, 6, v.dk[iz], v.dk[iz + 1], 2 * v.di[ix] * v.dj[iy]};
-    if (iz > 0) f[k++] = JFace{c - sz, c - sz, 2, -1, 5, v.dk[iz], v.dk[iz - 1], 2 * v.di[ix] * v.dj[iy]};
+    if (ix < v.nx - 1) f[k++] = JFace{c + sx, c, 0, 1, 2, di, ld(v.di + ix + 1), 2 * dj * dk};
+    if (ix > 0) f[k++] = JFace{c - sx, c - sx, 0, -1, 1, di, ld(v.di + ix - 1), 2 * dj * dk};
+    if (iy < v.ny - 1) f[k++] = JFace{c + sy, c, 1, 1, 4, dj, ld(v.dj + iy + 1), 2 * di * dk};
+    if (iy > 0) f[k++] = JFace{c - sy, c - sy, 1, -1, 3, dj, ld(v.dj + iy - 1), 2 * di * dk};
+    if (iz < v.nz - 1) f[k++] = JFace{c + sz, c, 2, 1, 6, dk, ld(v.dk + iz + 1), 2 * di * dj};
+    if (iz > 0) f[k++] = JFace{c - sz, c - sz, 2, -1, 5, dk, ld(v.dk + iz - 1), 2 * di * dj};
     return k;
 }
 
@@ -233,11 +391,15 @@ struct FaceData {
 OSR_HD inline FaceData face_data(const JacView &v, const JMed &F, long c, const JFace &e) {
     FaceData fd;
     const long n = v.n;
-    for (int t = 0; t < 12; t++) fd.T[t] = F.trans[(long)(t * 3 + e.d) * n + e.tc];
-    for (int p = 0; p < 3; p++) fd.ts[p] = F.transS[(long)(p * 3 + e.d) * n + e.tc];
-    fd.ift = F.iftran[(long)e.d * n + e.tc];
-    for (int p = 0; p < 3; p++) fd.dP[p] = e.sgn > 0 ? F.P[p * n + e.nb] - F.P[p * n + c] : F.P[p * n + c] - F.P[p * n + e.nb];
-    fd.dH = e.sgn > 0 ? v.blockH[e.nb] - v.blockH[c] : v.blockH[c] - v.blockH[e.nb];
+    for (int t = 0; t < 12; t++) fd.T[t] = ld(F.trans + (long)(t * 3 + e.d) * n + e.tc);
+    for (int p = 0; p < 3; p++) fd.ts[p] = ld(F.transS + (long)(p * 3 + e.d) * n + e.tc);
+    fd.ift = ld(F.iftran + (long)e.d * n + e.tc);
+    for (int p = 0; p < 3; p++) {
+        const double a = ld(F.P + p * n + e.nb), b = ld(F.P + p * n + c);
+        fd.dP[p] = e.sgn > 0 ? a - b : b - a;
+    }
+    const double hn = ld(v.blockH + e.nb), hc = ld(v.blockH + c);
+    fd.dH = e.sgn > 0 ? hn - hc : hc - hn;
     return fd;
 }
 
@@ -247,45 +409,48 @@ OSR_HD inline long upstream(const JFace &e, const FaceData &fd, long c, int p) {
     return fd.ts[p] ? c : e.nb;
 }
 
-// Columns of a cell's own unknowns by phase state (the reference's reCol /
-// reCol3 offsets): a one-phase cell has no column for the absent phase's
-// composition and saturation, and an oil-only or gas-only cell emits its own
-// saturation derivatives only for the phases it carries.
+// Which of a cell's own unknowns the reference's rows address by phase state
+// (its reCol / reCol3 offsets): a one-phase cell has no column for the
+// absent phase's composition and saturation, and an oil-only or gas-only cell
+// emits its own saturation derivatives only for the phases it carries.
 struct OwnLayout {
-    int P, Sw, So, Sg, X, Y;
     bool swso, sg, x, y;
 };
 
-OSR_HD inline OwnLayout own_layout(int N, int lab) {
-    if (lab == 0) return OwnLayout{2 * N, 2 * N + 1, 2 * N + 2, 2 * N + 3, 0, N, true, true, true, true};
-    if (lab == 1) return OwnLayout{N, N + 1, N + 2, -1, 0, -1, true, false, true, false};
-    return OwnLayout{N, N + 1, -1, N + 2, -1, 0, false, true, false, true};
+OSR_HD inline OwnLayout own_layout(int lab) {
+    if (lab == 0) return OwnLayout{true, true, true, true};
+    if (lab == 1) return OwnLayout{true, false, true, false};
+    return OwnLayout{false, true, false, true};
 }
+
+// One phase of one cell as the mobility factors see it.
+struct Side {
+    double rho, mu, gam;
+};
 
 // Mobility-ratio derivative factors of one phase across a face: the
 // derivatives of (rho_c dl + rho_n dn C) / (mu_c dl + mu_n dn C) and of the
 // face-averaged gravity with respect to a variable of this cell (M, MG) and
-// of the neighbour (B, BG).  k = N: pressure; k < N: component k.
+// of the neighbour (B, BG).  comp: a composition variable with molar mass
+// mwk (else pressure).
 struct Mob {
     double Sur, Mak, M, B, MG, BG, tempdx;
 };
 
-OSR_HD inline Mob mobility(const Cell &q, const Cell &nb, const JFace &e, int ph, int k, double coef, double dmu_c,
-                           double dmu_n, bool coef_in_bg) {
-    const int N = q.v->nc;
+OSR_HD inline Mob mobility(const Side &q, const Side &nb, double dEq, double dEn, bool comp, double mwk, const JFace &e,
+                           double coef, double dmu_c, double dmu_n) {
     Mob m;
-    m.Sur = q.rho(ph) * e.dl + nb.rho(ph) * e.dn * coef;
-    m.Mak = q.mu(ph) * e.dl + nb.mu(ph) * e.dn * coef;
-    m.M = (q.dE(k, ph) * e.dl * m.Mak - dmu_c * e.dl * m.Sur) / (m.Mak * m.Mak);
-    m.B = (nb.dE(k, ph) * e.dn * coef * m.Mak - dmu_n * e.dn * coef * m.Sur) / (m.Mak * m.Mak);
-    const double gk_c = k < N ? kGAccG * q.rho(ph) * q.v->mw[k] : 0.0;
-    const double gk_n = k < N ? kGAccG * nb.rho(ph) * q.v->mw[k] : 0.0;
-    m.MG = e.dl * (gk_c + q.gam(ph) * q.dE(k, ph) / q.rho(ph)) / (e.dl + e.dn * coef);
-    m.BG = (coef_in_bg ? coef : 1.0) * e.dn * (gk_n + nb.gam(ph) * nb.dE(k, ph) / nb.rho(ph)) / (e.dl + e.dn * coef);
-    m.tempdx = (q.gam(ph) * e.dl + nb.gam(ph) * e.dn * coef) / (e.dl + e.dn * coef);
+    m.Sur = q.rho * e.dl + nb.rho * e.dn * coef;
+    m.Mak = q.mu * e.dl + nb.mu * e.dn * coef;
+    m.M = (dEq * e.dl * m.Mak - dmu_c * e.dl * m.Sur) / (m.Mak * m.Mak);
+    m.B = (dEn * e.dn * coef * m.Mak - dmu_n * e.dn * coef * m.Sur) / (m.Mak * m.Mak);
+    const double gk_c = comp ? kGAccG * q.rho * mwk : 0.0;
+    const double gk_n = comp ? kGAccG * nb.rho * mwk : 0.0;
+    m.MG = e.dl * (gk_c + q.gam * dEq / q.rho) / (e.dl + e.dn * coef);
+    m.BG = coef * e.dn * (gk_n + nb.gam * dEn / nb.rho) / (e.dl + e.dn * coef);
+    m.tempdx = (q.gam * e.dl + nb.gam * e.dn * coef) / (e.dl + e.dn * coef);
     return m;
 }
-
 
 // ---------------------------------------------------------------------------
 // Matrix-fracture transfer quantities of a cell (the "sadeq" region of the
@@ -303,7 +468,7 @@ struct Transfer {
 
 OSR_HD inline Transfer transfer_terms(const JacView &v, long c) {
     Transfer t;
-    const Cell M{&v, &v.m[0], c}, F{&v, &v.m[1], c};
+    const Cell M{&v, &v.m[0], c, 0}, F{&v, &v.m[1], c, 1};
     t.pm = M.porpor();
     t.pf = F.porpor();
     t.dpm = M.dpordp();
@@ -326,9 +491,9 @@ OSR_HD inline Transfer transfer_terms(const JacView &v, long c) {
     t.dPg = (F.P(2) - M.P(2)) + (F.pc(1) - M.pc(1));
     t.dPw = (F.P(0) - M.P(0)) + (M.pc(0) - F.pc(0));
     const int ix = (int)(c % v.nx), iy = (int)((c / v.nx) % v.ny), iz = (int)(c / ((long)v.nx * v.ny));
-    const double di = v.di[ix], dj = v.dj[iy], dk = v.dk[iz];
+    const double di = ld(v.di + ix), dj = ld(v.dj + iy), dk = ld(v.dk + iz);
     t.Vb = di * dj * dk;
-    t.SF2 = 4 * v.sigma * (M.F->perm[c] / (di * di) + M.F->perm[v.n + c] / (dj * dj) + M.F->perm[2 * v.n + c] / (dk * dk));
+    t.SF2 = 4 * v.sigma * (ld(M.F->perm + c) / (di * di) + ld(M.F->perm + v.n + c) / (dj * dj) + ld(M.F->perm + 2 * v.n + c) / (dk * dk));
     t.SF1 = v.diff_off ? 0.0 : 4 * v.sigma * ((1 / (di * di)) + (1 / (dj * dj)) + (1 / (dk * dk)));
     t.SF3 = v.diff_off ? 0.0 : 4 * v.sigma * ((1 / di) + (1 / dj) + (1 / dk)) / v.lf;
     return t;
@@ -359,6 +524,19 @@ OSR_HD inline int matrix_diff_targets(int lm, int lf, int ph, int *kinds) {
     return n;
 }
 
+// Fracture-side diffusive transfer pairings.  fsf1: the matrix-side (SF1)
+// terms toward the fracture composition a fracture row carries for phase ph;
+// fsf3: the interface (SF3) terms of the fracture's own phase ph.
+OSR_HD inline bool fsf1(int lm, int lf, int ph) {
+    if (lm == 0 && lf == 0) return true;
+    if (ph == 0) return (lm == 1 && lf == 1) || (lm == 0 && lf == 1) || (lm == 1 && lf == 0);
+    return (lm == -1 && lf == -1) || (lm == 0 && lf == -1) || (lm == -1 && lf == 0);
+}
+OSR_HD inline bool fsf3(int lm, int lf, int ph) {
+    if (ph == 0) return (lm == -1 && lf == 1) || (lm == 0 && lf == 1) || (lm == -1 && lf == 0);
+    return (lm == 1 && lf == -1) || (lm == 0 && lf == -1) || (lm == 1 && lf == 0);
+}
+
 // Direction-dependent deviations of the reference's face blocks.
 struct FaceQuirks {
     bool gas_dB_assign_up;     // - faces, gas upstream = this cell: dB = ... instead of dB -= ...
@@ -367,65 +545,63 @@ struct FaceQuirks {
     bool gas_coef_any_1ph;     // k != i, gas: neighbour weight zero for any one-phase neighbour
     bool oil_grav_assign_down; // - faces, oil upstream = neighbour: gravity term assigned to dB
     bool shifted_block;        // neighbour P / S columns counted from the block after the neighbour's
-    bool matrix_kr_offdiag_up; // k != i, oil upstream = this cell: the matrix relative permeability
 };
 
-OSR_HD inline FaceQuirks matrix_total_quirks(const JFace &e) {
-    FaceQuirks q{false, false, false, false, false, false, false};
+// the total rows' pressure / saturation face blocks
+OSR_HD inline FaceQuirks total_quirks(const JFace &e) {
+    FaceQuirks q{false, false, false, false, false, false};
     if (e.sgn < 0 && e.d == 1) { q.gas_dB_assign_down = true; q.oil_grav_assign_down = true; q.shifted_block = true; }
     if (e.sgn < 0 && e.d == 2) q.shifted_block = true;
     return q;
 }
 
-OSR_HD inline FaceQuirks fracture_comp_quirks(const JFace &e);
-
-OSR_HD inline FaceQuirks matrix_comp_quirks(const JFace &e) {
-    FaceQuirks q{false, false, false, false, false, false, false};
+// the component rows' face blocks (both continua)
+OSR_HD inline FaceQuirks comp_quirks(const JFace &e) {
+    FaceQuirks q{false, false, false, false, false, false};
     if (e.sgn < 0 && e.d == 0) { q.gas_dB_assign_up = true; q.gas_dB_assign_down = true; q.gas_coef_any_1ph = true; }
     if (e.sgn > 0 && e.d == 2) q.ift_y_in_diag_grav = true;
     return q;
 }
 
-
 // ---------------------------------------------------------------------------
-// Component balance rows of a cell (matrix continuum).
+// Accumulators of one component or total row.  The per-component ones live
+// in shared memory on the device (one column per thread: element k at
+// X[k * stride]).
 // ---------------------------------------------------------------------------
-
-OSR_HD inline FaceQuirks fracture_comp_quirks(const JFace &e) {
-    return matrix_comp_quirks(e);
-}
-
-// Derivatives of row i's face terms with respect to the neighbour's pressure
-// and saturations (emitted) and this cell's pressure and saturations
-// (accumulated): the first face block of the reference's component rows.
-struct OwnPS {
+struct Acc {
     double dp, dSw, dSo, dSg;
+    double *X, *Y;   // d(flux + transfer) / d x_k, d y_k of this cell
+    double *Z;       // a one-phase neighbour's composition entries between the two phases
+    int stride;
+    OSR_HD double &x(int k) { return X[k * stride]; }
+    OSR_HD double &y(int k) { return Y[k * stride]; }
+    OSR_HD double &z(int k) { return Z[k * stride]; }
 };
 
-OSR_HD inline void comp_face_ps(const JacView &v, const Cell &q, int i, const JFace &e, const FaceQuirks &qk,
-                                const BlockRow &out, int row, OwnPS &acc, bool fracture, bool total = false) {
+// Derivatives of row i's face terms with respect to the neighbour's pressure
+// and saturations (ps, canonical P Sw So Sg, or ov when the reference counts
+// them from the following block) and this cell's pressure and saturations
+// (accumulated).
+OSR_HD inline void face_ps(const JacView &v, const Cell &q, const Cell &nb, int i, const JFace &e, const FaceData &fd,
+                           const FaceQuirks &qk, bool fracture, bool total, Acc &acc, double *ps, double *ov) {
     const int N = v.nc;
-    const JMed &F = *q.F;
-    const Cell nb{&v, &F, e.nb};
-    const FaceData fd = face_data(v, F, q.c, e);
     const double s = e.sgn;
-    const int lnb = nb.label();
-    const int nbase = lnb ? -N : 0, reCol4 = lnb ? 1 : 0;
-    const long upo = upstream(e, fd, q.c, 0), upg = upstream(e, fd, q.c, 1);
-    const bool nb_o = upo == e.nb, nb_g = upg == e.nb;
-    const Cell Uo{&v, &F, upo}, Ug{&v, &F, upg};
-    const double xo = total ? 1.0 : Uo.w(0, i), yg = total ? 1.0 : Ug.w(1, i);
-    // the emitted neighbour columns; the reference counts some from the next block's offset
-    auto put = [&](int col, double val) {
-        if (qk.shifted_block) out.add_global(row, v.rowoff[(e.nb + (q.F == &v.m[1] ? v.n : 0)) + 1] + col, val);
-        else out.add(e.slot, row, col, val);
+    const int lnb = nb.label(), lq = q.label();
+    const bool nb_o = upstream(e, fd, q.c, 0) == e.nb, nb_g = upstream(e, fd, q.c, 1) == e.nb;
+    const double xo = total ? 1.0 : (nb_o ? nb : q).w(0, i), yg = total ? 1.0 : (nb_g ? nb : q).w(1, i);
+    // the reference's four neighbour columns: P, Sw, So, and the hydrocarbon
+    // saturation (Sg, or a one-phase neighbour's own saturation)
+    const int cS2 = lnb == -1 ? 3 : 2, cS3 = lnb == 1 ? 2 : 3;
+    auto put = [&](int t, int cc, double val) {
+        if (qk.shifted_block) ov[t] = val;
+        else ps[cc] += val;
     };
     // saturation factors
     const double dsw = s * (xo * fd.T[4] * fd.dP[1] + xo * fd.T[6] * fd.dH);
-    if (nb_o) put(nbase + 2 * N + 1, dsw);
+    if (nb_o) put(1, 1, dsw);
     else acc.dSw += dsw;
     const double dso = s * (xo * fd.T[10] * fd.dP[1] + xo * fd.T[11] * fd.dH);
-    if (nb_o) put(nbase + 2 * N + 2, lnb == -1 ? 0.0 : dso);
+    if (nb_o) put(2, cS2, lnb == -1 ? 0.0 : dso);
     else acc.dSo += dso;
     const double dsgo = s * (xo * fd.T[8] * fd.dP[1] + xo * fd.T[9] * fd.dH);
     const double dsgg = s * (yg * fd.T[5] * fd.dP[2] + yg * fd.T[7] * fd.dH);
@@ -434,24 +610,27 @@ OSR_HD inline void comp_face_ps(const JacView &v, const Cell &q, int i, const JF
     else acc.dSg += dsgo;
     if (nb_g) vsg += lnb == 1 ? 0.0 : dsgg;
     else acc.dSg += dsgg;
-    put(nbase + 2 * N + 3 - reCol4, vsg);
+    put(3, cS3, vsg);
     // mobility and diffusion derivatives with respect to the two pressures
-    const double tor_c = fracture ? 1.0 : v.tor[q.c], tor_n = fracture ? 1.0 : v.tor[e.nb];
+    const double tor_c = fracture ? 1.0 : ld(v.tor + q.c), tor_n = fracture ? 1.0 : ld(v.tor + e.nb);
     const double pm = q.porpor(), dpm = q.dpordp();
     const double pn = nb.porpor(), dpn = nb.dpordp();
     const double NNd = e.area2 / (e.dn + e.dl);
+    const bool inactive = q.por() < 1e-10 || nb.por() < 1e-10;
     double dB = 0;
     for (int ph = 0; ph < 2; ph++) {
         const double coef = ph == 0 ? (lnb == -1 ? 0.0 : 1.0) : (lnb == 1 ? 0.0 : 1.0);
-        const double dC = ph == 0 ? (q.label() == -1 ? 0.0 : 1.0) : (q.label() == 1 ? 0.0 : 1.0);
-        const Mob m = mobility(q, nb, e, ph, N, coef, visc_deriv(q, N, ph), visc_deriv(nb, N, ph), true);
+        const double dC = ph == 0 ? (lq == -1 ? 0.0 : 1.0) : (lq == 1 ? 0.0 : 1.0);
+        const Side sq{q.rho(ph), q.mu(ph), q.gam(ph)}, sn{nb.rho(ph), nb.mu(ph), nb.gam(ph)};
+        const double dEq = q.dE(N, ph), dEn = nb.dE(N, ph);
+        const Mob m = mobility(sq, sn, dEq, dEn, false, 0.0, e, coef, dmu(q, N, ph), dmu(nb, N, ph));
         const bool up_nb = ph == 0 ? nb_o : nb_g;
         const Cell &U = up_nb ? nb : q;
         const double wk = total ? 1.0 : U.w(ph, i), krk = U.kr(1 + ph);
         const double dPp = fd.dP[1 + ph];
         const double a = wk * fd.ift * krk;
         acc.dp -= s * (a * m.M * dPp);
-        double vB = s * (a * m.B * dPp);
+        const double vB = s * (a * m.B * dPp);
         if (ph == 1 && e.sgn < 0) {
             const bool assign = up_nb ? qk.gas_dB_assign_down : qk.gas_dB_assign_up;
             dB = assign ? vB : dB + vB;
@@ -465,25 +644,26 @@ OSR_HD inline void comp_face_ps(const JacView &v, const Cell &q, int i, const JF
             if (ph == 0 && e.sgn < 0 && up_nb && qk.oil_grav_assign_down) dB = gB;
             else dB += gB;
         }
-        if (total) continue;
+        if (total || v.diff_off) continue;   // CDIF 0: the coefficient and its derivatives vanish
         // intra-continuum diffusion
+        const double wq = q.w(ph, i), wn = nb.w(ph, i);
         double Dup, dDdp, dDdp2;
-        if (nb.w(ph, i) > q.w(ph, i)) {
+        if (wn > wq) {
             Dup = nb.D(i, ph);
             dDdp = 0;
-            dDdp2 = diff_deriv(nb, i, N, ph);
+            dDdp2 = dD(nb, i, N, ph);
         } else {
             Dup = q.D(i, ph);
-            dDdp = diff_deriv(q, i, N, ph);
+            dDdp = dD(q, i, N, ph);
             dDdp2 = 0;
         }
-        if (q.por() < 1e-10 || nb.por() < 1e-10) Dup = dDdp = dDdp2 = 0;
-        double AAd = nb.rho(ph) * e.dn * coef + q.rho(ph) * e.dl * dC;
+        if (inactive) Dup = dDdp = dDdp2 = 0;
+        double AAd = sn.rho * e.dn * coef + sq.rho * e.dl * dC;
         AAd *= (nb.S(1 + ph) * e.dn * coef + q.S(1 + ph) * e.dl * dC) / (e.dn + e.dl);
         const double BBd = tor_n * e.dn * coef / pn + tor_c * e.dl * dC / pm;
         const double MMd = AAd / BBd;
-        const double DX = nb.w(ph, i) - q.w(ph, i);
-        const double dAA = q.dE(N, ph) * e.dl * dC, dAA2 = nb.dE(N, ph) * e.dn * coef;
+        const double DX = wn - wq;
+        const double dAA = dEq * e.dl * dC, dAA2 = dEn * e.dn * coef;
         const double dBB = -dpm * tor_c * e.dl * dC / (pm * pm), dBB2 = -dpn * tor_n * e.dn * coef / (pn * pn);
         const double dMM = (dAA * BBd - dBB * AAd) / (BBd * BBd), dMM2 = (dAA2 * BBd - dBB2 * AAd) / (BBd * BBd);
         if (coef != 0 && dC != 0) {
@@ -491,100 +671,182 @@ OSR_HD inline void comp_face_ps(const JacView &v, const Cell &q, int i, const JF
             dB += NNd * DX * (MMd * dDdp2 + Dup * dMM2);
         }
     }
-    put(nbase + 2 * N, v.pcoeff * (-xo * fd.T[0] - yg * fd.T[1] - dB));
+    put(0, 0, v.pcoeff * (-xo * fd.T[0] - yg * fd.T[1] - dB));
 }
 
-// Derivatives of row i's face terms with respect to component k of both
-// cells (the second and third face blocks: k == i and k != i).
-OSR_HD inline void comp_face_x(const JacView &v, const Cell &q, int i, int k, const JFace &e, const FaceQuirks &qk,
-                               const BlockRow &out, int row, double &dRxl, double &dRxg, bool fracture,
-                               bool total = false) {
+// k-independent factors of one phase across one face for the composition
+// derivatives (the mobility-ratio and gravity denominators, the upstream
+// weights and the diffusion factors) at neighbour weight coef.
+struct PhFace {
+    double coef, Sur, Mak, iMak2, iden, tempdx, SurMak, gq, gn;
+    double BBd, iBB, MMd;
+};
+
+OSR_HD inline PhFace ph_face(const Side &sq, const Side &sn, const JFace &e, double coef, double dC, double Sq,
+                             double Sn, double tor_c, double tor_n, double pm, double pn) {
+    PhFace P;
+    P.coef = coef;
+    P.Sur = sq.rho * e.dl + sn.rho * e.dn * coef;
+    P.Mak = sq.mu * e.dl + sn.mu * e.dn * coef;
+    P.iMak2 = 1 / (P.Mak * P.Mak);
+    P.iden = 1 / (e.dl + e.dn * coef);
+    P.tempdx = (sq.gam * e.dl + sn.gam * e.dn * coef) * P.iden;
+    P.SurMak = P.Sur / P.Mak;
+    P.gq = sq.gam / sq.rho;
+    P.gn = sn.gam / sn.rho;
+    double AAd = sn.rho * e.dn * coef + sq.rho * e.dl * dC;
+    AAd *= (Sn * e.dn * coef + Sq * e.dl * dC) / (e.dn + e.dl);
+    P.BBd = tor_n * e.dn * coef / pn + tor_c * e.dl * dC / pm;
+    P.iBB = 1 / P.BBd;
+    P.MMd = AAd * P.iBB;
+    return P;
+}
+
+// Derivatives of row i's face terms with respect to the compositions of both
+// cells: the neighbour's entries are stored (both phases of a one-phase
+// neighbour land in its one composition column), this cell's accumulated.
+OSR_HD inline void face_x(const JacView &v, const Cell &q, const Cell &nb, int i, const JFace &e, const FaceData &fd,
+                          const FaceQuirks &qk, bool fracture, bool total, Acc &acc, const Out &out, int row) {
     const int N = v.nc;
-    const JMed &F = *q.F;
-    const Cell nb{&v, &F, e.nb};
-    const FaceData fd = face_data(v, F, q.c, e);
+    const Layout L(N);
     const double s = e.sgn;
-    const bool diag = !total && k == i;
-    const int lnb = nb.label();
-    const double tor_c = fracture ? 1.0 : v.tor[q.c], tor_n = fracture ? 1.0 : v.tor[e.nb];
+    const int lnb = nb.label(), lq = q.label();
+    const double tor_c = fracture ? 1.0 : ld(v.tor + q.c), tor_n = fracture ? 1.0 : ld(v.tor + e.nb);
     const double pm = q.porpor(), pn = nb.porpor();
     const double NNd = e.area2 / (e.dn + e.dl);
+    const double ift_y = ld(q.F->iftran + v.n + q.c);
+    const bool idiff = !total && !v.diff_off;   // intra-continuum diffusion present
     for (int ph = 0; ph < 2; ph++) {
-        double coef;
-        if (ph == 0) coef = lnb == -1 ? 0.0 : 1.0;
-        else if (!diag && qk.gas_coef_any_1ph) coef = lnb != 0 ? 0.0 : 1.0;
-        else coef = lnb == 1 ? 0.0 : 1.0;
-        const double dC = ph == 0 ? (q.label() == -1 ? 0.0 : 1.0) : (q.label() == 1 ? 0.0 : 1.0);
-        const Mob m = mobility(q, nb, e, ph, k, coef, visc_deriv(q, k, ph), visc_deriv(nb, k, ph), true);
         const bool up_nb = upstream(e, fd, q.c, ph) == e.nb;
-        const double Tp = diag ? fd.T[ph] : 0.0, Tg = diag ? fd.T[2 + ph] : 0.0;
-        const double dPp = fd.dP[1 + ph];
-        double dR = 0, dB;
+        const Side sq{q.rho(ph), q.mu(ph), q.gam(ph)}, sn{nb.rho(ph), nb.mu(ph), nb.gam(ph)};
         const double wc = total ? 1.0 : q.w(ph, i), wn = total ? 1.0 : nb.w(ph, i);
-        const double krc = (ph == 0 && !diag && !total && qk.matrix_kr_offdiag_up) ? v.m[0].kr[v.n + q.c] : q.kr(1 + ph);
-        const double ac = wc * fd.ift * krc, an = wn * fd.ift * nb.kr(1 + ph);
-        const double gM = m.M * m.tempdx + m.MG * m.Sur / m.Mak, gB = m.B * m.tempdx + m.BG * m.Sur / m.Mak;
-        if (up_nb) {
-            dR += s * (an * m.M * dPp);
-            dB = s * ((Tp + an * m.B) * dPp);
-        } else {
-            dR += s * ((Tp + ac * m.M) * dPp);
-            dB = s * (ac * m.B * dPp);
+        const double krq = q.kr(1 + ph), krn = nb.kr(1 + ph);
+        const double Sq = q.S(1 + ph), Sn = nb.S(1 + ph);
+        const double dC = ph == 0 ? (lq == -1 ? 0.0 : 1.0) : (lq == 1 ? 0.0 : 1.0);
+        // the neighbour weight off the diagonal (k != i) and on it
+        double coef_nd, coef_d;
+        if (ph == 0) coef_nd = coef_d = lnb == -1 ? 0.0 : 1.0;
+        else {
+            coef_d = lnb == 1 ? 0.0 : 1.0;
+            coef_nd = qk.gas_coef_any_1ph ? (lnb != 0 ? 0.0 : 1.0) : coef_d;
         }
-        // gravity (nonzero across z faces only)
-        if (e.sgn > 0) {
-            if (up_nb) {
-                const double ift_r = (diag && ph == 0 && qk.ift_y_in_diag_grav)
-                                         ? F.iftran[v.n + q.c] : fd.ift;
-                dR += wn * ift_r * nb.kr(1 + ph) * gM * fd.dH;
-                dB += (Tg + an * gB) * fd.dH;
-            } else {
-                dR += (Tg + ac * gM) * fd.dH;
-                dB += ac * gB * fd.dH;
-            }
-        } else {
-            // - faces: the gas terms exchange the two cells' factors; with k != i
-            // the oil terms of a downstream cell change sign
-            const double g1 = ph == 1 ? gB : gM, g2 = ph == 1 ? gM : gB;
-            if (!up_nb) {
-                dR -= (Tg + ac * g1) * fd.dH;
-                dB -= ac * g2 * fd.dH;
-            } else {
-                const double flip = (!diag && !total && ph == 0) ? -1.0 : 1.0;
-                dR -= flip * (an * g1 * fd.dH);
-                dB -= flip * ((Tg + an * g2) * fd.dH);
-            }
-        }
-        // intra-continuum diffusion (component rows only)
-        double Dup = 0, dDdx = 0, dDdx2 = 0;
-        if (total) {
-        } else if (wn > wc) {
-            Dup = nb.D(i, ph);
-            dDdx = 0;
-            dDdx2 = diff_deriv(nb, i, k, ph);
-        } else {
-            Dup = q.D(i, ph);
-            dDdx = diff_deriv(q, i, k, ph);
-            dDdx2 = 0;
-        }
-        double AAd = nb.rho(ph) * e.dn * coef + q.rho(ph) * e.dl * dC;
-        AAd *= (nb.S(1 + ph) * e.dn * coef + q.S(1 + ph) * e.dl * dC) / (e.dn + e.dl);
-        const double BBd = tor_n * e.dn * coef / pn + tor_c * e.dl * dC / pm;
-        const double MMd = AAd / BBd;
+        const PhFace base = ph_face(sq, sn, e, coef_nd, dC, Sq, Sn, tor_c, tor_n, pm, pn);
+        const double ac = wc * fd.ift * krq, an = wn * fd.ift * krn;
+        const double dPp = fd.dP[1 + ph];
+        // intra-continuum diffusion: the coefficient of the upstream (richer) cell
+        const bool dn_up = wn > wc;
+        const double Dup = idiff ? (dn_up ? nb.D(i, ph) : q.D(i, ph)) : 0.0;
         const double DX = wn - wc;
-        const double dMM = q.dE(k, ph) * e.dl * dC / BBd, dMM2 = nb.dE(k, ph) * e.dn * coef / BBd;
-        if (!total && coef != 0 && dC != 0) {
-            dR += s * NNd * ((diag ? -MMd * Dup : 0.0) + dDdx * MMd * DX + dMM * Dup * DX);
-            dB += s * NNd * ((diag ? MMd * Dup : 0.0) + dDdx2 * MMd * DX + dMM2 * Dup * DX);
-        }
-        if (ph == 0) {
-            dRxl += dR;
-            out.add(e.slot, row, k, -dB * coef);
-        } else {
-            dRxg += dR;
-            out.add(e.slot, row, (lnb ? -N : 0) + k + N, -dB * coef);
+        DDer dd;
+        dd.zero = true;
+        if (idiff) dd = make_dder(dn_up ? nb : q, i, ph);
+        // this phase's column of the neighbour (a one-phase neighbour has one composition set)
+        const bool to_x = ph == 0 ? lnb != -1 : lnb == 1;
+        for (int k = 0; k < N; k++) {
+            const bool diag = !total && k == i;
+            PhFace P = base;
+            if (diag && coef_d != coef_nd) P = ph_face(sq, sn, e, coef_d, dC, Sq, Sn, tor_c, tor_n, pm, pn);
+            const double coef = P.coef;
+            const double dEq = q.dE(k, ph), dEn = nb.dE(k, ph);
+            const double mwk = v.mw[k];
+            const double M = (dEq * e.dl * P.Mak - dmu(q, k, ph) * e.dl * P.Sur) * P.iMak2;
+            const double B = (dEn * e.dn * coef * P.Mak - dmu(nb, k, ph) * e.dn * coef * P.Sur) * P.iMak2;
+            const double MG = e.dl * (kGAccG * sq.rho * mwk + P.gq * dEq) * P.iden;
+            const double BG = coef * e.dn * (kGAccG * sn.rho * mwk + P.gn * dEn) * P.iden;
+            const double gM = M * P.tempdx + MG * P.SurMak, gB = B * P.tempdx + BG * P.SurMak;
+            const double Tp = diag ? fd.T[ph] : 0.0, Tg = diag ? fd.T[2 + ph] : 0.0;
+            double dR = 0, dB;
+            if (up_nb) {
+                dR += s * (an * M * dPp);
+                dB = s * ((Tp + an * B) * dPp);
+            } else {
+                dR += s * ((Tp + ac * M) * dPp);
+                dB = s * (ac * B * dPp);
+            }
+            // gravity (nonzero across z faces only)
+            if (e.sgn > 0) {
+                if (up_nb) {
+                    const double ift_r = (diag && ph == 0 && qk.ift_y_in_diag_grav) ? ift_y : fd.ift;
+                    dR += wn * ift_r * krn * gM * fd.dH;
+                    dB += (Tg + an * gB) * fd.dH;
+                } else {
+                    dR += (Tg + ac * gM) * fd.dH;
+                    dB += ac * gB * fd.dH;
+                }
+            } else {
+                // - faces: the gas terms exchange the two cells' factors; with k != i
+                // the oil terms of a downstream cell change sign
+                const double g1 = ph == 1 ? gB : gM, g2 = ph == 1 ? gM : gB;
+                if (!up_nb) {
+                    dR -= (Tg + ac * g1) * fd.dH;
+                    dB -= ac * g2 * fd.dH;
+                } else {
+                    const double flip = (!diag && !total && ph == 0) ? -1.0 : 1.0;
+                    dR -= flip * (an * g1 * fd.dH);
+                    dB -= flip * ((Tg + an * g2) * fd.dH);
+                }
+            }
+            if (idiff && coef != 0 && dC != 0) {
+                const double dDx = dd_k(v, dd, i, k, dn_up ? dEn : dEq);
+                const double dDdx = dn_up ? 0.0 : dDx, dDdx2 = dn_up ? dDx : 0.0;
+                const double dMM = dEq * e.dl * dC * P.iBB, dMM2 = dEn * e.dn * coef * P.iBB;
+                dR += s * NNd * ((diag ? -P.MMd * Dup : 0.0) + dDdx * P.MMd * DX + dMM * Dup * DX);
+                dB += s * NNd * ((diag ? P.MMd * Dup : 0.0) + dDdx2 * P.MMd * DX + dMM2 * Dup * DX);
+            }
+            const double nv = -dB * coef;
+            if (ph == 0) {
+                acc.x(k) += dR;
+                if (lnb == 0) out.st(L.cr(row, e.slot, k), nv);
+                else acc.z(k) = nv;
+            } else {
+                acc.y(k) += dR;
+                if (lnb == 0) {
+                    out.st(L.cr(row, e.slot, N + k), nv);
+                } else {
+                    // both phases land in the neighbour's one composition column
+                    const double w = acc.z(k) + nv;
+                    out.st(L.cr(row, e.slot, k), to_x ? w : 0.0);
+                    out.st(L.cr(row, e.slot, N + k), to_x ? 0.0 : w);
+                }
+            }
         }
     }
+}
+
+// The face part of a component (total: the total) row: the advective terms of
+// this cell's pressure, then every face's neighbour block.  Slots of absent
+// faces are stored as zeros; the total row's shifted entries go to ov[8]
+// (-y face 0..3, -z face 4..7).
+OSR_HD inline void row_faces(const JacView &v, const Cell &q, int i, bool fracture, bool total, Acc &acc,
+                             const Out &out, int row, double *ov) {
+    const int N = v.nc;
+    const Layout L(N);
+    JFace fc[6];
+    const int nf = jac_faces(v, q.c, fc);
+    unsigned present = 0;
+    for (int f = 0; f < nf; f++) present |= 1u << fc[f].slot;
+    // advective flux, this cell's pressure
+    for (int ph = 0; ph < 2; ph++)
+        for (int f = 0; f < nf; f++) {
+            const FaceData fd = face_data(v, *q.F, q.c, fc[f]);
+            const double T = fd.T[ph];
+            acc.dp += total ? T : Cell{&v, q.F, upstream(fc[f], fd, q.c, ph), q.med}.w(ph, i) * T;
+        }
+    for (int f = 0; f < nf; f++) {
+        const JFace &e = fc[f];
+        const Cell nb{&v, q.F, e.nb, q.med};
+        const FaceData fd = face_data(v, *q.F, q.c, e);
+        const FaceQuirks qps = total ? total_quirks(e) : comp_quirks(e);
+        double ps[4] = {0, 0, 0, 0};
+        double *o = ov ? ov + (e.d == 1 ? 0 : 4) : nullptr;
+        face_ps(v, q, nb, i, e, fd, qps, fracture, total, acc, ps, o);
+        for (int t = 0; t < 4; t++) out.st(L.cr(row, e.slot, 2 * N + t), ps[t]);
+        const FaceQuirks qx = total ? FaceQuirks{false, false, false, false, false, false} : comp_quirks(e);
+        face_x(v, q, nb, i, e, fd, qx, fracture, total, acc, out, row);
+    }
+    for (int s = 1; s <= 6; s++)
+        if (!(present & (1u << s)))
+            for (int c = 0; c < L.BS; c++) out.st(L.cr(row, s, c), 0.0);
 }
 
 // Well rates of a completion cell at the linearisation point (written by the
@@ -599,25 +861,56 @@ OSR_HD inline WellAt well_at(const JacView &v, int med, long c, int i, double ow
     WellAt w{0, 0, 0, 0, 0, 0, own_y, -1};
     if (!v.well_q) return w;
     const long b = med ? v.n + c : c;
-    w.Qw = v.well_q[3 * b];
-    w.Qo = v.well_q[3 * b + 1];
-    w.Qg = v.well_q[3 * b + 2];
-    w.PIw = v.well_pi[3 * b];
-    w.PIo = v.well_pi[3 * b + 1];
-    w.PIg = v.well_pi[3 * b + 2];
-    w.iwell = v.well_comp[b];
-    if (w.iwell >= 0) w.gcomp = v.stream_y[w.iwell * kMaxNc + i];
+    w.Qw = ld(v.well_q + 3 * b);
+    w.Qo = ld(v.well_q + 3 * b + 1);
+    w.Qg = ld(v.well_q + 3 * b + 2);
+    w.PIw = ld(v.well_pi + 3 * b);
+    w.PIo = ld(v.well_pi + 3 * b + 1);
+    w.PIg = ld(v.well_pi + 3 * b + 2);
+    w.iwell = ld(v.well_comp + b);
+    if (w.iwell >= 0) w.gcomp = ld(v.stream_y + w.iwell * kMaxNc + i);
     return w;
 }
 
-// Component balance row i (0 <= i < N-1) of a two-phase matrix cell.
-OSR_HD inline void matrix_comp_row_2ph(const JacView &v, long c, int i, const BlockRow &out, int row) {
+// This cell's P and saturation entries of a component or total row; unused
+// columns of a one-phase cell are stored as zeros.
+OSR_HD inline void store_own_ps(int N, const Out &out, int row, int lab, double P, double Sw, double So, double Sg) {
+    const Layout L(N);
+    const OwnLayout O = own_layout(lab);
+    out.st(L.cr(row, 0, 2 * N), P);
+    out.st(L.cr(row, 0, 2 * N + 1), O.swso ? Sw : 0.0);
+    out.st(L.cr(row, 0, 2 * N + 2), O.swso ? So : 0.0);
+    out.st(L.cr(row, 0, 2 * N + 3), O.sg ? Sg : 0.0);
+}
+
+// The other continuum's block of a component or total row (slot 7): P, Sw,
+// the saturation(s) and compositions its phase state carries.
+OSR_HD inline void store_other_ps(int N, const Out &out, int row, int lo, double P, double Sw, double So, double Sg) {
+    const Layout L(N);
+    out.st(L.cr(row, 7, 2 * N), P);
+    out.st(L.cr(row, 7, 2 * N + 1), Sw);
+    out.st(L.cr(row, 7, 2 * N + 2), lo == -1 ? 0.0 : So);
+    out.st(L.cr(row, 7, 2 * N + 3), lo == 1 ? 0.0 : Sg);
+}
+
+OSR_HD inline void store_other_x(int N, const Out &out, int row, int lo, int k, double xl, double xg) {
+    const Layout L(N);
+    out.st(L.cr(row, 7, k), lo == -1 ? 0.0 : xl);
+    out.st(L.cr(row, 7, N + k), lo == 1 ? 0.0 : xg);
+}
+
+// ---------------------------------------------------------------------------
+// Component balance row i (0 <= i < N-1) of a matrix cell.
+// ---------------------------------------------------------------------------
+OSR_HD inline void matrix_comp_row(const JacView &v, long c, int i, const Out &out, Acc &a) {
     const int N = v.nc;
-    const Cell M{&v, &v.m[0], c}, Fr{&v, &v.m[1], c};
+    const Layout L(N);
+    const int row = N + i;
+    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
     const Transfer t = transfer_terms(v, c);
     const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
     const double Vb = t.Vb, SF1 = t.SF1, SF2 = t.SF2;
-    const double tor = v.tor[c];
+    const double tor = ld(v.tor + c);
     const int lm = M.label(), lf = Fr.label();
     const double xi = M.w(0, i), yi = M.w(1, i);
     const double ro = M.rho(0), rg = M.rho(1);
@@ -625,22 +918,23 @@ OSR_HD inline void matrix_comp_row_2ph(const JacView &v, long c, int i, const Bl
     const double dLdp = (Vb / v.dt) * (xi * M.S(1) * (ro * dpm + M.dE(N, 0) * pm) + yi * M.S(2) * (rg * dpm + M.dE(N, 1) * pm));
     const double dLdSo = (Vb / v.dt) * (xi * pm * ro), dLdSg = (Vb / v.dt) * (yi * pm * rg);
     double dRfdp = 0;
-    OwnPS a{0, 0, 0, 0};
+    a.dp = a.dSw = a.dSo = a.dSg = 0;
     // transfer, this cell's pressure
     a.dp += kSIC * M.dE(N, 0) * xi * SF2 * Vb * t.kro / mubar_o * t.dPo;
     a.dp += -kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    a.dp += -kSIC * (visc_deriv(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+    a.dp += -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
     a.dp += kSIC * dpm * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
     a.dp += kSIC * M.dE(N, 1) * yi * SF2 * Vb * t.krg / mubar_g * t.dPg;
     a.dp += -kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    a.dp += -kSIC * (visc_deriv(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+    a.dp += -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
     a.dp += kSIC * dpm * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
     // diffusive transfer, this cell's pressure
     for (int ph = 0; ph < 2; ph++) {
         int kinds[2];
         const int nt = matrix_diff_targets(lm, lf, ph, kinds);
+        if (!nt) continue;
         const double sat = M.S(1 + ph), rho = M.rho(ph), D = M.D(i, ph), w = M.w(ph, i);
-        const double dDdp = diff_deriv(M, i, N, ph);
+        const double dDdp = dD(M, i, N, ph);
         for (int j = 0; j < nt; j++) {
             const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
             a.dp += dpm * SF1 * sat * Vb / tor * rho * D * (tgt - w);
@@ -650,20 +944,11 @@ OSR_HD inline void matrix_comp_row_2ph(const JacView &v, long c, int i, const Bl
     }
     // transfer, the fracture's pressure
     dRfdp += kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    dRfdp += -kSIC * (visc_deriv(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+    dRfdp += -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
     dRfdp += kSIC * dpf * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
     dRfdp += kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    dRfdp += -kSIC * (visc_deriv(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+    dRfdp += -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
     dRfdp += kSIC * dpf * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    // advective flux, this cell's pressure
-    JFace fc[6];
-    const int nf = jac_faces(v, c, fc);
-    for (int ph = 0; ph < 2; ph++)
-        for (int q = 0; q < nf; q++) {
-            const FaceData fd = face_data(v, v.m[0], c, fc[q]);
-            const Cell U{&v, &v.m[0], upstream(fc[q], fd, c, ph)};
-            a.dp += U.w(ph, i) * fd.T[ph];
-        }
     // saturations (transfer and diffusive transfer)
     double dRfdSw = 0, dRfdSo = 0, dRfdSg = 0;
     const double po = xi * ro * SF2 * Vb / mubar_o * t.dPo, pg = yi * rg * SF2 * Vb / mubar_g * t.dPg;
@@ -693,319 +978,81 @@ OSR_HD inline void matrix_comp_row_2ph(const JacView &v, long c, int i, const Bl
     dRfdSg += kSIC * t.dkf[3] * pg;
     a.dSw += kSIC * t.dkm[1] * po;
     dRfdSw += kSIC * t.dkf[1] * po;
-    // faces: neighbour pressures and saturations
-    for (int q = 0; q < nf; q++) comp_face_ps(v, M, i, fc[q], matrix_comp_quirks(fc[q]), out, row, a, false);
-    // this cell's pressure and saturations (with the completion's productivity terms)
-    const WellAt W = well_at(v, 0, c, i, yi);
-    const OwnLayout L = own_layout(N, lm);
-    out.add(0, row, L.P, v.pcoeff * (dLdp + a.dp + xi * W.PIo + W.gcomp * W.PIg));
-    if (L.swso) {
-        out.add(0, row, L.Sw, -a.dSw);
-        out.add(0, row, L.So, dLdSo - a.dSo);
+    // compositions: transfer terms and the fracture's block; the factors that
+    // do not depend on k first
+    double cdg[2], cx1[2], cx2[2], cf2[2], cd1[2], cdd[2], cd2[2], cfd[2];
+    bool dtr[2];
+    for (int ph = 0; ph < 2; ph++) {
+        const double w = ph ? yi : xi, rho = ph ? rg : ro, kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
+        const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
+        cdg[ph] = kSIC * rho * SF2 * Vb * kr / mub * dPp;
+        cx1[ph] = kSIC * w * SF2 * Vb * kr / mub * dPp;
+        cx2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pm + pf);
+        cf2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pm + pf);
+        cd1[ph] = cdd[ph] = cd2[ph] = cfd[ph] = 0;
+        int kinds[2];
+        const int nt = v.diff_off ? 0 : matrix_diff_targets(lm, lf, ph, kinds);
+        dtr[ph] = nt > 0;
+        const double sat = M.S(1 + ph), D = M.D(i, ph);
+        for (int j = 0; j < nt; j++) {
+            const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
+            cd1[ph] += SF1 * sat * pm * Vb / tor * D * (tgt - w);
+            cdd[ph] += -SF1 * sat * pm * Vb / tor * rho * D;
+            cd2[ph] += SF1 * sat * pm * Vb / tor * rho * (tgt - w);
+        }
+        // towards the fracture composition of the same phase (k == i)
+        bool on = (lm == 0 && lf == 0);
+        if (ph == 0) on = on || (lm == 1 && lf == 1) || (lm == 0 && lf == 1) || (lm == 1 && lf == 0);
+        else on = on || (lm == -1 && lf == -1) || (lm == 0 && lf == -1) || (lm == -1 && lf == 0);
+        if (on && !v.diff_off) cfd[ph] = SF1 * sat * pm * Vb / tor * rho * D;
     }
-    if (L.sg) out.add(0, row, L.Sg, dLdSg - a.dSg);
-    // the fracture's pressure and saturations
-    const int rf = lf ? N : 0;
-    if (lf == 1) out.add(7, row, 2 * N + 2 - rf, dRfdSo);
-    else if (lf == -1) out.add(7, row, 2 * N + 2 - rf, dRfdSg);
-    else {
-        out.add(7, row, 2 * N + 2, dRfdSo);
-        out.add(7, row, 2 * N + 3, dRfdSg);
-    }
-    out.add(7, row, 2 * N - rf, v.pcoeff * dRfdp);
-    out.add(7, row, 2 * N + 1 - rf, dRfdSw);
-    // compositions
     for (int k = 0; k < N; k++) {
-        double dRxl = 0, dRxg = 0, dRfxl = 0, dRfxg = 0;
+        double dRx[2], dRfx[2];
         const bool diag = k == i;
         for (int ph = 0; ph < 2; ph++) {
-            const double w = M.w(ph, i), rho = M.rho(ph), kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
-            const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
-            double &dR = ph ? dRxg : dRxl;
-            double &dRf = ph ? dRfxg : dRfxl;
-            if (diag) dR += kSIC * rho * SF2 * Vb * kr / mub * dPp;
-            dR += kSIC * M.dE(k, ph) * w * SF2 * Vb * kr / mub * dPp;
-            dR += -kSIC * visc_deriv(M, k, ph) * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pm + pf);
-            int kinds[2];
-            const int nt = matrix_diff_targets(lm, lf, ph, kinds);
-            const double sat = M.S(1 + ph), D = M.D(i, ph), dDdx = diff_deriv(M, i, k, ph);
-            for (int j = 0; j < nt; j++) {
-                const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
-                dR += M.dE(k, ph) * SF1 * sat * pm * Vb / tor * D * (tgt - w);
-                if (diag) dR += -SF1 * sat * pm * Vb / tor * rho * D;
-                dR += dDdx * SF1 * sat * pm * Vb / tor * rho * (tgt - w);
-            }
-            dRf += -kSIC * visc_deriv(Fr, k, ph) * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pm + pf);
-            if (diag) {
-                // towards the fracture composition of the same phase
-                bool on = (lm == 0 && lf == 0);
-                if (ph == 0) on = on || (lm == 1 && lf == 1) || (lm == 0 && lf == 1) || (lm == 1 && lf == 0);
-                else on = on || (lm == -1 && lf == -1) || (lm == 0 && lf == -1) || (lm == -1 && lf == 0);
-                if (on) dRf += SF1 * sat * pm * Vb / tor * rho * D;
-            }
+            const double dEk = M.dE(k, ph);
+            double dR = (diag ? cdg[ph] : 0.0) + dEk * cx1[ph] + dmu(M, k, ph) * cx2[ph];
+            if (dtr[ph]) dR += dEk * cd1[ph] + (diag ? cdd[ph] : 0.0) + dD(M, i, k, ph) * cd2[ph];
+            dRx[ph] = dR;
+            dRfx[ph] = dmu(Fr, k, ph) * cf2[ph] + (diag ? cfd[ph] : 0.0);
         }
+        a.x(k) = dRx[0];
+        a.y(k) = dRx[1];
+        store_other_x(N, out, row, lf, k, dRfx[0], dRfx[1]);
+    }
+    // faces
+    row_faces(v, M, i, false, false, a, out, row, nullptr);
+    // this cell's block (with the completion's productivity terms)
+    const WellAt W = well_at(v, 0, c, i, yi);
+    store_own_ps(N, out, row, lm, v.pcoeff * (dLdp + a.dp + xi * W.PIo + W.gcomp * W.PIg), -a.dSw, dLdSo - a.dSo,
+                 dLdSg - a.dSg);
+    const OwnLayout O = own_layout(lm);
+    const double aol = (Vb / v.dt) * pm * M.S(1), aog = (Vb / v.dt) * pm * M.S(2);
+    for (int k = 0; k < N; k++) {
+        const bool diag = k == i;
         const double dLxl = diag ? ro + xi * M.dE(k, 0) : xi * M.dE(k, 0);
         const double dLxg = diag ? rg + yi * M.dE(k, 1) : yi * M.dE(k, 1);
         const double dQxl = (diag && W.iwell < 0) ? W.Qo : 0.0, dQxg = (diag && W.iwell < 0) ? W.Qg : 0.0;
-        for (int q = 0; q < nf; q++) comp_face_x(v, M, i, k, fc[q], matrix_comp_quirks(fc[q]), out, row, dRxl, dRxg, false);
-        if (lf == 1) out.add(7, row, k, dRfxl);
-        else if (lf == -1) out.add(7, row, k, dRfxg);
-        else {
-            out.add(7, row, k, dRfxl);
-            out.add(7, row, N + k, dRfxg);
-        }
-        if (L.x) out.add(0, row, L.X + k, (Vb / v.dt) * pm * M.S(1) * dLxl - dQxl - dRxl);
-        if (L.y) out.add(0, row, L.Y + k, (Vb / v.dt) * pm * M.S(2) * dLxg - dQxg - dRxg);
+        out.st(L.cr(row, 0, k), O.x ? aol * dLxl - dQxl - a.x(k) : 0.0);
+        out.st(L.cr(row, 0, N + k), O.y ? aog * dLxg - dQxg - a.y(k) : 0.0);
     }
+    // the fracture's block
+    store_other_ps(N, out, row, lf, v.pcoeff * dRfdp, dRfdSw, dRfdSo, dRfdSg);
 }
 
-// Fugacity rows of a two-phase cell (compsim/Petsc_Functions.cpp:30240-30406
-// for the matrix): x_i P_o phi_i^L - y_i P_g phi_i^V with Z from the stored
-// density and dZ from dE.
-OSR_HD inline void fugacity_rows(const JacView &v, const Cell &q, const BlockRow &out) {
-    const int N = v.nc;
-    const double RT = kR * v.T;
-    const double Pl = q.P(1), Pg = q.P(2);
-    double Al = 0, Bl = 0, Ag = 0, Bg = 0;
-    for (int i = 0; i < N; i++) {
-        Bl += q.w(0, i) * v.b[i];
-        Bg += q.w(1, i) * v.b[i];
-        for (int j = 0; j < N; j++) {
-            const double t = v.sa[i] * v.sa[j] * v.bic[i * N + j];
-            Al += q.w(0, i) * q.w(0, j) * t;
-            Ag += q.w(1, i) * q.w(1, j) * t;
-        }
-    }
-    const double Cal = Al, Cbl = Bl, Cag = Ag, Cbg = Bg;
-    Al *= Pl / (RT * RT);
-    Bl *= Pl / RT;
-    Ag *= Pg / (RT * RT);
-    Bg *= Pg / RT;
-    const double dAdpl = Cal / (RT * RT), dAdpg = Cag / (RT * RT), dBdpl = Cbl / RT, dBdpg = Cbg / RT;
-    const double Zl = Pl / (q.rho(0) * RT), Zg = Pg / (q.rho(1) * RT);
-    const double dZdpl = (1 - q.dE(N, 0) * RT * Zl) * (Zl / Pl), dZdpg = (1 - q.dE(N, 1) * RT * Zg) * (Zg / Pg);
-    const double d1 = v.srk ? 1.0 : 1 + kSqrt2, d2 = v.srk ? 0.0 : 1 - kSqrt2;
-    for (int i = 0; i < N; i++) {
-        double tl = 0, tg = 0;
-        for (int j = 0; j < N; j++) {
-            const double t = v.sa[i] * v.sa[j] * v.bic[i * N + j];
-            tl += q.w(0, j) * t;
-            tg += q.w(1, j) * t;
-        }
-        const double t1l = v.b[i] / Cbl, t1g = v.b[i] / Cbg;
-        const double EEl = 2 * tl / Cal - t1l, EEg = 2 * tg / Cag - t1g;
-        const double DDl = Al / (Bl * (d1 - d2)), DDg = Ag / (Bg * (d1 - d2));
-        const double FFl = log((Zl + d2 * Bl) / (Zl + d1 * Bl)), FFg = log((Zg + d2 * Bg) / (Zg + d1 * Bg));
-        const double phiL = exp(t1l * (Zl - 1) - log(Zl - Bl) + DDl * EEl * FFl);
-        const double phiG = exp(t1g * (Zg - 1) - log(Zg - Bg) + DDg * EEg * FFg);
-        const double dAAl = v.b[i] * dZdpl / Cbl, dAAg = v.b[i] * dZdpg / Cbg;
-        const double dBBl = (dBdpl - dZdpl) / (Zl - Bl), dBBg = (dBdpg - dZdpg) / (Zg - Bg);
-        const double dDDl = (Bl * dAdpl - Al * dBdpl) / (Bl * Bl * (d1 - d2)), dDDg = (Bg * dAdpg - Ag * dBdpg) / (Bg * Bg * (d1 - d2));
-        const double dFFl = (dZdpl + d2 * dBdpl) / (Zl + d2 * Bl) - (dZdpl + d1 * dBdpl) / (Zl + d1 * Bl);
-        const double dFFg = (dZdpg + d2 * dBdpg) / (Zg + d2 * Bg) - (dZdpg + d1 * dBdpg) / (Zg + d1 * Bg);
-        const double dPhil = phiL * (dAAl + dBBl + EEl * (dDDl * FFl + DDl * dFFl));
-        const double dPhig = phiG * (dAAg + dBBg + EEg * (dDDg * FFg + DDg * dFFg));
-        const double xi = q.w(0, i), yi = q.w(1, i);
-        out.add(0, i, 2 * N, v.pcoeff * (xi * (phiL + Pl * dPhil) - yi * (phiG + Pg * dPhig)));
-        for (int k = 0; k < N; k++) {
-            double dAl = 0, dAg = 0;
-            for (int n = 0; n < N; n++) {
-                const double t = v.sa[k] * v.sa[n] * v.bic[k * N + n];
-                dAl += q.w(0, n) * t;
-                dAg += q.w(1, n) * t;
-            }
-            dAl *= 2 * Pl / (RT * RT);
-            dAg *= 2 * Pg / (RT * RT);
-            const double dBl = v.b[k] * Pl / RT, dBg = v.b[k] * Pg / RT;
-            const double dZl = -q.dE(k, 0) * RT * Zl * Zl / Pl, dZg = -q.dE(k, 1) * RT * Zg * Zg / Pg;
-            const double dAAxl = -v.b[k] * v.b[i] * (Zl - 1) / (Cbl * Cbl) + v.b[i] * dZl / Cbl;
-            const double dAAxg = -v.b[k] * v.b[i] * (Zg - 1) / (Cbg * Cbg) + v.b[i] * dZg / Cbg;
-            const double dBBxl = (dBl - dZl) / (Zl - Bl), dBBxg = (dBg - dZg) / (Zg - Bg);
-            const double dDDxl = (dAl * Bl - dBl * Al) / (Bl * Bl * (d1 - d2)), dDDxg = (dAg * Bg - dBg * Ag) / (Bg * Bg * (d1 - d2));
-            const double dFFxl = (dZl + d2 * dBl) / (Zl + d2 * Bl) - (dZl + d1 * dBl) / (Zl + d1 * Bl);
-            const double dFFxg = (dZg + d2 * dBg) / (Zg + d2 * Bg) - (dZg + d1 * dBg) / (Zg + d1 * Bg);
-            const double tik = v.sa[i] * v.sa[k] * v.bic[i * N + k];
-            const double dEEl = 2 * (tik / Cal - dAl * RT * RT * tl / (Pl * Cal * Cal)) + v.b[i] * v.b[k] / (Cbl * Cbl);
-            const double dEEg = 2 * (tik / Cag - dAg * RT * RT * tg / (Pg * Cag * Cag)) + v.b[i] * v.b[k] / (Cbg * Cbg);
-            const double dPxl = phiL * (dAAxl + dBBxl + dDDxl * EEl * FFl + DDl * dEEl * FFl + DDl * EEl * dFFxl);
-            const double dPxg = phiG * (dAAxg + dBBxg + dDDxg * EEg * FFg + DDg * dEEg * FFg + DDg * EEg * dFFxg);
-            if (i == k) {
-                out.add(0, i, k, Pl * phiL + Pl * xi * dPxl);
-                out.add(0, i, N + k, -(Pg * phiG + Pg * yi * dPxg));
-            } else {
-                out.add(0, i, k, Pl * xi * dPxl);
-                out.add(0, i, N + k, -Pg * yi * dPxg);
-            }
-        }
-    }
-}
-
-// Rows sum x - 1, sum y - 1, sum S - 1 of a two-phase cell.
-OSR_HD inline void constraint_rows_2ph(const JacView &v, const BlockRow &out) {
-    const int N = v.nc;
-    for (int k = 0; k < N; k++) {
-        out.add(0, 2 * N + 1, k, 1.0);
-        out.add(0, 2 * N + 2, N + k, 1.0);
-    }
-    for (int j = 0; j < 3; j++) out.add(0, 2 * N + 3, 2 * N + 1 + j, 1.0);
-}
-
-
-// Total hydrocarbon row (2N-1) of a two-phase cell.  The matrix-fracture
-// transfer derivatives are formed from the matrix side; a fracture row takes
-// them negated with the roles of the two continua exchanged.
-OSR_HD inline void total_row_2ph(const JacView &v, int med, long c, const BlockRow &out, int row) {
-    const int N = v.nc;
-    const Cell M{&v, &v.m[0], c}, Fr{&v, &v.m[1], c};
-    const Cell &O = med ? Fr : M;          // this row's continuum
-    const Transfer t = transfer_terms(v, c);
-    const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
-    const double Vb = t.Vb, SF2 = t.SF2;
-    const double po_ = med ? pf : pm, dpo_ = med ? dpf : dpm;
-    const int lo = (med ? M : Fr).label();   // the other continuum's label
-    const double ro = M.rho(0), rg = M.rho(1);
-    const double mubar_o = t.Do / (pm + pf), mubar_g = t.Dg / (pm + pf);
-    const double dLdp = (Vb / v.dt) * (O.S(1) * (O.rho(0) * dpo_ + O.dE(N, 0) * po_) + O.S(2) * (O.rho(1) * dpo_ + O.dE(N, 1) * po_));
-    const double dLdSo = (Vb / v.dt) * (po_ * O.rho(0)), dLdSg = (Vb / v.dt) * (po_ * O.rho(1));
-    // matrix-side derivatives of the (matrix-row) transfer terms
-    double tm = 0, tf = 0;
-    tm += kSIC * M.dE(N, 0) * SF2 * Vb * t.kro / mubar_o * t.dPo;
-    tm += -kSIC * ro * SF2 * Vb * t.kro / mubar_o;
-    tm += -kSIC * (visc_deriv(M, N, 0) * pm + dpm * M.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
-    tm += kSIC * dpm * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    tm += kSIC * M.dE(N, 1) * SF2 * Vb * t.krg / mubar_g * t.dPg;
-    tm += -kSIC * rg * SF2 * Vb * t.krg / mubar_g;
-    tm += -kSIC * (visc_deriv(M, N, 1) * pm + dpm * M.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    tm += kSIC * dpm * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    tf += kSIC * ro * SF2 * Vb * t.kro / mubar_o;
-    tf += -kSIC * (visc_deriv(Fr, N, 0) * pf + dpf * Fr.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
-    tf += kSIC * dpf * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    tf += kSIC * rg * SF2 * Vb * t.krg / mubar_g;
-    tf += -kSIC * (visc_deriv(Fr, N, 1) * pf + dpf * Fr.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    tf += kSIC * dpf * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    const double sg = med ? -1.0 : 1.0;
-    OwnPS a{0, 0, 0, 0};
-    a.dp += sg * (med ? tf : tm);
-    const double dROdp = sg * (med ? tm : tf);   // the other continuum's pressure
-    JFace fc[6];
-    const int nf = jac_faces(v, c, fc);
-    for (int ph = 0; ph < 2; ph++)
-        for (int q = 0; q < nf; q++) a.dp += face_data(v, v.m[med], c, fc[q]).T[ph];
-    const double po = ro * SF2 * Vb / mubar_o * t.dPo, pg = rg * SF2 * Vb / mubar_g * t.dPg;
-    const double smSo = kSIC * t.dkm[4] * po, sfSo = kSIC * t.dkf[4] * po;
-    const double smSg = kSIC * t.dkm[2] * po + kSIC * t.dkm[3] * pg, sfSg = kSIC * t.dkf[2] * po + kSIC * t.dkf[3] * pg;
-    const double smSw = kSIC * t.dkm[1] * po, sfSw = kSIC * t.dkf[1] * po;
-    a.dSo += sg * (med ? sfSo : smSo);
-    a.dSg += sg * (med ? sfSg : smSg);
-    a.dSw += sg * (med ? sfSw : smSw);
-    const double dROSo = sg * (med ? smSo : sfSo), dROSg = sg * (med ? smSg : sfSg), dROSw = sg * (med ? smSw : sfSw);
-    for (int q = 0; q < nf; q++) comp_face_ps(v, O, 0, fc[q], matrix_total_quirks(fc[q]), out, row, a, med == 1, true);
-    const WellAt W = well_at(v, med, c, 0, 0.0);
-    const OwnLayout L = own_layout(N, O.label());
-    out.add(0, row, L.P, v.pcoeff * (dLdp + a.dp + W.PIo + W.PIg));
-    if (L.swso) {
-        out.add(0, row, L.Sw, -a.dSw);
-        out.add(0, row, L.So, dLdSo - a.dSo);
-    }
-    if (L.sg) out.add(0, row, L.Sg, dLdSg - a.dSg);
-    const int rf = lo ? N : 0;
-    if (lo == 1) out.add(7, row, 2 * N + 2 - rf, dROSo);
-    else if (lo == -1) out.add(7, row, 2 * N + 2 - rf, dROSg);
-    else {
-        out.add(7, row, 2 * N + 2, dROSo);
-        out.add(7, row, 2 * N + 3, dROSg);
-    }
-    out.add(7, row, 2 * N - rf, v.pcoeff * dROdp);
-    out.add(7, row, 2 * N + 1 - rf, dROSw);
-    for (int k = 0; k < N; k++) {
-        double xm = 0, ym = 0;
-        xm += kSIC * M.dE(k, 0) * SF2 * Vb * t.kro / mubar_o * t.dPo;
-        xm += -kSIC * visc_deriv(M, k, 0) * ro * SF2 * Vb * t.kro * pm / (t.Do * t.Do) * t.dPo * (pm + pf);
-        const double xf = -kSIC * visc_deriv(Fr, k, 0) * ro * SF2 * Vb * t.kro * pf / (t.Do * t.Do) * t.dPo * (pm + pf);
-        ym += kSIC * M.dE(k, 1) * SF2 * Vb * t.krg / mubar_g * t.dPg;
-        ym += -kSIC * visc_deriv(M, k, 1) * rg * SF2 * Vb * t.krg * pm / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-        const double yf = -kSIC * visc_deriv(Fr, k, 1) * rg * SF2 * Vb * t.krg * pf / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-        double dRxl = sg * (med ? xf : xm), dRxg = sg * (med ? yf : ym);
-        const double dROxl = sg * (med ? xm : xf), dROxg = sg * (med ? ym : yf);
-        const FaceQuirks none{false, false, false, false, false, false, false};
-        for (int q = 0; q < nf; q++) comp_face_x(v, O, 0, k, fc[q], none, out, row, dRxl, dRxg, med == 1, true);
-        if (L.x) out.add(0, row, L.X + k, (Vb / v.dt) * po_ * O.S(1) * O.dE(k, 0) - dRxl);
-        if (L.y) out.add(0, row, L.Y + k, (Vb / v.dt) * po_ * O.S(2) * O.dE(k, 1) - dRxg);
-        if (lo == 1) out.add(7, row, k, dROxl);
-        else if (lo == -1) out.add(7, row, k, dROxg);
-        else {
-            out.add(7, row, k, dROxl);
-            out.add(7, row, N + k, dROxg);
-        }
-    }
-}
-
-// Water row (2N) of a two-phase cell.
-OSR_HD inline void water_row_2ph(const JacView &v, int med, long c, const BlockRow &out, int row) {
-    const int N = v.nc;
-    const Cell M{&v, &v.m[0], c}, Fr{&v, &v.m[1], c};
-    const Cell &O = med ? Fr : M;
-    const JMed &F = v.m[med];
-    const Transfer t = transfer_terms(v, c);
-    const double wr = v.wat_ro * kWatMRo;
-    const double po_ = med ? t.pf : t.pm, dpo_ = med ? t.dpf : t.dpm;
-    const double sg = med ? -1.0 : 1.0;
-    const double dLdp = (t.Vb / v.dt) * wr * O.S(0) * dpo_;
-    const double dLdSw = (t.Vb / v.dt) * (po_ * wr);
-    const double tr = kSIC * v.wat_ro * kWatMRo * t.SF2 * t.krw / v.wat_mu * t.Vb;
-    // both continua's water rows take -tr for their own pressure, +tr for the other's
-    double dRdp = -tr;
-    const double dROdp = tr;
-    JFace fc[6];
-    const int nf = jac_faces(v, c, fc);
-    const long n = v.n;
-    for (int q = 0; q < nf; q++) dRdp += F.wtran[(long)fc[q].d * n + fc[q].tc];
-    const WellAt W = well_at(v, med, c, 0, 0.0);
-    const OwnLayout L = own_layout(N, O.label());
-    out.add(0, row, L.P, v.pcoeff * (dLdp + dRdp + W.PIw));
-    const double smw = kSIC * kWatMRo * t.dkm[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
-    const double sfw = kSIC * kWatMRo * t.dkf[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
-    double dRdSw = sg * (med ? sfw : smw);
-    const double dROSw = sg * (med ? smw : sfw);
-    for (int q = 0; q < nf; q++) {
-        const JFace &e = fc[q];
-        const FaceData fd = face_data(v, F, c, e);
-        const int lnb = F.label[e.nb];
-        const int nbase = lnb ? -N : 0;
-        const double Tw = F.wtran[(long)e.d * n + e.tc], dTw = F.dwtran[(long)e.d * n + e.tc];
-        out.add(e.slot, row, nbase + 2 * N, v.pcoeff * (-Tw));
-        const double dsw = e.sgn * (dTw * fd.dP[0] + kGAcc * v.wat_ro * dTw * fd.dH);
-        if (upstream(e, fd, c, 2) == e.nb) out.add(e.slot, row, nbase + 2 * N + 1, dsw);
-        else dRdSw += dsw;
-    }
-    out.add(0, row, L.P + 1, dLdSw - dRdSw);
-    const int rf = (med ? M : Fr).label() ? N : 0;
-    out.add(7, row, 2 * N - rf, v.pcoeff * dROdp);
-    out.add(7, row, 2 * N + 1 - rf, dROSw);
-}
-
-// Fracture-side diffusive transfer pairings.  fsf1: the matrix-side (SF1)
-// terms toward the fracture composition a fracture row carries for phase ph;
-// fsf3: the interface (SF3) terms of the fracture's own phase ph.
-OSR_HD inline bool fsf1(int lm, int lf, int ph) {
-    if (lm == 0 && lf == 0) return true;
-    if (ph == 0) return (lm == 1 && lf == 1) || (lm == 0 && lf == 1) || (lm == 1 && lf == 0);
-    return (lm == -1 && lf == -1) || (lm == 0 && lf == -1) || (lm == -1 && lf == 0);
-}
-OSR_HD inline bool fsf3(int lm, int lf, int ph) {
-    if (ph == 0) return (lm == -1 && lf == 1) || (lm == 0 && lf == 1) || (lm == -1 && lf == 0);
-    return (lm == 1 && lf == -1) || (lm == 0 && lf == -1) || (lm == 1 && lf == 0);
-}
-
-// Component balance row i of a two-phase fracture cell (the fracture case of
+// ---------------------------------------------------------------------------
+// Component balance row i of a fracture cell (the fracture case of
 // IteratorJacobian, compsim/Petsc_Functions.cpp:12756-18666).
-OSR_HD inline void fracture_comp_row_2ph(const JacView &v, long c, int i, const BlockRow &out, int row) {
+// ---------------------------------------------------------------------------
+OSR_HD inline void fracture_comp_row(const JacView &v, long c, int i, const Out &out, Acc &a) {
     const int N = v.nc;
-    const Cell M{&v, &v.m[0], c}, Fr{&v, &v.m[1], c};
+    const Layout L(N);
+    const int row = N + i;
+    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
     const Transfer t = transfer_terms(v, c);
     const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
     const double Vb = t.Vb, SF1 = t.SF1, SF2 = t.SF2, SF3 = t.SF3;
-    const double tor = v.tor[c];
+    const double tor = ld(v.tor + c);
     const int lm = M.label(), lf = Fr.label();
     const double xi = M.w(0, i), yi = M.w(1, i);         // matrix compositions (transfer terms)
     const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
@@ -1014,45 +1061,37 @@ OSR_HD inline void fracture_comp_row_2ph(const JacView &v, long c, int i, const 
     const double dLdp = (Vb / v.dt) * (fxi * Fr.S(1) * (Fr.rho(0) * dpf + Fr.dE(N, 0) * pf) + fyi * Fr.S(2) * (Fr.rho(1) * dpf + Fr.dE(N, 1) * pf));
     const double dLdSo = (Vb / v.dt) * (fxi * pf * Fr.rho(0)), dLdSg = (Vb / v.dt) * (fyi * pf * Fr.rho(1));
     double dRMdp = 0;
-    OwnPS a{0, 0, 0, 0};
+    a.dp = a.dSw = a.dSo = a.dSg = 0;
     // transfer, the matrix pressure
     dRMdp -= kSIC * M.dE(N, 0) * xi * SF2 * Vb * t.kro / mubar_o * t.dPo;
     dRMdp -= -kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    dRMdp -= -kSIC * (visc_deriv(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
+    dRMdp -= -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
     dRMdp -= kSIC * dpm * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
     dRMdp -= kSIC * M.dE(N, 1) * yi * SF2 * Vb * t.krg / mubar_g * t.dPg;
     dRMdp -= -kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    dRMdp -= -kSIC * (visc_deriv(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
+    dRMdp -= -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
     dRMdp -= kSIC * dpm * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
     for (int ph = 0; ph < 2; ph++) {
         if (!fsf1(lm, lf, ph)) continue;
         const double sat = M.S(1 + ph), rho = M.rho(ph), D = M.D(i, ph), dlt = Fr.w(ph, i) - M.w(ph, i);
         dRMdp -= dpm * SF1 * sat * Vb / tor * rho * D * dlt;
         dRMdp -= M.dE(N, ph) * SF1 * sat * pm * Vb / tor * D * dlt;
-        dRMdp -= diff_deriv(M, i, N, ph) * SF1 * sat * pm * Vb / tor * rho * dlt;
+        dRMdp -= dD(M, i, N, ph) * SF1 * sat * pm * Vb / tor * rho * dlt;
     }
     // transfer, this (fracture) cell's pressure
     a.dp -= kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    a.dp -= -kSIC * (visc_deriv(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
+    a.dp -= -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
     a.dp -= kSIC * dpf * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
     a.dp -= kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    a.dp -= -kSIC * (visc_deriv(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
+    a.dp -= -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
     a.dp -= kSIC * dpf * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
     for (int ph = 0; ph < 2; ph++) {
         if (!fsf3(lm, lf, ph)) continue;
         const double sat = Fr.S(1 + ph), rho = Fr.rho(ph), D = Fr.D(i, ph), w = Fr.w(ph, i);
         a.dp -= dpf * SF3 * sat * Vb / tor * rho * D * (w - 0.0);
         a.dp -= Fr.dE(N, ph) * SF3 * sat * pf * Vb / tor * D * (w - 0.0);
-        a.dp -= diff_deriv(Fr, i, N, ph) * SF3 * sat * pf * Vb / tor * rho * (w - 0.0);
+        a.dp -= dD(Fr, i, N, ph) * SF3 * sat * pf * Vb / tor * rho * (w - 0.0);
     }
-    JFace fc[6];
-    const int nf = jac_faces(v, c, fc);
-    for (int ph = 0; ph < 2; ph++)
-        for (int q = 0; q < nf; q++) {
-            const FaceData fd = face_data(v, v.m[1], c, fc[q]);
-            const Cell U{&v, &v.m[1], upstream(fc[q], fd, c, ph)};
-            a.dp += U.w(ph, i) * fd.T[ph];
-        }
     // saturations
     double dRMdSo = 0, dRMdSg = 0, dRMdSw = 0;
     const double po = xi * ro * SF2 * Vb / mubar_o * t.dPo, pg = yi * rg * SF2 * Vb / mubar_g * t.dPg;
@@ -1068,109 +1107,483 @@ OSR_HD inline void fracture_comp_row_2ph(const JacView &v, long c, int i, const 
     if (fsf3(lm, lf, 1)) a.dSg -= SF3 * Vb * pf / tor * Fr.rho(1) * Fr.D(i, 1) * (fyi - 0.0);
     dRMdSw -= kSIC * t.dkm[1] * po;
     a.dSw -= kSIC * t.dkf[1] * po;
-    for (int q = 0; q < nf; q++) comp_face_ps(v, Fr, i, fc[q], fracture_comp_quirks(fc[q]), out, row, a, true);
-    const WellAt W = well_at(v, 1, c, i, fyi);
-    const OwnLayout L = own_layout(N, lf);
-    out.add(0, row, L.P, v.pcoeff * (dLdp + a.dp + fxi * W.PIo + W.gcomp * W.PIg));
-    if (L.swso) {
-        out.add(0, row, L.Sw, -a.dSw);
-        out.add(0, row, L.So, dLdSo - a.dSo);
+    // compositions: transfer terms and the matrix's block; the factors that do
+    // not depend on k first (the matrix-side SF1 and the fracture's SF3 terms)
+    double cdg[2], cx1[2], cx2[2], cf2[2], m1[2], mdd[2], m2[2], f1d[2], f3[2], f3d[2], f32[2];
+    bool s1on[2], s3on[2];
+    for (int ph = 0; ph < 2; ph++) {
+        const double w = ph ? yi : xi, rho = ph ? rg : ro, kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
+        const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
+        cdg[ph] = kSIC * rho * SF2 * Vb * kr / mub * dPp;
+        cx1[ph] = kSIC * w * SF2 * Vb * kr / mub * dPp;
+        cx2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pf + pm);
+        cf2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pf + pm);
+        s1on[ph] = !v.diff_off && fsf1(lm, lf, ph);
+        s3on[ph] = !v.diff_off && fsf3(lm, lf, ph);
+        m1[ph] = mdd[ph] = m2[ph] = f1d[ph] = f3[ph] = f3d[ph] = f32[ph] = 0;
+        const double msat = M.S(1 + ph), mD = M.D(i, ph);
+        if (s1on[ph]) {
+            const double dlt = Fr.w(ph, i) - w;
+            m1[ph] = SF1 * msat * pm * Vb / tor * mD * dlt;
+            mdd[ph] = -SF1 * msat * pm * Vb / tor * rho * mD;
+            m2[ph] = SF1 * msat * pm * Vb / tor * rho * dlt;
+            f1d[ph] = SF1 * msat * pm * Vb / tor * rho * mD;
+        }
+        if (s3on[ph]) {
+            const double fsat = Fr.S(1 + ph), frho = Fr.rho(ph), fD = Fr.D(i, ph), fw = Fr.w(ph, i);
+            f3[ph] = SF3 * fsat * pf * Vb / tor * fD * (fw - 0.0);
+            f3d[ph] = SF3 * fsat * pf * Vb / tor * frho * fD;
+            f32[ph] = SF3 * fsat * pf * Vb / tor * frho * (fw - 0.0);
+        }
     }
-    if (L.sg) out.add(0, row, L.Sg, dLdSg - a.dSg);
-    const int rm = lm ? N : 0;
-    if (lm == 1) out.add(7, row, 2 * N + 2 - rm, dRMdSo);
-    else if (lm == -1) out.add(7, row, 2 * N + 2 - rm, dRMdSg);
-    else {
-        out.add(7, row, 2 * N + 2, dRMdSo);
-        out.add(7, row, 2 * N + 3, dRMdSg);
-    }
-    out.add(7, row, 2 * N - rm, v.pcoeff * dRMdp);
-    out.add(7, row, 2 * N + 1 - rm, dRMdSw);
     for (int k = 0; k < N; k++) {
-        double dRxl = 0, dRxg = 0, dRMxl = 0, dRMxg = 0;
+        double dRx[2], dRMx[2];
         const bool diag = k == i;
         for (int ph = 0; ph < 2; ph++) {
-            const double w = M.w(ph, i), rho = M.rho(ph), kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
-            const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
-            double &dR = ph ? dRxg : dRxl;
-            double &dRM = ph ? dRMxg : dRMxl;
-            if (diag) dRM -= kSIC * rho * SF2 * Vb * kr / mub * dPp;
-            dRM -= kSIC * M.dE(k, ph) * w * SF2 * Vb * kr / mub * dPp;
-            dRM -= -kSIC * visc_deriv(M, k, ph) * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pf + pm);
-            if (fsf1(lm, lf, ph)) {
-                const double sat = M.S(1 + ph), D = M.D(i, ph), dlt = Fr.w(ph, i) - w;
-                dRM -= M.dE(k, ph) * SF1 * sat * pm * Vb / tor * D * dlt;
-                if (diag) dRM -= -SF1 * sat * pm * Vb / tor * rho * D;
-                dRM -= diff_deriv(M, i, k, ph) * SF1 * sat * pm * Vb / tor * rho * dlt;
-            }
-            dR -= -kSIC * visc_deriv(Fr, k, ph) * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pf + pm);
-            // the fracture's own SF1 / SF3 composition dependences, in the reference's order
-            const double msat = M.S(1 + ph), mD = M.D(i, ph);
-            const double fsat = Fr.S(1 + ph), frho = Fr.rho(ph), fD = Fr.D(i, ph), fw = Fr.w(ph, i);
-            const bool s1 = fsf1(lm, lf, ph) && diag, s3 = fsf3(lm, lf, ph);
-            auto sf1_term = [&]() { if (s1) dR -= SF1 * msat * pm * Vb / tor * rho * mD; };
-            auto sf3_term = [&]() {
-                if (!s3) return;
-                dR -= Fr.dE(k, ph) * SF3 * fsat * pf * Vb / tor * fD * (fw - 0.0);
-                if (diag) dR -= SF3 * fsat * pf * Vb / tor * frho * fD;
-                dR -= diff_deriv(Fr, i, k, ph) * SF3 * fsat * pf * Vb / tor * frho * (fw - 0.0);
-            };
-            // both-phase pairings list the interface term first
-            if ((ph == 0 && lm == 0 && lf == 1) || (ph == 1 && lm == 0 && lf == -1)) {
-                if (ph == 0) { sf3_term(); sf1_term(); }
-                else { sf1_term(); sf3_term(); }
-            } else {
-                sf1_term();
-                sf3_term();
-            }
+            const double dEk = M.dE(k, ph);
+            double dRM = -((diag ? cdg[ph] : 0.0) + dEk * cx1[ph] + dmu(M, k, ph) * cx2[ph]);
+            if (s1on[ph]) dRM -= dEk * m1[ph] + (diag ? mdd[ph] : 0.0) + dD(M, i, k, ph) * m2[ph];
+            double dR = -(dmu(Fr, k, ph) * cf2[ph]);
+            // the fracture's own SF1 / SF3 composition dependences
+            if (s1on[ph] && diag) dR -= f1d[ph];
+            if (s3on[ph]) dR -= Fr.dE(k, ph) * f3[ph] + (diag ? f3d[ph] : 0.0) + dD(Fr, i, k, ph) * f32[ph];
+            dRx[ph] = dR;
+            dRMx[ph] = dRM;
         }
-        const double dLxl = diag ? Fr.rho(0) + fxi * Fr.dE(k, 0) : fxi * Fr.dE(k, 0);
-        const double dLxg = diag ? Fr.rho(1) + fyi * Fr.dE(k, 1) : fyi * Fr.dE(k, 1);
+        a.x(k) = dRx[0];
+        a.y(k) = dRx[1];
+        store_other_x(N, out, row, lm, k, dRMx[0], dRMx[1]);
+    }
+    row_faces(v, Fr, i, true, false, a, out, row, nullptr);
+    const WellAt W = well_at(v, 1, c, i, fyi);
+    store_own_ps(N, out, row, lf, v.pcoeff * (dLdp + a.dp + fxi * W.PIo + W.gcomp * W.PIg), -a.dSw, dLdSo - a.dSo,
+                 dLdSg - a.dSg);
+    const OwnLayout O = own_layout(lf);
+    const double aol = (Vb / v.dt) * pf * Fr.S(1), aog = (Vb / v.dt) * pf * Fr.S(2);
+    const double frl = Fr.rho(0), frg = Fr.rho(1);
+    for (int k = 0; k < N; k++) {
+        const bool diag = k == i;
+        const double dLxl = diag ? frl + fxi * Fr.dE(k, 0) : fxi * Fr.dE(k, 0);
+        const double dLxg = diag ? frg + fyi * Fr.dE(k, 1) : fyi * Fr.dE(k, 1);
         const double dQxl = (diag && W.iwell < 0) ? W.Qo : 0.0, dQxg = (diag && W.iwell < 0) ? W.Qg : 0.0;
-        for (int q = 0; q < nf; q++) comp_face_x(v, Fr, i, k, fc[q], fracture_comp_quirks(fc[q]), out, row, dRxl, dRxg, true);
-        if (lm == 1) out.add(7, row, k, dRMxl);
-        else if (lm == -1) out.add(7, row, k, dRMxg);
-        else {
-            out.add(7, row, k, dRMxl);
-            out.add(7, row, N + k, dRMxg);
+        out.st(L.cr(row, 0, k), O.x ? aol * dLxl - dQxl - a.x(k) : 0.0);
+        out.st(L.cr(row, 0, N + k), O.y ? aog * dLxg - dQxg - a.y(k) : 0.0);
+    }
+    store_other_ps(N, out, row, lm, v.pcoeff * dRMdp, dRMdSw, dRMdSo, dRMdSg);
+}
+
+// ---------------------------------------------------------------------------
+// Total hydrocarbon row (canonical 2N-1).  The matrix-fracture transfer
+// derivatives are formed from the matrix side; a fracture row takes them
+// negated with the roles of the two continua exchanged.  Also stores the
+// eight shifted entries of this block row.
+// ---------------------------------------------------------------------------
+OSR_HD inline void total_row(const JacView &v, int med, long c, const Out &out, Acc &a) {
+    const int N = v.nc;
+    const Layout L(N);
+    const int row = 2 * N - 1;
+    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
+    const Cell &O = med ? Fr : M;          // this row's continuum
+    const Transfer t = transfer_terms(v, c);
+    const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
+    const double Vb = t.Vb, SF2 = t.SF2;
+    const double po_ = med ? pf : pm, dpo_ = med ? dpf : dpm;
+    const int lo = (med ? M : Fr).label();   // the other continuum's label
+    const double ro = M.rho(0), rg = M.rho(1);
+    const double mubar_o = t.Do / (pm + pf), mubar_g = t.Dg / (pm + pf);
+    const double dLdp = (Vb / v.dt) * (O.S(1) * (O.rho(0) * dpo_ + O.dE(N, 0) * po_) + O.S(2) * (O.rho(1) * dpo_ + O.dE(N, 1) * po_));
+    const double dLdSo = (Vb / v.dt) * (po_ * O.rho(0)), dLdSg = (Vb / v.dt) * (po_ * O.rho(1));
+    // matrix-side derivatives of the (matrix-row) transfer terms
+    double tm = 0, tf = 0;
+    tm += kSIC * M.dE(N, 0) * SF2 * Vb * t.kro / mubar_o * t.dPo;
+    tm += -kSIC * ro * SF2 * Vb * t.kro / mubar_o;
+    tm += -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+    tm += kSIC * dpm * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+    tm += kSIC * M.dE(N, 1) * SF2 * Vb * t.krg / mubar_g * t.dPg;
+    tm += -kSIC * rg * SF2 * Vb * t.krg / mubar_g;
+    tm += -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+    tm += kSIC * dpm * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+    tf += kSIC * ro * SF2 * Vb * t.kro / mubar_o;
+    tf += -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+    tf += kSIC * dpf * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+    tf += kSIC * rg * SF2 * Vb * t.krg / mubar_g;
+    tf += -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+    tf += kSIC * dpf * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+    const double sg = med ? -1.0 : 1.0;
+    a.dp = a.dSw = a.dSo = a.dSg = 0;
+    a.dp += sg * (med ? tf : tm);
+    const double dROdp = sg * (med ? tm : tf);   // the other continuum's pressure
+    const double po = ro * SF2 * Vb / mubar_o * t.dPo, pg = rg * SF2 * Vb / mubar_g * t.dPg;
+    const double smSo = kSIC * t.dkm[4] * po, sfSo = kSIC * t.dkf[4] * po;
+    const double smSg = kSIC * t.dkm[2] * po + kSIC * t.dkm[3] * pg, sfSg = kSIC * t.dkf[2] * po + kSIC * t.dkf[3] * pg;
+    const double smSw = kSIC * t.dkm[1] * po, sfSw = kSIC * t.dkf[1] * po;
+    a.dSo += sg * (med ? sfSo : smSo);
+    a.dSg += sg * (med ? sfSg : smSg);
+    a.dSw += sg * (med ? sfSw : smSw);
+    const double dROSo = sg * (med ? smSo : sfSo), dROSg = sg * (med ? smSg : sfSg), dROSw = sg * (med ? smSw : sfSw);
+    const double t1o = kSIC * SF2 * Vb * t.kro / mubar_o * t.dPo;
+    const double t2o = -kSIC * ro * SF2 * Vb * t.kro * pm / (t.Do * t.Do) * t.dPo * (pm + pf);
+    const double t3o = -kSIC * ro * SF2 * Vb * t.kro * pf / (t.Do * t.Do) * t.dPo * (pm + pf);
+    const double t1g = kSIC * SF2 * Vb * t.krg / mubar_g * t.dPg;
+    const double t2g = -kSIC * rg * SF2 * Vb * t.krg * pm / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+    const double t3g = -kSIC * rg * SF2 * Vb * t.krg * pf / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+    for (int k = 0; k < N; k++) {
+        const double xm = M.dE(k, 0) * t1o + dmu(M, k, 0) * t2o;
+        const double xf = dmu(Fr, k, 0) * t3o;
+        const double ym = M.dE(k, 1) * t1g + dmu(M, k, 1) * t2g;
+        const double yf = dmu(Fr, k, 1) * t3g;
+        a.x(k) = sg * (med ? xf : xm);
+        a.y(k) = sg * (med ? yf : ym);
+        store_other_x(N, out, row, lo, k, sg * (med ? xm : xf), sg * (med ? ym : yf));
+    }
+    double ov[kOverflow];
+    for (int j = 0; j < kOverflow; j++) ov[j] = 0;
+    row_faces(v, O, 0, med == 1, true, a, out, row, ov);
+    for (int j = 0; j < kOverflow; j++) out.st(L.o(j), ov[j]);
+    const WellAt W = well_at(v, med, c, 0, 0.0);
+    const int lab = O.label();
+    store_own_ps(N, out, row, lab, v.pcoeff * (dLdp + a.dp + W.PIo + W.PIg), -a.dSw, dLdSo - a.dSo, dLdSg - a.dSg);
+    const OwnLayout OL = own_layout(lab);
+    const double aol = (Vb / v.dt) * po_ * O.S(1), aog = (Vb / v.dt) * po_ * O.S(2);
+    for (int k = 0; k < N; k++) {
+        out.st(L.cr(row, 0, k), OL.x ? aol * O.dE(k, 0) - a.x(k) : 0.0);
+        out.st(L.cr(row, 0, N + k), OL.y ? aog * O.dE(k, 1) - a.y(k) : 0.0);
+    }
+    store_other_ps(N, out, row, lo, v.pcoeff * dROdp, dROSw, dROSo, dROSg);
+}
+
+// ---------------------------------------------------------------------------
+// Water row (canonical 2N).
+// ---------------------------------------------------------------------------
+OSR_HD inline void water_row(const JacView &v, int med, long c, const Out &out) {
+    const int N = v.nc;
+    const Layout L(N);
+    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
+    const Cell &O = med ? Fr : M;
+    const JMed &F = v.m[med];
+    const Transfer t = transfer_terms(v, c);
+    const double wr = v.wat_ro * kWatMRo;
+    const double po_ = med ? t.pf : t.pm, dpo_ = med ? t.dpf : t.dpm;
+    const double sg = med ? -1.0 : 1.0;
+    const double dLdp = (t.Vb / v.dt) * wr * O.S(0) * dpo_;
+    const double dLdSw = (t.Vb / v.dt) * (po_ * wr);
+    const double tr = kSIC * v.wat_ro * kWatMRo * t.SF2 * t.krw / v.wat_mu * t.Vb;
+    // both continua's water rows take -tr for their own pressure, +tr for the other's
+    double dRdp = -tr;
+    const double dROdp = tr;
+    JFace fc[6];
+    const int nf = jac_faces(v, c, fc);
+    const long n = v.n;
+    for (int q = 0; q < nf; q++) dRdp += ld(F.wtran + (long)fc[q].d * n + fc[q].tc);
+    const WellAt W = well_at(v, med, c, 0, 0.0);
+    out.st(L.w(0, 2 * N), v.pcoeff * (dLdp + dRdp + W.PIw));
+    const double smw = kSIC * kWatMRo * t.dkm[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
+    const double sfw = kSIC * kWatMRo * t.dkf[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
+    double dRdSw = sg * (med ? sfw : smw);
+    const double dROSw = sg * (med ? smw : sfw);
+    unsigned present = 0;
+    for (int q = 0; q < nf; q++) {
+        const JFace &e = fc[q];
+        present |= 1u << e.slot;
+        const FaceData fd = face_data(v, F, c, e);
+        const double Tw = ld(F.wtran + (long)e.d * n + e.tc), dTw = ld(F.dwtran + (long)e.d * n + e.tc);
+        out.st(L.w(e.slot, 2 * N), v.pcoeff * (-Tw));
+        const double dsw = e.sgn * (dTw * fd.dP[0] + kGAcc * v.wat_ro * dTw * fd.dH);
+        const bool up_nb = upstream(e, fd, c, 2) == e.nb;
+        out.st(L.w(e.slot, 2 * N + 1), up_nb ? dsw : 0.0);
+        if (!up_nb) dRdSw += dsw;
+    }
+    for (int s = 1; s <= 6; s++)
+        if (!(present & (1u << s))) {
+            out.st(L.w(s, 2 * N), 0.0);
+            out.st(L.w(s, 2 * N + 1), 0.0);
         }
-        if (L.x) out.add(0, row, L.X + k, (Vb / v.dt) * pf * Fr.S(1) * dLxl - dQxl - dRxl);
-        if (L.y) out.add(0, row, L.Y + k, (Vb / v.dt) * pf * Fr.S(2) * dLxg - dQxg - dRxg);
+    out.st(L.w(0, 2 * N + 1), dLdSw - dRdSw);
+    out.st(L.w(7, 2 * N), v.pcoeff * dROdp);
+    out.st(L.w(7, 2 * N + 1), dROSw);
+}
+
+// ---------------------------------------------------------------------------
+// Fugacity rows of a two-phase cell (compsim/Petsc_Functions.cpp:30240-30406
+// for the matrix): x_i P_o phi_i^L - y_i P_g phi_i^V with Z from the stored
+// density and dZ from dE.
+// ---------------------------------------------------------------------------
+OSR_HD inline void fugacity_rows(const JacView &v, const Cell &q, const Out &out) {
+    const int N = v.nc;
+    const Layout L(N);
+    const double RT = kR * v.T;
+    const double Pl = q.P(1), Pg = q.P(2);
+    double xl[kMaxNc], yg[kMaxNc], tl[kMaxNc], tg[kMaxNc];
+    for (int i = 0; i < N; i++) {
+        xl[i] = q.w(0, i);
+        yg[i] = q.w(1, i);
+    }
+    double Al = 0, Bl = 0, Ag = 0, Bg = 0;
+    for (int i = 0; i < N; i++) {
+        Bl += xl[i] * v.b[i];
+        Bg += yg[i] * v.b[i];
+        for (int j = 0; j < N; j++) {
+            const double t = v.sa[i] * v.sa[j] * v.bic[i * N + j];
+            Al += xl[i] * xl[j] * t;
+            Ag += yg[i] * yg[j] * t;
+        }
+    }
+    // sum_j w_j sqrt(a_i a_j) bic_ij of each component
+    for (int i = 0; i < N; i++) {
+        double a = 0, g = 0;
+        for (int j = 0; j < N; j++) {
+            const double t = v.sa[i] * v.sa[j] * v.bic[i * N + j];
+            a += xl[j] * t;
+            g += yg[j] * t;
+        }
+        tl[i] = a;
+        tg[i] = g;
+    }
+    const double Cal = Al, Cbl = Bl, Cag = Ag, Cbg = Bg;
+    Al *= Pl / (RT * RT);
+    Bl *= Pl / RT;
+    Ag *= Pg / (RT * RT);
+    Bg *= Pg / RT;
+    const double dAdpl = Cal / (RT * RT), dAdpg = Cag / (RT * RT), dBdpl = Cbl / RT, dBdpg = Cbg / RT;
+    const double Zl = Pl / (q.rho(0) * RT), Zg = Pg / (q.rho(1) * RT);
+    const double dZdpl = (1 - q.dE(N, 0) * RT * Zl) * (Zl / Pl), dZdpg = (1 - q.dE(N, 1) * RT * Zg) * (Zg / Pg);
+    const double d1 = v.srk ? 1.0 : 1 + kSqrt2, d2 = v.srk ? 0.0 : 1 - kSqrt2;
+    const double DDl = Al / (Bl * (d1 - d2)), DDg = Ag / (Bg * (d1 - d2));
+    const double FFl = log((Zl + d2 * Bl) / (Zl + d1 * Bl)), FFg = log((Zg + d2 * Bg) / (Zg + d1 * Bg));
+    const double lZBl = log(Zl - Bl), lZBg = log(Zg - Bg);
+    for (int i = 0; i < N; i++) {
+        const double t1l = v.b[i] / Cbl, t1g = v.b[i] / Cbg;
+        const double EEl = 2 * tl[i] / Cal - t1l, EEg = 2 * tg[i] / Cag - t1g;
+        const double phiL = exp(t1l * (Zl - 1) - lZBl + DDl * EEl * FFl);
+        const double phiG = exp(t1g * (Zg - 1) - lZBg + DDg * EEg * FFg);
+        const double dAAl = v.b[i] * dZdpl / Cbl, dAAg = v.b[i] * dZdpg / Cbg;
+        const double dBBl = (dBdpl - dZdpl) / (Zl - Bl), dBBg = (dBdpg - dZdpg) / (Zg - Bg);
+        const double dDDl = (Bl * dAdpl - Al * dBdpl) / (Bl * Bl * (d1 - d2)), dDDg = (Bg * dAdpg - Ag * dBdpg) / (Bg * Bg * (d1 - d2));
+        const double dFFl = (dZdpl + d2 * dBdpl) / (Zl + d2 * Bl) - (dZdpl + d1 * dBdpl) / (Zl + d1 * Bl);
+        const double dFFg = (dZdpg + d2 * dBdpg) / (Zg + d2 * Bg) - (dZdpg + d1 * dBdpg) / (Zg + d1 * Bg);
+        const double dPhil = phiL * (dAAl + dBBl + EEl * (dDDl * FFl + DDl * dFFl));
+        const double dPhig = phiG * (dAAg + dBBg + EEg * (dDDg * FFg + DDg * dFFg));
+        const double xi = xl[i], yi = yg[i];
+        out.st(L.f(i, 2 * N), v.pcoeff * (xi * (phiL + Pl * dPhil) - yi * (phiG + Pg * dPhig)));
+        for (int k = 0; k < N; k++) {
+            const double dAl = tl[k] * (2 * Pl / (RT * RT)), dAg = tg[k] * (2 * Pg / (RT * RT));
+            const double dBl = v.b[k] * Pl / RT, dBg = v.b[k] * Pg / RT;
+            const double dZl = -q.dE(k, 0) * RT * Zl * Zl / Pl, dZg = -q.dE(k, 1) * RT * Zg * Zg / Pg;
+            const double dAAxl = -v.b[k] * v.b[i] * (Zl - 1) / (Cbl * Cbl) + v.b[i] * dZl / Cbl;
+            const double dAAxg = -v.b[k] * v.b[i] * (Zg - 1) / (Cbg * Cbg) + v.b[i] * dZg / Cbg;
+            const double dBBxl = (dBl - dZl) / (Zl - Bl), dBBxg = (dBg - dZg) / (Zg - Bg);
+            const double dDDxl = (dAl * Bl - dBl * Al) / (Bl * Bl * (d1 - d2)), dDDxg = (dAg * Bg - dBg * Ag) / (Bg * Bg * (d1 - d2));
+            const double dFFxl = (dZl + d2 * dBl) / (Zl + d2 * Bl) - (dZl + d1 * dBl) / (Zl + d1 * Bl);
+            const double dFFxg = (dZg + d2 * dBg) / (Zg + d2 * Bg) - (dZg + d1 * dBg) / (Zg + d1 * Bg);
+            const double tik = v.sa[i] * v.sa[k] * v.bic[i * N + k];
+            const double dEEl = 2 * (tik / Cal - dAl * RT * RT * tl[i] / (Pl * Cal * Cal)) + v.b[i] * v.b[k] / (Cbl * Cbl);
+            const double dEEg = 2 * (tik / Cag - dAg * RT * RT * tg[i] / (Pg * Cag * Cag)) + v.b[i] * v.b[k] / (Cbg * Cbg);
+            const double dPxl = phiL * (dAAxl + dBBxl + dDDxl * EEl * FFl + DDl * dEEl * FFl + DDl * EEl * dFFxl);
+            const double dPxg = phiG * (dAAxg + dBBxg + dDDxg * EEg * FFg + DDg * dEEg * FFg + DDg * EEg * dFFxg);
+            if (i == k) {
+                out.st(L.f(i, k), Pl * phiL + Pl * xi * dPxl);
+                out.st(L.f(i, N + k), -(Pg * phiG + Pg * yi * dPxg));
+            } else {
+                out.st(L.f(i, k), Pl * xi * dPxl);
+                out.st(L.f(i, N + k), -Pg * yi * dPxg);
+            }
+        }
     }
 }
 
-// Block row b (cell-medium) of the Jacobian.  Returns false when this
-// cell-medium's case is not covered.
-OSR_HD inline bool jacobian_block(const JacView &v, long b) {
+// ---------------------------------------------------------------------------
+// Row tasks
+// ---------------------------------------------------------------------------
+
+// A component or total row of an inactive cell-medium: its unit entry and
+// zeros (the reference writes a unit diagonal only).
+OSR_HD inline void inactive_c_row(int N, const Out &out, int lab, int row) {
+    const Layout L(N);
+    const int uc = unit_col(N, lab, row);
+    for (int s = 0; s < 8; s++)
+        for (int c = 0; c < L.BS; c++) out.st(L.cr(row, s, c), (s == 0 && c == uc) ? 1.0 : 0.0);
+}
+
+// Task N: the fugacity rows (or a one-phase cell's unused rows), the water row
+// and the constraint rows.
+OSR_HD inline void misc_rows(const JacView &v, int med, long c, const Out &out) {
     const int N = v.nc;
-    const int med = b >= v.n;
-    const long c = med ? b - v.n : b;
-    const BlockRow out{&v, b};
-    const Cell q{&v, &v.m[med], c};
+    const Layout L(N);
+    const Cell q{&v, &v.m[med], c, med};
     const int lab = q.label();
-    const int rows = lab == 0 ? 2 * N + 4 : N + 3;
-    if (q.por() < 1e-10) {
-        // an inactive cell-medium: unit diagonal
-        for (int r = 0; r < rows; r++) out.add(0, r, r, 1.0);
-        return true;
-    }
-    const int r0 = lab == 0 ? N : 0;
-    if (lab == 0) fugacity_rows(v, q, out);
-    if (med == 0)
-        for (int i = 0; i < N - 1; i++) matrix_comp_row_2ph(v, c, i, out, r0 + i);
-    else
-        for (int i = 0; i < N - 1; i++) fracture_comp_row_2ph(v, c, i, out, r0 + i);
-    total_row_2ph(v, med, c, out, r0 + N - 1);
-    water_row_2ph(v, med, c, out, r0 + N);
-    if (lab == 0) {
-        constraint_rows_2ph(v, out);
+    const bool inactive = q.por() < 1e-10;
+    // F region
+    if (lab == 0 && !inactive) {
+        fugacity_rows(v, q, out);
     } else {
-        const OwnLayout L = own_layout(N, lab);
-        for (int k = 0; k < N; k++) out.add(0, N + 1, (lab == 1 ? L.X : L.Y) + k, 1.0);
-        out.add(0, N + 2, L.Sw, 1.0);
-        out.add(0, N + 2, lab == 1 ? L.So : L.Sg, 1.0);
+        for (int r = 0; r < N; r++) {
+            const int uc = unit_col(N, lab, r);
+            for (int cc = 0; cc <= 2 * N; cc++) out.st(L.f(r, cc), cc == uc ? 1.0 : 0.0);
+        }
     }
-    return true;
+    // W region
+    if (inactive) {
+        for (int s = 0; s < 8; s++) {
+            out.st(L.w(s, 2 * N), s == 0 ? 1.0 : 0.0);
+            out.st(L.w(s, 2 * N + 1), 0.0);
+        }
+    } else {
+        water_row(v, med, c, out);
+    }
+    // K region: the constraint rows, or unit entries where a row is unused
+    for (int r = 2 * N + 1; r <= 2 * N + 3; r++) {
+        const bool used = ref_row(N, lab, r) >= 0;
+        const int uc = unit_col(N, lab, r);
+        for (int cc = 0; cc < L.BS; cc++) {
+            double val;
+            if (inactive || !used) val = cc == uc ? 1.0 : 0.0;
+            else if (r == 2 * N + 3) val = (cc == 2 * N + 1 || (cc == 2 * N + 2 && lab != -1) || (cc == 2 * N + 3 && lab != 1)) ? 1.0 : 0.0;
+            else if (r == 2 * N + 1) val = cc < N ? 1.0 : 0.0;           // sum x (an oil-only cell's sum w)
+            else val = (cc >= N && cc < 2 * N) ? 1.0 : 0.0;              // sum y (a gas-only cell's sum w)
+            out.st(L.k(r, cc), val);
+        }
+    }
+}
+
+// The values row task `task` owns, stored as zeros (lanes of the last chunk
+// beyond the grid).
+OSR_HD inline void zero_task(int N, const Out &out, int task) {
+    const Layout L(N);
+    if (task == N) {
+        for (int e = 0; e < L.EF; e++) out.st(e, 0.0);
+        for (int e = L.EF + L.EC; e < L.E; e++) out.st(e, 0.0);
+        return;
+    }
+    const int row = N + task;
+    for (int s = 0; s < 8; s++)
+        for (int c = 0; c < L.BS; c++) out.st(L.cr(row, s, c), 0.0);
+    if (task == N - 1)
+        for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
+}
+
+// Row task `task` of block row bm (cell-medium).
+OSR_HD inline void jacobian_task(const JacView &v, long bm, int task, Acc &a) {
+    const int N = v.nc;
+    const int med = bm >= v.n;
+    const long c = med ? bm - v.n : bm;
+    const Out out{v.vals, v.entries, bm};
+    const Layout L(N);
+    if (task == N) {
+        misc_rows(v, med, c, out);
+        return;
+    }
+    const Cell q{&v, &v.m[med], c, med};
+    const int row = N + task;
+    if (q.por() < 1e-10) {
+        inactive_c_row(N, out, q.label(), row);
+        if (task == N - 1)
+            for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
+        return;
+    }
+    if (task == N - 1) total_row(v, med, c, out, a);
+    else if (med == 0) matrix_comp_row(v, c, task, out, a);
+    else fracture_comp_row(v, c, task, out, a);
+}
+
+// Row tasks by kind, for launches that each run one code path: 0 matrix
+// component rows, 1 fracture component rows, 2 total rows, 3 fugacity /
+// water / constraint rows.  The kind's lanes only; padding lanes of the last
+// chunk store zeros.
+template <int KIND>
+OSR_HD inline void jacobian_task_kind(const JacView &v, long bm, int task, Acc &a) {
+    const int N = v.nc;
+    const long nb = 2 * v.n;
+    const Out out{v.vals, v.entries, bm};
+    if (bm >= nb) {
+        if (KIND != 0) zero_task(N, out, task);
+        return;
+    }
+    const int med = bm >= v.n;
+    if ((KIND == 0 && med) || (KIND == 1 && !med)) return;
+    const long c = med ? bm - v.n : bm;
+    if (KIND == 3) {
+        misc_rows(v, med, c, out);
+        return;
+    }
+    const Cell q{&v, &v.m[med], c, med};
+    if (q.por() < 1e-10) {
+        inactive_c_row(N, out, q.label(), N + task);
+        if (KIND == 2) {
+            const Layout L(N);
+            for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
+        }
+        return;
+    }
+    if (KIND == 0) matrix_comp_row(v, c, task, out, a);
+    else if (KIND == 1) fracture_comp_row(v, c, task, out, a);
+    else total_row(v, med, c, out, a);
+}
+
+// Reference (global row, global column) of entry e of block row bm, or -1 for
+// an entry the reference does not have (unit entries of unused rows, absent
+// neighbours and unknowns).  rowoff: the row offsets of the row layout;
+// lab_m, lab_f: per cell phase state of the two continua.
+OSR_HD inline void entry_position(int N, int nx, int ny, int nz, long n, const long *rowoff, const signed char *lab_m,
+                                  const signed char *lab_f, long bm, int e, long *grow, long *gcol) {
+    const Layout L(N);
+    *grow = *gcol = -1;
+    const int med = bm >= n;
+    const long c = med ? bm - n : bm;
+    const signed char *lab = med ? lab_f : lab_m;
+    const int lb = lab[c];
+    const int ix = (int)(c % nx), iy = (int)((c / nx) % ny), iz = (int)(c / ((long)nx * ny));
+    const long sy = nx, sz = (long)nx * ny;
+    if (e >= L.E) {
+        // shifted entries of the total row: face -y (0..3) or -z (4..7)
+        const int j = e - L.E, f = j / 4, t = j % 4;
+        if (f == 0 ? iy == 0 : iz == 0) return;
+        const long stride = f == 0 ? sy : sz;
+        const int lnb = lab[c - stride];
+        const int nbase = lnb ? -N : 0, reCol4 = lnb ? 1 : 0;
+        const int col = nbase + 2 * N + (t == 3 ? 3 - reCol4 : t);
+        *grow = rowoff[bm] + ref_row(N, lb, 2 * N - 1);
+        *gcol = rowoff[bm - stride + 1] + col;
+        return;
+    }
+    int r, s, cc;
+    if (e < L.EF) {
+        r = e / (2 * N + 1);
+        cc = e % (2 * N + 1);
+        s = 0;
+    } else if (e < L.EF + L.EC) {
+        const int q = e - L.EF;
+        r = N + q / (8 * L.BS);
+        s = (q / L.BS) % 8;
+        cc = q % L.BS;
+    } else if (e < L.EF + L.EC + L.EW) {
+        const int q = e - L.EF - L.EC;
+        r = 2 * N;
+        s = q / 2;
+        cc = 2 * N + q % 2;
+    } else {
+        const int q = e - L.EF - L.EC - L.EW;
+        r = 2 * N + 1 + q / L.BS;
+        s = 0;
+        cc = q % L.BS;
+    }
+    const int rr = ref_row(N, lb, r);
+    if (rr < 0) return;
+    long tb;   // target block row (cell-medium)
+    switch (s) {
+        case 0: tb = bm; break;
+        case 1: if (ix == 0) return; tb = bm - 1; break;
+        case 2: if (ix == nx - 1) return; tb = bm + 1; break;
+        case 3: if (iy == 0) return; tb = bm - sy; break;
+        case 4: if (iy == ny - 1) return; tb = bm + sy; break;
+        case 5: if (iz == 0) return; tb = bm - sz; break;
+        case 6: if (iz == nz - 1) return; tb = bm + sz; break;
+        default: tb = med ? c : n + c; break;
+    }
+    const int lt = tb >= n ? lab_f[tb - n] : lab_m[tb];
+    const int rc = ref_col(N, lt, cc);
+    if (rc < 0) return;
+    *grow = rowoff[bm] + rr;
+    *gcol = rowoff[tb] + rc;
 }
 
 }  // namespace osrj
