@@ -19,6 +19,10 @@ static osr_status jfail(cudaError_t) { return OSR_ERR_CUDA; }
     } while (0)
 
 constexpr int kRowThreads = 128;
+// Resident CTAs per SM the row kernels are compiled for (bounds their registers).
+#ifndef OSR_JAC_MIN_BLOCKS
+#define OSR_JAC_MIN_BLOCKS 4
+#endif
 
 template <int N>
 __global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_constant__ osrj::JacView v) {
@@ -32,7 +36,7 @@ __global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_cons
 // N-1, the fugacity / water / constraint rows task N.  Each thread's
 // per-component accumulators: 3N doubles of dynamic shared memory.
 template <int KIND>
-__global__ void __launch_bounds__(kRowThreads) jacobian_rows_kernel(const __grid_constant__ osrj::JacView v,
+__global__ void __launch_bounds__(kRowThreads, OSR_JAC_MIN_BLOCKS) jacobian_rows_kernel(const __grid_constant__ osrj::JacView v,
                                                                    long chunk0, long chunks) {
     extern __shared__ double s_acc[];
     const int N = v.nc;
