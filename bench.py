@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-assembly", action="store_true")
+    ap.add_argument("--part", choices=["all", "assembly"], default="all",
+                    help="assembly: only the Newton-step assembly object (profiling)")
+    ap.add_argument("--assembly-grid", default=None, help="NX,NY,NZ of the assembly grid (default 128,128,32)")
     return ap.parse_args()
 
 
@@ -216,7 +219,8 @@ def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier,
     workload, each part timed with CUDA events on the launching stream."""
     import numpy as np
     from osiris_b200 import workloads
-    nx, ny, nz = workloads.ASSEMBLY_GRID
+    nx, ny, nz = (tuple(int(v) for v in args.assembly_grid.split(",")) if args.assembly_grid
+                  else workloads.ASSEMBLY_GRID)
     d = workloads.assembly_deck(nx, ny, nz)
     G = osr.Grid(d)
     p0 = workloads.assembly_state(G, d, dev, seed=4 + rank)
@@ -323,6 +327,16 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     n = args.cells or workloads.FLASH_CELLS
+
+    if args.part == "assembly":
+        dev = torch.device("cuda", local)
+        torch.cuda.set_device(dev)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        a = measure_assembly(osr, torch, dev, torch.cuda.current_stream(dev), flush, args, rank, world,
+                             lambda: None, lambda x: x, _gpu_id(torch, dev))
+        if rank == 0:
+            print(json.dumps(a), flush=True)
+        return 0
 
     # the CPU pool is spawned before the first GPU call
     cpu = None

@@ -17,6 +17,12 @@
 // two-phase cell, [w, P/PCoeff, Sw, S_present] for a one-phase cell
 // (UpdateAll/InitGuess2, compsim/PetscAUX.cpp:176-498, 878-964).
 #pragma once
+
+// Resident 128-thread CTAs per SM the residual kernel is compiled for (bounds
+// its registers).
+#ifndef OSR_RES_MIN_BLOCKS
+#define OSR_RES_MIN_BLOCKS 4
+#endif
 #include "grid_kernels.cuh"
 
 namespace osr {
@@ -653,7 +659,7 @@ __device__ __forceinline__ double porpor_at(const MediumFields &F, const GridSca
 }
 
 template <int N>
-__global__ void __launch_bounds__(128) residual_kernel(const __grid_constant__ AsmArgs<N> A) {
+__global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const __grid_constant__ AsmArgs<N> A) {
     const GridScalars &s = A.a.s;
     const GridGeom &geo = A.a.geo;
     const long n = s.cells;
