@@ -292,6 +292,34 @@ osr_status osr_grid_jacobian(osr_grid *grid, double sim_time, double *d_vals, vo
 osr_status osr_grid_form_jacobian(osr_grid *grid, const double *d_x, double sim_time, double *d_vals,
                                   void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Phase appearance after an accepted time step.
+ * ------------------------------------------------------------------------- */
+
+/* Saturation pressure of every one-phase cell of one continuum (0 matrix, 1
+ * fracture): the bubble pressure of an oil-only cell from its oil pressure,
+ * the dew pressure of a gas-only cell from its gas pressure (Bubl_Succ,
+ * Dew_Succ, fBubl_Succ, fDew_Succ, compsim/Minor_NR.cpp:491-2015: successive
+ * substitution, then a Newton fallback with a dense (N+1)^2 solve).
+ * d_psat [cells]: the pressure, -1 where the reference's function returns -1
+ * (no convergence in 20 iterations, trivial solution), 0 for two-phase
+ * cells.  d_xm [nc][cells] (optional): the incipient phase's composition.
+ * DEVICE pointers; asynchronous on `stream`. */
+osr_status osr_grid_saturation_pressure(osr_grid *grid, int medium, double *d_psat, double *d_xm, void *stream);
+
+/* PhaseCtrl and fPhaseCtrl (compsim/Do_Cycle.cpp:1558-1721) on the current
+ * state: phase appearance at 0.95 of the saturation pressure with a new-phase
+ * saturation of 1e-3 and the incipient composition, phase disappearance at
+ * zero saturation, saturations renormalised.  Changes labels, saturations
+ * and compositions; the row layout follows with osr_grid_refresh_layout. */
+osr_status osr_grid_phase_ctrl(osr_grid *grid, void *stream);
+
+/* UpdateAll(x, true) after an accepted Newton solve (compsim/PetscAUX.cpp:
+ * 176-498, UpdateDependencies(true) :500-545): unpack x, PhaseCtrl and
+ * fPhaseCtrl, PCoeff and the row layout, then the property sweeps.
+ * Synchronises `stream` (the new row count and PCoeff come back to the host). */
+osr_status osr_grid_update_all_full(osr_grid *grid, const double *d_x, void *stream);
+
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The
  * denominator of the flash kernel's roofline.  No reference counterpart. */

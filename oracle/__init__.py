@@ -302,6 +302,8 @@ class RefDeck:
         lib.ref_get.restype = ctypes.c_long
         lib.ref_scalar.restype = ctypes.c_double
         lib.ref_form_jacobian.restype = ctypes.c_long
+        lib.ref_set.restype = ctypes.c_long
+        lib.ref_sat_pressure.restype = ctypes.c_double
         rc = lib.ref_deck_open(path.encode())
         if rc:
             raise RuntimeError(f"reference could not open {path}")
@@ -353,6 +355,23 @@ class RefDeck:
         info = np.zeros(10, np.int32)
         self.lib.ref_deck_info(_p(info))
         return info
+
+    def set(self, name: str, values):
+        """Overwrite a state array (m./f. + P, sat, x, y, z, label) in the
+        layout ``get`` returns."""
+        v = np.ascontiguousarray(values, np.float64).ravel().copy()
+        if self.lib.ref_set(name.encode(), _p(v)) < 0:
+            raise KeyError(name)
+
+    def sat_pressure(self, medium: int, cell: int):
+        """(saturation pressure, incipient composition) of one cell as the
+        reference's PhaseCtrl computes it."""
+        xm = np.zeros(self.nc)
+        p = self.lib.ref_sat_pressure(int(medium), ctypes.c_long(int(cell)), _p(xm))
+        return float(p), xm
+
+    def phase_ctrl(self):
+        self.lib.ref_phase_ctrl()
 
     def update_all(self, x, full: bool):
         x = np.ascontiguousarray(x, np.float64).copy()

@@ -308,6 +308,58 @@ long ref_get(const char *name, double *out) {
     return w;
 }
 
+/* Overwrite a named state array (the layout of ref_get): m./f. + P, sat,
+ * x, y, z or label.  Returns the values read, or -1. */
+long ref_set(const char *name, const double *in) {
+    std::string s(name);
+    const long n = ncell();
+    bool fr = s.size() > 2 && s[0] == 'f' && s[1] == '.';
+    std::string k = s.size() > 2 ? s.substr(2) : s;
+    FType *****cp = fr ? fcomp : comp;
+    FType ****pp = fr ? fP : P;
+    FType ****st = fr ? fsat : sat;
+    signed char ***ps = fr ? fphaseStat : phaseStat;
+    if (k == "P") {
+        for (int p = 0; p < 3; p++) each_cell([&](int i, int j, int l, long c) { pp[i + 1][j + 1][l + 1][p] = in[p * n + c]; });
+        return 3 * n;
+    }
+    if (k == "sat") {
+        for (int p = 0; p < 3; p++) each_cell([&](int i, int j, int l, long c) { st[i][j][l][p] = in[p * n + c]; });
+        return 3 * n;
+    }
+    if (k == "x" || k == "y" || k == "z") {
+        int ph = k == "x" ? 0 : (k == "y" ? 1 : 2);
+        for (int q = 0; q < Nc; q++) each_cell([&](int i, int j, int l, long c) { cp[i][j][l][q][ph] = in[q * n + c]; });
+        return (long)Nc * n;
+    }
+    if (k == "label") {
+        each_cell([&](int i, int j, int l, long c) { ps[i][j][l] = (signed char)in[c]; });
+        return n;
+    }
+    return -1;
+}
+
+/* Saturation pressure of cell c of one continuum as PhaseCtrl computes it
+ * (Bubl_Succ / Dew_Succ, or the fracture's fBubl_Succ / fDew_Succ,
+ * compsim/Minor_NR.cpp:491-2015) by its phase label; xm receives Xm[0..Nc-1].
+ * Two-phase cells return 0. */
+double ref_sat_pressure(int med, long c, double *xm) {
+    const int Ix = (int)(c % Nx), Iy = (int)((c / Nx) % Ny), Iz = (int)(c / ((long)Nx * Ny));
+    const int lab = med ? fphaseStat[Ix][Iy][Iz] : phaseStat[Ix][Iy][Iz];
+    double p = 0;
+    if (lab == 1) p = med ? fBubl_Succ(Ix, Iy, Iz) : Bubl_Succ(Ix, Iy, Iz);
+    else if (lab == -1) p = med ? fDew_Succ(Ix, Iy, Iz) : Dew_Succ(Ix, Iy, Iz);
+    for (int i = 0; i < Nc; i++) xm[i] = lab ? Xm[i] : 0.0;
+    return p;
+}
+
+/* PhaseCtrl and fPhaseCtrl (compsim/Do_Cycle.cpp:1558-1721). */
+int ref_phase_ctrl(void) {
+    PhaseCtrl();
+    fPhaseCtrl();
+    return 0;
+}
+
 /* UpdateAll(x, full) (compsim/PetscAUX.cpp:176-498). */
 int ref_update_all(double *x, int full) {
     _p_Vec v{x, MatrixSize};

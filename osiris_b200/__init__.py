@@ -334,6 +334,26 @@ class Grid:
                                             ctypes.c_double(sim_time), None if stream is None else _vp(stream)),
                "osr_grid_form_function")
 
+    # -- phase appearance ----------------------------------------------------
+    def saturation_pressure(self, medium: int, device, stream=None):
+        """(pressure [cells], incipient composition [nc, cells]) of every
+        one-phase cell of one continuum (0 for two-phase cells, -1 where no
+        saturation pressure is found), device tensors."""
+        import torch
+        p = torch.empty(self.cells, dtype=torch.float64, device=device)
+        xm = torch.empty((self.nc, self.cells), dtype=torch.float64, device=device)
+        _check(lib().osr_grid_saturation_pressure(self._h, int(medium), _vp(p.data_ptr()), _vp(xm.data_ptr()),
+                                                  None if stream is None else _vp(stream)),
+               "osr_grid_saturation_pressure")
+        return p, xm
+
+    def phase_ctrl(self, stream=None):
+        _check(lib().osr_grid_phase_ctrl(self._h, None if stream is None else _vp(stream)), "osr_grid_phase_ctrl")
+
+    def update_all_full(self, d_x, stream=None):
+        _check(lib().osr_grid_update_all_full(self._h, _vp(d_x.data_ptr()), None if stream is None else _vp(stream)),
+               "osr_grid_update_all_full")
+
     # -- Jacobian path -------------------------------------------------------
     def jacobian_shape(self):
         """(block size, values per block row, shifted entries per block row)."""

@@ -406,6 +406,17 @@ osr_status osr_grid_well_radius(osr_grid *g, int well, double *re) {
     return OSR_OK;
 }
 
+}  // extern "C"
+
+namespace osr {
+osr_status grid_unpack(osr_grid &grid, const double *d_x, cudaStream_t st) {
+    osr_grid *g = &grid;
+    ASM_SWITCH(update_all_n<K>(*g, d_x, st))
+}
+}  // namespace osr
+
+extern "C" {
+
 osr_status osr_grid_init_guess(osr_grid *g, double *d_x, void *stream) {
     if (!g || !d_x || !(g->pcoeff > 0)) return OSR_ERR_ARG;
     ASM_SWITCH(init_guess_n<K>(*g, d_x, (cudaStream_t)stream))
@@ -413,11 +424,7 @@ osr_status osr_grid_init_guess(osr_grid *g, double *d_x, void *stream) {
 
 osr_status osr_grid_update_all(osr_grid *g, const double *d_x, void *stream) {
     if (!g || !d_x || !(g->pcoeff > 0)) return OSR_ERR_ARG;
-    osr_status s;
-    {
-        auto run = [&]() -> osr_status { ASM_SWITCH(update_all_n<K>(*g, d_x, (cudaStream_t)stream)) };
-        s = run();
-    }
+    osr_status s = grid_unpack(*g, d_x, (cudaStream_t)stream);
     if (s != OSR_OK) return s;
     return grid_update(*g, (cudaStream_t)stream);
 }

@@ -48,6 +48,8 @@ struct osr_grid {
 namespace osr {
 GridScalars grid_scalars(const osr_grid &g);
 osr_status grid_update(osr_grid &g, cudaStream_t st);
+// UpdateAll's unpacking of the unknowns into the state (no property sweeps).
+osr_status grid_unpack(osr_grid &g, const double *d_x, cudaStream_t st);
 double peaceman_re(const double *di, const double *dj, int nx, int ny, int ix, int iy);
 osr_status grid_assembly_init(osr_grid &g, const osr_model *md);
 void grid_assembly_free(osr_grid &g);

@@ -1,0 +1,145 @@
+"""GPU parity of the phase-appearance step against the reference.
+
+Both sides start from the same deck state; the test then writes the same
+constructed state into both: two-phase cells relabelled oil-only with the
+feed as the oil composition (their bubble pressure lies above the cell
+pressure), relabelled gas-only with the feed as the gas composition, and
+two-phase cells whose oil or gas saturation is set to zero.  Checked:
+
+* saturation pressures of every one-phase cell of both continua against the
+  reference's own Bubl_Succ / Dew_Succ / fBubl_Succ / fDew_Succ on the same
+  cell: the same failure cells (-1), else within 1e-9 relative; incipient
+  compositions within 1e-9;
+* PhaseCtrl + fPhaseCtrl: labels identical, saturations within 1e-12,
+  compositions within 1e-9;
+* UpdateAll(x, true) after a perturbed unknown vector: labels, row layout
+  and PCoeff identical, and the state and property planes within the grid
+  tests' bar.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+import osiris_b200 as osr
+from osiris_b200 import deck
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle.ref_available(), reason="reference library missing")]
+
+G_, O_ = (0.9, 0.07, 0.03), (0.5, 0.2, 0.3)
+_ST = {-1: (8e6, G_), 1: (2e7, O_), 0: (8e6, O_)}
+_PAIRS = [(a, b) for a in (-1, 0, 1) for b in (-1, 0, 1)]
+
+DECKS = {
+    "state_pairs": lambda: deck.config_deck(nx=3, ny=3, nz=9, ipress=[_ST[a][0] for a, _ in _PAIRS],
+                                            igc=[_ST[a][1] for a, _ in _PAIRS],
+                                            fipress=[_ST[b][0] for _, b in _PAIRS],
+                                            figc=[_ST[b][1] for _, b in _PAIRS], wells=False, cdif=0.0),
+    "sample_6MPa": lambda: deck.sample_deck(ipress=6e6),
+    "twophase_8MPa": lambda: deck.config_deck(nx=4, ny=4, nz=3, cdif=None, ipress=8e6, wells=False, seed=8),
+}
+
+
+def open_pair(tmp_path, name):
+    path = os.path.join(str(tmp_path), name + ".dat")
+    deck.write_deck(path, DECKS[name]())
+    R = oracle.RefDeck(path)
+    G = osr.Grid(deck.parse_deck(path))
+    for mi, m in enumerate("mf"):
+        G.set_state(mi, R.get(f"{m}.P")[1], R.get(f"{m}.sat"), R.get(f"{m}.x"), R.get(f"{m}.y"), R.get(f"{m}.z"),
+                    R.get(f"{m}.label"), R.get(f"{m}.rho"))
+    G.update_dependencies()
+    return R, G
+
+
+def construct_changes(R, G):
+    """The same phase-change candidates on both sides (see the module doc)."""
+    for mi, m in enumerate("mf"):
+        lab = R.get(f"{m}.label").copy()
+        sat = R.get(f"{m}.sat").copy()
+        x, y, z = R.get(f"{m}.x").copy(), R.get(f"{m}.y").copy(), R.get(f"{m}.z").copy()
+        two = np.nonzero(lab == 0)[0]
+        for j, c in enumerate(two):
+            kind = (j + mi) % 5
+            if kind == 0:                      # oil-only with the feed as its composition
+                lab[c] = 1
+                x[:, c] = z[:, c]
+            elif kind == 1:                    # gas-only with the feed as its composition
+                lab[c] = -1
+                y[:, c] = z[:, c]
+            elif kind == 2:                    # vanished oil
+                sat[1, c] = 0
+                sat[2, c] = 1 - sat[0, c]
+            elif kind == 3:                    # vanished gas
+                sat[2, c] = 0
+                sat[1, c] = 1 - sat[0, c]
+        for name, v in (("label", lab), ("sat", sat), ("x", x), ("y", y)):
+            R.set(f"{m}.{name}", v)
+        G.set_state(mi, G.get(f"{m}.P")[1], sat, x, y, z, lab.astype(np.int8))
+        R.set(f"{m}.P", G.get(f"{m}.P"))   # the phase pressures of the device's last property sweep
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_saturation_pressure_matches_reference(name, tmp_path, cuda_device):
+    import torch
+    R, G = open_pair(tmp_path, name)
+    construct_changes(R, G)
+    checked = 0
+    for mi, m in enumerate("mf"):
+        p, xm = G.saturation_pressure(mi, cuda_device)
+        torch.cuda.synchronize()
+        p, xm = p.cpu().numpy(), xm.cpu().numpy()
+        lab = R.get(f"{m}.label")
+        for c in np.nonzero(lab != 0)[0]:
+            pr, xr = R.sat_pressure(mi, int(c))
+            checked += 1
+            if pr == -1 or p[c] == -1:
+                assert pr == p[c], (m, int(c), p[c], pr)
+                continue
+            assert abs(p[c] - pr) <= 1e-9 * abs(pr), (m, int(c), p[c], pr)
+            assert np.abs(xm[:, c] - xr).max() <= 1e-9, (m, int(c), xm[:, c], xr)
+    assert checked > 0
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_phase_ctrl_matches_reference(name, tmp_path, cuda_device):
+    import torch
+    R, G = open_pair(tmp_path, name)
+    any_two_phase = any(bool((R.get(f"{m}.label") == 0).any()) for m in "mf")
+    construct_changes(R, G)
+    before = [R.get(f"{m}.label").copy() for m in "mf"]
+    R.phase_ctrl()
+    G.phase_ctrl()
+    torch.cuda.synchronize()
+    changed = 0
+    for mi, m in enumerate("mf"):
+        lr, lg = R.get(f"{m}.label"), G.get(f"{m}.label")
+        assert np.array_equal(lr, lg), (m, np.nonzero(lr != lg)[0][:10])
+        changed += int((lr != before[mi]).sum())
+        assert np.abs(G.get(f"{m}.sat") - R.get(f"{m}.sat")).max() <= 1e-12
+        for k in ("x", "y"):
+            assert np.abs(G.get(f"{m}.{k}") - R.get(f"{m}.{k}")).max() <= 1e-9, (m, k)
+    assert changed > 0 or not any_two_phase
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_update_all_full_matches_reference(name, tmp_path, cuda_device):
+    import torch
+    R, G = open_pair(tmp_path, name)
+    G.refresh_layout()
+    x0 = R.init_guess()
+    rng = np.random.default_rng(3)
+    xp = x0 * (1 + 2e-3 * rng.uniform(-1, 1, x0.shape))
+    R.update_all(xp, True)
+    G.update_all_full(torch.tensor(xp, device=cuda_device))
+    torch.cuda.synchronize()
+    rows, pcoeff = G.layout()
+    assert pcoeff == R.scalar("PCoeff")
+    assert np.array_equal(G.row_offsets(), R.get("rowoff").astype(np.int64))
+    for m in "mf":
+        assert np.array_equal(G.get(f"{m}.label"), R.get(f"{m}.label")), m
+        for k in ("P", "sat", "x", "y", "rho", "mu", "kr", "pc"):
+            g, r = G.get(f"{m}.{k}"), R.get(f"{m}.{k}")
+            scale = np.maximum(np.abs(r).max(axis=-1, keepdims=True), 1e-300)
+            assert np.all(np.abs(g - r) <= 1e-9 * np.abs(r) + 1e-12 * scale), (m, k)
