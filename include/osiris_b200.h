@@ -98,6 +98,18 @@ osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const doub
 osr_status osr_flash_batch_noalloc(const osr_fluid *fluid, const double *d_P, const double *d_T,
                                    const double *d_z, long n, const osr_flash_out *out, void *stream);
 
+/* Many independent instances in one batched call: instance i owns cells
+ * [inst_start[i], inst_start[i+1]) of the inputs and outputs and has its own
+ * fluid (EOS, criticals, kij); all instances have the same component count.
+ * inst_start: HOST [n_inst + 1], inst_start[0] = 0, inst_start[n_inst] = n.
+ * Each cell gets exactly the result osr_flash_batch gives it with its own
+ * instance's fluid; the work queue spans all instances, so uneven
+ * iteration counts across instances are absorbed as within one.  A caller
+ * with several component counts makes one call per count. */
+osr_status osr_flash_batch_instances(const osr_fluid *fluids, int n_inst, const long *inst_start, const double *d_P,
+                                     const double *d_T, const double *d_z, long n, const osr_flash_out *out,
+                                     void *stream);
+
 /* Same results, plain form: one thread per cell, no work queue.  Kept as the
  * baseline the batched form is measured against. */
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T,

@@ -21,7 +21,7 @@ import numpy as np
 
 from .build import INCLUDE, LIB
 
-__all__ = ["Fluid", "lib", "flash", "flash_host", "set_shape", "get_shape", "header_symbols", "OsrError",
+__all__ = ["Fluid", "lib", "flash", "flash_host", "flash_instances", "set_shape", "get_shape", "header_symbols", "OsrError",
            "FLASH_OUTPUTS"]
 
 _vp = ctypes.c_void_p
@@ -204,6 +204,30 @@ def flash_passes() -> int:
         n += 1
         s *= 2
     return n + 1
+
+
+def flash_instances(fluids, start, P, T, z, derivs: bool = True, out: dict | None = None, stream=None,
+                    iters: bool = True):
+    """Flash several instances of one component count in one batched call
+    (``osr_flash_batch_instances``): ``fluids`` a list of Fluid, ``start``
+    host int64 [len(fluids) + 1] cell offsets, P/T/z device tensors of all
+    instances' cells.  Returns (or fills) the output dict."""
+    import torch
+    n = int(P.shape[0])
+    nc = fluids[0].nc
+    start = np.ascontiguousarray(start, dtype=np.int64)
+    if start.shape != (len(fluids) + 1,):
+        raise OsrError("start must have len(fluids) + 1 entries")
+    arr = (_CFluid * len(fluids))(*[f._c for f in fluids])
+    if out is None:
+        out = alloc_flash_outputs(nc, n, derivs, P.device, iters)
+    if stream is None:
+        stream = torch.cuda.current_stream(P.device)
+    co = _out_struct(out, lambda t: _vp(t.data_ptr()))
+    _check(lib().osr_flash_batch_instances(arr, len(fluids), _vp(start.ctypes.data), _vp(P.data_ptr()),
+                                           _vp(T.data_ptr()), _vp(z.data_ptr()), ctypes.c_long(n),
+                                           ctypes.byref(co), _vp(stream.cuda_stream)), "osr_flash_batch_instances")
+    return out
 
 
 def set_shape(ss_batch: int, tail_batch: int, ctas_per_sm: int, park_after: int):

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <vector>
 #include "osiris_b200.h"
 #include "flash_kernels.cuh"
 
@@ -164,11 +165,11 @@ static int pass_limits(int park_after, int *lim) {
     return np;
 }
 
-template <int N>
+template <int N, bool MULTI>
 static int queue_blocks(long n) {
     long warps_needed = (n + 31) / 32;
     int per_sm = g_ctas_per_sm.load(), fit = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N>, 128, 0) == cudaSuccess &&
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N, MULTI>, 128, 0) == cudaSuccess &&
         fit > 0 && per_sm > fit)
         per_sm = fit;
     long blocks = (long)sm_count() * per_sm;
@@ -178,11 +179,22 @@ static int queue_blocks(long n) {
     return (int)blocks;
 }
 
+// Several instances of one component count in one call: instance i owns
+// cells [start[i], start[i+1]) and its own component table (device copies).
+template <int N>
+struct Instances {
+    const FluidTable<N> *tables = nullptr;
+    const long *start = nullptr;
+    int n = 0;
+};
+
 template <int N>
 static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double *T, const double *z, long n,
-                              const osr_flash_out &o, cudaStream_t s, Form form, char *scratch) {
+                              const osr_flash_out &o, cudaStream_t s, Form form, char *scratch,
+                              Instances<N> inst = Instances<N>()) {
     FluidTable<N> table;
     make_table<N>(fl, table);
+    const bool multi = inst.tables != nullptr;
     FlashIO io{P, T, z, n, o.label, o.L, o.x, o.y, o.Zl, o.Zg, o.iters, o.rr_iters};
     if (form == Form::kPlain) {
         FlashArgs<N> a;
@@ -202,7 +214,10 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
         q.f = table;
         q.io = io;
         q.max_wait = g_max_wait.load();
-        const int blocks = queue_blocks<N>(n);
+        q.tables = inst.tables;
+        q.inst_start = inst.start;
+        q.n_inst = inst.n;
+        const int blocks = multi ? queue_blocks<N, true>(n) : queue_blocks<N, false>(n);
         for (int p = 0; p < np; p++) {
             q.first = p == 0;
             q.src = park_view(scratch, n, N, (p + 1) & 1);
@@ -212,7 +227,8 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
             q.head = heads + p;
             q.park_at = lim[p];
             q.ss_batch = p == 0 ? g_ss_batch.load() : g_tail_batch.load();
-            flash_queue_kernel<N><<<blocks, 128, 0, s>>>(q);
+            if (multi) flash_queue_kernel<N, true><<<blocks, 128, 0, s>>>(q);
+            else flash_queue_kernel<N, false><<<blocks, 128, 0, s>>>(q);
             OSR_CUDA(cudaGetLastError());
         }
     }
@@ -228,10 +244,14 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
         d.n = n;
         d.dlnphi_dx = o.dlnphi_dx;
         d.dlnphi_dP = o.dlnphi_dP;
+        d.tables = inst.tables;
+        d.inst_start = inst.start;
+        d.n_inst = inst.n;
         long blocks = (n + 127) / 128;
         long cap = (long)sm_count() * 8;
         if (blocks > cap) blocks = cap;
-        flash_deriv_kernel<N><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+        if (multi) flash_deriv_kernel<N, true><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+        else flash_deriv_kernel<N, false><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
         OSR_CUDA(cudaGetLastError());
     }
     return OSR_OK;
@@ -266,6 +286,34 @@ static osr_status flash_device(const osr_fluid *fluid, const double *P, const do
         cudaError_t e = cudaFreeAsync(scratch, s);
         if (st == OSR_OK && e != cudaSuccess) return cuda_fail(e);
     }
+    return st;
+}
+
+// Tables and instance offsets to the device, then the batched passes.
+template <int N>
+static osr_status run_instances_n(const osr_fluid *fluids, int n_inst, const long *start, const double *P,
+                                  const double *T, const double *z, long n, const osr_flash_out &o, cudaStream_t s,
+                                  char *scratch) {
+    std::vector<FluidTable<N>> tabs((size_t)n_inst);
+    for (int i = 0; i < n_inst; i++) make_table<N>(fluids[i], tabs[i]);
+    const size_t tb = (size_t)n_inst * sizeof(FluidTable<N>), sb = (size_t)(n_inst + 1) * sizeof(long);
+    char *dev = nullptr;
+    OSR_CUDA(pool_alloc((void **)&dev, ((tb + 255) & ~(size_t)255) + sb, s));
+    FluidTable<N> *dt = (FluidTable<N> *)dev;
+    long *ds = (long *)(dev + ((tb + 255) & ~(size_t)255));
+    osr_status st = OSR_OK;
+    cudaError_t e = cudaMemcpyAsync(dt, tabs.data(), tb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, start, sb, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) st = cuda_fail(e);
+    Instances<N> inst;
+    inst.tables = dt;
+    inst.start = ds;
+    inst.n = n_inst;
+    if (st == OSR_OK) st = run_flash_n<N>(fluids[0], P, T, z, n, o, s, Form::kQueue, scratch, inst);
+    // pageable-memory copies above are staged before they return, so the
+    // host tables may go out of scope
+    cudaError_t ef = cudaFreeAsync(dev, s);
+    if (st == OSR_OK && ef != cudaSuccess) return cuda_fail(ef);
     return st;
 }
 
@@ -323,6 +371,40 @@ osr_status osr_flash_batch_noalloc(const osr_fluid *fluid, const double *d_P, co
     // run_flash clears the scratch header (queue heads, parked counts) on
     // `stream` before the first pass; the parked lists are written before read.
     return run_flash(*fluid, d_P, d_T, d_z, n, *out, (cudaStream_t)stream, Form::kQueue, scratch);
+}
+
+osr_status osr_flash_batch_instances(const osr_fluid *fluids, int n_inst, const long *inst_start, const double *d_P,
+                                     const double *d_T, const double *d_z, long n, const osr_flash_out *out,
+                                     void *stream) {
+    if (!fluids || n_inst < 1 || !inst_start) return OSR_ERR_ARG;
+    const int nc = fluids[0].nc;
+    for (int i = 0; i < n_inst; i++) {
+        osr_status st = check_fluid(&fluids[i]);
+        if (st) return st;
+        if (fluids[i].nc != nc) return OSR_ERR_ARG;
+        if (inst_start[i + 1] < inst_start[i]) return OSR_ERR_ARG;
+    }
+    if (inst_start[0] != 0 || inst_start[n_inst] != n || n < 0) return OSR_ERR_ARG;
+    if (!out) return OSR_ERR_ARG;
+    if (n == 0) return OSR_OK;
+    osr_status st = check_out(out);
+    if (st) return st;
+    if (!d_P || !d_T || !d_z) return OSR_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *scratch = nullptr;
+    OSR_CUDA(pool_alloc((void **)&scratch, queue_scratch_bytes(n, nc), s));
+    switch (nc) {
+#define OSR_NC_CASE(K) \
+    case K: st = run_instances_n<K>(fluids, n_inst, inst_start, d_P, d_T, d_z, n, *out, s, scratch); break;
+        OSR_NC_CASE(1) OSR_NC_CASE(2) OSR_NC_CASE(3) OSR_NC_CASE(4) OSR_NC_CASE(5) OSR_NC_CASE(6)
+        OSR_NC_CASE(7) OSR_NC_CASE(8) OSR_NC_CASE(9) OSR_NC_CASE(10) OSR_NC_CASE(11) OSR_NC_CASE(12)
+        OSR_NC_CASE(13) OSR_NC_CASE(14) OSR_NC_CASE(15) OSR_NC_CASE(16)
+#undef OSR_NC_CASE
+        default: st = OSR_ERR_NC;
+    }
+    cudaError_t e = cudaFreeAsync(scratch, s);
+    if (st == OSR_OK && e != cudaSuccess) return cuda_fail(e);
+    return st;
 }
 
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,

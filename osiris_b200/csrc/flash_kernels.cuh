@@ -23,6 +23,12 @@
 // The plain kernel (one thread per cell, no queue) is kept as the baseline the
 // batched form is measured against.
 #pragma once
+
+// Resident 128-thread CTAs per SM the queue kernel is compiled for (bounds
+// its registers).
+#ifndef OSR_FLASH_MIN_BLOCKS
+#define OSR_FLASH_MIN_BLOCKS 3
+#endif
 #include "eos_device.cuh"
 
 namespace osr {
@@ -321,7 +327,30 @@ struct QueueArgs {
     int max_wait;                // ... or Newton trips the ready lanes have waited
     int park_at;                 // park a cell still running once it reaches this many SS steps
     int first;                   // 1: take cells [0, n) fresh; 0: resume src
+    // several instances (fluids) of one component count: cells
+    // [inst_start[i], inst_start[i+1]) use tables[i]
+    const FluidTable<N> *tables;
+    const long *inst_start;
+    int n_inst;
 };
+
+// Instance of cell c: the largest i with start[i] <= c.
+__device__ __forceinline__ int find_instance(const long *start, int n_inst, long c) {
+    int lo = 0, hi = n_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The component table of a cell: the kernel parameter, or its instance's.
+template <int N, bool MULTI, class Args>
+__device__ __forceinline__ const FluidTable<N> &table_of(const Args &a, int inst) {
+    if constexpr (MULTI) return a.tables[inst];
+    else return a.f;
+}
 
 // Batched form: persistent warps, a per-lane state machine and a global work
 // queue, run as a sequence of passes.  The first pass takes every cell; a
@@ -330,8 +359,8 @@ struct QueueArgs {
 // pass resumes the parked cells of the previous one with a doubled limit, so
 // every pass starts with fully populated warps instead of draining a few
 // long cells through mostly idle warps.
-template <int N>
-__global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant__ QueueArgs<N> a) {
+template <int N, bool MULTI>
+__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_queue_kernel(const __grid_constant__ QueueArgs<N> a) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const FlashIO &io = a.io;
@@ -342,6 +371,7 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
     double z[N], K[N], sa[N];
     int j = 0, k = 0, rr = 0;
     int waited = 0;  // warp-uniform: Newton trips since ready lanes appeared
+    int inst = 0;
     double big = 0;
 #pragma unroll
     for (int i = 0; i < N; i++) z[i] = K[i] = sa[i] = 0;
@@ -372,8 +402,9 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
                     T = io.T[c];
 #pragma unroll
                     for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
-                    if (a.first) flash_init<N>(a.f, P, T, K, sa);
-                    else sqrt_a<N>(a.f, T, sa);
+                    if constexpr (MULTI) inst = find_instance(a.inst_start, a.n_inst, c);
+                    if (a.first) flash_init<N>(table_of<N, MULTI>(a, inst), P, T, K, sa);
+                    else sqrt_a<N>(table_of<N, MULTI>(a, inst), T, sa);
                     L = 0.6;
                     j = 0;
                     big = rr_bound<N>(K);
@@ -401,7 +432,7 @@ __global__ void __launch_bounds__(128) flash_queue_kernel(const __grid_constant_
             waited = 0;
             if (mode == kReady) {
                 double x[N], y[N], Zl, Zg;
-                double es = ss_update<N>(a.f, sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
+                double es = ss_update<N>(table_of<N, MULTI>(a, inst), sa, P, T, z, K, L, Lb, x, y, Zl, Zg);
                 rr += j;
                 k++;
                 if ((es > kSSTol) && (k < kSSMaxIt)) {
@@ -440,6 +471,9 @@ struct DerivArgs {
     const double *P, *T, *x, *y, *Zl, *Zg;
     long n;
     double *dlnphi_dx, *dlnphi_dP;
+    const FluidTable<N> *tables;   // several instances (see QueueArgs)
+    const long *inst_start;
+    int n_inst;
 };
 
 template <int N>
@@ -524,7 +558,7 @@ __device__ __forceinline__ void phase_derivs(const FluidTable<N> &f, const doubl
 }
 
 // One thread per (cell, phase); blockIdx.y selects the phase.
-template <int N>
+template <int N, bool MULTI>
 __global__ void __launch_bounds__(128) flash_deriv_kernel(const __grid_constant__ DerivArgs<N> a) {
     const int ph = blockIdx.y;
     const double *comp = ph ? a.y : a.x;
@@ -535,10 +569,13 @@ __global__ void __launch_bounds__(128) flash_deriv_kernel(const __grid_constant_
     for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += stride) {
         double sa[N], w[N];
         double T = a.T[c];
-        sqrt_a<N>(a.f, T, sa);
+        int inst = 0;
+        if constexpr (MULTI) inst = find_instance(a.inst_start, a.n_inst, c);
+        const FluidTable<N> &f = table_of<N, MULTI>(a, inst);
+        sqrt_a<N>(f, T, sa);
 #pragma unroll
         for (int i = 0; i < N; i++) w[i] = comp[(long)i * a.n + c];
-        phase_derivs<N>(a.f, sa, a.P[c], T, w, Zp[c], odx, odp, a.n, c);
+        phase_derivs<N>(f, sa, a.P[c], T, w, Zp[c], odx, odp, a.n, c);
     }
 }
 

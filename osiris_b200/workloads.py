@@ -49,6 +49,44 @@ def flash_cells(n: int, nc: int, seed: int = 3):
     return P, T, z
 
 
+INSTANCES = 4096
+
+
+def batched_instances(n_inst: int = INSTANCES, seed: int = 4, cells_lo: float = 1e3, cells_hi: float = 6.4e4,
+                      nc_lo: int = 3, nc_hi: int = 12):
+    """The uneven-instance workload: n_inst independent flash instances, each
+    with log-uniform cell count in [cells_lo, cells_hi], component count
+    uniform in {nc_lo..nc_hi}, PR or SRK with equal odds, and its own seeded
+    component table drawn as ``flash_table``'s.  Returns a list of dicts
+    (nc, eos, tc, pc, acf, kij, cells, seed)."""
+    rng = np.random.default_rng(seed)
+    cells = np.exp(rng.uniform(np.log(cells_lo), np.log(cells_hi), n_inst)).astype(np.int64)
+    ncs = rng.integers(nc_lo, nc_hi + 1, n_inst)
+    eos = rng.integers(0, 2, n_inst)
+    out = []
+    for i in range(n_inst):
+        s = int(seed) * 1_000_003 + i
+        tc, pc, acf, kij = flash_table(int(ncs[i]), s)
+        out.append(dict(nc=int(ncs[i]), eos=int(eos[i]), tc=tc, pc=pc, acf=acf, kij=kij, cells=int(cells[i]), seed=s))
+    return out
+
+
+def instance_group(instances, nc: int, seed: int = 5):
+    """The instances with nc components, concatenated: (members, start [m+1],
+    P [n], T [n], z [nc, n]) with P ~ U(5, 40) MPa, T ~ U(300, 450) K and
+    z ~ Dirichlet(1) per cell (seeded per group)."""
+    members = [d for d in instances if d["nc"] == nc]
+    start = np.zeros(len(members) + 1, np.int64)
+    start[1:] = np.cumsum([d["cells"] for d in members])
+    n = int(start[-1])
+    rng = np.random.default_rng(seed * 1000 + nc)
+    P = rng.uniform(5e6, 40e6, n)
+    T = rng.uniform(300.0, 450.0, n)
+    g = rng.standard_gamma(1.0, (nc, n))
+    z = np.ascontiguousarray(g / g.sum(axis=0, keepdims=True))
+    return members, start, P, T, z
+
+
 def fluid_c1_nc4_nc10():
     tc = np.array([190.6, 425.1, 617.7])
     pc = np.array([4.599e6, 3.796e6, 2.110e6])
