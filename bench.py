@@ -7,6 +7,13 @@ phase labels, phase fractions, compositions, compressibilities and the
 fugacity derivative blocks of both phases.  Inputs are resident in HBM when
 the timed region starts; L2 is flushed (256 MiB write) before every step.
 
+A third object, ``instances``, flashes 4,096 independent instances of uneven
+size (log-uniform 1,000-64,000 cells, 3-12 components, PR or SRK, each with
+its own seeded component table; about 62 M cells) with one multi-instance
+batched call per component count, the calls on separate streams; beside it
+the one-instance-per-launch forms and the reference's CPU flash, each
+measured on a sample of instances and extrapolated.
+
 A second measured object, ``assembly``, times the full Newton-step assembly
 (FormFunction then FormJacobian) on a 128x128x32 dual-porosity grid (2 x
 524,288 cell-media), PR, 8 components, all cells two-phase: UpdateAll, the
@@ -50,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-assembly", action="store_true")
+    ap.add_argument("--no-instances", action="store_true")
+    ap.add_argument("--instances", type=int, default=None, help="instances of the uneven-instance object (4096)")
     ap.add_argument("--part", choices=["all", "assembly"], default="all",
                     help="assembly: only the Newton-step assembly object (profiling)")
     ap.add_argument("--assembly-grid", default=None, help="NX,NY,NZ of the assembly grid (default 128,128,32)")
@@ -71,6 +80,41 @@ def _cpu_worker_init(lo, hi, n_total):
     _W["P"] = np.ascontiguousarray(P[lo:hi])
     _W["T"] = np.ascontiguousarray(T[lo:hi])
     _W["z"] = np.ascontiguousarray(z[:, lo:hi])
+
+
+def _cpu_inst_init(items):
+    import oracle
+    _W["inst"] = [(oracle.Fluid(d["tc"], d["pc"], d["acf"], d["kij"], d["eos"]), P, T, z) for d, P, T, z in items]
+
+
+def _cpu_inst_run(_):
+    import oracle
+    t = time.perf_counter()
+    for fl, P, T, z in _W["inst"]:
+        oracle.ref_flash_batch(fl, P, T, z)
+    return time.perf_counter() - t
+
+
+class CpuInstances:
+    """The reference's SuccFalsh over a sample of instances, the instances
+    dealt round-robin to one spawned process per core."""
+
+    def __init__(self, items, cores: int | None = None):
+        self.cores = cores or len(os.sched_getaffinity(0))
+        ctx = mp.get_context("spawn")
+        shards = [items[i::self.cores] for i in range(self.cores)]
+        self.pools = [ctx.Pool(1, initializer=_cpu_inst_init, initargs=(sh,)) for sh in shards if sh]
+
+    def step(self) -> float:
+        t = time.perf_counter()
+        rs = [p.apply_async(_cpu_inst_run, (0,)) for p in self.pools]
+        for r in rs:
+            r.get()
+        return time.perf_counter() - t
+
+    def close(self):
+        for p in self.pools:
+            p.terminate()
 
 
 def _cpu_worker_run(_):
@@ -199,6 +243,124 @@ def _traffic_from_profiles():
             except ValueError:
                 return None
     return None
+
+
+def instance_groups(args, rank):
+    """The uneven-instance workload grouped by component count (host arrays)."""
+    from osiris_b200 import workloads
+    insts = workloads.batched_instances(n_inst=args.instances or workloads.INSTANCES, seed=4)
+    groups = []
+    for nc in sorted({d["nc"] for d in insts}):
+        members, start, P, T, z = workloads.instance_group(insts, nc, seed=5 + rank)
+        groups.append(dict(nc=nc, members=members, start=start, P=P, T=T, z=z))
+    return insts, groups
+
+
+def cpu_instance_sample(groups, k: int = 64):
+    """Every (n_inst / k)-th instance with its cells, for the CPU baseline."""
+    flat = [(g, i) for g in groups for i in range(len(g["members"]))]
+    step = max(1, len(flat) // k)
+    items = []
+    for g, i in flat[::step][:k]:
+        a, b = int(g["start"][i]), int(g["start"][i + 1])
+        items.append((g["members"][i], g["P"][a:b].copy(), g["T"][a:b].copy(), g["z"][:, a:b].copy()))
+    return items
+
+
+def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max_over_ranks, gpu_id, world, cpu):
+    """The uneven-instance flash: one osr_flash_batch_instances call per
+    component count, the calls on separate streams inside one timed step."""
+    import numpy as np
+    G = []
+    for g in groups:
+        fl = [osr.Fluid(d["tc"], d["pc"], d["acf"], d["kij"], d["eos"]) for d in g["members"]]
+        t = dict(nc=g["nc"], start=g["start"], fluids=fl, n=int(g["start"][-1]),
+                 P=torch.from_numpy(g["P"]).to(dev), T=torch.from_numpy(g["T"]).to(dev),
+                 z=torch.from_numpy(g["z"]).to(dev), stream=torch.cuda.Stream(dev))
+        t["out"] = osr.alloc_flash_outputs(g["nc"], t["n"], True, dev)
+        G.append(t)
+    n_total = sum(t["n"] for t in G)
+    n_inst = sum(len(t["fluids"]) for t in G)
+
+    def step():
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        ends = []
+        for t in G:
+            t["stream"].wait_event(ev)
+            osr.flash_instances(t["fluids"], t["start"], t["P"], t["T"], t["z"], derivs=True, out=t["out"],
+                                stream=t["stream"])
+            e = torch.cuda.Event()
+            e.record(t["stream"])
+            ends.append(e)
+        for e in ends:
+            stream.wait_event(e)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = ClockSampler(gpu_id)
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        step()
+        s1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(s0.elapsed_time(s1))
+    clk = clocks.stop()
+    barrier()
+    m = max_over_ranks(sum(ms) / len(ms))
+    two_phase = float(sum(float((t["out"]["label"] == 0).sum().item()) for t in G) / n_total)
+    # one instance per launch (plain kernel; batched kernel), on every 16th instance
+    flat = [(t, i) for t in G for i in range(len(t["fluids"]))]
+    sample = flat[::16]
+    prep = []
+    for t, i in sample:
+        a, b = int(t["start"][i]), int(t["start"][i + 1])
+        prep.append((t["fluids"][i], t["P"][a:b].contiguous(), t["T"][a:b].contiguous(),
+                     t["z"][:, a:b].contiguous()))
+    forms = {}
+    for form in ("plain", "batched"):
+        osr.flash(*prep[0], derivs=True, form=form)
+        torch.cuda.synchronize(dev)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for fl, P, T, z in prep:
+            osr.flash(fl, P, T, z, derivs=True, form=form)
+        s1.record(stream)
+        torch.cuda.synchronize(dev)
+        sample_cells = sum(int(P.shape[0]) for _, P, _, _ in prep)
+        sec = s0.elapsed_time(s1) * 1e-3
+        forms[form] = {"value": sample_cells / sec, "instances_sampled": len(prep), "cells_sampled": sample_cells,
+                       "ms_sample": sec * 1e3}
+    cpu_line = None
+    if cpu is not None:
+        cpu.step()
+        sec = cpu.step()
+        cpu.close()
+        cpu_cells = cpu.cells
+        cpu_line = {"value": cpu_cells / sec, "unit": "cells/s", "cores": cpu.cores, "kind": "reference",
+                    "sample": f"{cpu.n_inst} instances ({cpu_cells} cells), every {n_inst // cpu.n_inst}-th, "
+                              f"reference SuccFalsh, one process per core"}
+    for t in G:
+        del t["out"], t["P"], t["T"], t["z"]
+    torch.cuda.empty_cache()
+    return {
+        "metric": "uneven-instance flash+Jacobian cells/s", "value": world * n_total / (m * 1e-3), "unit": "cells/s",
+        "ms_per_step": m,
+        "config": {"workload": f"{n_inst} instances, log-uniform 1,000-64,000 cells, 3-12 components, PR or SRK, "
+                               "seeded tables; P~U(5,40) MPa, T~U(300,450) K, z~Dirichlet(1); with fugacity "
+                               "derivatives", "cells": n_total, "instances": n_inst,
+                   "calls_per_step": len(G), "streams": len(G), "two_phase_fraction": two_phase,
+                   "l2": "flushed before every step (256 MiB write)"},
+        "one_instance_per_launch": forms,
+        "batched_over_plain": (world * n_total / (m * 1e-3)) / forms["plain"]["value"],
+        "cpu_baseline": cpu_line,
+        "clocks": clk,
+    }
 
 
 def structural_values(nx: int, ny: int, nz: int, nc: int) -> int:
@@ -338,12 +500,20 @@ def run_ours(args):
             print(json.dumps(a), flush=True)
         return 0
 
-    # the CPU pool is spawned before the first GPU call
+    # the CPU pools are spawned before the first GPU call
     cpu = None
+    inst_groups, cpu_inst = None, None
+    if not args.no_instances:
+        _, inst_groups = instance_groups(args, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
             cpu = CpuReference(n)
+            if inst_groups is not None:
+                items = cpu_instance_sample(inst_groups)
+                cpu_inst = CpuInstances(items)
+                cpu_inst.cells = sum(int(P.shape[0]) for _, P, _, _ in items)
+                cpu_inst.n_inst = len(items)
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -462,6 +632,11 @@ def run_ours(args):
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         assembly = measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier, max_over_ranks, gpu_id)
 
+    instances = None
+    if inst_groups is not None:
+        instances = measure_instances(osr, torch, dev, stream, flush, args, inst_groups, barrier, max_over_ranks,
+                                      gpu_id, world, cpu_inst)
+
     cpu_line = None
     if cpu is not None:
         cpu.step()  # warm the workers (library load, first-touch)
@@ -504,6 +679,8 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_line
     if assembly is not None:
         line["assembly"] = assembly
+    if instances is not None:
+        line["instances"] = instances
     try:
         import json as _j
         peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
