@@ -42,7 +42,7 @@ struct osr_grid {
     // injection-well index, injected gas compositions, unsupported-cell count
     double *jw_q = nullptr, *jw_pi = nullptr, *j_stream_y = nullptr;
     int *jw_iw = nullptr;
-    double *j_dmu = nullptr, *j_dh = nullptr;   // Jacobian derivative tables [2][N+1][2 cells], [2][5+N][2 cells]
+    double *j_dmu = nullptr, *j_dh = nullptr;   // Jacobian derivative tables [2][N+1][2 cells], [2][8+2N][2 cells]
 };
 
 namespace osr {

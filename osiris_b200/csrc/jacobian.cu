@@ -31,39 +31,36 @@ __global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_cons
         osrj::prep_cell<N>(v, b);
 }
 
-// One warp per (32 consecutive block rows, row task) of one kind (see
-// jacobian_task_kind): component rows take tasks 0..N-2, the total rows task
-// N-1, the fugacity / water / constraint rows task N.  Each thread's
-// per-component accumulators: 3N doubles of dynamic shared memory.
+// One warp per (32 consecutive block rows, task) of one kind (see
+// jacobian_task_kind): column kinds take tasks k = 0..N-1, the others one
+// task.  Each thread's per-row sums: 3N (columns) or 4N (pressure and
+// saturations) doubles of dynamic shared memory.
 template <int KIND>
 __global__ void __launch_bounds__(kRowThreads, OSR_JAC_MIN_BLOCKS) jacobian_rows_kernel(const __grid_constant__ osrj::JacView v,
                                                                    long chunk0, long chunks) {
     extern __shared__ double s_acc[];
-    const int N = v.nc;
-    const int T = KIND <= 1 ? N - 1 : 1;
+    const int T = KIND <= 1 ? v.nc : 1;
     const int lane = threadIdx.x & 31;
     const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-    osrj::Acc a;
-    a.X = s_acc + threadIdx.x;
-    a.Y = s_acc + N * kRowThreads + threadIdx.x;
-    a.Z = s_acc + 2 * N * kRowThreads + threadIdx.x;
-    a.stride = kRowThreads;
     const long items = chunks * T;
     for (long it = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nwarps) {
         const long cq = it / T;
-        const int tt = (int)(it - cq * T);
-        const int task = KIND <= 1 ? tt : (KIND == 2 ? N - 1 : N);
-        osrj::jacobian_task_kind<KIND>(v, (chunk0 + cq) * 32 + lane, task, a);
+        const int task = (int)(it - cq * T);
+        osrj::jacobian_task_kind<KIND>(v, (chunk0 + cq) * 32 + lane, task, s_acc + threadIdx.x, kRowThreads);
     }
 }
 
 template <int KIND>
-static osr_status launch_rows(const osrj::JacView &v, long chunk0, long chunks, int tasks, cudaStream_t st) {
+static osr_status launch_rows(const osrj::JacView &v, long chunk0, long chunks, cudaStream_t st) {
+    const int tasks = KIND <= 1 ? v.nc : 1;
     const long items = chunks * tasks;
     if (items <= 0) return OSR_OK;
     long rb = (items * 32 + kRowThreads - 1) / kRowThreads;
     if (rb > 148L * 64) rb = 148L * 64;
-    jacobian_rows_kernel<KIND><<<(unsigned)rb, kRowThreads, (size_t)3 * v.nc * kRowThreads * 8, st>>>(v, chunk0, chunks);
+    const size_t smem = KIND == 4 ? 0 : (size_t)(KIND <= 1 ? 3 : 4) * v.nc * kRowThreads * 8;
+    if (smem > 48 * 1024)
+        JAC_CUDA(cudaFuncSetAttribute(jacobian_rows_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    jacobian_rows_kernel<KIND><<<(unsigned)rb, kRowThreads, smem, st>>>(v, chunk0, chunks);
     JAC_CUDA(cudaGetLastError());
     return OSR_OK;
 }
@@ -211,10 +208,11 @@ static osr_status jacobian_n(osr_grid &g, double sim_time, double *vals, cudaStr
     jac_prep_kernel<N><<<(unsigned)blocks, kRowThreads, 0, st>>>(v);
     JAC_CUDA(cudaGetLastError());
     const long chunks = (nb + 31) / 32, mchunks = (g.cells + 31) / 32, fchunk0 = g.cells / 32;
-    if ((s = launch_rows<0>(v, 0, mchunks, N - 1, st)) != OSR_OK) return s;
-    if ((s = launch_rows<1>(v, fchunk0, chunks - fchunk0, N - 1, st)) != OSR_OK) return s;
-    if ((s = launch_rows<2>(v, 0, chunks, 1, st)) != OSR_OK) return s;
-    return launch_rows<3>(v, 0, chunks, 1, st);
+    if ((s = launch_rows<0>(v, 0, mchunks, st)) != OSR_OK) return s;
+    if ((s = launch_rows<1>(v, fchunk0, chunks - fchunk0, st)) != OSR_OK) return s;
+    if ((s = launch_rows<2>(v, 0, mchunks, st)) != OSR_OK) return s;
+    if ((s = launch_rows<3>(v, fchunk0, chunks - fchunk0, st)) != OSR_OK) return s;
+    return launch_rows<4>(v, 0, chunks, st);
 }
 
 static osr_status ensure_jacobian_scratch(osr_grid &g) {
@@ -224,7 +222,7 @@ static osr_status ensure_jacobian_scratch(osr_grid &g) {
     JAC_CUDA(cudaMalloc((void **)&g.jw_pi, nb * 3 * 8));
     JAC_CUDA(cudaMalloc((void **)&g.jw_iw, nb * sizeof(int)));
     JAC_CUDA(cudaMalloc((void **)&g.j_dmu, (size_t)nb * 2 * (g.nc + 1) * 8));
-    if (!g.const_dif) JAC_CUDA(cudaMalloc((void **)&g.j_dh, (size_t)nb * 2 * (g.nc + 5) * 8));
+    if (!g.const_dif) JAC_CUDA(cudaMalloc((void **)&g.j_dh, (size_t)nb * 2 * (2 * g.nc + 8) * 8));
     const int nw = g.nwells > 0 ? g.nwells : 1;
     JAC_CUDA(cudaMalloc((void **)&g.j_stream_y, (size_t)nw * osrj::kMaxNc * 8));
     JAC_CUDA(cudaMemset(g.j_stream_y, 0, (size_t)nw * osrj::kMaxNc * 8));

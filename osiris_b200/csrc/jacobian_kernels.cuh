@@ -38,9 +38,11 @@
 // lanes of the last chunk beyond the grid): no clearing pass, no
 // read-modify-write.
 //
-// Work decomposition: a warp takes 32 consecutive block rows and one row task
-// -- component row i (tasks 0..N-2), the total row (task N-1), or the
-// fugacity, water and constraint rows together (task N).  Viscosity
+// Work decomposition: a warp takes 32 consecutive block rows and one task --
+// a composition column k of all component and total rows, their pressure
+// and saturation columns, or the fugacity, water and constraint rows.  The
+// face factors of a (face, phase, column) are shared by all rows, so a
+// column task evaluates them once and applies them row by row.  Viscosity
 // derivatives and the composition sums of the diffusion-coefficient
 // derivatives are tabulated per cell-medium by a preparation kernel, so an
 // entry costs O(1).
@@ -106,7 +108,7 @@ struct JacView {
     const double *stream_y;   // [wells][kMaxNc] injected gas composition
     // derivative tables (written by the preparation kernel)
     double *dmu;   // [2 phases][N+1][2 cells]: d mu / d w_k (k < N), d mu / d P (k = N)
-    double *dh;    // [2 phases][5+N][2 cells]: composition sums of d D / d w (see prep_cell)
+    double *dh;    // [2 phases][8+2N][2 cells]: factors of d D / d w (see prep_cell)
     // output
     double *vals;  // [chunks of 32 block rows][entries][32]
     int entries;   // values per block row
@@ -217,10 +219,11 @@ struct Cell {
 
 // One cell-medium's tables.  dmu: d mu / d w_k (k < N) or d mu / d P (k == N)
 // of each phase (DiffVisco / fDiffVisco, compsim/Mass_Tran.cpp:307-399).
-// dh: the composition sums of the diffusion-coefficient derivative
-// (DifDiffusion / fDifDiffusion, compsim/Mass_Tran.cpp:107-305):
-// s1 = sum w_j Vc_j^(5/3), s2 = sum w_j Vc_j^(2/3), Er = rho s1 / s2, AA(Er),
-// AA / rho and, per component i, Sm_i = sum_{j != i} w_j / pD_ji.
+// dh: the factors of the diffusion-coefficient derivative (DifDiffusion /
+// fDifDiffusion, compsim/Mass_Tran.cpp:107-305) that do not depend on the
+// column: s1 = sum w_j Vc_j^(5/3), s2 = sum w_j Vc_j^(2/3), s1/s2, 1/s2^2,
+// cA = dAA/dEr at Er = rho s1/s2, AA(Er), 1/rho^2, rho/AA, and per component
+// i, a2_i = Sm_i rho/AA with Sm_i = sum_{j != i} w_j / pD_ji, and 1/a2_i^2.
 template <int N>
 OSR_HD inline void prep_cell(const JacView &v, long bm) {
     const int med = bm >= v.n;
@@ -275,18 +278,24 @@ OSR_HD inline void prep_cell(const JacView &v, long bm) {
         }
         const double Ed = rho * d1 / d2;
         const double AA = 0.99589 + 0.096016 * Ed - 0.22035 * Ed * Ed + 0.032874 * Ed * Ed * Ed;
-        double *h = v.dh + (long)ph * (5 + N) * nb2 + bm;
+        const double iroRD = 1 / (AA / rho);
+        double *h = v.dh + (long)ph * (8 + 2 * N) * nb2 + bm;
         h[0] = d1;
         h[nb2] = d2;
-        h[2 * nb2] = Ed;
-        h[3 * nb2] = AA;
-        h[4 * nb2] = AA / rho;
+        h[2 * nb2] = d1 / d2;
+        h[3 * nb2] = 1 / (d2 * d2);
+        h[4 * nb2] = 0.096016 - 0.4407 * Ed + 0.098622 * Ed * Ed;
+        h[5 * nb2] = AA;
+        h[6 * nb2] = 1 / (rho * rho);
+        h[7 * nb2] = iroRD;
         for (int i = 0; i < N; i++) {
             double sm = 0;
 #pragma unroll
             for (int j = 0; j < N; j++)
                 if (j != i) sm += w[j] / v.pD[j * N + i];
-            h[(5 + i) * nb2] = sm;
+            const double a2 = sm * iroRD;
+            h[(8 + 2 * i) * nb2] = a2;
+            h[(9 + 2 * i) * nb2] = 1 / (a2 * a2);
         }
     }
 }
@@ -301,56 +310,46 @@ OSR_HD inline double dmu(const Cell &q, int k, int ph) {
 //   a2 = Sm_i / (AA/rho),  a1 = [k != i] / (pD_ki AA/rho) - G Sm_i / (AA/rho)^2,
 //   dD = -(a2 [k == i] + a1 (1 - w_i)) / a2^2.
 // Unlike the coefficient itself (CalcDiffusion) it carries no 1e-4 factor.
-// DDer holds the k-independent factors of one (cell-medium, phase, i).
-struct DDer {
-    double s1, s2, r12, is22, Er, cA, AA, rho, irho2, iroRD, a2, ia2sq, omw;
+// DCol is the part of one (cell-medium, phase, k): G and rho/AA; a row adds
+// a2_i, 1/a2_i^2 and w_i (dd_col).
+struct DCol {
+    double G, iroRD;
     bool zero;
 };
 
-OSR_HD inline DDer make_dder(const Cell &q, int i, int ph) {
+OSR_HD inline DCol make_dcol(const Cell &q, int k, int ph, double dEk) {
     const JacView &v = *q.v;
-    const int N = v.nc;
-    const long nb2 = 2 * v.n;
-    DDer d;
+    DCol d;
     if (v.const_dif) {
         d.zero = true;
         return d;
     }
-    const double *h = v.dh + (long)ph * (5 + N) * nb2 + q.bm();
-    d.s1 = ld(h);
-    d.s2 = ld(h + nb2);
-    d.Er = ld(h + 2 * nb2);
-    d.AA = ld(h + 3 * nb2);
-    const double roRD = ld(h + 4 * nb2), Sm = ld(h + (5 + i) * nb2);
-    d.rho = q.rho(ph);
-    d.r12 = d.s1 / d.s2;
-    d.is22 = 1 / (d.s2 * d.s2);
-    d.cA = 0.096016 - 0.4407 * d.Er + 0.098622 * d.Er * d.Er;
-    d.irho2 = 1 / (d.rho * d.rho);
-    d.iroRD = 1 / roRD;
-    d.a2 = Sm * d.iroRD;
-    d.ia2sq = 1 / (d.a2 * d.a2);
-    d.omw = 1 - q.w(ph, i);
-    d.zero = d.AA < 0 || d.a2 == 0;
+    const int N = v.nc;
+    const long nb2 = 2 * v.n;
+    const double *h = v.dh + (long)ph * (8 + 2 * N) * nb2 + q.bm();
+    const double s1 = ld(h), s2 = ld(h + nb2), r12 = ld(h + 2 * nb2), is22 = ld(h + 3 * nb2), cA = ld(h + 4 * nb2);
+    const double AA = ld(h + 5 * nb2), irho2 = ld(h + 6 * nb2);
+    const double rho = q.rho(ph);
+    double dEr = dEk * r12;
+    if (k < N) dEr += rho * (v.vc53[k] * s2 - v.vc23[k] * s1) * is22;
+    d.G = (dEr * cA * rho - dEk * AA) * irho2;
+    d.iroRD = ld(h + 7 * nb2);
+    d.zero = AA < 0;
     return d;
 }
 
-// dEk: d rho / d w_k (k < N) or d rho / d P (k == N) of the same cell and phase.
-OSR_HD inline double dd_k(const JacView &v, const DDer &d, int i, int k, double dEk) {
+OSR_HD inline double dd_col(const JacView &v, const DCol &d, const Cell &q, int i, int k, int ph) {
     if (d.zero) return 0;
     const int N = v.nc;
-    double dEr = dEk * d.r12;
-    if (k < N) dEr += d.rho * (v.vc53[k] * d.s2 - v.vc23[k] * d.s1) * d.is22;
-    const double G = (dEr * d.cA * d.rho - dEk * d.AA) * d.irho2;
-    double a1 = -G * d.a2 * d.iroRD;
+    const long nb2 = 2 * v.n;
+    const double *h = v.dh + (long)ph * (8 + 2 * N) * nb2 + q.bm();
+    const double a2 = ld(h + (8 + 2 * i) * nb2);
+    if (a2 == 0) return 0;
+    const double ia2sq = ld(h + (9 + 2 * i) * nb2), omw = 1 - q.w(ph, i);
+    double a1 = -d.G * a2 * d.iroRD;
     if (k < N && k != i) a1 += v.ipD[k * N + i] * d.iroRD;
-    if (k == i) return -(d.a2 + a1 * d.omw) * d.ia2sq;
-    return -a1 * d.omw * d.ia2sq;
-}
-
-OSR_HD inline double dD(const Cell &q, int i, int k, int ph) {
-    if (q.v->const_dif) return 0;
-    return dd_k(*q.v, make_dder(q, i, ph), i, k, q.dE(k < q.v->nc ? k : q.v->nc, ph));
+    if (k == i) return -(a2 + a1 * omw) * ia2sq;
+    return -a1 * omw * ia2sq;
 }
 
 // ---------------------------------------------------------------------------
@@ -563,117 +562,6 @@ OSR_HD inline FaceQuirks comp_quirks(const JFace &e) {
     return q;
 }
 
-// ---------------------------------------------------------------------------
-// Accumulators of one component or total row.  The per-component ones live
-// in shared memory on the device (one column per thread: element k at
-// X[k * stride]).
-// ---------------------------------------------------------------------------
-struct Acc {
-    double dp, dSw, dSo, dSg;
-    double *X, *Y;   // d(flux + transfer) / d x_k, d y_k of this cell
-    double *Z;       // a one-phase neighbour's composition entries between the two phases
-    int stride;
-    OSR_HD double &x(int k) { return X[k * stride]; }
-    OSR_HD double &y(int k) { return Y[k * stride]; }
-    OSR_HD double &z(int k) { return Z[k * stride]; }
-};
-
-// Derivatives of row i's face terms with respect to the neighbour's pressure
-// and saturations (ps, canonical P Sw So Sg, or ov when the reference counts
-// them from the following block) and this cell's pressure and saturations
-// (accumulated).
-OSR_HD inline void face_ps(const JacView &v, const Cell &q, const Cell &nb, int i, const JFace &e, const FaceData &fd,
-                           const FaceQuirks &qk, bool fracture, bool total, Acc &acc, double *ps, double *ov) {
-    const int N = v.nc;
-    const double s = e.sgn;
-    const int lnb = nb.label(), lq = q.label();
-    const bool nb_o = upstream(e, fd, q.c, 0) == e.nb, nb_g = upstream(e, fd, q.c, 1) == e.nb;
-    const double xo = total ? 1.0 : (nb_o ? nb : q).w(0, i), yg = total ? 1.0 : (nb_g ? nb : q).w(1, i);
-    // the reference's four neighbour columns: P, Sw, So, and the hydrocarbon
-    // saturation (Sg, or a one-phase neighbour's own saturation)
-    const int cS2 = lnb == -1 ? 3 : 2, cS3 = lnb == 1 ? 2 : 3;
-    auto put = [&](int t, int cc, double val) {
-        if (qk.shifted_block) ov[t] = val;
-        else ps[cc] += val;
-    };
-    // saturation factors
-    const double dsw = s * (xo * fd.T[4] * fd.dP[1] + xo * fd.T[6] * fd.dH);
-    if (nb_o) put(1, 1, dsw);
-    else acc.dSw += dsw;
-    const double dso = s * (xo * fd.T[10] * fd.dP[1] + xo * fd.T[11] * fd.dH);
-    if (nb_o) put(2, cS2, lnb == -1 ? 0.0 : dso);
-    else acc.dSo += dso;
-    const double dsgo = s * (xo * fd.T[8] * fd.dP[1] + xo * fd.T[9] * fd.dH);
-    const double dsgg = s * (yg * fd.T[5] * fd.dP[2] + yg * fd.T[7] * fd.dH);
-    double vsg = 0;
-    if (nb_o) vsg = lnb == 1 ? 0.0 : dsgo;
-    else acc.dSg += dsgo;
-    if (nb_g) vsg += lnb == 1 ? 0.0 : dsgg;
-    else acc.dSg += dsgg;
-    put(3, cS3, vsg);
-    // mobility and diffusion derivatives with respect to the two pressures
-    const double tor_c = fracture ? 1.0 : ld(v.tor + q.c), tor_n = fracture ? 1.0 : ld(v.tor + e.nb);
-    const double pm = q.porpor(), dpm = q.dpordp();
-    const double pn = nb.porpor(), dpn = nb.dpordp();
-    const double NNd = e.area2 / (e.dn + e.dl);
-    const bool inactive = q.por() < 1e-10 || nb.por() < 1e-10;
-    double dB = 0;
-    for (int ph = 0; ph < 2; ph++) {
-        const double coef = ph == 0 ? (lnb == -1 ? 0.0 : 1.0) : (lnb == 1 ? 0.0 : 1.0);
-        const double dC = ph == 0 ? (lq == -1 ? 0.0 : 1.0) : (lq == 1 ? 0.0 : 1.0);
-        const Side sq{q.rho(ph), q.mu(ph), q.gam(ph)}, sn{nb.rho(ph), nb.mu(ph), nb.gam(ph)};
-        const double dEq = q.dE(N, ph), dEn = nb.dE(N, ph);
-        const Mob m = mobility(sq, sn, dEq, dEn, false, 0.0, e, coef, dmu(q, N, ph), dmu(nb, N, ph));
-        const bool up_nb = ph == 0 ? nb_o : nb_g;
-        const Cell &U = up_nb ? nb : q;
-        const double wk = total ? 1.0 : U.w(ph, i), krk = U.kr(1 + ph);
-        const double dPp = fd.dP[1 + ph];
-        const double a = wk * fd.ift * krk;
-        acc.dp -= s * (a * m.M * dPp);
-        const double vB = s * (a * m.B * dPp);
-        if (ph == 1 && e.sgn < 0) {
-            const bool assign = up_nb ? qk.gas_dB_assign_down : qk.gas_dB_assign_up;
-            dB = assign ? vB : dB + vB;
-            // the reference exchanges this cell's and the neighbour's gravity factors here
-            acc.dp -= s * (a * (m.B * m.tempdx + m.BG * m.Sur / m.Mak) * fd.dH);
-            dB += s * (a * (m.M * m.tempdx + m.MG * m.Sur / m.Mak) * fd.dH);
-        } else {
-            dB = ph == 0 ? vB : dB + vB;
-            acc.dp -= s * (a * (m.M * m.tempdx + m.MG * m.Sur / m.Mak) * fd.dH);
-            const double gB = s * (a * (m.B * m.tempdx + m.BG * m.Sur / m.Mak) * fd.dH);
-            if (ph == 0 && e.sgn < 0 && up_nb && qk.oil_grav_assign_down) dB = gB;
-            else dB += gB;
-        }
-        if (total || v.diff_off) continue;   // CDIF 0: the coefficient and its derivatives vanish
-        // intra-continuum diffusion
-        const double wq = q.w(ph, i), wn = nb.w(ph, i);
-        double Dup, dDdp, dDdp2;
-        if (wn > wq) {
-            Dup = nb.D(i, ph);
-            dDdp = 0;
-            dDdp2 = dD(nb, i, N, ph);
-        } else {
-            Dup = q.D(i, ph);
-            dDdp = dD(q, i, N, ph);
-            dDdp2 = 0;
-        }
-        if (inactive) Dup = dDdp = dDdp2 = 0;
-        double AAd = sn.rho * e.dn * coef + sq.rho * e.dl * dC;
-        AAd *= (nb.S(1 + ph) * e.dn * coef + q.S(1 + ph) * e.dl * dC) / (e.dn + e.dl);
-        const double BBd = tor_n * e.dn * coef / pn + tor_c * e.dl * dC / pm;
-        const double MMd = AAd / BBd;
-        const double DX = wn - wq;
-        const double dAA = dEq * e.dl * dC, dAA2 = dEn * e.dn * coef;
-        const double dBB = -dpm * tor_c * e.dl * dC / (pm * pm), dBB2 = -dpn * tor_n * e.dn * coef / (pn * pn);
-        const double dMM = (dAA * BBd - dBB * AAd) / (BBd * BBd), dMM2 = (dAA2 * BBd - dBB2 * AAd) / (BBd * BBd);
-        if (coef != 0 && dC != 0) {
-            acc.dp += -NNd * DX * (MMd * dDdp + Dup * dMM);
-            dB += NNd * DX * (MMd * dDdp2 + Dup * dMM2);
-        }
-    }
-    put(0, 0, v.pcoeff * (-xo * fd.T[0] - yg * fd.T[1] - dB));
-}
-
 // k-independent factors of one phase across one face for the composition
 // derivatives (the mobility-ratio and gravity denominators, the upstream
 // weights and the diffusion factors) at neighbour weight coef.
@@ -700,153 +588,6 @@ OSR_HD inline PhFace ph_face(const Side &sq, const Side &sn, const JFace &e, dou
     P.iBB = 1 / P.BBd;
     P.MMd = AAd * P.iBB;
     return P;
-}
-
-// Derivatives of row i's face terms with respect to the compositions of both
-// cells: the neighbour's entries are stored (both phases of a one-phase
-// neighbour land in its one composition column), this cell's accumulated.
-OSR_HD inline void face_x(const JacView &v, const Cell &q, const Cell &nb, int i, const JFace &e, const FaceData &fd,
-                          const FaceQuirks &qk, bool fracture, bool total, Acc &acc, const Out &out, int row) {
-    const int N = v.nc;
-    const Layout L(N);
-    const double s = e.sgn;
-    const int lnb = nb.label(), lq = q.label();
-    const double tor_c = fracture ? 1.0 : ld(v.tor + q.c), tor_n = fracture ? 1.0 : ld(v.tor + e.nb);
-    const double pm = q.porpor(), pn = nb.porpor();
-    const double NNd = e.area2 / (e.dn + e.dl);
-    const double ift_y = ld(q.F->iftran + v.n + q.c);
-    const bool idiff = !total && !v.diff_off;   // intra-continuum diffusion present
-    for (int ph = 0; ph < 2; ph++) {
-        const bool up_nb = upstream(e, fd, q.c, ph) == e.nb;
-        const Side sq{q.rho(ph), q.mu(ph), q.gam(ph)}, sn{nb.rho(ph), nb.mu(ph), nb.gam(ph)};
-        const double wc = total ? 1.0 : q.w(ph, i), wn = total ? 1.0 : nb.w(ph, i);
-        const double krq = q.kr(1 + ph), krn = nb.kr(1 + ph);
-        const double Sq = q.S(1 + ph), Sn = nb.S(1 + ph);
-        const double dC = ph == 0 ? (lq == -1 ? 0.0 : 1.0) : (lq == 1 ? 0.0 : 1.0);
-        // the neighbour weight off the diagonal (k != i) and on it
-        double coef_nd, coef_d;
-        if (ph == 0) coef_nd = coef_d = lnb == -1 ? 0.0 : 1.0;
-        else {
-            coef_d = lnb == 1 ? 0.0 : 1.0;
-            coef_nd = qk.gas_coef_any_1ph ? (lnb != 0 ? 0.0 : 1.0) : coef_d;
-        }
-        const PhFace base = ph_face(sq, sn, e, coef_nd, dC, Sq, Sn, tor_c, tor_n, pm, pn);
-        const double ac = wc * fd.ift * krq, an = wn * fd.ift * krn;
-        const double dPp = fd.dP[1 + ph];
-        // intra-continuum diffusion: the coefficient of the upstream (richer) cell
-        const bool dn_up = wn > wc;
-        const double Dup = idiff ? (dn_up ? nb.D(i, ph) : q.D(i, ph)) : 0.0;
-        const double DX = wn - wc;
-        DDer dd;
-        dd.zero = true;
-        if (idiff) dd = make_dder(dn_up ? nb : q, i, ph);
-        // this phase's column of the neighbour (a one-phase neighbour has one composition set)
-        const bool to_x = ph == 0 ? lnb != -1 : lnb == 1;
-        for (int k = 0; k < N; k++) {
-            const bool diag = !total && k == i;
-            PhFace P = base;
-            if (diag && coef_d != coef_nd) P = ph_face(sq, sn, e, coef_d, dC, Sq, Sn, tor_c, tor_n, pm, pn);
-            const double coef = P.coef;
-            const double dEq = q.dE(k, ph), dEn = nb.dE(k, ph);
-            const double mwk = v.mw[k];
-            const double M = (dEq * e.dl * P.Mak - dmu(q, k, ph) * e.dl * P.Sur) * P.iMak2;
-            const double B = (dEn * e.dn * coef * P.Mak - dmu(nb, k, ph) * e.dn * coef * P.Sur) * P.iMak2;
-            const double MG = e.dl * (kGAccG * sq.rho * mwk + P.gq * dEq) * P.iden;
-            const double BG = coef * e.dn * (kGAccG * sn.rho * mwk + P.gn * dEn) * P.iden;
-            const double gM = M * P.tempdx + MG * P.SurMak, gB = B * P.tempdx + BG * P.SurMak;
-            const double Tp = diag ? fd.T[ph] : 0.0, Tg = diag ? fd.T[2 + ph] : 0.0;
-            double dR = 0, dB;
-            if (up_nb) {
-                dR += s * (an * M * dPp);
-                dB = s * ((Tp + an * B) * dPp);
-            } else {
-                dR += s * ((Tp + ac * M) * dPp);
-                dB = s * (ac * B * dPp);
-            }
-            // gravity (nonzero across z faces only)
-            if (e.sgn > 0) {
-                if (up_nb) {
-                    const double ift_r = (diag && ph == 0 && qk.ift_y_in_diag_grav) ? ift_y : fd.ift;
-                    dR += wn * ift_r * krn * gM * fd.dH;
-                    dB += (Tg + an * gB) * fd.dH;
-                } else {
-                    dR += (Tg + ac * gM) * fd.dH;
-                    dB += ac * gB * fd.dH;
-                }
-            } else {
-                // - faces: the gas terms exchange the two cells' factors; with k != i
-                // the oil terms of a downstream cell change sign
-                const double g1 = ph == 1 ? gB : gM, g2 = ph == 1 ? gM : gB;
-                if (!up_nb) {
-                    dR -= (Tg + ac * g1) * fd.dH;
-                    dB -= ac * g2 * fd.dH;
-                } else {
-                    const double flip = (!diag && !total && ph == 0) ? -1.0 : 1.0;
-                    dR -= flip * (an * g1 * fd.dH);
-                    dB -= flip * ((Tg + an * g2) * fd.dH);
-                }
-            }
-            if (idiff && coef != 0 && dC != 0) {
-                const double dDx = dd_k(v, dd, i, k, dn_up ? dEn : dEq);
-                const double dDdx = dn_up ? 0.0 : dDx, dDdx2 = dn_up ? dDx : 0.0;
-                const double dMM = dEq * e.dl * dC * P.iBB, dMM2 = dEn * e.dn * coef * P.iBB;
-                dR += s * NNd * ((diag ? -P.MMd * Dup : 0.0) + dDdx * P.MMd * DX + dMM * Dup * DX);
-                dB += s * NNd * ((diag ? P.MMd * Dup : 0.0) + dDdx2 * P.MMd * DX + dMM2 * Dup * DX);
-            }
-            const double nv = -dB * coef;
-            if (ph == 0) {
-                acc.x(k) += dR;
-                if (lnb == 0) out.st(L.cr(row, e.slot, k), nv);
-                else acc.z(k) = nv;
-            } else {
-                acc.y(k) += dR;
-                if (lnb == 0) {
-                    out.st(L.cr(row, e.slot, N + k), nv);
-                } else {
-                    // both phases land in the neighbour's one composition column
-                    const double w = acc.z(k) + nv;
-                    out.st(L.cr(row, e.slot, k), to_x ? w : 0.0);
-                    out.st(L.cr(row, e.slot, N + k), to_x ? 0.0 : w);
-                }
-            }
-        }
-    }
-}
-
-// The face part of a component (total: the total) row: the advective terms of
-// this cell's pressure, then every face's neighbour block.  Slots of absent
-// faces are stored as zeros; the total row's shifted entries go to ov[8]
-// (-y face 0..3, -z face 4..7).
-OSR_HD inline void row_faces(const JacView &v, const Cell &q, int i, bool fracture, bool total, Acc &acc,
-                             const Out &out, int row, double *ov) {
-    const int N = v.nc;
-    const Layout L(N);
-    JFace fc[6];
-    const int nf = jac_faces(v, q.c, fc);
-    unsigned present = 0;
-    for (int f = 0; f < nf; f++) present |= 1u << fc[f].slot;
-    // advective flux, this cell's pressure
-    for (int ph = 0; ph < 2; ph++)
-        for (int f = 0; f < nf; f++) {
-            const FaceData fd = face_data(v, *q.F, q.c, fc[f]);
-            const double T = fd.T[ph];
-            acc.dp += total ? T : Cell{&v, q.F, upstream(fc[f], fd, q.c, ph), q.med}.w(ph, i) * T;
-        }
-    for (int f = 0; f < nf; f++) {
-        const JFace &e = fc[f];
-        const Cell nb{&v, q.F, e.nb, q.med};
-        const FaceData fd = face_data(v, *q.F, q.c, e);
-        const FaceQuirks qps = total ? total_quirks(e) : comp_quirks(e);
-        double ps[4] = {0, 0, 0, 0};
-        double *o = ov ? ov + (e.d == 1 ? 0 : 4) : nullptr;
-        face_ps(v, q, nb, i, e, fd, qps, fracture, total, acc, ps, o);
-        for (int t = 0; t < 4; t++) out.st(L.cr(row, e.slot, 2 * N + t), ps[t]);
-        const FaceQuirks qx = total ? FaceQuirks{false, false, false, false, false, false} : comp_quirks(e);
-        face_x(v, q, nb, i, e, fd, qx, fracture, total, acc, out, row);
-    }
-    for (int s = 1; s <= 6; s++)
-        if (!(present & (1u << s)))
-            for (int c = 0; c < L.BS; c++) out.st(L.cr(row, s, c), 0.0);
 }
 
 // Well rates of a completion cell at the linearisation point (written by the
@@ -900,356 +641,683 @@ OSR_HD inline void store_other_x(int N, const Out &out, int row, int lo, int k, 
 }
 
 // ---------------------------------------------------------------------------
-// Component balance row i (0 <= i < N-1) of a matrix cell.
+// Column decomposition of the component and total rows.
+//
+// Canonical rows N..2N-1 of a block row are the component balances i = 0..N-2
+// and the total row (i = N-1).  Their face terms share one factor set per
+// (face, phase, column): the mobility-ratio and gravity derivatives depend on
+// the two cells and the column, not on the row.  A column task computes the
+// x_k and y_k columns of all N rows in every block (own, six faces, the other
+// continuum), evaluating those factors once per (face, phase) and applying
+// them row by row; the pressure-saturation task does the same for the P, Sw,
+// So, Sg columns and the eight shifted entries.  Per-row sums are kept in
+// shared memory (SmemVec), in the order the reference adds their terms.
 // ---------------------------------------------------------------------------
-OSR_HD inline void matrix_comp_row(const JacView &v, long c, int i, const Out &out, Acc &a) {
-    const int N = v.nc;
-    const Layout L(N);
-    const int row = N + i;
-    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
-    const Transfer t = transfer_terms(v, c);
-    const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
-    const double Vb = t.Vb, SF1 = t.SF1, SF2 = t.SF2;
-    const double tor = ld(v.tor + c);
-    const int lm = M.label(), lf = Fr.label();
-    const double xi = M.w(0, i), yi = M.w(1, i);
-    const double ro = M.rho(0), rg = M.rho(1);
-    const double mubar_o = t.Do / (pm + pf), mubar_g = t.Dg / (pm + pf);
-    const double dLdp = (Vb / v.dt) * (xi * M.S(1) * (ro * dpm + M.dE(N, 0) * pm) + yi * M.S(2) * (rg * dpm + M.dE(N, 1) * pm));
-    const double dLdSo = (Vb / v.dt) * (xi * pm * ro), dLdSg = (Vb / v.dt) * (yi * pm * rg);
-    double dRfdp = 0;
-    a.dp = a.dSw = a.dSo = a.dSg = 0;
-    // transfer, this cell's pressure
-    a.dp += kSIC * M.dE(N, 0) * xi * SF2 * Vb * t.kro / mubar_o * t.dPo;
-    a.dp += -kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    a.dp += -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
-    a.dp += kSIC * dpm * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    a.dp += kSIC * M.dE(N, 1) * yi * SF2 * Vb * t.krg / mubar_g * t.dPg;
-    a.dp += -kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    a.dp += -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    a.dp += kSIC * dpm * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    // diffusive transfer, this cell's pressure
-    for (int ph = 0; ph < 2; ph++) {
-        int kinds[2];
-        const int nt = matrix_diff_targets(lm, lf, ph, kinds);
-        if (!nt) continue;
-        const double sat = M.S(1 + ph), rho = M.rho(ph), D = M.D(i, ph), w = M.w(ph, i);
-        const double dDdp = dD(M, i, N, ph);
-        for (int j = 0; j < nt; j++) {
-            const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
-            a.dp += dpm * SF1 * sat * Vb / tor * rho * D * (tgt - w);
-            a.dp += M.dE(N, ph) * SF1 * sat * pm * Vb / tor * D * (tgt - w);
-            a.dp += dDdp * SF1 * sat * pm * Vb / tor * rho * (tgt - w);
-        }
-    }
-    // transfer, the fracture's pressure
-    dRfdp += kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    dRfdp += -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
-    dRfdp += kSIC * dpf * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    dRfdp += kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    dRfdp += -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    dRfdp += kSIC * dpf * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    // saturations (transfer and diffusive transfer)
-    double dRfdSw = 0, dRfdSo = 0, dRfdSg = 0;
-    const double po = xi * ro * SF2 * Vb / mubar_o * t.dPo, pg = yi * rg * SF2 * Vb / mubar_g * t.dPg;
-    a.dSo += kSIC * t.dkm[4] * po;
-    {
-        int kinds[2];
-        const int nt = matrix_diff_targets(lm, lf, 0, kinds);
-        for (int j = 0; j < nt; j++) {
-            const double tgt = kinds[j] ? Fr.w(0, i) : 0.0;
-            a.dSo += SF1 * Vb * pm / tor * ro * M.D(i, 0) * (tgt - xi);
-        }
-    }
-    dRfdSo += kSIC * t.dkf[4] * po;
-    a.dSg += kSIC * t.dkm[2] * po;
-    a.dSg += kSIC * t.dkm[3] * pg;
-    {
-        // the gas saturation derivative omits the two-phase matrix / oil fracture pairing
-        int kinds[2];
-        int nt = matrix_diff_targets(lm, lf, 1, kinds);
-        if (lm == 0 && lf == 1) nt = 0;
-        for (int j = 0; j < nt; j++) {
-            const double tgt = kinds[j] ? Fr.w(1, i) : 0.0;
-            a.dSg += SF1 * Vb * pm / tor * rg * M.D(i, 1) * (tgt - yi);
-        }
-    }
-    dRfdSg += kSIC * t.dkf[2] * po;
-    dRfdSg += kSIC * t.dkf[3] * pg;
-    a.dSw += kSIC * t.dkm[1] * po;
-    dRfdSw += kSIC * t.dkf[1] * po;
-    // compositions: transfer terms and the fracture's block; the factors that
-    // do not depend on k first
-    double cdg[2], cx1[2], cx2[2], cf2[2], cd1[2], cdd[2], cd2[2], cfd[2];
-    bool dtr[2];
-    for (int ph = 0; ph < 2; ph++) {
-        const double w = ph ? yi : xi, rho = ph ? rg : ro, kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
-        const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
-        cdg[ph] = kSIC * rho * SF2 * Vb * kr / mub * dPp;
-        cx1[ph] = kSIC * w * SF2 * Vb * kr / mub * dPp;
-        cx2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pm + pf);
-        cf2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pm + pf);
-        cd1[ph] = cdd[ph] = cd2[ph] = cfd[ph] = 0;
-        int kinds[2];
-        const int nt = v.diff_off ? 0 : matrix_diff_targets(lm, lf, ph, kinds);
-        dtr[ph] = nt > 0;
-        const double sat = M.S(1 + ph), D = M.D(i, ph);
-        for (int j = 0; j < nt; j++) {
-            const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
-            cd1[ph] += SF1 * sat * pm * Vb / tor * D * (tgt - w);
-            cdd[ph] += -SF1 * sat * pm * Vb / tor * rho * D;
-            cd2[ph] += SF1 * sat * pm * Vb / tor * rho * (tgt - w);
-        }
-        // towards the fracture composition of the same phase (k == i)
-        bool on = (lm == 0 && lf == 0);
-        if (ph == 0) on = on || (lm == 1 && lf == 1) || (lm == 0 && lf == 1) || (lm == 1 && lf == 0);
-        else on = on || (lm == -1 && lf == -1) || (lm == 0 && lf == -1) || (lm == -1 && lf == 0);
-        if (on && !v.diff_off) cfd[ph] = SF1 * sat * pm * Vb / tor * rho * D;
-    }
-    for (int k = 0; k < N; k++) {
-        double dRx[2], dRfx[2];
-        const bool diag = k == i;
-        for (int ph = 0; ph < 2; ph++) {
-            const double dEk = M.dE(k, ph);
-            double dR = (diag ? cdg[ph] : 0.0) + dEk * cx1[ph] + dmu(M, k, ph) * cx2[ph];
-            if (dtr[ph]) dR += dEk * cd1[ph] + (diag ? cdd[ph] : 0.0) + dD(M, i, k, ph) * cd2[ph];
-            dRx[ph] = dR;
-            dRfx[ph] = dmu(Fr, k, ph) * cf2[ph] + (diag ? cfd[ph] : 0.0);
-        }
-        a.x(k) = dRx[0];
-        a.y(k) = dRx[1];
-        store_other_x(N, out, row, lf, k, dRfx[0], dRfx[1]);
-    }
-    // faces
-    row_faces(v, M, i, false, false, a, out, row, nullptr);
-    // this cell's block (with the completion's productivity terms)
-    const WellAt W = well_at(v, 0, c, i, yi);
-    store_own_ps(N, out, row, lm, v.pcoeff * (dLdp + a.dp + xi * W.PIo + W.gcomp * W.PIg), -a.dSw, dLdSo - a.dSo,
-                 dLdSg - a.dSg);
-    const OwnLayout O = own_layout(lm);
-    const double aol = (Vb / v.dt) * pm * M.S(1), aog = (Vb / v.dt) * pm * M.S(2);
-    for (int k = 0; k < N; k++) {
-        const bool diag = k == i;
-        const double dLxl = diag ? ro + xi * M.dE(k, 0) : xi * M.dE(k, 0);
-        const double dLxg = diag ? rg + yi * M.dE(k, 1) : yi * M.dE(k, 1);
-        const double dQxl = (diag && W.iwell < 0) ? W.Qo : 0.0, dQxg = (diag && W.iwell < 0) ? W.Qg : 0.0;
-        out.st(L.cr(row, 0, k), O.x ? aol * dLxl - dQxl - a.x(k) : 0.0);
-        out.st(L.cr(row, 0, N + k), O.y ? aog * dLxg - dQxg - a.y(k) : 0.0);
-    }
-    // the fracture's block
-    store_other_ps(N, out, row, lf, v.pcoeff * dRfdp, dRfdSw, dRfdSo, dRfdSg);
+
+// A per-thread vector in shared memory: element j at p[j * stride].
+struct SmemVec {
+    double *p;
+    int stride;
+    OSR_HD double &operator[](int j) const { return p[j * stride]; }
+};
+
+// This cell's factors of one phase across a face for column k at neighbour
+// weight coef: d(mobility ratio)/d w_k of this cell (M) and the neighbour (B)
+// and the gravity-weighted forms gM, gB.
+struct ColFac {
+    PhFace P;
+    double M, B, gM, gB;
+};
+
+OSR_HD inline ColFac col_fac(const Side &sq, const Side &sn, const JFace &e, double coef, double dC, double Sq,
+                             double Sn, double tor_c, double tor_n, double pm, double pn, double dEq, double dEn,
+                             double dmq, double dmn, double mwk) {
+    ColFac f;
+    f.P = ph_face(sq, sn, e, coef, dC, Sq, Sn, tor_c, tor_n, pm, pn);
+    const PhFace &P = f.P;
+    f.M = (dEq * e.dl * P.Mak - dmq * e.dl * P.Sur) * P.iMak2;
+    f.B = (dEn * e.dn * coef * P.Mak - dmn * e.dn * coef * P.Sur) * P.iMak2;
+    const double MG = e.dl * (kGAccG * sq.rho * mwk + P.gq * dEq) * P.iden;
+    const double BG = coef * e.dn * (kGAccG * sn.rho * mwk + P.gn * dEn) * P.iden;
+    f.gM = f.M * P.tempdx + MG * P.SurMak;
+    f.gB = f.B * P.tempdx + BG * P.SurMak;
+    return f;
 }
 
-// ---------------------------------------------------------------------------
-// Component balance row i of a fracture cell (the fracture case of
-// IteratorJacobian, compsim/Petsc_Functions.cpp:12756-18666).
-// ---------------------------------------------------------------------------
-OSR_HD inline void fracture_comp_row(const JacView &v, long c, int i, const Out &out, Acc &a) {
+// Column k (x_k and y_k) of all component and total rows of block row
+// (med, c): the transfer terms, the other continuum's block, every face, and
+// this cell's block.  accX, accY, accZ: N doubles each.
+OSR_HD inline void column_task(const JacView &v, int med, long c, int k, const Out &out, SmemVec accX, SmemVec accY,
+                               SmemVec accZ) {
     const int N = v.nc;
     const Layout L(N);
-    const int row = N + i;
     const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
+    const Cell &q = med ? Fr : M;
+    const int lm = M.label(), lf = Fr.label(), lq = q.label(), lo = med ? lm : lf;
+    const Transfer t = transfer_terms(v, c);
+    const double Vb = t.Vb, SF1 = t.SF1, SF2 = t.SF2, SF3 = t.SF3, pm = t.pm, pf = t.pf;
+    const double tor = ld(v.tor + c);
+    const double mubar_o = t.Do / (pm + pf), mubar_g = t.Dg / (pm + pf);
+    const double ro = M.rho(0), rg = M.rho(1);
+    const double dEkM[2] = {M.dE(k, 0), M.dE(k, 1)}, dEkF[2] = {Fr.dE(k, 0), Fr.dE(k, 1)};
+    const double dmM[2] = {dmu(M, k, 0), dmu(M, k, 1)}, dmF[2] = {dmu(Fr, k, 0), dmu(Fr, k, 1)};
+    const bool idiff = !v.diff_off;
+    DCol dcM[2], dcF[2];
+    for (int ph = 0; ph < 2; ph++) {
+        dcM[ph] = make_dcol(M, k, ph, dEkM[ph]);
+        dcF[ph] = make_dcol(Fr, k, ph, dEkF[ph]);
+    }
+    // 1) transfer terms of every row and the other continuum's block
+    for (int i = 0; i < N; i++) {
+        const int row = N + i;
+        const bool total = i == N - 1, diag = !total && i == k;
+        double rx[2], ox[2];
+        if (total) {
+            const double sg = med ? -1.0 : 1.0;
+            const double t1o = kSIC * SF2 * Vb * t.kro / mubar_o * t.dPo;
+            const double t2o = -kSIC * ro * SF2 * Vb * t.kro * pm / (t.Do * t.Do) * t.dPo * (pm + pf);
+            const double t3o = -kSIC * ro * SF2 * Vb * t.kro * pf / (t.Do * t.Do) * t.dPo * (pm + pf);
+            const double t1g = kSIC * SF2 * Vb * t.krg / mubar_g * t.dPg;
+            const double t2g = -kSIC * rg * SF2 * Vb * t.krg * pm / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+            const double t3g = -kSIC * rg * SF2 * Vb * t.krg * pf / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+            const double xm = dEkM[0] * t1o + dmM[0] * t2o, xf = dmF[0] * t3o;
+            const double ym = dEkM[1] * t1g + dmM[1] * t2g, yf = dmF[1] * t3g;
+            rx[0] = sg * (med ? xf : xm);
+            rx[1] = sg * (med ? yf : ym);
+            ox[0] = sg * (med ? xm : xf);
+            ox[1] = sg * (med ? ym : yf);
+        } else if (med == 0) {
+            // matrix component row i
+            const double xi = M.w(0, i), yi = M.w(1, i);
+            for (int ph = 0; ph < 2; ph++) {
+                const double w = ph ? yi : xi, rho = ph ? rg : ro, kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
+                const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
+                const double cdg = kSIC * rho * SF2 * Vb * kr / mub * dPp;
+                const double cx1 = kSIC * w * SF2 * Vb * kr / mub * dPp;
+                const double cx2 = -kSIC * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pm + pf);
+                const double cf2 = -kSIC * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pm + pf);
+                double dR = (diag ? cdg : 0.0) + dEkM[ph] * cx1 + dmM[ph] * cx2;
+                double dRf = dmF[ph] * cf2;
+                if (idiff) {
+                    int kinds[2];
+                    const int nt = matrix_diff_targets(lm, lf, ph, kinds);
+                    const double sat = M.S(1 + ph), D = M.D(i, ph);
+                    if (nt) {
+                        double cd1 = 0, cdd = 0, cd2 = 0;
+                        for (int j = 0; j < nt; j++) {
+                            const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
+                            cd1 += SF1 * sat * pm * Vb / tor * D * (tgt - w);
+                            cdd += -SF1 * sat * pm * Vb / tor * rho * D;
+                            cd2 += SF1 * sat * pm * Vb / tor * rho * (tgt - w);
+                        }
+                        dR += dEkM[ph] * cd1 + (diag ? cdd : 0.0) + dd_col(v, dcM[ph], M, i, k, ph) * cd2;
+                    }
+                    if (diag) {
+                        // towards the fracture composition of the same phase
+                        bool on = (lm == 0 && lf == 0);
+                        if (ph == 0) on = on || (lm == 1 && lf == 1) || (lm == 0 && lf == 1) || (lm == 1 && lf == 0);
+                        else on = on || (lm == -1 && lf == -1) || (lm == 0 && lf == -1) || (lm == -1 && lf == 0);
+                        if (on) dRf += SF1 * sat * pm * Vb / tor * rho * D;
+                    }
+                }
+                rx[ph] = dR;
+                ox[ph] = dRf;
+            }
+        } else {
+            // fracture component row i
+            const double xi = M.w(0, i), yi = M.w(1, i);
+            for (int ph = 0; ph < 2; ph++) {
+                const double w = ph ? yi : xi, rho = ph ? rg : ro, kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
+                const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
+                const double cdg = kSIC * rho * SF2 * Vb * kr / mub * dPp;
+                const double cx1 = kSIC * w * SF2 * Vb * kr / mub * dPp;
+                const double cx2 = -kSIC * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pf + pm);
+                const double cf2 = -kSIC * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pf + pm);
+                double dRM = -((diag ? cdg : 0.0) + dEkM[ph] * cx1 + dmM[ph] * cx2);
+                double dR = -(dmF[ph] * cf2);
+                if (idiff && fsf1(lm, lf, ph)) {
+                    const double msat = M.S(1 + ph), mD = M.D(i, ph), dlt = Fr.w(ph, i) - w;
+                    const double m1 = SF1 * msat * pm * Vb / tor * mD * dlt;
+                    const double mdd = -SF1 * msat * pm * Vb / tor * rho * mD;
+                    const double m2 = SF1 * msat * pm * Vb / tor * rho * dlt;
+                    dRM -= dEkM[ph] * m1 + (diag ? mdd : 0.0) + dd_col(v, dcM[ph], M, i, k, ph) * m2;
+                    if (diag) dR -= SF1 * msat * pm * Vb / tor * rho * mD;
+                }
+                if (idiff && fsf3(lm, lf, ph)) {
+                    const double fsat = Fr.S(1 + ph), frho = Fr.rho(ph), fD = Fr.D(i, ph), fw = Fr.w(ph, i);
+                    const double f3 = SF3 * fsat * pf * Vb / tor * fD * (fw - 0.0);
+                    const double f3d = SF3 * fsat * pf * Vb / tor * frho * fD;
+                    const double f32 = SF3 * fsat * pf * Vb / tor * frho * (fw - 0.0);
+                    dR -= dEkF[ph] * f3 + (diag ? f3d : 0.0) + dd_col(v, dcF[ph], Fr, i, k, ph) * f32;
+                }
+                rx[ph] = dR;
+                ox[ph] = dRM;
+            }
+        }
+        accX[i] = rx[0];
+        accY[i] = rx[1];
+        store_other_x(N, out, row, lo, k, ox[0], ox[1]);
+    }
+    // 2) faces: one factor set per (face, phase), applied to every row
+    JFace fc[6];
+    const int nf = jac_faces(v, c, fc);
+    unsigned present = 0;
+    const double ift_y = ld(q.F->iftran + v.n + c);
+    const double mwk = v.mw[k];
+    for (int f = 0; f < nf; f++) {
+        const JFace &e = fc[f];
+        present |= 1u << e.slot;
+        const Cell nb{&v, q.F, e.nb, med};
+        const FaceData fd = face_data(v, *q.F, c, e);
+        const int lnb = nb.label();
+        const FaceQuirks qk = comp_quirks(e);   // component rows; the total row has none
+        const double s = e.sgn;
+        const double tor_c = med ? 1.0 : tor, tor_n = med ? 1.0 : ld(v.tor + e.nb);
+        const double pq = q.porpor(), pn = nb.porpor();
+        const double NNd = e.area2 / (e.dn + e.dl);
+        for (int ph = 0; ph < 2; ph++) {
+            const bool up_nb = upstream(e, fd, c, ph) == e.nb;
+            const Side sq{q.rho(ph), q.mu(ph), q.gam(ph)}, sn{nb.rho(ph), nb.mu(ph), nb.gam(ph)};
+            const double krq = q.kr(1 + ph), krn = nb.kr(1 + ph), Sq = q.S(1 + ph), Sn = nb.S(1 + ph);
+            const double dC = ph == 0 ? (lq == -1 ? 0.0 : 1.0) : (lq == 1 ? 0.0 : 1.0);
+            // neighbour weight: standard (total row, diagonal row), and off the diagonal of the
+            // component rows, where the -x gas term drops any one-phase neighbour
+            const double coef_d = ph == 0 ? (lnb == -1 ? 0.0 : 1.0) : (lnb == 1 ? 0.0 : 1.0);
+            const double coef_nd = (ph == 1 && qk.gas_coef_any_1ph) ? (lnb != 0 ? 0.0 : 1.0) : coef_d;
+            const double dEq = q.dE(k, ph), dEn = nb.dE(k, ph), dmq = dmu(q, k, ph), dmn = dmu(nb, k, ph);
+            const ColFac fs = col_fac(sq, sn, e, coef_d, dC, Sq, Sn, tor_c, tor_n, pq, pn, dEq, dEn, dmq, dmn, mwk);
+            DCol dcn;
+            dcn.zero = true;
+            if (idiff) dcn = make_dcol(nb, k, ph, dEn);
+            const DCol &dcq = med ? dcF[ph] : dcM[ph];
+            const double dPp = fd.dP[1 + ph];
+            const bool to_x = ph == 0 ? lnb != -1 : lnb == 1;
+            for (int i = 0; i < N; i++) {
+                const int row = N + i;
+                const bool total = i == N - 1, diag = !total && i == k;
+                ColFac F = fs;
+                if (!total && !diag && coef_nd != coef_d)
+                    F = col_fac(sq, sn, e, coef_nd, dC, Sq, Sn, tor_c, tor_n, pq, pn, dEq, dEn, dmq, dmn, mwk);
+                const double coef = F.P.coef;
+                const double wc = total ? 1.0 : q.w(ph, i), wn = total ? 1.0 : nb.w(ph, i);
+                const double ac = wc * fd.ift * krq, an = wn * fd.ift * krn;
+                const double Tp = diag ? fd.T[ph] : 0.0, Tg = diag ? fd.T[2 + ph] : 0.0;
+                double dR = 0, dB;
+                if (up_nb) {
+                    dR += s * (an * F.M * dPp);
+                    dB = s * ((Tp + an * F.B) * dPp);
+                } else {
+                    dR += s * ((Tp + ac * F.M) * dPp);
+                    dB = s * (ac * F.B * dPp);
+                }
+                // gravity (nonzero across z faces only)
+                if (e.sgn > 0) {
+                    if (up_nb) {
+                        const double ift_r = (diag && ph == 0 && qk.ift_y_in_diag_grav) ? ift_y : fd.ift;
+                        dR += wn * ift_r * krn * F.gM * fd.dH;
+                        dB += (Tg + an * F.gB) * fd.dH;
+                    } else {
+                        dR += (Tg + ac * F.gM) * fd.dH;
+                        dB += ac * F.gB * fd.dH;
+                    }
+                } else {
+                    // - faces: the gas terms exchange the two cells' factors; with k != i
+                    // the oil terms of a downstream cell change sign
+                    const double g1 = ph == 1 ? F.gB : F.gM, g2 = ph == 1 ? F.gM : F.gB;
+                    if (!up_nb) {
+                        dR -= (Tg + ac * g1) * fd.dH;
+                        dB -= ac * g2 * fd.dH;
+                    } else {
+                        const double flip = (!diag && !total && ph == 0) ? -1.0 : 1.0;
+                        dR -= flip * (an * g1 * fd.dH);
+                        dB -= flip * ((Tg + an * g2) * fd.dH);
+                    }
+                }
+                // intra-continuum diffusion (component rows only)
+                if (idiff && !total && coef != 0 && dC != 0) {
+                    const bool dn_up = wn > wc;
+                    const double Dup = dn_up ? nb.D(i, ph) : q.D(i, ph);
+                    const double dDx = dn_up ? dd_col(v, dcn, nb, i, k, ph) : dd_col(v, dcq, q, i, k, ph);
+                    const double dDdx = dn_up ? 0.0 : dDx, dDdx2 = dn_up ? dDx : 0.0;
+                    const double DX = wn - wc;
+                    const double dMM = dEq * e.dl * dC * F.P.iBB, dMM2 = dEn * e.dn * coef * F.P.iBB;
+                    dR += s * NNd * ((diag ? -F.P.MMd * Dup : 0.0) + dDdx * F.P.MMd * DX + dMM * Dup * DX);
+                    dB += s * NNd * ((diag ? F.P.MMd * Dup : 0.0) + dDdx2 * F.P.MMd * DX + dMM2 * Dup * DX);
+                }
+                const double nv = -dB * coef;
+                if (ph == 0) {
+                    accX[i] += dR;
+                    if (lnb == 0) out.st(L.cr(row, e.slot, k), nv);
+                    else accZ[i] = nv;
+                } else {
+                    accY[i] += dR;
+                    if (lnb == 0) {
+                        out.st(L.cr(row, e.slot, N + k), nv);
+                    } else {
+                        // both phases land in the neighbour's one composition column
+                        const double w = accZ[i] + nv;
+                        out.st(L.cr(row, e.slot, k), to_x ? w : 0.0);
+                        out.st(L.cr(row, e.slot, N + k), to_x ? 0.0 : w);
+                    }
+                }
+            }
+        }
+    }
+    for (int sl = 1; sl <= 6; sl++)
+        if (!(present & (1u << sl)))
+            for (int i = 0; i < N; i++) {
+                out.st(L.cr(N + i, sl, k), 0.0);
+                out.st(L.cr(N + i, sl, N + k), 0.0);
+            }
+    // 3) this cell's block
+    const OwnLayout O = own_layout(lq);
+    const WellAt W = well_at(v, med, c, 0, 0.0);
+    for (int i = 0; i < N; i++) {
+        const int row = N + i;
+        const bool total = i == N - 1, diag = !total && i == k;
+        double X, Y;
+        if (total) {
+            const double po_ = med ? pf : pm;
+            const double dEq0 = med ? dEkF[0] : dEkM[0], dEq1 = med ? dEkF[1] : dEkM[1];
+            X = (Vb / v.dt) * po_ * q.S(1) * dEq0 - accX[i];
+            Y = (Vb / v.dt) * po_ * q.S(2) * dEq1 - accY[i];
+        } else {
+            const double dQxl = (diag && W.iwell < 0) ? W.Qo : 0.0, dQxg = (diag && W.iwell < 0) ? W.Qg : 0.0;
+            if (med == 0) {
+                const double xi = M.w(0, i), yi = M.w(1, i);
+                const double dLxl = diag ? ro + xi * dEkM[0] : xi * dEkM[0];
+                const double dLxg = diag ? rg + yi * dEkM[1] : yi * dEkM[1];
+                X = (Vb / v.dt) * pm * M.S(1) * dLxl - dQxl - accX[i];
+                Y = (Vb / v.dt) * pm * M.S(2) * dLxg - dQxg - accY[i];
+            } else {
+                const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
+                const double dLxl = diag ? Fr.rho(0) + fxi * dEkF[0] : fxi * dEkF[0];
+                const double dLxg = diag ? Fr.rho(1) + fyi * dEkF[1] : fyi * dEkF[1];
+                X = (Vb / v.dt) * pf * Fr.S(1) * dLxl - dQxl - accX[i];
+                Y = (Vb / v.dt) * pf * Fr.S(2) * dLxg - dQxg - accY[i];
+            }
+        }
+        out.st(L.cr(row, 0, k), O.x ? X : 0.0);
+        out.st(L.cr(row, 0, N + k), O.y ? Y : 0.0);
+    }
+}
+
+// The pressure and saturation columns (P, Sw, So, Sg) of all component and
+// total rows of block row (med, c) in every block, and the total row's eight
+// shifted entries.  dp, dSw, dSo, dSg: N doubles each.
+OSR_HD inline void ps_task(const JacView &v, int med, long c, const Out &out, SmemVec dp, SmemVec dSw, SmemVec dSo,
+                           SmemVec dSg) {
+    const int N = v.nc;
+    const Layout L(N);
+    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
+    const Cell &q = med ? Fr : M;
+    const int lm = M.label(), lf = Fr.label(), lq = q.label(), lo = med ? lm : lf;
     const Transfer t = transfer_terms(v, c);
     const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
     const double Vb = t.Vb, SF1 = t.SF1, SF2 = t.SF2, SF3 = t.SF3;
     const double tor = ld(v.tor + c);
-    const int lm = M.label(), lf = Fr.label();
-    const double xi = M.w(0, i), yi = M.w(1, i);         // matrix compositions (transfer terms)
-    const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
-    const double ro = M.rho(0), rg = M.rho(1);
-    const double mubar_o = t.Do / (pf + pm), mubar_g = t.Dg / (pf + pm);
-    const double dLdp = (Vb / v.dt) * (fxi * Fr.S(1) * (Fr.rho(0) * dpf + Fr.dE(N, 0) * pf) + fyi * Fr.S(2) * (Fr.rho(1) * dpf + Fr.dE(N, 1) * pf));
-    const double dLdSo = (Vb / v.dt) * (fxi * pf * Fr.rho(0)), dLdSg = (Vb / v.dt) * (fyi * pf * Fr.rho(1));
-    double dRMdp = 0;
-    a.dp = a.dSw = a.dSo = a.dSg = 0;
-    // transfer, the matrix pressure
-    dRMdp -= kSIC * M.dE(N, 0) * xi * SF2 * Vb * t.kro / mubar_o * t.dPo;
-    dRMdp -= -kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    dRMdp -= -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
-    dRMdp -= kSIC * dpm * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    dRMdp -= kSIC * M.dE(N, 1) * yi * SF2 * Vb * t.krg / mubar_g * t.dPg;
-    dRMdp -= -kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    dRMdp -= -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
-    dRMdp -= kSIC * dpm * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    for (int ph = 0; ph < 2; ph++) {
-        if (!fsf1(lm, lf, ph)) continue;
-        const double sat = M.S(1 + ph), rho = M.rho(ph), D = M.D(i, ph), dlt = Fr.w(ph, i) - M.w(ph, i);
-        dRMdp -= dpm * SF1 * sat * Vb / tor * rho * D * dlt;
-        dRMdp -= M.dE(N, ph) * SF1 * sat * pm * Vb / tor * D * dlt;
-        dRMdp -= dD(M, i, N, ph) * SF1 * sat * pm * Vb / tor * rho * dlt;
-    }
-    // transfer, this (fracture) cell's pressure
-    a.dp -= kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
-    a.dp -= -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
-    a.dp -= kSIC * dpf * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    a.dp -= kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
-    a.dp -= -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
-    a.dp -= kSIC * dpf * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    for (int ph = 0; ph < 2; ph++) {
-        if (!fsf3(lm, lf, ph)) continue;
-        const double sat = Fr.S(1 + ph), rho = Fr.rho(ph), D = Fr.D(i, ph), w = Fr.w(ph, i);
-        a.dp -= dpf * SF3 * sat * Vb / tor * rho * D * (w - 0.0);
-        a.dp -= Fr.dE(N, ph) * SF3 * sat * pf * Vb / tor * D * (w - 0.0);
-        a.dp -= dD(Fr, i, N, ph) * SF3 * sat * pf * Vb / tor * rho * (w - 0.0);
-    }
-    // saturations
-    double dRMdSo = 0, dRMdSg = 0, dRMdSw = 0;
-    const double po = xi * ro * SF2 * Vb / mubar_o * t.dPo, pg = yi * rg * SF2 * Vb / mubar_g * t.dPg;
-    dRMdSo -= kSIC * t.dkm[4] * po;
-    if (fsf1(lm, lf, 0)) dRMdSo -= SF1 * Vb * pm / tor * ro * M.D(i, 0) * (fxi - xi);
-    a.dSo -= kSIC * t.dkf[4] * po;
-    if (fsf3(lm, lf, 0)) a.dSo -= SF3 * Vb * pf / tor * Fr.rho(0) * Fr.D(i, 0) * (fxi - 0.0);
-    dRMdSg -= kSIC * t.dkm[2] * po;
-    dRMdSg -= kSIC * t.dkm[3] * pg;
-    if (fsf1(lm, lf, 1)) dRMdSg -= SF1 * Vb * pm / tor * rg * M.D(i, 1) * (fyi - yi);
-    a.dSg -= kSIC * t.dkf[2] * po;
-    a.dSg -= kSIC * t.dkf[3] * pg;
-    if (fsf3(lm, lf, 1)) a.dSg -= SF3 * Vb * pf / tor * Fr.rho(1) * Fr.D(i, 1) * (fyi - 0.0);
-    dRMdSw -= kSIC * t.dkm[1] * po;
-    a.dSw -= kSIC * t.dkf[1] * po;
-    // compositions: transfer terms and the matrix's block; the factors that do
-    // not depend on k first (the matrix-side SF1 and the fracture's SF3 terms)
-    double cdg[2], cx1[2], cx2[2], cf2[2], m1[2], mdd[2], m2[2], f1d[2], f3[2], f3d[2], f32[2];
-    bool s1on[2], s3on[2];
-    for (int ph = 0; ph < 2; ph++) {
-        const double w = ph ? yi : xi, rho = ph ? rg : ro, kr = ph ? t.krg : t.kro, mub = ph ? mubar_g : mubar_o;
-        const double Dd = ph ? t.Dg : t.Do, dPp = ph ? t.dPg : t.dPo;
-        cdg[ph] = kSIC * rho * SF2 * Vb * kr / mub * dPp;
-        cx1[ph] = kSIC * w * SF2 * Vb * kr / mub * dPp;
-        cx2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pm / (Dd * Dd) * dPp * (pf + pm);
-        cf2[ph] = -kSIC * w * rho * SF2 * Vb * kr * pf / (Dd * Dd) * dPp * (pf + pm);
-        s1on[ph] = !v.diff_off && fsf1(lm, lf, ph);
-        s3on[ph] = !v.diff_off && fsf3(lm, lf, ph);
-        m1[ph] = mdd[ph] = m2[ph] = f1d[ph] = f3[ph] = f3d[ph] = f32[ph] = 0;
-        const double msat = M.S(1 + ph), mD = M.D(i, ph);
-        if (s1on[ph]) {
-            const double dlt = Fr.w(ph, i) - w;
-            m1[ph] = SF1 * msat * pm * Vb / tor * mD * dlt;
-            mdd[ph] = -SF1 * msat * pm * Vb / tor * rho * mD;
-            m2[ph] = SF1 * msat * pm * Vb / tor * rho * dlt;
-            f1d[ph] = SF1 * msat * pm * Vb / tor * rho * mD;
-        }
-        if (s3on[ph]) {
-            const double fsat = Fr.S(1 + ph), frho = Fr.rho(ph), fD = Fr.D(i, ph), fw = Fr.w(ph, i);
-            f3[ph] = SF3 * fsat * pf * Vb / tor * fD * (fw - 0.0);
-            f3d[ph] = SF3 * fsat * pf * Vb / tor * frho * fD;
-            f32[ph] = SF3 * fsat * pf * Vb / tor * frho * (fw - 0.0);
-        }
-    }
-    for (int k = 0; k < N; k++) {
-        double dRx[2], dRMx[2];
-        const bool diag = k == i;
-        for (int ph = 0; ph < 2; ph++) {
-            const double dEk = M.dE(k, ph);
-            double dRM = -((diag ? cdg[ph] : 0.0) + dEk * cx1[ph] + dmu(M, k, ph) * cx2[ph]);
-            if (s1on[ph]) dRM -= dEk * m1[ph] + (diag ? mdd[ph] : 0.0) + dD(M, i, k, ph) * m2[ph];
-            double dR = -(dmu(Fr, k, ph) * cf2[ph]);
-            // the fracture's own SF1 / SF3 composition dependences
-            if (s1on[ph] && diag) dR -= f1d[ph];
-            if (s3on[ph]) dR -= Fr.dE(k, ph) * f3[ph] + (diag ? f3d[ph] : 0.0) + dD(Fr, i, k, ph) * f32[ph];
-            dRx[ph] = dR;
-            dRMx[ph] = dRM;
-        }
-        a.x(k) = dRx[0];
-        a.y(k) = dRx[1];
-        store_other_x(N, out, row, lm, k, dRMx[0], dRMx[1]);
-    }
-    row_faces(v, Fr, i, true, false, a, out, row, nullptr);
-    const WellAt W = well_at(v, 1, c, i, fyi);
-    store_own_ps(N, out, row, lf, v.pcoeff * (dLdp + a.dp + fxi * W.PIo + W.gcomp * W.PIg), -a.dSw, dLdSo - a.dSo,
-                 dLdSg - a.dSg);
-    const OwnLayout O = own_layout(lf);
-    const double aol = (Vb / v.dt) * pf * Fr.S(1), aog = (Vb / v.dt) * pf * Fr.S(2);
-    const double frl = Fr.rho(0), frg = Fr.rho(1);
-    for (int k = 0; k < N; k++) {
-        const bool diag = k == i;
-        const double dLxl = diag ? frl + fxi * Fr.dE(k, 0) : fxi * Fr.dE(k, 0);
-        const double dLxg = diag ? frg + fyi * Fr.dE(k, 1) : fyi * Fr.dE(k, 1);
-        const double dQxl = (diag && W.iwell < 0) ? W.Qo : 0.0, dQxg = (diag && W.iwell < 0) ? W.Qg : 0.0;
-        out.st(L.cr(row, 0, k), O.x ? aol * dLxl - dQxl - a.x(k) : 0.0);
-        out.st(L.cr(row, 0, N + k), O.y ? aog * dLxg - dQxg - a.y(k) : 0.0);
-    }
-    store_other_ps(N, out, row, lm, v.pcoeff * dRMdp, dRMdSw, dRMdSo, dRMdSg);
-}
-
-// ---------------------------------------------------------------------------
-// Total hydrocarbon row (canonical 2N-1).  The matrix-fracture transfer
-// derivatives are formed from the matrix side; a fracture row takes them
-// negated with the roles of the two continua exchanged.  Also stores the
-// eight shifted entries of this block row.
-// ---------------------------------------------------------------------------
-OSR_HD inline void total_row(const JacView &v, int med, long c, const Out &out, Acc &a) {
-    const int N = v.nc;
-    const Layout L(N);
-    const int row = 2 * N - 1;
-    const Cell M{&v, &v.m[0], c, 0}, Fr{&v, &v.m[1], c, 1};
-    const Cell &O = med ? Fr : M;          // this row's continuum
-    const Transfer t = transfer_terms(v, c);
-    const double pm = t.pm, pf = t.pf, dpm = t.dpm, dpf = t.dpf;
-    const double Vb = t.Vb, SF2 = t.SF2;
-    const double po_ = med ? pf : pm, dpo_ = med ? dpf : dpm;
-    const int lo = (med ? M : Fr).label();   // the other continuum's label
     const double ro = M.rho(0), rg = M.rho(1);
     const double mubar_o = t.Do / (pm + pf), mubar_g = t.Dg / (pm + pf);
-    const double dLdp = (Vb / v.dt) * (O.S(1) * (O.rho(0) * dpo_ + O.dE(N, 0) * po_) + O.S(2) * (O.rho(1) * dpo_ + O.dE(N, 1) * po_));
-    const double dLdSo = (Vb / v.dt) * (po_ * O.rho(0)), dLdSg = (Vb / v.dt) * (po_ * O.rho(1));
-    // matrix-side derivatives of the (matrix-row) transfer terms
-    double tm = 0, tf = 0;
-    tm += kSIC * M.dE(N, 0) * SF2 * Vb * t.kro / mubar_o * t.dPo;
-    tm += -kSIC * ro * SF2 * Vb * t.kro / mubar_o;
-    tm += -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
-    tm += kSIC * dpm * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    tm += kSIC * M.dE(N, 1) * SF2 * Vb * t.krg / mubar_g * t.dPg;
-    tm += -kSIC * rg * SF2 * Vb * t.krg / mubar_g;
-    tm += -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    tm += kSIC * dpm * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    tf += kSIC * ro * SF2 * Vb * t.kro / mubar_o;
-    tf += -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
-    tf += kSIC * dpf * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
-    tf += kSIC * rg * SF2 * Vb * t.krg / mubar_g;
-    tf += -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    tf += kSIC * dpf * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
-    const double sg = med ? -1.0 : 1.0;
-    a.dp = a.dSw = a.dSo = a.dSg = 0;
-    a.dp += sg * (med ? tf : tm);
-    const double dROdp = sg * (med ? tm : tf);   // the other continuum's pressure
-    const double po = ro * SF2 * Vb / mubar_o * t.dPo, pg = rg * SF2 * Vb / mubar_g * t.dPg;
-    const double smSo = kSIC * t.dkm[4] * po, sfSo = kSIC * t.dkf[4] * po;
-    const double smSg = kSIC * t.dkm[2] * po + kSIC * t.dkm[3] * pg, sfSg = kSIC * t.dkf[2] * po + kSIC * t.dkf[3] * pg;
-    const double smSw = kSIC * t.dkm[1] * po, sfSw = kSIC * t.dkf[1] * po;
-    a.dSo += sg * (med ? sfSo : smSo);
-    a.dSg += sg * (med ? sfSg : smSg);
-    a.dSw += sg * (med ? sfSw : smSw);
-    const double dROSo = sg * (med ? smSo : sfSo), dROSg = sg * (med ? smSg : sfSg), dROSw = sg * (med ? smSw : sfSw);
-    const double t1o = kSIC * SF2 * Vb * t.kro / mubar_o * t.dPo;
-    const double t2o = -kSIC * ro * SF2 * Vb * t.kro * pm / (t.Do * t.Do) * t.dPo * (pm + pf);
-    const double t3o = -kSIC * ro * SF2 * Vb * t.kro * pf / (t.Do * t.Do) * t.dPo * (pm + pf);
-    const double t1g = kSIC * SF2 * Vb * t.krg / mubar_g * t.dPg;
-    const double t2g = -kSIC * rg * SF2 * Vb * t.krg * pm / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    const double t3g = -kSIC * rg * SF2 * Vb * t.krg * pf / (t.Dg * t.Dg) * t.dPg * (pm + pf);
-    for (int k = 0; k < N; k++) {
-        const double xm = M.dE(k, 0) * t1o + dmu(M, k, 0) * t2o;
-        const double xf = dmu(Fr, k, 0) * t3o;
-        const double ym = M.dE(k, 1) * t1g + dmu(M, k, 1) * t2g;
-        const double yf = dmu(Fr, k, 1) * t3g;
-        a.x(k) = sg * (med ? xf : xm);
-        a.y(k) = sg * (med ? yf : ym);
-        store_other_x(N, out, row, lo, k, sg * (med ? xm : xf), sg * (med ? ym : yf));
+    const bool idiff = !v.diff_off;
+    // pressure parts of the diffusion-coefficient derivatives of both cells
+    DCol dpM[2], dpF[2];
+    for (int ph = 0; ph < 2; ph++) {
+        dpM[ph] = make_dcol(M, N, ph, M.dE(N, ph));
+        dpF[ph] = make_dcol(Fr, N, ph, Fr.dE(N, ph));
     }
+    // 1) transfer terms of every row (this cell's accumulations) and the other continuum's block
+    for (int i = 0; i < N; i++) {
+        const int row = N + i;
+        const bool total = i == N - 1;
+        double a_dp = 0, a_dSw = 0, a_dSo = 0, a_dSg = 0;
+        double oP, oSw, oSo, oSg;
+        if (total) {
+            double tm = 0, tf = 0;
+            tm += kSIC * M.dE(N, 0) * SF2 * Vb * t.kro / mubar_o * t.dPo;
+            tm += -kSIC * ro * SF2 * Vb * t.kro / mubar_o;
+            tm += -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+            tm += kSIC * dpm * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+            tm += kSIC * M.dE(N, 1) * SF2 * Vb * t.krg / mubar_g * t.dPg;
+            tm += -kSIC * rg * SF2 * Vb * t.krg / mubar_g;
+            tm += -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+            tm += kSIC * dpm * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+            tf += kSIC * ro * SF2 * Vb * t.kro / mubar_o;
+            tf += -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+            tf += kSIC * dpf * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+            tf += kSIC * rg * SF2 * Vb * t.krg / mubar_g;
+            tf += -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+            tf += kSIC * dpf * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+            const double sg = med ? -1.0 : 1.0;
+            a_dp += sg * (med ? tf : tm);
+            oP = sg * (med ? tm : tf);
+            const double po = ro * SF2 * Vb / mubar_o * t.dPo, pg = rg * SF2 * Vb / mubar_g * t.dPg;
+            const double smSo = kSIC * t.dkm[4] * po, sfSo = kSIC * t.dkf[4] * po;
+            const double smSg = kSIC * t.dkm[2] * po + kSIC * t.dkm[3] * pg, sfSg = kSIC * t.dkf[2] * po + kSIC * t.dkf[3] * pg;
+            const double smSw = kSIC * t.dkm[1] * po, sfSw = kSIC * t.dkf[1] * po;
+            a_dSo += sg * (med ? sfSo : smSo);
+            a_dSg += sg * (med ? sfSg : smSg);
+            a_dSw += sg * (med ? sfSw : smSw);
+            oSo = sg * (med ? smSo : sfSo);
+            oSg = sg * (med ? smSg : sfSg);
+            oSw = sg * (med ? smSw : sfSw);
+        } else if (med == 0) {
+            // matrix component row i
+            const double xi = M.w(0, i), yi = M.w(1, i);
+            double dRfdp = 0;
+            a_dp += kSIC * M.dE(N, 0) * xi * SF2 * Vb * t.kro / mubar_o * t.dPo;
+            a_dp += -kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
+            a_dp += -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+            a_dp += kSIC * dpm * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+            a_dp += kSIC * M.dE(N, 1) * yi * SF2 * Vb * t.krg / mubar_g * t.dPg;
+            a_dp += -kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
+            a_dp += -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+            a_dp += kSIC * dpm * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+            for (int ph = 0; ph < 2 && idiff; ph++) {
+                int kinds[2];
+                const int nt = matrix_diff_targets(lm, lf, ph, kinds);
+                if (!nt) continue;
+                const double sat = M.S(1 + ph), rho = M.rho(ph), D = M.D(i, ph), w = M.w(ph, i);
+                const double dDdp = dd_col(v, dpM[ph], M, i, N, ph);
+                for (int j = 0; j < nt; j++) {
+                    const double tgt = kinds[j] ? Fr.w(ph, i) : 0.0;
+                    a_dp += dpm * SF1 * sat * Vb / tor * rho * D * (tgt - w);
+                    a_dp += M.dE(N, ph) * SF1 * sat * pm * Vb / tor * D * (tgt - w);
+                    a_dp += dDdp * SF1 * sat * pm * Vb / tor * rho * (tgt - w);
+                }
+            }
+            dRfdp += kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
+            dRfdp += -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pm + pf);
+            dRfdp += kSIC * dpf * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+            dRfdp += kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
+            dRfdp += -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pm + pf);
+            dRfdp += kSIC * dpf * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+            double dRfdSw = 0, dRfdSo = 0, dRfdSg = 0;
+            const double po = xi * ro * SF2 * Vb / mubar_o * t.dPo, pg = yi * rg * SF2 * Vb / mubar_g * t.dPg;
+            a_dSo += kSIC * t.dkm[4] * po;
+            if (idiff) {
+                int kinds[2];
+                const int nt = matrix_diff_targets(lm, lf, 0, kinds);
+                for (int j = 0; j < nt; j++) {
+                    const double tgt = kinds[j] ? Fr.w(0, i) : 0.0;
+                    a_dSo += SF1 * Vb * pm / tor * ro * M.D(i, 0) * (tgt - xi);
+                }
+            }
+            dRfdSo += kSIC * t.dkf[4] * po;
+            a_dSg += kSIC * t.dkm[2] * po;
+            a_dSg += kSIC * t.dkm[3] * pg;
+            if (idiff) {
+                // the gas saturation derivative omits the two-phase matrix / oil fracture pairing
+                int kinds[2];
+                int nt = matrix_diff_targets(lm, lf, 1, kinds);
+                if (lm == 0 && lf == 1) nt = 0;
+                for (int j = 0; j < nt; j++) {
+                    const double tgt = kinds[j] ? Fr.w(1, i) : 0.0;
+                    a_dSg += SF1 * Vb * pm / tor * rg * M.D(i, 1) * (tgt - yi);
+                }
+            }
+            dRfdSg += kSIC * t.dkf[2] * po;
+            dRfdSg += kSIC * t.dkf[3] * pg;
+            a_dSw += kSIC * t.dkm[1] * po;
+            dRfdSw += kSIC * t.dkf[1] * po;
+            oP = dRfdp;
+            oSw = dRfdSw;
+            oSo = dRfdSo;
+            oSg = dRfdSg;
+        } else {
+            // fracture component row i
+            const double xi = M.w(0, i), yi = M.w(1, i);
+            const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
+            double dRMdp = 0;
+            dRMdp -= kSIC * M.dE(N, 0) * xi * SF2 * Vb * t.kro / mubar_o * t.dPo;
+            dRMdp -= -kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
+            dRMdp -= -kSIC * (dmu(M, N, 0) * pm + dpm * M.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
+            dRMdp -= kSIC * dpm * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+            dRMdp -= kSIC * M.dE(N, 1) * yi * SF2 * Vb * t.krg / mubar_g * t.dPg;
+            dRMdp -= -kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
+            dRMdp -= -kSIC * (dmu(M, N, 1) * pm + dpm * M.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
+            dRMdp -= kSIC * dpm * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+            for (int ph = 0; ph < 2 && idiff; ph++) {
+                if (!fsf1(lm, lf, ph)) continue;
+                const double sat = M.S(1 + ph), rho = M.rho(ph), D = M.D(i, ph), dlt = Fr.w(ph, i) - M.w(ph, i);
+                dRMdp -= dpm * SF1 * sat * Vb / tor * rho * D * dlt;
+                dRMdp -= M.dE(N, ph) * SF1 * sat * pm * Vb / tor * D * dlt;
+                dRMdp -= dd_col(v, dpM[ph], M, i, N, ph) * SF1 * sat * pm * Vb / tor * rho * dlt;
+            }
+            a_dp -= kSIC * xi * ro * SF2 * Vb * t.kro / mubar_o;
+            a_dp -= -kSIC * (dmu(Fr, N, 0) * pf + dpf * Fr.mu(0)) * xi * ro * SF2 * Vb * t.kro / (t.Do * t.Do) * t.dPo * (pf + pm);
+            a_dp -= kSIC * dpf * xi * ro * SF2 * Vb * t.kro / t.Do * t.dPo;
+            a_dp -= kSIC * yi * rg * SF2 * Vb * t.krg / mubar_g;
+            a_dp -= -kSIC * (dmu(Fr, N, 1) * pf + dpf * Fr.mu(1)) * yi * rg * SF2 * Vb * t.krg / (t.Dg * t.Dg) * t.dPg * (pf + pm);
+            a_dp -= kSIC * dpf * yi * rg * SF2 * Vb * t.krg / t.Dg * t.dPg;
+            for (int ph = 0; ph < 2 && idiff; ph++) {
+                if (!fsf3(lm, lf, ph)) continue;
+                const double sat = Fr.S(1 + ph), rho = Fr.rho(ph), D = Fr.D(i, ph), w = Fr.w(ph, i);
+                a_dp -= dpf * SF3 * sat * Vb / tor * rho * D * (w - 0.0);
+                a_dp -= Fr.dE(N, ph) * SF3 * sat * pf * Vb / tor * D * (w - 0.0);
+                a_dp -= dd_col(v, dpF[ph], Fr, i, N, ph) * SF3 * sat * pf * Vb / tor * rho * (w - 0.0);
+            }
+            double dRMdSo = 0, dRMdSg = 0, dRMdSw = 0;
+            const double po = xi * ro * SF2 * Vb / mubar_o * t.dPo, pg = yi * rg * SF2 * Vb / mubar_g * t.dPg;
+            dRMdSo -= kSIC * t.dkm[4] * po;
+            if (idiff && fsf1(lm, lf, 0)) dRMdSo -= SF1 * Vb * pm / tor * ro * M.D(i, 0) * (fxi - xi);
+            a_dSo -= kSIC * t.dkf[4] * po;
+            if (idiff && fsf3(lm, lf, 0)) a_dSo -= SF3 * Vb * pf / tor * Fr.rho(0) * Fr.D(i, 0) * (fxi - 0.0);
+            dRMdSg -= kSIC * t.dkm[2] * po;
+            dRMdSg -= kSIC * t.dkm[3] * pg;
+            if (idiff && fsf1(lm, lf, 1)) dRMdSg -= SF1 * Vb * pm / tor * rg * M.D(i, 1) * (fyi - yi);
+            a_dSg -= kSIC * t.dkf[2] * po;
+            a_dSg -= kSIC * t.dkf[3] * pg;
+            if (idiff && fsf3(lm, lf, 1)) a_dSg -= SF3 * Vb * pf / tor * Fr.rho(1) * Fr.D(i, 1) * (fyi - 0.0);
+            dRMdSw -= kSIC * t.dkm[1] * po;
+            a_dSw -= kSIC * t.dkf[1] * po;
+            oP = dRMdp;
+            oSw = dRMdSw;
+            oSo = dRMdSo;
+            oSg = dRMdSg;
+        }
+        dp[i] = a_dp;
+        dSw[i] = a_dSw;
+        dSo[i] = a_dSo;
+        dSg[i] = a_dSg;
+        store_other_ps(N, out, row, lo, v.pcoeff * oP, oSw, oSo, oSg);
+    }
+    // 2) faces
+    JFace fc[6];
+    const int nf = jac_faces(v, c, fc);
+    unsigned present = 0;
+    for (int f = 0; f < nf; f++) present |= 1u << fc[f].slot;
+    // advective flux, this cell's pressure
+    for (int ph = 0; ph < 2; ph++)
+        for (int f = 0; f < nf; f++) {
+            const FaceData fd = face_data(v, *q.F, c, fc[f]);
+            const double T = fd.T[ph];
+            const Cell U{&v, q.F, upstream(fc[f], fd, c, ph), med};
+            for (int i = 0; i < N; i++) dp[i] += i == N - 1 ? T : U.w(ph, i) * T;
+        }
     double ov[kOverflow];
     for (int j = 0; j < kOverflow; j++) ov[j] = 0;
-    row_faces(v, O, 0, med == 1, true, a, out, row, ov);
-    for (int j = 0; j < kOverflow; j++) out.st(L.o(j), ov[j]);
-    const WellAt W = well_at(v, med, c, 0, 0.0);
-    const int lab = O.label();
-    store_own_ps(N, out, row, lab, v.pcoeff * (dLdp + a.dp + W.PIo + W.PIg), -a.dSw, dLdSo - a.dSo, dLdSg - a.dSg);
-    const OwnLayout OL = own_layout(lab);
-    const double aol = (Vb / v.dt) * po_ * O.S(1), aog = (Vb / v.dt) * po_ * O.S(2);
-    for (int k = 0; k < N; k++) {
-        out.st(L.cr(row, 0, k), OL.x ? aol * O.dE(k, 0) - a.x(k) : 0.0);
-        out.st(L.cr(row, 0, N + k), OL.y ? aog * O.dE(k, 1) - a.y(k) : 0.0);
+    const double tor_c = med ? 1.0 : tor;
+    const double pq = q.porpor(), dpq = q.dpordp();
+    const bool q_inactive = q.por() < 1e-10;
+    for (int f = 0; f < nf; f++) {
+        const JFace &e = fc[f];
+        const Cell nb{&v, q.F, e.nb, med};
+        const FaceData fd = face_data(v, *q.F, c, e);
+        const int lnb = nb.label();
+        const double s = e.sgn;
+        const bool nb_o = upstream(e, fd, c, 0) == e.nb, nb_g = upstream(e, fd, c, 1) == e.nb;
+        const double tor_n = med ? 1.0 : ld(v.tor + e.nb);
+        const double pn = nb.porpor(), dpn = nb.dpordp();
+        const double NNd = e.area2 / (e.dn + e.dl);
+        const bool inactive = q_inactive || nb.por() < 1e-10;
+        // the pressure factors of both phases (shared by every row)
+        Mob m[2];
+        double coefs[2], dCs[2], MMd[2], dMM[2], dMM2[2];
+        DCol dcnb[2];
+        for (int ph = 0; ph < 2; ph++) {
+            const double coef = ph == 0 ? (lnb == -1 ? 0.0 : 1.0) : (lnb == 1 ? 0.0 : 1.0);
+            const double dC = ph == 0 ? (lq == -1 ? 0.0 : 1.0) : (lq == 1 ? 0.0 : 1.0);
+            const Side sq{q.rho(ph), q.mu(ph), q.gam(ph)}, sn{nb.rho(ph), nb.mu(ph), nb.gam(ph)};
+            const double dEq = q.dE(N, ph), dEn = nb.dE(N, ph);
+            m[ph] = mobility(sq, sn, dEq, dEn, false, 0.0, e, coef, dmu(q, N, ph), dmu(nb, N, ph));
+            dcnb[ph].zero = true;
+            if (idiff) dcnb[ph] = make_dcol(nb, N, ph, dEn);
+            coefs[ph] = coef;
+            dCs[ph] = dC;
+            double AAd = sn.rho * e.dn * coef + sq.rho * e.dl * dC;
+            AAd *= (nb.S(1 + ph) * e.dn * coef + q.S(1 + ph) * e.dl * dC) / (e.dn + e.dl);
+            const double BBd = tor_n * e.dn * coef / pn + tor_c * e.dl * dC / pq;
+            MMd[ph] = AAd / BBd;
+            const double dAA = dEq * e.dl * dC, dAA2 = dEn * e.dn * coef;
+            const double dBB = -dpq * tor_c * e.dl * dC / (pq * pq), dBB2 = -dpn * tor_n * e.dn * coef / (pn * pn);
+            dMM[ph] = (dAA * BBd - dBB * AAd) / (BBd * BBd);
+            dMM2[ph] = (dAA2 * BBd - dBB2 * AAd) / (BBd * BBd);
+        }
+        const int cS2 = lnb == -1 ? 3 : 2, cS3 = lnb == 1 ? 2 : 3;
+        for (int i = 0; i < N; i++) {
+            const int row = N + i;
+            const bool total = i == N - 1;
+            const FaceQuirks qk = total ? total_quirks(e) : comp_quirks(e);
+            const double xo = total ? 1.0 : (nb_o ? nb : q).w(0, i), yg = total ? 1.0 : (nb_g ? nb : q).w(1, i);
+            double ps[4] = {0, 0, 0, 0}, ovl[4] = {0, 0, 0, 0};
+            auto put = [&](int tt, int cc, double val) {
+                if (qk.shifted_block) ovl[tt] = val;
+                else ps[cc] += val;
+            };
+            // saturation factors
+            const double dsw = s * (xo * fd.T[4] * fd.dP[1] + xo * fd.T[6] * fd.dH);
+            if (nb_o) put(1, 1, dsw);
+            else dSw[i] += dsw;
+            const double dso = s * (xo * fd.T[10] * fd.dP[1] + xo * fd.T[11] * fd.dH);
+            if (nb_o) put(2, cS2, lnb == -1 ? 0.0 : dso);
+            else dSo[i] += dso;
+            const double dsgo = s * (xo * fd.T[8] * fd.dP[1] + xo * fd.T[9] * fd.dH);
+            const double dsgg = s * (yg * fd.T[5] * fd.dP[2] + yg * fd.T[7] * fd.dH);
+            double vsg = 0;
+            if (nb_o) vsg = lnb == 1 ? 0.0 : dsgo;
+            else dSg[i] += dsgo;
+            if (nb_g) vsg += lnb == 1 ? 0.0 : dsgg;
+            else dSg[i] += dsgg;
+            put(3, cS3, vsg);
+            // mobility and diffusion derivatives with respect to the two pressures
+            double dB = 0;
+            for (int ph = 0; ph < 2; ph++) {
+                const Mob &mb = m[ph];
+                const bool up_nb = ph == 0 ? nb_o : nb_g;
+                const Cell &U = up_nb ? nb : q;
+                const double wk = total ? 1.0 : U.w(ph, i), krk = U.kr(1 + ph);
+                const double dPp = fd.dP[1 + ph];
+                const double a = wk * fd.ift * krk;
+                dp[i] -= s * (a * mb.M * dPp);
+                const double vB = s * (a * mb.B * dPp);
+                if (ph == 1 && e.sgn < 0) {
+                    const bool assign = up_nb ? qk.gas_dB_assign_down : qk.gas_dB_assign_up;
+                    dB = assign ? vB : dB + vB;
+                    // the reference exchanges this cell's and the neighbour's gravity factors here
+                    dp[i] -= s * (a * (mb.B * mb.tempdx + mb.BG * mb.Sur / mb.Mak) * fd.dH);
+                    dB += s * (a * (mb.M * mb.tempdx + mb.MG * mb.Sur / mb.Mak) * fd.dH);
+                } else {
+                    dB = ph == 0 ? vB : dB + vB;
+                    dp[i] -= s * (a * (mb.M * mb.tempdx + mb.MG * mb.Sur / mb.Mak) * fd.dH);
+                    const double gB = s * (a * (mb.B * mb.tempdx + mb.BG * mb.Sur / mb.Mak) * fd.dH);
+                    if (ph == 0 && e.sgn < 0 && up_nb && qk.oil_grav_assign_down) dB = gB;
+                    else dB += gB;
+                }
+                if (total || !idiff) continue;
+                // intra-continuum diffusion
+                const double wq = q.w(ph, i), wn = nb.w(ph, i);
+                double Dup, dDdp, dDdp2;
+                if (wn > wq) {
+                    Dup = nb.D(i, ph);
+                    dDdp = 0;
+                    dDdp2 = dd_col(v, dcnb[ph], nb, i, N, ph);
+                } else {
+                    Dup = q.D(i, ph);
+                    dDdp = dd_col(v, med ? dpF[ph] : dpM[ph], q, i, N, ph);
+                    dDdp2 = 0;
+                }
+                if (inactive) Dup = dDdp = dDdp2 = 0;
+                const double DX = wn - wq;
+                if (coefs[ph] != 0 && dCs[ph] != 0) {
+                    dp[i] += -NNd * DX * (MMd[ph] * dDdp + Dup * dMM[ph]);
+                    dB += NNd * DX * (MMd[ph] * dDdp2 + Dup * dMM2[ph]);
+                }
+            }
+            put(0, 0, v.pcoeff * (-xo * fd.T[0] - yg * fd.T[1] - dB));
+            for (int tt = 0; tt < 4; tt++) out.st(L.cr(row, e.slot, 2 * N + tt), ps[tt]);
+            if (total && qk.shifted_block)
+                for (int tt = 0; tt < 4; tt++) ov[(e.d == 1 ? 0 : 4) + tt] = ovl[tt];
+        }
     }
-    store_other_ps(N, out, row, lo, v.pcoeff * dROdp, dROSw, dROSo, dROSg);
+    for (int sl = 1; sl <= 6; sl++)
+        if (!(present & (1u << sl)))
+            for (int i = 0; i < N; i++)
+                for (int tt = 0; tt < 4; tt++) out.st(L.cr(N + i, sl, 2 * N + tt), 0.0);
+    for (int j = 0; j < kOverflow; j++) out.st(L.o(j), ov[j]);
+    // 3) this cell's block, with the accumulation and the completion's productivity terms
+    for (int i = 0; i < N; i++) {
+        const int row = N + i;
+        double dLdp, dLdSo, dLdSg, well;
+        if (i == N - 1) {
+            const double po_ = med ? pf : pm, dpo_ = med ? dpf : dpm;
+            dLdp = (Vb / v.dt) * (q.S(1) * (q.rho(0) * dpo_ + q.dE(N, 0) * po_) + q.S(2) * (q.rho(1) * dpo_ + q.dE(N, 1) * po_));
+            dLdSo = (Vb / v.dt) * (po_ * q.rho(0));
+            dLdSg = (Vb / v.dt) * (po_ * q.rho(1));
+            const WellAt W = well_at(v, med, c, 0, 0.0);
+            well = W.PIo + W.PIg;
+        } else if (med == 0) {
+            const double xi = M.w(0, i), yi = M.w(1, i);
+            dLdp = (Vb / v.dt) * (xi * M.S(1) * (ro * dpm + M.dE(N, 0) * pm) + yi * M.S(2) * (rg * dpm + M.dE(N, 1) * pm));
+            dLdSo = (Vb / v.dt) * (xi * pm * ro);
+            dLdSg = (Vb / v.dt) * (yi * pm * rg);
+            const WellAt W = well_at(v, 0, c, i, yi);
+            well = xi * W.PIo + W.gcomp * W.PIg;
+        } else {
+            const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
+            dLdp = (Vb / v.dt) * (fxi * Fr.S(1) * (Fr.rho(0) * dpf + Fr.dE(N, 0) * pf) + fyi * Fr.S(2) * (Fr.rho(1) * dpf + Fr.dE(N, 1) * pf));
+            dLdSo = (Vb / v.dt) * (fxi * pf * Fr.rho(0));
+            dLdSg = (Vb / v.dt) * (fyi * pf * Fr.rho(1));
+            const WellAt W = well_at(v, 1, c, i, fyi);
+            well = fxi * W.PIo + W.gcomp * W.PIg;
+        }
+        store_own_ps(N, out, row, lq, v.pcoeff * (dLdp + dp[i] + well), -dSw[i], dLdSo - dSo[i], dLdSg - dSg[i]);
+    }
+}
+
+// Inactive cell-media (porosity < 1e-10): the unit entries of the reference's
+// diagonal in the columns a task owns, zeros elsewhere.
+OSR_HD inline void inactive_column(int N, const Out &out, int lab, int k) {
+    const Layout L(N);
+    for (int i = 0; i < N; i++) {
+        const int row = N + i, uc = unit_col(N, lab, row);
+        for (int sl = 0; sl < 8; sl++) {
+            out.st(L.cr(row, sl, k), (sl == 0 && uc == k) ? 1.0 : 0.0);
+            out.st(L.cr(row, sl, N + k), (sl == 0 && uc == N + k) ? 1.0 : 0.0);
+        }
+    }
+}
+
+OSR_HD inline void zero_ps(int N, const Out &out) {
+    const Layout L(N);
+    for (int i = 0; i < N; i++)
+        for (int sl = 0; sl < 8; sl++)
+            for (int tt = 0; tt < 4; tt++) out.st(L.cr(N + i, sl, 2 * N + tt), 0.0);
+    for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
+}
+
+OSR_HD inline void zero_column(int N, const Out &out, int k) {
+    const Layout L(N);
+    for (int i = 0; i < N; i++)
+        for (int sl = 0; sl < 8; sl++) {
+            out.st(L.cr(N + i, sl, k), 0.0);
+            out.st(L.cr(N + i, sl, N + k), 0.0);
+        }
+}
+
+OSR_HD inline void zero_misc(int N, const Out &out) {
+    const Layout L(N);
+    for (int e = 0; e < L.EF; e++) out.st(e, 0.0);
+    for (int e = L.EF + L.EC; e < L.E; e++) out.st(e, 0.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1395,15 +1463,6 @@ OSR_HD inline void fugacity_rows(const JacView &v, const Cell &q, const Out &out
 // Row tasks
 // ---------------------------------------------------------------------------
 
-// A component or total row of an inactive cell-medium: its unit entry and
-// zeros (the reference writes a unit diagonal only).
-OSR_HD inline void inactive_c_row(int N, const Out &out, int lab, int row) {
-    const Layout L(N);
-    const int uc = unit_col(N, lab, row);
-    for (int s = 0; s < 8; s++)
-        for (int c = 0; c < L.BS; c++) out.st(L.cr(row, s, c), (s == 0 && c == uc) ? 1.0 : 0.0);
-}
-
 // Task N: the fugacity rows (or a one-phase cell's unused rows), the water row
 // and the constraint rows.
 OSR_HD inline void misc_rows(const JacView &v, int med, long c, const Out &out) {
@@ -1445,78 +1504,40 @@ OSR_HD inline void misc_rows(const JacView &v, int med, long c, const Out &out) 
     }
 }
 
-// The values row task `task` owns, stored as zeros (lanes of the last chunk
-// beyond the grid).
-OSR_HD inline void zero_task(int N, const Out &out, int task) {
-    const Layout L(N);
-    if (task == N) {
-        for (int e = 0; e < L.EF; e++) out.st(e, 0.0);
-        for (int e = L.EF + L.EC; e < L.E; e++) out.st(e, 0.0);
-        return;
-    }
-    const int row = N + task;
-    for (int s = 0; s < 8; s++)
-        for (int c = 0; c < L.BS; c++) out.st(L.cr(row, s, c), 0.0);
-    if (task == N - 1)
-        for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
-}
-
-// Row task `task` of block row bm (cell-medium).
-OSR_HD inline void jacobian_task(const JacView &v, long bm, int task, Acc &a) {
-    const int N = v.nc;
-    const int med = bm >= v.n;
-    const long c = med ? bm - v.n : bm;
-    const Out out{v.vals, v.entries, bm};
-    const Layout L(N);
-    if (task == N) {
-        misc_rows(v, med, c, out);
-        return;
-    }
-    const Cell q{&v, &v.m[med], c, med};
-    const int row = N + task;
-    if (q.por() < 1e-10) {
-        inactive_c_row(N, out, q.label(), row);
-        if (task == N - 1)
-            for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
-        return;
-    }
-    if (task == N - 1) total_row(v, med, c, out, a);
-    else if (med == 0) matrix_comp_row(v, c, task, out, a);
-    else fracture_comp_row(v, c, task, out, a);
-}
-
-// Row tasks by kind, for launches that each run one code path: 0 matrix
-// component rows, 1 fracture component rows, 2 total rows, 3 fugacity /
-// water / constraint rows.  The kind's lanes only; padding lanes of the last
-// chunk store zeros.
+// Task kinds, one code path per launch: 0 matrix columns (task k = 0..N-1),
+// 1 fracture columns, 2 matrix pressure-saturation columns (one task), 3
+// fracture pressure-saturation columns, 4 fugacity / water / constraint rows.
+// A kind's lanes only; lanes of the last chunk beyond the grid store zeros.
+// smem: the thread's shared-memory column (3N or 4N doubles at stride).
 template <int KIND>
-OSR_HD inline void jacobian_task_kind(const JacView &v, long bm, int task, Acc &a) {
+OSR_HD inline void jacobian_task_kind(const JacView &v, long bm, int task, double *smem, int stride) {
     const int N = v.nc;
     const long nb = 2 * v.n;
     const Out out{v.vals, v.entries, bm};
-    if (bm >= nb) {
-        if (KIND != 0) zero_task(N, out, task);
-        return;
-    }
     const int med = bm >= v.n;
-    if ((KIND == 0 && med) || (KIND == 1 && !med)) return;
+    if (KIND == 4) {
+        if (bm >= nb) zero_misc(N, out);
+        else misc_rows(v, med, med ? bm - v.n : bm, out);
+        return;
+    }
+    const int want = (KIND == 1 || KIND == 3) ? 1 : 0;
+    if (bm >= nb) {
+        if (KIND == 1) zero_column(N, out, task);
+        if (KIND == 3) zero_ps(N, out);
+        return;
+    }
+    if (med != want) return;
     const long c = med ? bm - v.n : bm;
-    if (KIND == 3) {
-        misc_rows(v, med, c, out);
-        return;
-    }
     const Cell q{&v, &v.m[med], c, med};
-    if (q.por() < 1e-10) {
-        inactive_c_row(N, out, q.label(), N + task);
-        if (KIND == 2) {
-            const Layout L(N);
-            for (int j = 0; j < kOverflow; j++) out.st(L.o(j), 0.0);
-        }
-        return;
+    const SmemVec s0{smem, stride}, s1{smem + N * stride, stride}, s2{smem + 2 * N * stride, stride},
+        s3{smem + 3 * N * stride, stride};
+    if (KIND <= 1) {
+        if (q.por() < 1e-10) inactive_column(N, out, q.label(), task);
+        else column_task(v, med, c, task, out, s0, s1, s2);
+    } else {
+        if (q.por() < 1e-10) zero_ps(N, out);
+        else ps_task(v, med, c, out, s0, s1, s2, s3);
     }
-    if (KIND == 0) matrix_comp_row(v, c, task, out, a);
-    else if (KIND == 1) fracture_comp_row(v, c, task, out, a);
-    else total_row(v, med, c, out, a);
 }
 
 // Reference (global row, global column) of entry e of block row bm, or -1 for
