@@ -124,6 +124,47 @@ def _cpu_worker_run(_):
     return time.perf_counter() - t
 
 
+ASM_CPU_GRID = (128, 128, 16)
+ASM_CPU_ROWS = 40_000
+
+
+def _ref_assembly_sample(state_path: str, grid, k: int, seed: int = 6) -> dict:
+    """The reference's own assembly cost on the assembly deck family, timed
+    in a spawned process: open the deck (grid, rock, tables of
+    ``workloads.assembly_spec``), replace its component table with the
+    seeded one, load the device flash's two-phase state and unknowns, time
+    one UpdateAll(x, false), then IteratorFunction and IteratorJacobian on k
+    uniformly sampled global rows (in ascending order, as FormFunction and
+    FormJacobian visit them).  The reference's stdout chatter is discarded so
+    the bench's one JSON line stays alone on stdout."""
+    import numpy as np
+    import oracle
+    from osiris_b200 import deck, workloads
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    d = workloads.assembly_deck(*grid)
+    st = np.load(state_path)
+    path = state_path + ".dat"
+    deck.write_deck(path, workloads.assembly_spec(d))
+    R = oracle.RefDeck(path)
+    R.override_fluid(d)
+    for key in st.files:
+        if key != "x":
+            R.set(key, st[key])
+    rows = R.relayout()
+    x = st["x"]
+    if len(x) != rows:
+        raise RuntimeError(f"row layouts differ: {len(x)} unknowns for {rows} rows")
+    t0 = time.perf_counter()
+    R.update_all(x, False)
+    t_upd = time.perf_counter() - t0
+    sel = np.sort(np.random.default_rng(seed).choice(rows, min(k, rows), replace=False))
+    t_f = R.time_rows(sel, x, 0, d.dt)
+    t_j = R.time_rows(sel, x, 1, d.dt)
+    return {"rows": rows, "cell_media": 2 * d.cells, "k": int(len(sel)), "update_all_s": t_upd,
+            "function_s": t_f, "jacobian_s": t_j}
+
+
 class CpuReference:
     """The reference's SuccFalsh on every host core: one spawned process per
     core, each holding a contiguous shard of the cells (the reference keeps its
@@ -375,7 +416,8 @@ def structural_values(nx: int, ny: int, nz: int, nc: int) -> int:
     return int(2 * per.sum())
 
 
-def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier, max_over_ranks, gpu_id):
+def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier, max_over_ranks, gpu_id,
+                     cpu_sample=False):
     """The Newton-step assembly: UpdateAll + residual (FormFunction) and the
     Jacobian (FormJacobian's device part) of the 128x128x32, 8-component
     workload, each part timed with CUDA events on the launching stream."""
@@ -455,7 +497,10 @@ def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier,
     achieved = jac_bytes / (jac_max * 1e-3) / 1e9
     del J, G
     torch.cuda.empty_cache()
-    return {
+    cpu = None
+    if cpu_sample:
+        cpu = assembly_cpu_baseline(osr, torch, dev, cells, rows)
+    res = {
         "metric": "assembly cell-media/s (FormFunction + FormJacobian)", "value": world * cells / (total * 1e-3),
         "unit": "cells/s", "ms_per_step": total,
         "parts_ms": {"update_all": upd, "residual": res, "jacobian": jac},
@@ -463,7 +508,7 @@ def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier,
                                f"{nc} components, seeded properties, all cells two-phase (P0 {p0:.4g} Pa)",
                    "rows": rows, "two_phase_fraction": two_phase, "cdif": 0.0,
                    "l2": "flushed before every step (256 MiB write); values 12.6 GB per step exceed L2"},
-        "roofline": {"bound": "hbm", "kernel": "Jacobian: well pass, derivative tables, four row kernels",
+        "roofline": {"bound": "hbm", "kernel": "Jacobian: well pass, derivative tables, five column/row kernels",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if peak else None,
                      "bytes_per_launch": jac_bytes, "structural_values": sv,
@@ -473,9 +518,65 @@ def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier,
                 "h2d_bytes_per_step": rows * 8, "d2h_bytes_per_step": rows * 8, "ms_per_step": e2e,
                 "note": "unknowns in and residual out through pinned host memory; the Jacobian values stay "
                         "device-resident for a device linear solve"},
-        "gpu_launches": 10 * args.steps,
+        "gpu_launches": ASM_LAUNCHES * args.steps,
         "clocks": clk,
     }
+    if cpu is not None:
+        res["cpu_baseline"] = cpu
+    return res
+
+
+# kernels per assembly step: UpdateAll (unpack, cell properties, face
+# transmissibilities), the residual rows, the Jacobian (well pass, derivative
+# tables, five column/row kernels)
+ASM_LAUNCHES = 11
+
+
+def assembly_cpu_baseline(osr, torch, dev, cells_full: int, rows_full: int) -> dict:
+    """Reference CPU time of one Newton-step assembly (FormFunction +
+    FormJacobian: two UpdateAll calls and every row through IteratorFunction
+    and IteratorJacobian), from a sample.  The reference cannot open the
+    128x128x32 grid at 8 components: its CSR scratch allocation
+    (compsim/Data_Input.cpp:1803, 3*bCSRSize values in a 32-bit int)
+    overflows, so the sample runs on 128x128x16 of the same deck family.
+    Each of its rows first finds its block by a linear scan over the block
+    row offsets (compsim/Petsc_Functions.cpp:58-59), O(blocks) per row, so
+    per-row times on the half grid applied to the full grid's rows are a
+    lower bound on the reference's full-grid time; UpdateAll is O(cells) and
+    is scaled by the cell ratio."""
+    import tempfile
+
+    import numpy as np
+    import oracle
+    from osiris_b200 import workloads
+    if not oracle.ref_available():
+        return None
+    d = workloads.assembly_deck(*ASM_CPU_GRID)
+    G = osr.Grid(d)
+    workloads.assembly_state(G, d, dev)
+    rows, _ = G.refresh_layout()
+    x = torch.zeros(rows, dtype=torch.float64, device=dev)
+    G.init_guess(x)
+    st = {f"{m}.{k}": G.get(f"{m}.{k}") for m in "mf" for k in ("P", "sat", "x", "y", "z", "label", "rho")}
+    st["x"] = x.cpu().numpy()
+    del G, x
+    torch.cuda.empty_cache()
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "state.npz")
+        np.savez(path, **st)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(1) as pool:
+            r = pool.apply(_ref_assembly_sample, (path, ASM_CPU_GRID, ASM_CPU_ROWS))
+    scale = cells_full / r["cell_media"]
+    per_row = (r["function_s"] + r["jacobian_s"]) / r["k"]
+    sec = 2 * r["update_all_s"] * scale + per_row * rows_full
+    return {"value": cells_full / sec, "unit": "cells/s", "cores": 1, "kind": "reference",
+            "sample": (f"{r['k']} uniformly sampled rows of IteratorFunction and IteratorJacobian and one full "
+                       f"UpdateAll on the {'x'.join(map(str, ASM_CPU_GRID))} grid of the same deck family "
+                       f"({r['rows']} rows); per-row time x {rows_full} rows + 2 UpdateAll x {scale:g} "
+                       "(the reference cannot allocate the 128x128x32 grid; a lower bound on its time)"),
+            "seconds_per_step": sec, "per_row_us": per_row * 1e6,
+            "update_all_s": r["update_all_s"], "sample_rows": r["rows"]}
 
 
 def run_ours(args):
@@ -630,7 +731,8 @@ def run_ours(args):
         del out, flush
         torch.cuda.empty_cache()
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-        assembly = measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier, max_over_ranks, gpu_id)
+        assembly = measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier, max_over_ranks, gpu_id,
+                                    cpu_sample=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     instances = None
     if inst_groups is not None:

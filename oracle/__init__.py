@@ -357,8 +357,8 @@ class RefDeck:
         return info
 
     def set(self, name: str, values):
-        """Overwrite a state array (m./f. + P, sat, x, y, z, label) in the
-        layout ``get`` returns."""
+        """Overwrite a state array (m./f. + P, sat, x, y, z, label, rho) in
+        the layout ``get`` returns."""
         v = np.ascontiguousarray(values, np.float64).ravel().copy()
         if self.lib.ref_set(name.encode(), _p(v)) < 0:
             raise KeyError(name)
@@ -377,6 +377,33 @@ class RefDeck:
         x = np.ascontiguousarray(x, np.float64).copy()
         self.lib.ref_update_all(_p(x), int(full))
         self.rows = int(self.lib_info()[5])
+
+    def override_fluid(self, deck):
+        """Replace the component table with ``deck``'s (tc, pc, acf, mw, vc,
+        zc, parachor, kij) and redo EOS_Init / Tr_Mu; the reference's deck
+        keywords cannot carry arbitrary criticals."""
+        a = [np.ascontiguousarray(getattr(deck, k), np.float64) for k in
+             ("tc", "pc", "acf", "mw", "vc", "zc", "parachor")]
+        kij = np.ascontiguousarray(deck.kij, np.float64).ravel()
+        if self.lib.ref_override_fluid(int(self.nc), *(_p(v) for v in a), _p(kij)):
+            raise ValueError("component count differs from the deck's")
+
+    def relayout(self) -> int:
+        """CalcPCoeff + PJac for labels set through ``set``; returns the row count."""
+        self.lib.ref_relayout.restype = ctypes.c_long
+        self.rows = int(self.lib.ref_relayout())
+        return self.rows
+
+    def time_rows(self, rows, x, which: int, t: float = 0.0) -> float:
+        """Seconds the reference spends in IteratorFunction (which=0) or
+        IteratorJacobian (which=1) over the given global rows, at the state
+        of the last ``update_all``."""
+        rows = np.ascontiguousarray(rows, np.int64)
+        x = np.ascontiguousarray(x, np.float64).copy()
+        f = np.zeros(self.rows)
+        self.lib.ref_time_rows.restype = ctypes.c_double
+        return float(self.lib.ref_time_rows(_p(rows), ctypes.c_long(len(rows)), _p(x), _p(f), ctypes.c_double(t),
+                                            int(which)))
 
     def form_function(self, x, t: float = 0.0) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64).copy()

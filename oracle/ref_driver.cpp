@@ -9,6 +9,7 @@
  * Layout of the flat arrays (shared with the restated oracle and the CUDA
  * library): per-cell scalars are [n]; per-component fields are
  * component-major [nc][n]. */
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -309,7 +310,7 @@ long ref_get(const char *name, double *out) {
 }
 
 /* Overwrite a named state array (the layout of ref_get): m./f. + P, sat,
- * x, y, z or label.  Returns the values read, or -1. */
+ * x, y, z, label or rho.  Returns the values read, or -1. */
 long ref_set(const char *name, const double *in) {
     std::string s(name);
     const long n = ncell();
@@ -335,6 +336,11 @@ long ref_set(const char *name, const double *in) {
     if (k == "label") {
         each_cell([&](int i, int j, int l, long c) { ps[i][j][l] = (signed char)in[c]; });
         return n;
+    }
+    if (k == "rho") {  /* phase molar densities, read by the next CalcIFT */
+        FType *****bp = fr ? fblockFProps : blockFProps;
+        for (int p = 0; p < 2; p++) each_cell([&](int i, int j, int l, long c) { bp[i][j][l][RO][p] = in[p * n + c]; });
+        return 2 * n;
     }
     return -1;
 }
@@ -385,6 +391,62 @@ int ref_init_guess(double *x) {
     _p_Vec v{x, MatrixSize};
     InitGuess2(nullptr, &v, nullptr);
     return 0;
+}
+
+/* Replace the component table of an opened deck (fluidProp columns as the
+ * COMPNAME library sets them, compsim/Data_Input.cpp:653-952; bic = 1 - kij as
+ * the BIC keyword stores it, compsim/Data_Input.cpp:977-990) and redo the
+ * per-component initialisation that depends on it: EOS_Init (which divides
+ * VCRIT, given here in cm3/mol, by 1e6) and Tr_Mu
+ * (compsim/Init_Calcs.cpp:48-97).  The reference's own user-component path
+ * recomputes Tc, Pc and omega from SG/TB correlations (CPlus_Props), so a
+ * seeded table can only enter this way.  Call before setting the state. */
+int ref_override_fluid(int nc, const double *tc, const double *pc, const double *acf, const double *mw,
+                       const double *vc, const double *zc, const double *parachor, const double *kij) {
+    if (nc != Nc) return -1;
+    for (int i = 0; i < nc; i++) {
+        fluidProp[i][TCRIT] = tc[i];
+        fluidProp[i][PCRIT] = pc[i];
+        fluidProp[i][AC] = acf[i];
+        fluidProp[i][MW] = mw[i];
+        fluidProp[i][VCRIT] = vc[i];
+        fluidProp[i][ZCRIT] = zc[i];
+        fluidProp[i][PARACHOR] = parachor[i];
+        for (int j = 0; j < nc; j++) bic[i][j] = 1 - kij[i * nc + j];
+    }
+    EOS_Init();
+    Tr_Mu();
+    return 0;
+}
+
+/* PCoeff and the row layout of the current phase labels (CalcPCoeff, PJac),
+ * as UpdateAll(x, true) runs them after phase control
+ * (compsim/PetscAUX.cpp:505-506); for states set through ref_set. */
+long ref_relayout(void) {
+    CalcPCoeff();
+    PJac();
+    return MatrixSize;
+}
+
+/* Evaluate IteratorFunction (which = 0) or IteratorJacobian (which = 1) for
+ * the k listed global rows, as FormFunction / FormJacobian do for every row
+ * (compsim/PetscAUX.cpp:59-173), after the caller's UpdateAll; returns the
+ * wall time of the loop in seconds.  Values go to f (which = 0, MatrixSize
+ * doubles) or to a scratch matrix that is cleared first. */
+double ref_time_rows(const long *rows, long k, double *x, double *f, double t, int which) {
+    _p_Vec vx{x, MatrixSize}, vf{f, MatrixSize};
+    _p_Mat m;
+    SSimTime = t;
+    userData.SimulationTime = t;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (long q = 0; q < k; q++) {
+        userData.GlobalIndex = (int)rows[q];
+        userData.LocalIndex = (int)rows[q];
+        if (which == 0) IteratorFunction(&vx, &vf, &userData);
+        else IteratorJacobian(&vx, &m, &userData);
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
 }
 
 /* FormFunction(x) -> f (compsim/PetscAUX.cpp:59-104) at simulation time t. */

@@ -187,3 +187,31 @@ def assembly_state(grid, d, device, seed: int = 4):
         grid.set_state(med, P.cpu().numpy(), sat.cpu().numpy(), o["x"].cpu().numpy(), o["y"].cpu().numpy(),
                        z.cpu().numpy(), o["label"].cpu().numpy(), rho.cpu().numpy())
     return p0
+
+
+def assembly_spec(d) -> dict:
+    """``deck.write_deck`` spec of an assembly deck ``d`` for readers of the
+    reference's deck format: the same grid, rock, saturation tables and
+    controls.  The keywords cannot carry a seeded component table (named
+    components come from the library, user components from SG/TB
+    correlations), so the components are placeholder library names and the
+    table is replaced after loading; the initial state is likewise a
+    placeholder for ``assembly_state``'s.  ``parse_deck`` of the written text
+    with ``d``'s component table reproduces ``d``."""
+    from .deck import COMPONENT_LIBRARY, TIME_FACTOR
+    names = list(COMPONENT_LIBRARY)[:d.nc]
+    z = np.full(d.nc, 1.0 / d.nc)
+    return dict(grid=(d.nx, d.ny, d.nz), di=d.di, dj=d.dj, dk=d.dk, por=d.por, fpor=d.fpor, permi=d.perm[0],
+                permj=d.perm[1], permk=d.perm[2], fpermi=d.fperm[0], fpermj=d.fperm[1], fpermk=d.fperm[2],
+                lf=d.lf, re_f=d.re_f, model="PR" if d.eos == 0 else "SRK", comps=names, bic=np.zeros((d.nc, d.nc)),
+                sgt=d.sgt, swt=d.swt, refp=d.refp, cpor=d.cpor, dcpor=d.dcpor, wells=[],
+                restemp_c=d.restemp - 273.15, wat_ro=d.wat_ro, wat_mu=d.wat_mu, dt=d.dt / TIME_FACTOR,
+                cdif=d.cdif, ipress=2e7, iws=0.2, igc=z.tolist(), fipress=2e7, fiws=0.0, figc=z.tolist())
+
+
+def with_table(parsed, d):
+    """``parsed`` (a ``Deck`` read from ``assembly_spec(d)``'s text) with
+    ``d``'s component table."""
+    for k in ("tc", "pc", "acf", "mw", "vc", "zc", "parachor", "kij"):
+        setattr(parsed, k, np.array(getattr(d, k), dtype=float))
+    return parsed

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from osiris_b200 import deck
+from osiris_b200 import deck, workloads
 
 needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference library missing")
 
@@ -68,6 +68,20 @@ def test_write_parse_roundtrip(name, tmp_path):
     assert d.perm.shape == (3, d.cells) and (d.perm > 0).all()
     assert d.kij.shape == (d.nc, d.nc) and np.array_equal(d.kij, d.kij.T)
     assert d.wells_f.shape == (len(d.wells_i), d.nc + 6)
+
+
+def test_spec_round_trip(tmp_path):
+    """The written deck, read back with the seeded table, is the bench's deck
+    (apart from the placeholder initial state and the time controls)."""
+    d = workloads.assembly_deck(6, 5, 4)
+    path = os.path.join(str(tmp_path), "a.dat")
+    deck.write_deck(path, workloads.assembly_spec(d))
+    q = workloads.with_table(deck.parse_deck(path), d)
+    skip = {"p0", "fp0", "sw0", "fsw0", "z0", "fz0", "total_time", "dtmax", "extra", "initcond", "pnc", "unc"}
+    for k, v in vars(d).items():
+        if k not in skip:
+            assert np.array_equal(np.asarray(v), np.asarray(getattr(q, k))), k
+    assert q.nc == d.nc
 
 
 def test_missing_required_keyword(tmp_path):
