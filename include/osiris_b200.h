@@ -332,6 +332,47 @@ osr_status osr_grid_phase_ctrl(osr_grid *grid, void *stream);
  * Synchronises `stream` (the new row count and PCoeff come back to the host). */
 osr_status osr_grid_update_all_full(osr_grid *grid, const double *d_x, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Linear solve of the Newton system (replaces the KSPSolve inside SNESSolve
+ * of SolveNonLinear, compsim/PetscAUX.cpp:631-646, 672-698: SNESKSPONLY,
+ * KSPBCGS, PCVPBJACOBI over the PJac block sizes, KSPSetTolerances with the
+ * deck's RELTOL / ABSTOL / DIVTOL / MAXITERS, compsim/Data_Input.cpp:232-266).
+ * The matrix is the compact Jacobian of osr_grid_jacobian for the grid's
+ * current row layout; vectors are DEVICE arrays of the layout's row count.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    double rtol;      /* RELTOL, default 1e-18 */
+    double atol;      /* ABSTOL, default 1e-50 */
+    double dtol;      /* DIVTOL, default 1e3 */
+    int max_it;       /* MAXITERS, default 5000 */
+    int check_every;  /* iterations enqueued between host status reads (8) */
+} osr_ksp_opts;
+
+typedef struct {
+    int reason;       /* PETSc KSPConvergedReason: 2 CONVERGED_RTOL, 3 CONVERGED_ATOL,
+                         -3 DIVERGED_ITS, -4 DIVERGED_DTOL, -5 DIVERGED_BREAKDOWN,
+                         -9 DIVERGED_NANORINF, -11 DIVERGED_PC_FAILED (zero pivot) */
+    int its;          /* iterations taken */
+    double rnorm0;    /* |B b|_2, the initial preconditioned residual */
+    double rnorm;     /* final preconditioned residual 2-norm */
+} osr_ksp_info;
+
+/* The reference's defaults (compsim/Data_Input.cpp:232-266). */
+void osr_ksp_default_opts(osr_ksp_opts *opts);
+
+/* y = J x (MatMult) on the compact Jacobian d_vals.  Asynchronous. */
+osr_status osr_grid_jacobian_apply(osr_grid *grid, const double *d_vals, const double *d_x, double *d_y,
+                                   void *stream);
+
+/* Solve J d_sol = d_rhs from a zero initial guess with left-preconditioned
+ * BiCGStab and the inverse diagonal blocks of J (one block per cell-medium)
+ * as preconditioner, PETSc's KSPBCGS + PCVPBJACOBI.  opts may be null (the
+ * defaults).  Synchronises `stream` every opts->check_every iterations; the
+ * outcome is in info (may be null): a solve that does not converge returns
+ * OSR_OK with a negative info->reason, as KSPSolve does. */
+osr_status osr_grid_ksp_solve(osr_grid *grid, const double *d_vals, const double *d_rhs, double *d_sol,
+                              const osr_ksp_opts *opts, osr_ksp_info *info, void *stream);
+
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The
  * denominator of the flash kernel's roofline.  No reference counterpart. */

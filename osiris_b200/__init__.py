@@ -42,6 +42,27 @@ class _CFlashOut(ctypes.Structure):
                 ("rr_iters", _vp), ("dlnphi_dx", _vp), ("dlnphi_dP", _vp)]
 
 
+class KspOpts(ctypes.Structure):
+    """osr_ksp_opts: RELTOL, ABSTOL, DIVTOL, MAXITERS and the host poll interval."""
+    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("dtol", ctypes.c_double),
+                ("max_it", ctypes.c_int), ("check_every", ctypes.c_int)]
+
+
+class KspInfo(ctypes.Structure):
+    """osr_ksp_info: PETSc KSPConvergedReason, iterations, residual norms."""
+    _fields_ = [("reason", ctypes.c_int), ("its", ctypes.c_int), ("rnorm0", ctypes.c_double),
+                ("rnorm", ctypes.c_double)]
+
+
+def ksp_opts(**kw) -> KspOpts:
+    """The reference's KSP tolerances (osr_ksp_default_opts) with overrides."""
+    o = KspOpts()
+    lib().osr_ksp_default_opts(ctypes.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
 FLASH_OUTPUTS = ("label", "L", "x", "y", "Zl", "Zg", "iters", "rr_iters", "dlnphi_dx", "dlnphi_dP")
 
 
@@ -75,6 +96,8 @@ def _ctype(decl: str):
     Python int without this would truncate it to a C int."""
     if "*" in decl:
         return ctypes.c_char_p if re.match(r"(const\s+)?char\s*\*\s*\w*$", decl) else ctypes.c_void_p
+    if decl.strip() == "void":
+        return None
     base = re.sub(r"\s+\w+$", "", decl.strip()) if len(decl.split()) > 1 else decl.strip()
     if base not in _SCALARS:
         raise OsrError(f"unmapped C type in header: {decl!r}")
@@ -427,6 +450,24 @@ class Grid:
         r, c, v = rows.cpu().numpy().ravel(), cols.cpu().numpy().ravel(), vals.cpu().numpy().ravel()
         keep = r >= 0
         return r[keep], c[keep], v[keep]
+
+    # -- linear solve ----------------------------------------------------------
+    def jacobian_apply(self, vals, d_x, d_y, stream=None):
+        """d_y = J d_x on the compact Jacobian values (MatMult)."""
+        _check(lib().osr_grid_jacobian_apply(self._h, _vp(vals.data_ptr()), _vp(d_x.data_ptr()),
+                                             _vp(d_y.data_ptr()), None if stream is None else _vp(stream)),
+               "osr_grid_jacobian_apply")
+
+    def ksp_solve(self, vals, d_rhs, d_sol, stream=None, **opts) -> dict:
+        """Solve J d_sol = d_rhs (KSPBCGS + PCVPBJACOBI, zero initial guess);
+        keyword overrides of the reference's tolerances: rtol, atol, dtol,
+        max_it, check_every.  Returns reason, its, rnorm0, rnorm."""
+        o = ksp_opts(**opts)
+        info = KspInfo()
+        _check(lib().osr_grid_ksp_solve(self._h, _vp(vals.data_ptr()), _vp(d_rhs.data_ptr()),
+                                        _vp(d_sol.data_ptr()), ctypes.byref(o), ctypes.byref(info),
+                                        None if stream is None else _vp(stream)), "osr_grid_ksp_solve")
+        return {"reason": info.reason, "its": info.its, "rnorm0": info.rnorm0, "rnorm": info.rnorm}
 
     def get(self, name: str) -> np.ndarray:
         L = lib()

@@ -245,6 +245,7 @@ osr_status grid_assembly_init(osr_grid &g, const osr_model *md) {
 }
 
 void grid_assembly_free(osr_grid &g) {
+    ksp_free(g);
     void *ptrs[] = {g.tor, g.rowoff, g.sizes, g.pmax, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws,
                     g.jw_q, g.jw_pi, g.j_stream_y, g.jw_iw, g.j_dmu, g.j_dh};
     for (void *p : ptrs)

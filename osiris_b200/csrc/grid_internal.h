@@ -43,6 +43,8 @@ struct osr_grid {
     double *jw_q = nullptr, *jw_pi = nullptr, *j_stream_y = nullptr;
     int *jw_iw = nullptr;
     double *j_dmu = nullptr, *j_dh = nullptr;   // Jacobian derivative tables [2][N+1][2 cells], [2][8+2N][2 cells]
+    // linear-solve workspace (ksp.cu), allocated on first use
+    struct osr_ksp_work *ksp = nullptr;
 };
 
 namespace osr {
@@ -53,6 +55,7 @@ osr_status grid_unpack(osr_grid &g, const double *d_x, cudaStream_t st);
 double peaceman_re(const double *di, const double *dj, int nx, int ny, int ix, int iy);
 osr_status grid_assembly_init(osr_grid &g, const osr_model *md);
 void grid_assembly_free(osr_grid &g);
+void ksp_free(osr_grid &g);
 // Per-component constants at the reservoir temperature, formed with the
 // reference's expressions: EOS_Init (compsim/Init_Calcs.cpp:66-97), Tr_Mu
 // (:48-64) and the pair factors of CalcDiffusion (compsim/Mass_Tran.cpp:43-46).

@@ -1,0 +1,200 @@
+// Host side of the device linear solve (ksp_kernels.cuh): the KSPSolve of
+// SolveNonLinear (compsim/PetscAUX.cpp:631-646, 672-698) on the compact
+// Jacobian, and the matrix-vector product alone (MatMult).
+#include <cuda_runtime.h>
+#include <cstring>
+#include "grid_internal.h"
+#include "ksp_kernels.cuh"
+
+struct osr_ksp_work {
+    long rows_cap = 0, blocks = 0;
+    int nc = 0;
+    double *r = nullptr, *r0 = nullptr, *p = nullptr, *v = nullptr, *t = nullptr, *s = nullptr, *w = nullptr;
+    double *inv = nullptr;
+    double *part = nullptr;
+    osrk::KspScal *scal = nullptr;   // device
+    osrk::KspScal *host = nullptr;   // pinned
+};
+
+namespace osr {
+
+#define KSP_CUDA(call)                                     \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return OSR_ERR_CUDA;        \
+    } while (0)
+
+void ksp_free(osr_grid &g) {
+    osr_ksp_work *k = g.ksp;
+    if (!k) return;
+    void *ptrs[] = {k->r, k->r0, k->p, k->v, k->t, k->s, k->w, k->inv, k->part, k->scal};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    if (k->host) cudaFreeHost(k->host);
+    delete k;
+    g.ksp = nullptr;
+}
+
+// Vectors sized for the largest row layout (every cell-medium two-phase), so
+// phase changes never reallocate.
+static osr_status ksp_ensure(osr_grid &g) {
+    if (g.ksp) return OSR_OK;
+    osr_ksp_work *k = new osr_ksp_work();
+    g.ksp = k;
+    const int bs = 2 * g.nc + 4;
+    k->nc = g.nc;
+    k->blocks = 2 * g.cells;
+    k->rows_cap = k->blocks * bs;
+    const size_t vb = (size_t)k->rows_cap * sizeof(double);
+    double **vecs[] = {&k->r, &k->r0, &k->p, &k->v, &k->t, &k->s, &k->w};
+    for (double **q : vecs) KSP_CUDA(cudaMalloc((void **)q, vb));
+    KSP_CUDA(cudaMalloc((void **)&k->inv, (size_t)k->blocks * bs * bs * sizeof(double)));
+    KSP_CUDA(cudaMalloc((void **)&k->part, (size_t)osrk::kParts * osrk::kRedBlocks * sizeof(double)));
+    KSP_CUDA(cudaMalloc((void **)&k->scal, sizeof(osrk::KspScal)));
+    KSP_CUDA(cudaMallocHost((void **)&k->host, sizeof(osrk::KspScal)));
+    return OSR_OK;
+}
+
+static osrk::KView kview(const osr_grid &g, const double *vals) {
+    osrk::KView v;
+    v.nc = g.nc;
+    v.nx = g.nx;
+    v.ny = g.ny;
+    v.nz = g.nz;
+    v.n = g.cells;
+    v.rows = g.n_rows;
+    v.rowoff = g.rowoff;
+    v.lab_m = g.m[0].label;
+    v.lab_f = g.m[1].label;
+    v.vals = vals;
+    v.entries = osrj::Layout(g.nc).ET;
+    return v;
+}
+
+static unsigned spmv_blocks(long nb) {
+    long b = (nb + 127) / 128;
+    if (b > 148L * 32) b = 148L * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+static unsigned vec_blocks(long n) {
+    long b = (n + 255) / 256;
+    if (b > 148L * 16) b = 148L * 16;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+static unsigned inv_blocks(long nb) {
+    long b = (nb + osrk::kInvWarps - 1) / osrk::kInvWarps;
+    if (b > 148L * 64) b = 148L * 64;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+template <int N>
+static osr_status spmv_n(const osr_grid &g, const double *vals, const double *x, double *y, cudaStream_t st) {
+    const osrk::KView v = kview(g, vals);
+    osrk::spmv_kernel<N><<<spmv_blocks(2 * g.cells), 128, 0, st>>>(v, x, y, nullptr);
+    KSP_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
+template <int N>
+static osr_status solve_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
+                          osr_ksp_info *info, cudaStream_t st) {
+    osr_status rc = ksp_ensure(g);
+    if (rc != OSR_OK) return rc;
+    osr_ksp_work &k = *g.ksp;
+    const osrk::KView v = kview(g, vals);
+    const long n = g.n_rows, nb = 2 * g.cells;
+    osrk::KspScal h;
+    std::memset(&h, 0, sizeof(h));
+    h.rtol = o.rtol;
+    h.atol = o.atol;
+    h.dtol = o.dtol;
+    h.max_it = o.max_it;
+    *k.host = h;
+    KSP_CUDA(cudaMemcpyAsync(k.scal, k.host, sizeof(h), cudaMemcpyHostToDevice, st));
+    const unsigned sb = spmv_blocks(nb), vbk = vec_blocks(n), ib = inv_blocks(nb);
+    const unsigned tpb = 32 * osrk::kInvWarps;
+    osrk::bjac_invert_kernel<N><<<ib, tpb, 0, st>>>(v, k.inv, k.scal);
+    osrk::bjac_apply_kernel<N, 0><<<osrk::kRedBlocks, tpb, 0, st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
+    osrk::bcgs_setup_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.r0, k.p, k.v, x);
+    KSP_CUDA(cudaGetLastError());
+    const int every = o.check_every > 0 ? o.check_every : 8;
+    int launched = 0;
+    for (;;) {
+        for (int q = 0; q < every && launched < o.max_it; q++, launched++) {
+            osrk::bcgs_p_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.p, k.v, k.scal);
+            osrk::spmv_kernel<N><<<sb, 128, 0, st>>>(v, k.p, k.t, k.scal);
+            osrk::bjac_apply_kernel<N, 1><<<osrk::kRedBlocks, tpb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part,
+                                                                            k.scal);
+            osrk::bcgs_s_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.v, k.s, k.scal);
+            osrk::spmv_kernel<N><<<sb, 128, 0, st>>>(v, k.s, k.w, k.scal);
+            osrk::bjac_apply_kernel<N, 2><<<osrk::kRedBlocks, tpb, 0, st>>>(v, k.inv, k.w, k.t, k.s, k.part,
+                                                                            k.scal);
+            osrk::bcgs_xr_kernel<<<osrk::kRedBlocks, osrk::kRedThreads, 0, st>>>(n, x, k.p, k.s, k.t, k.r, k.r0,
+                                                                                 k.part, k.scal);
+        }
+        KSP_CUDA(cudaGetLastError());
+        KSP_CUDA(cudaMemcpyAsync(k.host, k.scal, sizeof(h), cudaMemcpyDeviceToHost, st));
+        KSP_CUDA(cudaStreamSynchronize(st));
+        if (k.host->reason != osrk::kItersRunning || launched >= o.max_it) break;
+    }
+    if (info) {
+        info->reason = k.host->reason == osrk::kItersRunning ? osrk::kDivergedIts : k.host->reason;
+        info->its = k.host->its;
+        info->rnorm0 = k.host->rnorm0;
+        info->rnorm = k.host->rnorm;
+    }
+    return OSR_OK;
+}
+
+#define KSP_SWITCH(call)                                                                                  \
+    switch (g->nc) {                                                                                      \
+        case 1: { constexpr int K = 1; return call; }                                                     \
+        case 2: { constexpr int K = 2; return call; }                                                     \
+        case 3: { constexpr int K = 3; return call; }                                                     \
+        case 4: { constexpr int K = 4; return call; }                                                     \
+        case 5: { constexpr int K = 5; return call; }                                                     \
+        case 6: { constexpr int K = 6; return call; }                                                     \
+        case 7: { constexpr int K = 7; return call; }                                                     \
+        case 8: { constexpr int K = 8; return call; }                                                     \
+        case 9: { constexpr int K = 9; return call; }                                                     \
+        case 10: { constexpr int K = 10; return call; }                                                   \
+        case 11: { constexpr int K = 11; return call; }                                                   \
+        case 12: { constexpr int K = 12; return call; }                                                   \
+        case 13: { constexpr int K = 13; return call; }                                                   \
+        case 14: { constexpr int K = 14; return call; }                                                   \
+        case 15: { constexpr int K = 15; return call; }                                                   \
+        case 16: { constexpr int K = 16; return call; }                                                   \
+        default: return OSR_ERR_NC;                                                                       \
+    }
+
+}  // namespace osr
+
+extern "C" {
+
+void osr_ksp_default_opts(osr_ksp_opts *o) {
+    if (!o) return;
+    o->rtol = 1e-18;
+    o->atol = 1e-50;
+    o->dtol = 1e3;
+    o->max_it = 5000;
+    o->check_every = 8;
+}
+
+osr_status osr_grid_jacobian_apply(osr_grid *g, const double *d_vals, const double *d_x, double *d_y, void *stream) {
+    if (!g || !d_vals || !d_x || !d_y || !g->rowoff || g->n_rows <= 0) return OSR_ERR_ARG;
+    KSP_SWITCH(osr::spmv_n<K>(*g, d_vals, d_x, d_y, (cudaStream_t)stream))
+}
+
+osr_status osr_grid_ksp_solve(osr_grid *g, const double *d_vals, const double *d_rhs, double *d_sol,
+                              const osr_ksp_opts *opts, osr_ksp_info *info, void *stream) {
+    if (!g || !d_vals || !d_rhs || !d_sol || !g->rowoff || g->n_rows <= 0) return OSR_ERR_ARG;
+    osr_ksp_opts o;
+    osr_ksp_default_opts(&o);
+    if (opts) o = *opts;
+    if (o.max_it < 0 || !(o.rtol >= 0) || !(o.atol >= 0)) return OSR_ERR_ARG;
+    KSP_SWITCH(osr::solve_n<K>(*g, d_vals, d_rhs, d_sol, o, info, (cudaStream_t)stream))
+}
+
+}  // extern "C"
