@@ -373,6 +373,51 @@ osr_status osr_grid_jacobian_apply(osr_grid *grid, const double *d_vals, const d
 osr_status osr_grid_ksp_solve(osr_grid *grid, const double *d_vals, const double *d_rhs, double *d_sol,
                               const osr_ksp_opts *opts, osr_ksp_info *info, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Time stepping: one osr_sim_step is one pass of the reference's main loop
+ * (compsim/PrimeSim.cpp:93-104).  SolveNonLinear (compsim/PetscAUX.cpp:
+ * 566-731): the unknowns of the current state, F and J there, one linear
+ * solve (osr_grid_ksp_solve), x - dx; accepted when the solve converged and
+ * |dx|_1 / rows <= 1e-2 (TOLMAIN), then UpdateAll(x, true) and CreateBackups.
+ * TimeStepCtrl (compsim/Do_Time_Step.cpp:391-470): the time advances by Dt,
+ * Dt x 1.03 after every 5 accepted steps, clamped to [1e-10 s, max_dt] and
+ * cut to the next marker; a rejected pass divides Dt by 1.5 and restores the
+ * backed-up state (RestoreBackups + PJac, :354-389).
+ * ------------------------------------------------------------------------- */
+typedef struct osr_sim osr_sim;
+
+typedef struct {
+    double sim_time;  /* simulation time after the pass (s) */
+    double dt;        /* Dt of the next pass (s) */
+    int accepted;     /* the pass's solve was accepted */
+    int finished;     /* the last time marker was reached (the reference's loop ends) */
+    int ksp_reason;   /* osr_ksp_info.reason of the pass's linear solve */
+    int ksp_its;
+    double vnorm;     /* |dx|_1 / rows */
+    long rows;        /* rows of the pass's system */
+} osr_step_info;
+
+/* A run on `grid` from its current state (set by the caller): markers are
+ * the ascending time markers (s) -- every well's start and end time and the
+ * total time, merged as ManageTSMarker does (compsim/Init_Calcs.cpp:
+ * 1133-1157) -- dt the first Dt, max_dt the deck's DTMAX.  Runs the property
+ * sweeps and the row layout of the current state and takes the first backup
+ * (compsim/PrimeSim.cpp:85-86).  The grid must outlive the run. */
+osr_status osr_sim_create(osr_grid *grid, const double *markers, int n_markers, double dt, double max_dt,
+                          osr_sim **sim);
+
+/* One pass (see above).  opts: the linear solve's tolerances (null: the
+ * reference's defaults).  Synchronises `stream`.  Returns
+ * OSR_ERR_UNSUPPORTED when Dt falls below 1e-10 s (the reference stops with
+ * "MINDT was hit"); after the last marker a call does nothing and reports
+ * finished. */
+osr_status osr_sim_step(osr_sim *sim, const osr_ksp_opts *opts, osr_step_info *info, void *stream);
+
+/* Current simulation time and Dt (either may be null). */
+osr_status osr_sim_time(osr_sim *sim, double *sim_time, double *dt);
+
+osr_status osr_sim_destroy(osr_sim *sim);
+
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA
  * counts 2): a dependent-FMA microbenchmark, best of 5 launches.  The
  * denominator of the flash kernel's roofline.  No reference counterpart. */

@@ -405,6 +405,22 @@ class RefDeck:
         return float(self.lib.ref_time_rows(_p(rows), ctypes.c_long(len(rows)), _p(x), _p(f), ctypes.c_double(t),
                                             int(which)))
 
+    def create_backups(self, t: float):
+        self.lib.ref_create_backups(ctypes.c_double(t))
+
+    def time_step_ctrl(self, t: float, rejected: bool):
+        """TimeStepCtrl after a pass: (flag, new time); Dt in scalar("Dt")."""
+        tt = ctypes.c_double(t)
+        flag = self.lib.ref_time_step_ctrl(ctypes.byref(tt), int(bool(rejected)))
+        self.rows = int(self.lib_info()[5])
+        return int(flag), tt.value
+
+    def time_markers(self):
+        out = np.zeros(2 * self.nwells + 1)
+        ctrl = ctypes.c_int()
+        k = self.lib.ref_time_markers(_p(out), ctypes.byref(ctrl))
+        return out[:k], ctrl.value
+
     def form_function(self, x, t: float = 0.0) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64).copy()
         f = np.zeros(self.rows)

@@ -165,6 +165,11 @@ int ref_deck_open(const char *path) {
     g_alloc_nc = -1;
     MPIsize = 1;
     MPIRank = 0;
+    /* time-control state as a fresh process starts with it */
+    incCount = 0;
+    TSMCtrl = 0;
+    repStat = 0;
+    maxNR = 0;
     Data_Input(fin);
     fin.close();
     ManageTSMarker();
@@ -447,6 +452,30 @@ double ref_time_rows(const long *rows, long k, double *x, double *f, double t, i
     }
     const auto t1 = std::chrono::steady_clock::now();
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+/* CreateBackups (compsim/Do_Time_Step.cpp:86-159). */
+int ref_create_backups(double t) {
+    CreateBackups(t);
+    return 0;
+}
+
+/* TimeStepCtrl (compsim/Do_Time_Step.cpp:391-470) after a pass whose solve was
+ * accepted (rejected = 0) or not (rejected = 1), as the main loop sets
+ * repStat (compsim/PrimeSim.cpp:95-101): advances *t, updates Dt, and after a
+ * rejection restores the backups and the row layout.  Returns its flag
+ * (1 when the last time marker is reached). */
+int ref_time_step_ctrl(double *t, int rejected) {
+    repStat = rejected ? 1 : 0;
+    return (int)TimeStepCtrl(t);
+}
+
+/* The time markers (TStepMarker[0..TSMSize), after ManageTSMarker) and the
+ * index of the next one; returns TSMSize. */
+int ref_time_markers(double *out, int *ctrl) {
+    for (int i = 0; i < TSMSize; i++) out[i] = TStepMarker[i];
+    if (ctrl) *ctrl = TSMCtrl;
+    return TSMSize;
 }
 
 /* FormFunction(x) -> f (compsim/PetscAUX.cpp:59-104) at simulation time t. */

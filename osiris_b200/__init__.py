@@ -63,6 +63,13 @@ def ksp_opts(**kw) -> KspOpts:
     return o
 
 
+class StepInfo(ctypes.Structure):
+    """osr_step_info of one pass of the main loop."""
+    _fields_ = [("sim_time", ctypes.c_double), ("dt", ctypes.c_double), ("accepted", ctypes.c_int),
+                ("finished", ctypes.c_int), ("ksp_reason", ctypes.c_int), ("ksp_its", ctypes.c_int),
+                ("vnorm", ctypes.c_double), ("rows", ctypes.c_long)]
+
+
 FLASH_OUTPUTS = ("label", "L", "x", "y", "Zl", "Zg", "iters", "rr_iters", "dlnphi_dx", "dlnphi_dP")
 
 
@@ -483,3 +490,46 @@ class Grid:
         if shape is None:
             shape = () if planes == 1 else ((12, 3) if key == "trans" else (3, 3) if key == "transS" else (planes,))
         return out.reshape(shape + (self.cells,))
+
+
+class Sim:
+    """A run of the reference's main loop on the device (osr_sim_*): one
+    ``step()`` is SolveNonLinear + TimeStepCtrl.  Starts from the grid's
+    current state; ``markers``/``dt`` as ``deck.time_markers`` gives them."""
+
+    def __init__(self, grid: "Grid", markers, dt: float, max_dt: float):
+        self.grid = grid   # the run uses the grid's device state
+        m = np.ascontiguousarray(markers, np.float64)
+        h = ctypes.c_void_p()
+        _check(lib().osr_sim_create(grid._h, m.ctypes.data, len(m), ctypes.c_double(dt), ctypes.c_double(max_dt),
+                                    ctypes.byref(h)), "osr_sim_create")
+        self._h = h
+
+    @classmethod
+    def from_deck(cls, grid: "Grid"):
+        from .deck import time_markers
+        m, dt = time_markers(grid.deck)
+        return cls(grid, m, dt, grid.deck.dtmax)
+
+    def step(self, stream=None, **ksp) -> dict:
+        o = ksp_opts(**ksp)
+        info = StepInfo()
+        _check(lib().osr_sim_step(self._h, ctypes.byref(o), ctypes.byref(info),
+                                  None if stream is None else _vp(stream)), "osr_sim_step")
+        return {k: getattr(info, k) for k, _ in StepInfo._fields_}
+
+    def time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _check(lib().osr_sim_time(self._h, ctypes.byref(t), ctypes.byref(dt)), "osr_sim_time")
+        return t.value, dt.value
+
+    def close(self):
+        if self._h:
+            lib().osr_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,264 @@
+// Time stepping on the device: one call of osr_sim_step is one pass of the
+// reference's main loop (compsim/PrimeSim.cpp:93-104):
+//
+//   SolveNonLinear (compsim/PetscAUX.cpp:566-731) with SNESKSPONLY: from the
+//   unknowns of the current state (InitGuess2), F(x0) (FormFunction), J(x0)
+//   (FormJacobian), one linear solve J dx = F (osr_grid_ksp_solve),
+//   x1 = x0 - dx; the step is accepted when the solve converged and
+//   |dx|_1 / rows <= TOLMAIN (1e-2) is a number; an accepted step ends with
+//   UpdateAll(x1, true) (phase control, PCoeff, PJac, properties) and
+//   CreateBackups (compsim/Do_Time_Step.cpp:86-159);
+//
+//   TimeStepCtrl (compsim/Do_Time_Step.cpp:391-470): after an accepted step
+//   the time advances by Dt, Dt grows by 1.03 after every 5 accepted steps
+//   (NTIMESTERINC, TIME_STEP_INC), is clamped to [MINDT, DTMAX] and cut to
+//   the next time marker (a well's start or end, the total time) when it
+//   would pass it or land within 1e-5 s of it; after a rejected step Dt is
+//   divided by 1.5 (TIME_STEP_DEC) and the backed-up state (pressures,
+//   saturations, phase compositions, labels, well latches) is restored and
+//   the row layout rebuilt (RestoreBackups, PJac).  A Dt below MINDT (1e-10 s)
+//   ends the run with an error, where the reference terminates.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "grid_internal.h"
+#include "jacobian_kernels.cuh"
+
+namespace {
+
+constexpr double kTolMain = 1e-2;       // TOLMAIN
+constexpr double kMinDt = 1e-10;        // MINDT
+constexpr double kStepInc = 1.03;       // TIME_STEP_INC
+constexpr double kStepDec = 1.5;        // TIME_STEP_DEC
+constexpr int kStepsPerInc = 5;         // NTIMESTERINC
+constexpr double kMarkerTol = 1e-5;     // TSTEPIF
+constexpr int kSumBlocks = 296;
+
+// x <- x - dx and per-CTA partial sums of |dx| (fixed order).
+__global__ void __launch_bounds__(256) update_norm1_kernel(long n, double *__restrict__ x,
+                                                           const double *__restrict__ dx, double *part) {
+    __shared__ double sm[8];
+    double a = 0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double d = dx[i];
+        x[i] -= d;
+        a += fabs(d);
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sm[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+__global__ void sum_parts_kernel(const double *part, int n, double *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double t = 0;
+        for (int i = 0; i < n; i++) t += part[i];
+        *out = t;
+    }
+}
+
+}  // namespace
+
+struct osr_sim {
+    osr_grid *g = nullptr;
+    double sim_time = 0, dt = 0, max_dt = 0;
+    int inc_count = 0, tsm_ctrl = 0;
+    std::vector<double> markers;
+    long rows_cap = 0;
+    double *x = nullptr, *f = nullptr, *dx = nullptr, *vals = nullptr, *part = nullptr;
+    double *bP[2] = {nullptr, nullptr}, *bsat[2] = {nullptr, nullptr}, *bx[2] = {nullptr, nullptr},
+           *by[2] = {nullptr, nullptr};
+    signed char *blab[2] = {nullptr, nullptr};
+    std::vector<unsigned char> bcond;
+    double *h_sum = nullptr;   // pinned
+};
+
+namespace {
+
+#define SIM_CUDA(call)                                     \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return OSR_ERR_CUDA;        \
+    } while (0)
+
+void sim_free(osr_sim *s) {
+    void *ptrs[] = {s->x, s->f, s->dx, s->vals, s->part, s->bP[0], s->bP[1], s->bsat[0], s->bsat[1],
+                    s->bx[0], s->bx[1], s->by[0], s->by[1], s->blab[0], s->blab[1]};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (s->h_sum) cudaFreeHost(s->h_sum);
+    delete s;
+}
+
+// CreateBackups / RestoreBackups: the primary state of both continua.
+osr_status copy_state(osr_sim &s, bool to_backup, cudaStream_t st) {
+    osr_grid &g = *s.g;
+    const long n = g.cells, nc = g.nc;
+    for (int m = 0; m < 2; m++) {
+        const osr::MediumFields &F = g.m[m];
+        struct {
+            void *live, *bak;
+            size_t bytes;
+        } items[] = {{F.P, s.bP[m], (size_t)3 * n * 8},
+                     {F.sat, s.bsat[m], (size_t)3 * n * 8},
+                     {F.x, s.bx[m], (size_t)nc * n * 8},
+                     {F.y, s.by[m], (size_t)nc * n * 8},
+                     {F.label, s.blab[m], (size_t)n}};
+        for (auto &it : items)
+            SIM_CUDA(cudaMemcpyAsync(to_backup ? it.bak : it.live, to_backup ? it.live : it.bak, it.bytes,
+                                     cudaMemcpyDeviceToDevice, st));
+    }
+    if (to_backup) {
+        s.bcond = g.cond_host;
+    } else {
+        for (int w = 0; w < g.nwells; w++)
+            if (g.cond_host[w] != s.bcond[w]) {
+                osr_status rc = osr_grid_set_well_condition(&g, w, s.bcond[w]);
+                if (rc != OSR_OK) return rc;
+            }
+    }
+    return OSR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+osr_status osr_sim_create(osr_grid *g, const double *markers, int n_markers, double dt, double max_dt,
+                          osr_sim **out) {
+    if (!g || !out || !markers || n_markers < 1 || !(dt > 0) || !(max_dt > 0)) return OSR_ERR_ARG;
+    *out = nullptr;
+    osr_sim *s = new osr_sim();
+    s->g = g;
+    s->dt = dt;
+    s->max_dt = max_dt;
+    s->markers.assign(markers, markers + n_markers);
+    const long n = g->cells, nc = g->nc;
+    s->rows_cap = 2 * n * (2 * nc + 4);
+    const long chunks = (2 * n + 31) / 32;
+    const size_t vals = (size_t)chunks * osrj::Layout((int)nc).ET * 32;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void **p, size_t b) {
+        if (e == cudaSuccess) e = cudaMalloc(p, b);
+    };
+    A((void **)&s->x, s->rows_cap * 8);
+    A((void **)&s->f, s->rows_cap * 8);
+    A((void **)&s->dx, s->rows_cap * 8);
+    A((void **)&s->vals, vals * 8);
+    A((void **)&s->part, kSumBlocks * 8 + 8);
+    for (int m = 0; m < 2; m++) {
+        A((void **)&s->bP[m], 3 * n * 8);
+        A((void **)&s->bsat[m], 3 * n * 8);
+        A((void **)&s->bx[m], nc * n * 8);
+        A((void **)&s->by[m], nc * n * 8);
+        A((void **)&s->blab[m], n);
+    }
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&s->h_sum, 8);
+    if (e != cudaSuccess) {
+        sim_free(s);
+        return OSR_ERR_CUDA;
+    }
+    // the state the caller set is the first backup (UpdateDependencies(true) +
+    // CreateBackups before the main loop, compsim/PrimeSim.cpp:85-86)
+    osr_status rc = osr_grid_refresh_layout(g, nullptr);
+    if (rc == OSR_OK) rc = osr_grid_update_dependencies(g, nullptr);
+    if (rc == OSR_OK) rc = copy_state(*s, true, nullptr);
+    if (rc == OSR_OK && cudaStreamSynchronize(nullptr) != cudaSuccess) rc = OSR_ERR_CUDA;
+    if (rc != OSR_OK) {
+        sim_free(s);
+        return rc;
+    }
+    *out = s;
+    return OSR_OK;
+}
+
+osr_status osr_sim_destroy(osr_sim *s) {
+    if (!s) return OSR_ERR_ARG;
+    sim_free(s);
+    return OSR_OK;
+}
+
+osr_status osr_sim_time(osr_sim *s, double *sim_time, double *dt) {
+    if (!s) return OSR_ERR_ARG;
+    if (sim_time) *sim_time = s->sim_time;
+    if (dt) *dt = s->dt;
+    return OSR_OK;
+}
+
+osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *info, void *stream) {
+    if (!s) return OSR_ERR_ARG;
+    osr_grid *g = s->g;
+    cudaStream_t st = (cudaStream_t)stream;
+    osr_status rc;
+    osr_step_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    if (s->tsm_ctrl >= (int)s->markers.size()) {
+        inf.finished = 1;
+        inf.sim_time = s->sim_time;
+        inf.dt = s->dt;
+        if (info) *info = inf;
+        return OSR_OK;
+    }
+    // SolveNonLinear
+    if ((rc = osr_grid_set_controls(g, s->dt, 0.0)) != OSR_OK) return rc;
+    const long rows = g->n_rows;
+    inf.rows = rows;
+    if ((rc = osr_grid_init_guess(g, s->x, stream)) != OSR_OK) return rc;
+    if ((rc = osr_grid_form_function(g, s->x, s->f, s->sim_time, stream)) != OSR_OK) return rc;
+    if ((rc = osr_grid_jacobian(g, s->sim_time, s->vals, stream)) != OSR_OK) return rc;
+    osr_ksp_info ki;
+    if ((rc = osr_grid_ksp_solve(g, s->vals, s->f, s->dx, opts, &ki, stream)) != OSR_OK) return rc;
+    inf.ksp_reason = ki.reason;
+    inf.ksp_its = ki.its;
+    long nb = (rows + 255) / 256;
+    if (nb > kSumBlocks) nb = kSumBlocks;
+    if (nb < 1) nb = 1;
+    update_norm1_kernel<<<(unsigned)nb, 256, 0, st>>>(rows, s->x, s->dx, s->part);
+    sum_parts_kernel<<<1, 32, 0, st>>>(s->part, (int)nb, s->part + kSumBlocks);
+    SIM_CUDA(cudaGetLastError());
+    SIM_CUDA(cudaMemcpyAsync(s->h_sum, s->part + kSumBlocks, 8, cudaMemcpyDeviceToHost, st));
+    SIM_CUDA(cudaStreamSynchronize(st));
+    const double vnorm = *s->h_sum / (double)rows;
+    inf.vnorm = vnorm;
+    const bool accepted = ki.reason > 0 && !(vnorm > kTolMain) && vnorm == vnorm;
+    inf.accepted = accepted ? 1 : 0;
+    if (accepted) {
+        if ((rc = osr_grid_update_all_full(g, s->x, stream)) != OSR_OK) return rc;
+        if ((rc = copy_state(*s, true, st)) != OSR_OK) return rc;
+    }
+    // TimeStepCtrl
+    if (accepted) {
+        s->sim_time += s->dt;
+        if (++s->inc_count > kStepsPerInc) {
+            s->dt *= kStepInc;
+            s->inc_count = 0;
+        }
+        if (s->dt < kMinDt) s->dt = kMinDt;
+        if (s->dt > s->max_dt) s->dt = s->max_dt;
+        const double mk = s->markers[s->tsm_ctrl];
+        if (s->sim_time + s->dt > mk || std::fabs(s->sim_time + s->dt - mk) < kMarkerTol) {
+            s->dt = mk - s->sim_time;
+            s->tsm_ctrl++;
+        }
+        if (s->tsm_ctrl == (int)s->markers.size()) inf.finished = 1;
+    } else {
+        s->inc_count = 0;
+        s->dt /= kStepDec;
+        if (s->dt < kMinDt) return OSR_ERR_UNSUPPORTED;
+        if ((rc = copy_state(*s, false, st)) != OSR_OK) return rc;
+        if ((rc = osr_grid_refresh_layout(g, stream)) != OSR_OK) return rc;
+    }
+    SIM_CUDA(cudaStreamSynchronize(st));
+    inf.sim_time = s->sim_time;
+    inf.dt = s->dt;
+    if (info) *info = inf;
+    return OSR_OK;
+}
+
+}  // extern "C"

@@ -366,6 +366,36 @@ def parse_deck(path: str) -> Deck:
 
 # ----------------------------------------------------------------------------- writer
 
+TSTEPTOL = 1.0   # markers closer than this (s) merge (compsim/Functions.h:264)
+
+
+def time_markers(d: Deck):
+    """The run's time markers and first step length: every well's start and
+    end time and the total time (compsim/Data_Input.cpp:1205-1344), sorted,
+    with zero markers and markers closer than TSTEPTOL to the next one removed,
+    and a first Dt cut to 1/2.1 of the first marker when it reaches it
+    (ManageTSMarker, compsim/Init_Calcs.cpp:1133-1157).  Returns (markers,
+    dt)."""
+    nw = len(d.wells_i)
+    m = []
+    for w in range(nw):
+        t = int(d.wells_i[w, 0])
+        ts = d.nc + 3 if t in (3, 8) else 3
+        m += [float(d.wells_f[w, ts + 1]), float(d.wells_f[w, ts + 2])]
+    m.append(float(d.total_time))
+    n = 2 * nw
+    m.sort()
+    j = 0
+    for i in range(n):
+        if abs(m[i - j] - m[i - j + 1]) < TSTEPTOL or not m[i - j]:
+            for k in range(i - j, n - j):
+                m[k] = m[k + 1]
+            j += 1
+    m = m[:n - j + 1]
+    dt = d.dt if d.dt < m[0] else m[0] / 2.1
+    return np.array(m), dt
+
+
 def _fmt(v) -> str:
     return repr(float(v)) if not float(v).is_integer() else str(int(v)) if abs(v) < 1e15 else repr(float(v))
 

@@ -91,3 +91,19 @@ def test_missing_required_keyword(tmp_path):
     open(bad, "w").write(text)
     with pytest.raises(deck.DeckError):
         deck.parse_deck(bad)
+
+
+@needs_ref
+@pytest.mark.parametrize("spec", ["plain", "all_wells", "sample", "no_wells"])
+def test_time_markers_match_reference(spec, tmp_path):
+    """The run's time markers and first Dt (Data_Input + ManageTSMarker)."""
+    s = {"plain": deck.config_deck, "all_wells": deck.all_wells_deck, "sample": deck.sample_deck,
+         "no_wells": lambda: deck.config_deck(wells=False)}[spec]()
+    path = os.path.join(str(tmp_path), spec + ".dat")
+    deck.write_deck(path, s)
+    R = oracle.RefDeck(path)
+    m_ref, ctrl = R.time_markers()
+    m, dt = deck.time_markers(deck.parse_deck(path))
+    assert ctrl == 0
+    assert np.array_equal(m, m_ref), (m, m_ref)
+    assert dt == R.scalar("Dt")
