@@ -70,6 +70,8 @@ class StepInfo(ctypes.Structure):
                 ("vnorm", ctypes.c_double), ("rows", ctypes.c_long)]
 
 
+R_GAS = 8.3144621   # RGAS, J/(mol K)
+
 FLASH_OUTPUTS = ("label", "L", "x", "y", "Zl", "Zg", "iters", "rr_iters", "dlnphi_dx", "dlnphi_dP")
 
 
@@ -333,6 +335,34 @@ class Grid:
         r = None if rho is None else np.ascontiguousarray(rho, np.float64)
         _check(lib().osr_grid_set_state(self._h, int(medium), *[a.ctypes.data for a in arrs], lab.ctypes.data,
                                         None if r is None else r.ctypes.data), "osr_grid_set_state")
+
+    def initialize(self, device, stream=None):
+        """The deck's initial state on the device, formed as the reference's
+        start-up forms it: the INITCOND pressures, water saturations and feed
+        compositions (compsim/Data_Input.cpp:1040-1181), a flash of every
+        cell-medium (AllFlash, compsim/Init_Calcs.cpp:949-962; label, phase
+        compositions, oil and gas saturations from the liquid volume fraction
+        and densities from the Z factors as SuccFalsh sets them, :715-737),
+        then UpdateDependencies(true) (compsim/PetscAUX.cpp:500-545): phase
+        control, PCoeff, the row layout and the property sweeps."""
+        import torch
+        d = self.deck
+        fl = Fluid(d.tc, d.pc, d.acf, d.kij, d.eos)
+        for med, (p0, sw0, z0) in enumerate(((d.p0, d.sw0, d.z0), (d.fp0, d.fsw0, d.fz0))):
+            P = torch.tensor(np.ascontiguousarray(p0, np.float64), device=device)
+            T = torch.full_like(P, d.restemp)
+            z = torch.tensor(np.ascontiguousarray(z0, np.float64), device=device)
+            o = flash(fl, P, T, z, derivs=False)
+            L, Zl, Zg = o["L"], o["Zl"], o["Zg"]
+            sw = torch.tensor(np.ascontiguousarray(sw0, np.float64), device=device)
+            liq = Zl * L / (Zl * L + Zg * (1 - L))
+            sat = torch.stack([sw, liq * (1 - sw), (1 - liq) * (1 - sw)])
+            rho = torch.stack([P / (Zl * R_GAS * T), P / (Zg * R_GAS * T)])
+            self.set_state(med, p0, sat.cpu().numpy(), o["x"].cpu().numpy(), o["y"].cpu().numpy(), z0,
+                           o["label"].cpu().numpy(), rho.cpu().numpy())
+        self.phase_ctrl(stream)
+        self.refresh_layout(stream)
+        self.update_dependencies(stream)
 
     def update_dependencies(self, stream=None):
         _check(lib().osr_grid_update_dependencies(self._h, None if stream is None else _vp(stream)),

@@ -150,13 +150,15 @@ def assembly_deck(nx: int = 128, ny: int = 128, nz: int = 32, nc: int = 8, seed:
     d.wells_i = np.zeros((0, 5), dtype=np.int32)
     d.wells_f = np.zeros((0, nc + 6))
     d.dt = 3600.0
+    d.total_time = 17520 * 3600.0   # the sample deck's TOTALT (2 years)
     return d
 
 
-def assembly_state(grid, d, device, seed: int = 4):
+def assembly_state(grid, d, device, seed: int = 4, noise: float = 0.005):
     """Initial two-phase state of the assembly workload on the device: one
     feed composition and the middle of its two-phase pressure range (found by
-    a flash sweep), +-0.5 % seeded pressure noise, water saturation 0.2 in the
+    a flash sweep), seeded pressure noise (+-0.5 % by default; the time-stepping
+    workload starts without it), water saturation 0.2 in the
     matrix and 0 in the fracture; phase split, compositions and densities from
     the device flash.  Returns the pressure the sweep chose."""
     import torch
@@ -176,7 +178,7 @@ def assembly_state(grid, d, device, seed: int = 4):
     p0 = float(np.median(two))
     R = 8.3144621
     for med, sw in ((0, 0.2), (1, 0.0)):
-        P = torch.tensor(p0 * (1 + 0.005 * rng.uniform(-1, 1, n)), device=device)
+        P = torch.tensor(p0 * (1 + noise * rng.uniform(-1, 1, n)), device=device)
         T = torch.full_like(P, d.restemp)
         z = torch.tensor(np.repeat(z0[:, None], n, axis=1), device=device)
         o = flash(fl, P, T, z)
@@ -206,6 +208,7 @@ def assembly_spec(d) -> dict:
                 lf=d.lf, re_f=d.re_f, model="PR" if d.eos == 0 else "SRK", comps=names, bic=np.zeros((d.nc, d.nc)),
                 sgt=d.sgt, swt=d.swt, refp=d.refp, cpor=d.cpor, dcpor=d.dcpor, wells=[],
                 restemp_c=d.restemp - 273.15, wat_ro=d.wat_ro, wat_mu=d.wat_mu, dt=d.dt / TIME_FACTOR,
+                totalt=d.total_time / TIME_FACTOR, dtmax=d.dtmax,
                 cdif=d.cdif, ipress=2e7, iws=0.2, igc=z.tolist(), fipress=2e7, fiws=0.0, figc=z.tolist())
 
 

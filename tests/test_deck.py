@@ -77,7 +77,7 @@ def test_spec_round_trip(tmp_path):
     path = os.path.join(str(tmp_path), "a.dat")
     deck.write_deck(path, workloads.assembly_spec(d))
     q = workloads.with_table(deck.parse_deck(path), d)
-    skip = {"p0", "fp0", "sw0", "fsw0", "z0", "fz0", "total_time", "dtmax", "extra", "initcond", "pnc", "unc"}
+    skip = {"p0", "fp0", "sw0", "fsw0", "z0", "fz0", "extra", "initcond", "pnc", "unc"}
     for k, v in vars(d).items():
         if k not in skip:
             assert np.array_equal(np.asarray(v), np.asarray(getattr(q, k))), k
