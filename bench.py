@@ -59,7 +59,9 @@ def parse():
     ap.add_argument("--no-assembly", action="store_true")
     ap.add_argument("--no-instances", action="store_true")
     ap.add_argument("--instances", type=int, default=None, help="instances of the uneven-instance object (4096)")
-    ap.add_argument("--part", choices=["all", "assembly"], default="all",
+    ap.add_argument("--no-steps", action="store_true")
+    ap.add_argument("--steps-grids", default=None, help="NX,NY,NZ[;...] of the scaled time-stepping runs")
+    ap.add_argument("--part", choices=["all", "assembly", "steps"], default="all",
                     help="assembly: only the Newton-step assembly object (profiling)")
     ap.add_argument("--assembly-grid", default=None, help="NX,NY,NZ of the assembly grid (default 128,128,32)")
     return ap.parse_args()
@@ -579,6 +581,126 @@ def assembly_cpu_baseline(osr, torch, dev, cells_full: int, rows_full: int) -> d
             "update_all_s": r["update_all_s"], "sample_rows": r["rows"]}
 
 
+# ----------------------------------------------------------------------------- time stepping
+
+STEP_ACCEPTED = 10          # accepted passes of the small plain case
+STEP_GRIDS = ((64, 64, 16), (128, 128, 32))
+STEP_PASSES_SCALED = 3      # passes timed on each scaled grid
+
+
+def _plain_case(nx=10, ny=10, nz=3):
+    """The small plain case's deck (10x10x3, C1/nC4/nC10 at 20 MPa, a gas
+    injector and a producer at opposite corners), or the same deck on a
+    larger grid, read through the deck reader."""
+    import tempfile
+    from osiris_b200 import deck
+    with tempfile.TemporaryDirectory() as t:
+        path = os.path.join(t, "plain.dat")
+        deck.write_deck(path, deck.config_deck(nx=nx, ny=ny, nz=nz, cdif=0.0))
+        return deck.parse_deck(path), open(path).read()
+
+
+def _ref_steps_worker(text: str, accepted: int) -> dict:
+    """The reference's main loop on the small plain case (oracle/steps.py:
+    its own callbacks, backups and time control, an exact sparse solve in
+    place of PETSc's KSP), timed pass by pass in a spawned process."""
+    import tempfile
+
+    import oracle
+    from oracle import steps
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    with tempfile.TemporaryDirectory() as t:
+        path = os.path.join(t, "plain.dat")
+        open(path, "w").write(text)
+        R = oracle.RefDeck(path)
+        sim_t = 0.0
+        R.create_backups(sim_t)
+        n_acc = passes = 0
+        cells = 2 * R.cells
+        t0 = time.perf_counter()
+        while n_acc < accepted and passes < 100:
+            o = steps.ref_pass(R, sim_t)
+            sim_t = o["sim_time"]
+            passes += 1
+            n_acc += int(o["accepted"])
+        sec = time.perf_counter() - t0
+    return {"seconds": sec, "passes": passes, "accepted": n_acc, "cell_media": cells, "sim_time": sim_t}
+
+
+def measure_steps(osr, torch, dev, args, cpu_sample=False):
+    """Time stepping through the public API (Grid.initialize + Sim.step):
+    the small plain case until ten passes are accepted (the whole run from
+    the deck, host state in and out), and a few passes of the same deck on
+    larger grids (per-pass cost: assembly, BiCGStab + block-Jacobi solve,
+    UpdateAll(x, true))."""
+    d, text = _plain_case()
+    t0 = time.perf_counter()
+    G = osr.Grid(d)
+    G.initialize(dev)
+    sim = osr.Sim.from_deck(G)
+    infos = []
+    while sum(i["accepted"] for i in infos) < STEP_ACCEPTED and len(infos) < 100:
+        infos.append(sim.step())
+    P = [G.get(f"{m}.P") for m in "mf"]
+    torch.cuda.synchronize(dev)
+    sec = time.perf_counter() - t0
+    cells = 2 * G.cells
+    acc = sum(i["accepted"] for i in infos)
+    h2d = sum(a.nbytes for a in (d.p0, d.fp0, d.sw0, d.fsw0, d.z0, d.fz0))
+    out = {
+        "metric": "accepted time steps x cell-media / s (SolveNonLinear + TimeStepCtrl)",
+        "value": acc * cells / sec, "unit": "cells/s",
+        "config": {"workload": "small plain case: 10x10x3 dual-porosity grid, PR, C1/nC4/nC10, 20 MPa, gas "
+                               "injector + producer, CDIF 0, from the deck's initial state to ten accepted steps",
+                   "cell_media": cells},
+        "passes": len(infos), "accepted": acc, "seconds": sec, "sim_time_s": infos[-1]["sim_time"],
+        "ksp_its": [i["ksp_its"] for i in infos],
+        "e2e": {"value": acc * cells / sec, "unit": "cells/s", "h2d_bytes_per_step": h2d // max(acc, 1),
+                "d2h_bytes_per_step": sum(p.nbytes for p in P) // max(acc, 1),
+                "note": "the whole run: deck state uploaded, initial flash, passes, pressures read back"},
+    }
+    del sim, G
+    if cpu_sample:
+        import oracle
+        if oracle.ref_available():
+            ctx = mp.get_context("spawn")
+            with ctx.Pool(1) as pool:
+                r = pool.apply(_ref_steps_worker, (text, STEP_ACCEPTED))
+            out["cpu_baseline"] = {
+                "value": r["accepted"] * r["cell_media"] / r["seconds"], "unit": "cells/s", "cores": 1,
+                "kind": "reference",
+                "sample": f"the same run: {r['passes']} passes of the reference's own main loop (InitGuess2, "
+                          "FormFunction, FormJacobian, UpdateAll, CreateBackups, TimeStepCtrl) with scipy's "
+                          "sparse LU in place of PETSc's KSP (not part of the reference); start-up excluded",
+                "seconds": r["seconds"], "passes": r["passes"]}
+    grids = (tuple(tuple(int(v) for v in g.split(",")) for g in args.steps_grids.split(";"))
+             if args.steps_grids else STEP_GRIDS)
+    scaled = []
+    for grid in grids:
+        d2, _ = _plain_case(*grid)
+        G = osr.Grid(d2)
+        G.initialize(dev)
+        sim = osr.Sim.from_deck(G)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(STEP_PASSES_SCALED + 1)]
+        rec = []
+        ev[0].record()
+        for k in range(STEP_PASSES_SCALED):
+            rec.append(sim.step())
+            ev[k + 1].record()
+        torch.cuda.synchronize(dev)
+        ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(STEP_PASSES_SCALED)]
+        c2 = 2 * G.cells
+        scaled.append({"grid": list(grid), "cell_media": c2, "rows": rec[0]["rows"], "ms_per_pass": ms,
+                       "accepted": [r["accepted"] for r in rec], "ksp_its": [r["ksp_its"] for r in rec],
+                       "ksp_reason": [r["ksp_reason"] for r in rec], "vnorm": [r["vnorm"] for r in rec],
+                       "cells_per_s_per_pass": c2 / (sum(ms) / len(ms) * 1e-3)})
+        del sim, G
+        torch.cuda.empty_cache()
+    out["scaled"] = scaled
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -590,6 +712,14 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     n = args.cells or workloads.FLASH_CELLS
+
+    if args.part == "steps":
+        dev = torch.device("cuda", local)
+        torch.cuda.set_device(dev)
+        st = measure_steps(osr, torch, dev, args, cpu_sample=rank == 0 and world == 1 and not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps(st), flush=True)
+        return 0
 
     if args.part == "assembly":
         dev = torch.device("cuda", local)
@@ -734,6 +864,10 @@ def run_ours(args):
         assembly = measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier, max_over_ranks, gpu_id,
                                     cpu_sample=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
+    steps_obj = None
+    if not args.no_steps:
+        steps_obj = measure_steps(osr, torch, dev, args, cpu_sample=rank == 0 and world == 1 and not args.no_cpu_baseline)
+
     instances = None
     if inst_groups is not None:
         instances = measure_instances(osr, torch, dev, stream, flush, args, inst_groups, barrier, max_over_ranks,
@@ -783,6 +917,8 @@ def run_ours(args):
         line["assembly"] = assembly
     if instances is not None:
         line["instances"] = instances
+    if steps_obj is not None:
+        line["time_stepping"] = steps_obj
     try:
         import json as _j
         peaks = _j.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
