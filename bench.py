@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--instances", type=int, default=None, help="instances of the uneven-instance object (4096)")
     ap.add_argument("--no-steps", action="store_true")
     ap.add_argument("--steps-grids", default=None, help="NX,NY,NZ[;...] of the scaled time-stepping runs")
+    ap.add_argument("--steps-passes", type=int, default=None, help="passes timed per scaled grid (3)")
+    ap.add_argument("--steps-scaled-only", action="store_true", help="skip the small plain case (profiling)")
     ap.add_argument("--part", choices=["all", "assembly", "steps"], default="all",
                     help="assembly: only the Newton-step assembly object (profiling)")
     ap.add_argument("--assembly-grid", default=None, help="NX,NY,NZ of the assembly grid (default 128,128,32)")
@@ -645,6 +647,38 @@ def measure_steps(osr, torch, dev, args, cpu_sample=False):
     the deck, host state in and out), and a few passes of the same deck on
     larger grids (per-pass cost: assembly, BiCGStab + block-Jacobi solve,
     UpdateAll(x, true))."""
+    out = {}
+    if not args.steps_scaled_only:
+        out = _small_plain_run(osr, torch, dev, cpu_sample)
+    grids = (tuple(tuple(int(v) for v in g.split(",")) for g in args.steps_grids.split(";"))
+             if args.steps_grids else STEP_GRIDS)
+    passes = args.steps_passes or STEP_PASSES_SCALED
+    scaled = []
+    for grid in grids:
+        d2, _ = _plain_case(*grid)
+        G = osr.Grid(d2)
+        G.initialize(dev)
+        sim = osr.Sim.from_deck(G)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(passes + 1)]
+        rec = []
+        ev[0].record()
+        for k in range(passes):
+            rec.append(sim.step())
+            ev[k + 1].record()
+        torch.cuda.synchronize(dev)
+        ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(passes)]
+        c2 = 2 * G.cells
+        scaled.append({"grid": list(grid), "cell_media": c2, "rows": rec[0]["rows"], "ms_per_pass": ms,
+                       "accepted": [r["accepted"] for r in rec], "ksp_its": [r["ksp_its"] for r in rec],
+                       "ksp_reason": [r["ksp_reason"] for r in rec], "vnorm": [r["vnorm"] for r in rec],
+                       "cells_per_s_per_pass": c2 / (sum(ms) / len(ms) * 1e-3)})
+        del sim, G
+        torch.cuda.empty_cache()
+    out["scaled"] = scaled
+    return out
+
+
+def _small_plain_run(osr, torch, dev, cpu_sample):
     d, text = _plain_case()
     t0 = time.perf_counter()
     G = osr.Grid(d)
@@ -685,30 +719,6 @@ def measure_steps(osr, torch, dev, args, cpu_sample=False):
                           "FormFunction, FormJacobian, UpdateAll, CreateBackups, TimeStepCtrl) with scipy's "
                           "sparse LU in place of PETSc's KSP (not part of the reference); start-up excluded",
                 "seconds": r["seconds"], "passes": r["passes"]}
-    grids = (tuple(tuple(int(v) for v in g.split(",")) for g in args.steps_grids.split(";"))
-             if args.steps_grids else STEP_GRIDS)
-    scaled = []
-    for grid in grids:
-        d2, _ = _plain_case(*grid)
-        G = osr.Grid(d2)
-        G.initialize(dev)
-        sim = osr.Sim.from_deck(G)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(STEP_PASSES_SCALED + 1)]
-        rec = []
-        ev[0].record()
-        for k in range(STEP_PASSES_SCALED):
-            rec.append(sim.step())
-            ev[k + 1].record()
-        torch.cuda.synchronize(dev)
-        ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(STEP_PASSES_SCALED)]
-        c2 = 2 * G.cells
-        scaled.append({"grid": list(grid), "cell_media": c2, "rows": rec[0]["rows"], "ms_per_pass": ms,
-                       "accepted": [r["accepted"] for r in rec], "ksp_its": [r["ksp_its"] for r in rec],
-                       "ksp_reason": [r["ksp_reason"] for r in rec], "vnorm": [r["vnorm"] for r in rec],
-                       "cells_per_s_per_pass": c2 / (sum(ms) / len(ms) * 1e-3)})
-        del sim, G
-        torch.cuda.empty_cache()
-    out["scaled"] = scaled
     return out
 
 

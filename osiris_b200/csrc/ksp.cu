@@ -48,7 +48,7 @@ static osr_status ksp_ensure(osr_grid &g) {
     const size_t vb = (size_t)k->rows_cap * sizeof(double);
     double **vecs[] = {&k->r, &k->r0, &k->p, &k->v, &k->t, &k->s, &k->w};
     for (double **q : vecs) KSP_CUDA(cudaMalloc((void **)q, vb));
-    KSP_CUDA(cudaMalloc((void **)&k->inv, (size_t)k->blocks * bs * bs * sizeof(double)));
+    KSP_CUDA(cudaMalloc((void **)&k->inv, (size_t)((k->blocks + 31) / 32) * 32 * bs * bs * sizeof(double)));
     KSP_CUDA(cudaMalloc((void **)&k->part, (size_t)osrk::kParts * osrk::kRedBlocks * sizeof(double)));
     KSP_CUDA(cudaMalloc((void **)&k->scal, sizeof(osrk::KspScal)));
     KSP_CUDA(cudaMallocHost((void **)&k->host, sizeof(osrk::KspScal)));
@@ -116,7 +116,8 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     const unsigned sb = spmv_blocks(nb), vbk = vec_blocks(n), ib = inv_blocks(nb);
     const unsigned tpb = 32 * osrk::kInvWarps;
     osrk::bjac_invert_kernel<N><<<ib, tpb, 0, st>>>(v, k.inv, k.scal);
-    osrk::bjac_apply_kernel<N, 0><<<osrk::kRedBlocks, tpb, 0, st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
+    const unsigned atb = osrk::kApplyThreads;
+    osrk::bjac_apply_kernel<N, 0><<<osrk::kRedBlocks, atb, 0, st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
     osrk::bcgs_setup_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.r0, k.p, k.v, x);
     KSP_CUDA(cudaGetLastError());
     const int every = o.check_every > 0 ? o.check_every : 8;
@@ -125,11 +126,11 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
         for (int q = 0; q < every && launched < o.max_it; q++, launched++) {
             osrk::bcgs_p_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.p, k.v, k.scal);
             osrk::spmv_kernel<N><<<sb, 128, 0, st>>>(v, k.p, k.t, k.scal);
-            osrk::bjac_apply_kernel<N, 1><<<osrk::kRedBlocks, tpb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part,
+            osrk::bjac_apply_kernel<N, 1><<<osrk::kRedBlocks, atb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part,
                                                                             k.scal);
             osrk::bcgs_s_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.v, k.s, k.scal);
             osrk::spmv_kernel<N><<<sb, 128, 0, st>>>(v, k.s, k.w, k.scal);
-            osrk::bjac_apply_kernel<N, 2><<<osrk::kRedBlocks, tpb, 0, st>>>(v, k.inv, k.w, k.t, k.s, k.part,
+            osrk::bjac_apply_kernel<N, 2><<<osrk::kRedBlocks, atb, 0, st>>>(v, k.inv, k.w, k.t, k.s, k.part,
                                                                             k.scal);
             osrk::bcgs_xr_kernel<<<osrk::kRedBlocks, osrk::kRedThreads, 0, st>>>(n, x, k.p, k.s, k.t, k.r, k.r0,
                                                                                  k.part, k.scal);

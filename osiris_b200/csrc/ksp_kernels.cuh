@@ -22,7 +22,7 @@
 // so the host may enqueue iterations in batches and poll the status rarely):
 //   bcgs_p       p <- r + beta (p - omega_old v)
 //   spmv         t <- A p                  (one thread per block row)
-//   bjac_apply   v <- B t, (v, r0)         (one warp per block row)  -> alpha
+//   bjac_apply   v <- B t, (v, r0)         (one thread per block row) -> alpha
 //   bcgs_s       s <- r - alpha v
 //   spmv         w <- A s
 //   bjac_apply   t <- B w, (s,t) (t,t) (s,s)                        -> omega
@@ -129,7 +129,9 @@ __device__ __forceinline__ int own_entry(const Layout &L, int r, int cc) {
 // block's unknowns are gathered once per slot into canonical positions, the
 // block row's canonical rows accumulate in registers and are stored at the
 // reference-local rows of the block (no atomics: every entry of a block row
-// lies in that block row's rows).
+// lies in that block row's rows).  Values whose row the block row does not
+// carry, or whose column the target block does not use (one-phase blocks),
+// are not fetched.
 // ---------------------------------------------------------------------------
 template <int N>
 __global__ void __launch_bounds__(128) spmv_kernel(const KView v, const double *__restrict__ x,
@@ -140,10 +142,18 @@ __global__ void __launch_bounds__(128) spmv_kernel(const KView v, const double *
     const long nb = 2 * v.n;
     for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long)gridDim.x * blockDim.x) {
         const int lb = label_of(v, b);
+        // canonical rows this block row carries (a one-phase block uses N+3 of 2N+4)
+        unsigned long long rm = 0;
+#pragma unroll
+        for (int r = 0; r < BS; r++) rm |= (unsigned long long)(ref_row(N, lb, r) >= 0) << r;
         double acc[BS];
 #pragma unroll
         for (int r = 0; r < BS; r++) acc[r] = 0;
         const double *val = v.vals + ((b >> 5) * v.entries) * 32 + (b & 31);
+        // a value is fetched only where both its row and its target column are used
+        auto mac = [&](int r, int cc, int e, const double *xs, unsigned long long cm) {
+            if (((rm >> r) & (cm >> cc)) & 1ull) acc[r] += __ldcs(val + 32 * e) * xs[cc];
+        };
 #pragma unroll 1
         for (int sl = 0; sl < 8; sl++) {
             const long tb = slot_block(v, b, sl);
@@ -151,28 +161,30 @@ __global__ void __launch_bounds__(128) spmv_kernel(const KView v, const double *
             const int lt = label_of(v, tb);
             const long toff = v.rowoff[tb];
             double xs[BS];
+            unsigned long long cm = 0;
 #pragma unroll
             for (int cc = 0; cc < BS; cc++) {
                 const int rc = ref_col(N, lt, cc);
                 xs[cc] = rc >= 0 ? __ldg(x + toff + rc) : 0.0;
+                cm |= (unsigned long long)(rc >= 0) << cc;
             }
             if (sl == 0) {
 #pragma unroll
                 for (int r = 0; r < N; r++)
 #pragma unroll
-                    for (int cc = 0; cc <= 2 * N; cc++) acc[r] += __ldcs(val + 32 * L.f(r, cc)) * xs[cc];
+                    for (int cc = 0; cc <= 2 * N; cc++) mac(r, cc, L.f(r, cc), xs, cm);
             }
 #pragma unroll
             for (int r = N; r < 2 * N; r++)
 #pragma unroll
-                for (int cc = 0; cc < BS; cc++) acc[r] += __ldcs(val + 32 * L.cr(r, sl, cc)) * xs[cc];
-            acc[2 * N] += __ldcs(val + 32 * L.w(sl, 2 * N)) * xs[2 * N] +
-                          __ldcs(val + 32 * L.w(sl, 2 * N + 1)) * xs[2 * N + 1];
+                for (int cc = 0; cc < BS; cc++) mac(r, cc, L.cr(r, sl, cc), xs, cm);
+            mac(2 * N, 2 * N, L.w(sl, 2 * N), xs, cm);
+            mac(2 * N, 2 * N + 1, L.w(sl, 2 * N + 1), xs, cm);
             if (sl == 0) {
 #pragma unroll
                 for (int r = 2 * N + 1; r < BS; r++)
 #pragma unroll
-                    for (int cc = 0; cc < BS; cc++) acc[r] += __ldcs(val + 32 * L.k(r, cc)) * xs[cc];
+                    for (int cc = 0; cc < BS; cc++) mac(r, cc, L.k(r, cc), xs, cm);
             }
         }
 #pragma unroll 1
@@ -194,9 +206,10 @@ __global__ void __launch_bounds__(128) spmv_kernel(const KView v, const double *
 // own-slot entries, plus any shifted entry whose column falls in the block)
 // is assembled in shared memory at reference-local rows and columns and
 // inverted in place by Gauss-Jordan elimination with partial pivoting (row
-// interchanges undone as column interchanges at the end).  Stored column by
-// column, inv[b][j][i] = (A^-1)_ij, BS x BS per block row.  A zero pivot sets
-// the solve's reason to PC_FAILED.
+// interchanges undone as column interchanges at the end).  Stored in chunks
+// of 32 block rows like the Jacobian values, inv[chunk][j BS + i][32] =
+// (A^-1)_ij, so the apply kernel's 32 lanes read 256 contiguous bytes per
+// entry.  A zero pivot sets the solve's reason to PC_FAILED.
 // ---------------------------------------------------------------------------
 constexpr int kInvWarps = 4;
 
@@ -293,9 +306,8 @@ __global__ void __launch_bounds__(32 * kInvWarps) bjac_invert_kernel(const KView
                 }
             __syncwarp();
         }
-        double *o = inv + b * (long)(BS * BS);
-        for (int j = 0; j < BS; j++)
-            for (int i = lane; i < BS; i += 32) o[j * BS + i] = A[i * BS + j];
+        double *o = inv + ((b >> 5) * (BS * BS)) * 32 + (b & 31);
+        for (int q = lane; q < BS * BS; q += 32) o[32 * q] = A[(q % BS) * BS + q / BS];
         __syncwarp();
     }
 }
@@ -363,31 +375,47 @@ __device__ __forceinline__ void converged_test(KspScal *s, double rnorm) {
 }
 
 // ---------------------------------------------------------------------------
-// z = B r (block-diagonal inverse), one warp per block row, with the dot
-// products the following step needs.
+// z = B r (block-diagonal inverse), one thread per block row (the block's r
+// in registers, the inverse read coalesced across the warp's 32 block rows,
+// loads beyond the block's own size predicated off), with the dot products
+// the following step needs.
 //   MODE 0 (setup):  (z, z)                  -> rnorm0, ttol, rho = (r0, r0)
 //   MODE 1 (v):      (z, a)                  -> alpha = rho / (v, r0)
 //   MODE 2 (t):      (a, z) (z, z) (a, a)    -> omega = (s,t) / (t,t)
 // ---------------------------------------------------------------------------
+constexpr int kApplyThreads = 128;
+
 template <int N, int MODE>
-__global__ void __launch_bounds__(32 * kInvWarps) bjac_apply_kernel(const KView v, const double *__restrict__ inv,
-                                                                     const double *__restrict__ r,
-                                                                     double *__restrict__ z,
-                                                                     const double *__restrict__ a, double *part,
-                                                                     KspScal *s) {
+__global__ void __launch_bounds__(kApplyThreads) bjac_apply_kernel(const KView v, const double *__restrict__ inv,
+                                                                    const double *__restrict__ r,
+                                                                    double *__restrict__ z,
+                                                                    const double *__restrict__ a, double *part,
+                                                                    KspScal *s) {
     if (s->reason != kItersRunning) return;
     constexpr int BS = 2 * N + 4;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long nb = 2 * v.n;
-    const long warps = (long)gridDim.x * kInvWarps;
     double acc[kParts] = {0, 0, 0};
-    for (long b = (long)blockIdx.x * kInvWarps + w; b < nb; b += warps) {
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long)gridDim.x * blockDim.x) {
         const long off = v.rowoff[b];
         const int bs = (int)(v.rowoff[b + 1] - off);
-        const double *ib = inv + b * (long)(BS * BS);
-        for (int i = lane; i < bs; i += 32) {
-            double t = 0;
-            for (int j = 0; j < bs; j++) t += ib[j * BS + i] * __ldg(r + off + j);
+        const double *ib = inv + ((b >> 5) * (BS * BS)) * 32 + (b & 31);
+        double rv[BS], zv[BS];
+#pragma unroll
+        for (int j = 0; j < BS; j++) {
+            rv[j] = j < bs ? __ldg(r + off + j) : 0.0;
+            zv[j] = 0;
+        }
+#pragma unroll
+        for (int j = 0; j < BS; j++) {
+            if (j >= bs) break;
+#pragma unroll
+            for (int i = 0; i < BS; i++)
+                if (i < bs) zv[i] += __ldg(ib + 32 * (j * BS + i)) * rv[j];
+        }
+#pragma unroll
+        for (int i = 0; i < BS; i++) {
+            if (i >= bs) break;
+            const double t = zv[i];
             z[off + i] = t;
             if (MODE == 0) {
                 acc[0] += t * t;
