@@ -49,7 +49,7 @@ static osr_status ksp_ensure(osr_grid &g) {
     double **vecs[] = {&k->r, &k->r0, &k->p, &k->v, &k->t, &k->s, &k->w};
     for (double **q : vecs) KSP_CUDA(cudaMalloc((void **)q, vb));
     KSP_CUDA(cudaMalloc((void **)&k->inv, (size_t)((k->blocks + 31) / 32) * 32 * bs * bs * sizeof(double)));
-    KSP_CUDA(cudaMalloc((void **)&k->part, (size_t)osrk::kParts * osrk::kRedBlocks * sizeof(double)));
+    KSP_CUDA(cudaMalloc((void **)&k->part, (size_t)osrk::kParts * osrk::kMaxRedBlocks * sizeof(double)));
     KSP_CUDA(cudaMalloc((void **)&k->scal, sizeof(osrk::KspScal)));
     KSP_CUDA(cudaMallocHost((void **)&k->host, sizeof(osrk::KspScal)));
     return OSR_OK;
@@ -72,8 +72,9 @@ static osrk::KView kview(const osr_grid &g, const double *vals) {
 }
 
 static unsigned spmv_blocks(long nb) {
-    long b = (nb + 127) / 128;
-    if (b > 148L * 32) b = 148L * 32;
+    const long per_cta = 8 * (osrk::kSpmvThreads / 32);   // block rows per CTA and sweep
+    long b = (nb + per_cta - 1) / per_cta;
+    if (b > 148L * 64) b = 148L * 64;
     return (unsigned)(b < 1 ? 1 : b);
 }
 
@@ -83,16 +84,39 @@ static unsigned vec_blocks(long n) {
     return (unsigned)(b < 1 ? 1 : b);
 }
 
+// CTAs of the reducing kernels: enough to cover the work in one sweep, at
+// most kMaxRedBlocks (the partial-sum buffer).
+static unsigned red_blocks(long work, int per_cta) {
+    long b = (work + per_cta - 1) / per_cta;
+    if (b > osrk::kMaxRedBlocks) b = osrk::kMaxRedBlocks;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
 static unsigned inv_blocks(long nb) {
     long b = (nb + osrk::kInvWarps - 1) / osrk::kInvWarps;
     if (b > 148L * 64) b = 148L * 64;
     return (unsigned)(b < 1 ? 1 : b);
 }
 
+// y = A x: one thread per block row on large grids, four lanes per block
+// row below osrk::kSpmvRowForm block rows.
+template <int N>
+static void spmv_launch(const osrk::KView &v, const double *x, double *y, const osrk::KspScal *sc,
+                        cudaStream_t st) {
+    const long nb = 2 * v.n;
+    if (nb >= osrk::kSpmvRowForm) {
+        long b = (nb + 127) / 128;
+        if (b > 148L * 64) b = 148L * 64;
+        osrk::spmv_row_kernel<N><<<(unsigned)b, 128, 0, st>>>(v, x, y, sc);
+    } else {
+        osrk::spmv_kernel<N><<<spmv_blocks(nb), osrk::kSpmvThreads, 0, st>>>(v, x, y, sc);
+    }
+}
+
 template <int N>
 static osr_status spmv_n(const osr_grid &g, const double *vals, const double *x, double *y, cudaStream_t st) {
     const osrk::KView v = kview(g, vals);
-    osrk::spmv_kernel<N><<<spmv_blocks(2 * g.cells), 128, 0, st>>>(v, x, y, nullptr);
+    spmv_launch<N>(v, x, y, nullptr, st);
     KSP_CUDA(cudaGetLastError());
     return OSR_OK;
 }
@@ -113,11 +137,12 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     h.max_it = o.max_it;
     *k.host = h;
     KSP_CUDA(cudaMemcpyAsync(k.scal, k.host, sizeof(h), cudaMemcpyHostToDevice, st));
-    const unsigned sb = spmv_blocks(nb), vbk = vec_blocks(n), ib = inv_blocks(nb);
+    const unsigned vbk = vec_blocks(n), ib = inv_blocks(nb);
     const unsigned tpb = 32 * osrk::kInvWarps;
     osrk::bjac_invert_kernel<N><<<ib, tpb, 0, st>>>(v, k.inv, k.scal);
     const unsigned atb = osrk::kApplyThreads;
-    osrk::bjac_apply_kernel<N, 0><<<osrk::kRedBlocks, atb, 0, st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
+    const unsigned ab = red_blocks(nb, osrk::kApplyThreads), xb = red_blocks(n, 4 * osrk::kRedThreads);
+    osrk::bjac_apply_kernel<N, 0><<<ab, atb, 0, st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
     osrk::bcgs_setup_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.r0, k.p, k.v, x);
     KSP_CUDA(cudaGetLastError());
     const int every = o.check_every > 0 ? o.check_every : 8;
@@ -125,14 +150,14 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     for (;;) {
         for (int q = 0; q < every && launched < o.max_it; q++, launched++) {
             osrk::bcgs_p_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.p, k.v, k.scal);
-            osrk::spmv_kernel<N><<<sb, 128, 0, st>>>(v, k.p, k.t, k.scal);
-            osrk::bjac_apply_kernel<N, 1><<<osrk::kRedBlocks, atb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part,
+            spmv_launch<N>(v, k.p, k.t, k.scal, st);
+            osrk::bjac_apply_kernel<N, 1><<<ab, atb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part,
                                                                             k.scal);
             osrk::bcgs_s_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.v, k.s, k.scal);
-            osrk::spmv_kernel<N><<<sb, 128, 0, st>>>(v, k.s, k.w, k.scal);
-            osrk::bjac_apply_kernel<N, 2><<<osrk::kRedBlocks, atb, 0, st>>>(v, k.inv, k.w, k.t, k.s, k.part,
+            spmv_launch<N>(v, k.s, k.w, k.scal, st);
+            osrk::bjac_apply_kernel<N, 2><<<ab, atb, 0, st>>>(v, k.inv, k.w, k.t, k.s, k.part,
                                                                             k.scal);
-            osrk::bcgs_xr_kernel<<<osrk::kRedBlocks, osrk::kRedThreads, 0, st>>>(n, x, k.p, k.s, k.t, k.r, k.r0,
+            osrk::bcgs_xr_kernel<<<xb, osrk::kRedThreads, 0, st>>>(n, x, k.p, k.s, k.t, k.r, k.r0,
                                                                                  k.part, k.scal);
         }
         KSP_CUDA(cudaGetLastError());

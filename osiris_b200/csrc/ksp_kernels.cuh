@@ -21,7 +21,7 @@
 // Kernels, per iteration (each returns at once when the solve has ended,
 // so the host may enqueue iterations in batches and poll the status rarely):
 //   bcgs_p       p <- r + beta (p - omega_old v)
-//   spmv         t <- A p                  (one thread per block row)
+//   spmv         t <- A p                  (four lanes per block row)
 //   bjac_apply   v <- B t, (v, r0)         (one thread per block row) -> alpha
 //   bcgs_s       s <- r - alpha v
 //   spmv         w <- A s
@@ -54,7 +54,7 @@ enum : int {
     kFinishWithP = -100,   // internal: t = s = 0, the update is x += alpha p
 };
 
-constexpr int kRedBlocks = 592;   // 4 x 148 SMs
+constexpr int kMaxRedBlocks = 148 * 64;   // CTAs of a reducing kernel (partials buffer size)
 constexpr int kRedThreads = 256;
 constexpr int kParts = 3;         // partial sums per reduction kernel
 
@@ -125,7 +125,9 @@ __device__ __forceinline__ int own_entry(const Layout &L, int r, int cc) {
 }
 
 // ---------------------------------------------------------------------------
-// y = A x on the compact layout, one thread per block row: the target
+// y = A x, one thread per block row (the form for large grids, where the
+// grid alone fills the GPU and each entry a warp reads is one 256-byte run of
+// 32 block rows; spmv_kernel below serves smaller grids): the target
 // block's unknowns are gathered once per slot into canonical positions, the
 // block row's canonical rows accumulate in registers and are stored at the
 // reference-local rows of the block (no atomics: every entry of a block row
@@ -134,8 +136,8 @@ __device__ __forceinline__ int own_entry(const Layout &L, int r, int cc) {
 // are not fetched.
 // ---------------------------------------------------------------------------
 template <int N>
-__global__ void __launch_bounds__(128) spmv_kernel(const KView v, const double *__restrict__ x,
-                                                    double *__restrict__ y, const KspScal *s) {
+__global__ void __launch_bounds__(128) spmv_row_kernel(const KView v, const double *__restrict__ x,
+                                                        double *__restrict__ y, const KspScal *s) {
     if (s && s->reason != kItersRunning) return;
     constexpr int BS = 2 * N + 4;
     const Layout L(N);
@@ -197,6 +199,116 @@ __global__ void __launch_bounds__(128) spmv_kernel(const KView v, const double *
         for (int r = 0; r < BS; r++) {
             const int rr = ref_row(N, lb, r);
             if (rr >= 0) y[off + rr] = acc[r];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// y = A x on the compact layout.  Four lanes per block row and eight block
+// rows per warp: lane = 8 g + q serves block row base + q and target slots g
+// and g + 4 (slot 0 this cell, 1..6 the -x, +x, -y, +y, -z, +z neighbours,
+// 7 the other continuum).  Each entry a warp reads is then four runs of 64
+// contiguous bytes (eight block rows of one slot), whole DRAM access units.
+// A lane gathers its target block's unknowns into canonical positions and
+// accumulates the block row's canonical rows in registers; the four partial
+// rows are summed by a butterfly over the lanes of the same q and stored at
+// the reference-local rows (no atomics: every entry of a block row lies in
+// that block row's rows).  The own-slot lane also takes the fugacity and
+// constraint rows, the -y and -z lanes the shifted entries of their faces.
+// Values whose row the block row does not carry, or whose column the target
+// block does not use (one-phase blocks), are not fetched.
+// ---------------------------------------------------------------------------
+constexpr int kSpmvThreads = 128;
+// block rows from which the one-thread-per-block-row form is used
+constexpr long kSpmvRowForm = 148L * 2048;
+
+template <int N>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_kernel(const KView v, const double *__restrict__ x,
+                                                             double *__restrict__ y, const KspScal *s) {
+    if (s && s->reason != kItersRunning) return;
+    constexpr int BS = 2 * N + 4;
+    const Layout L(N);
+    const long nb = 2 * v.n;
+    const int lane = threadIdx.x & 31, g = lane >> 3, q = lane & 7;
+    const long groups = (nb + 7) / 8;
+    const long gstride = (long)gridDim.x * (kSpmvThreads / 32);
+    for (long grp = (long)blockIdx.x * (kSpmvThreads / 32) + (threadIdx.x >> 5); grp < groups; grp += gstride) {
+        const long b = grp * 8 + q;
+        const bool valid = b < nb;
+        double acc[BS];
+#pragma unroll
+        for (int r = 0; r < BS; r++) acc[r] = 0;
+        int lb = 0;
+        if (valid) {
+            lb = label_of(v, b);
+            unsigned long long rm = 0;
+#pragma unroll
+            for (int r = 0; r < BS; r++) rm |= (unsigned long long)(ref_row(N, lb, r) >= 0) << r;
+            const double *val = v.vals + ((b >> 5) * v.entries) * 32 + (b & 31);
+#pragma unroll 1
+            for (int h = 0; h < 2; h++) {
+                const int sl = g + 4 * h;
+                const long tb = slot_block(v, b, sl);
+                if (tb < 0) continue;
+                const int lt = label_of(v, tb);
+                const long toff = v.rowoff[tb];
+                double xs[BS];
+                unsigned long long cm = 0;
+#pragma unroll
+                for (int cc = 0; cc < BS; cc++) {
+                    const int rc = ref_col(N, lt, cc);
+                    xs[cc] = rc >= 0 ? __ldg(x + toff + rc) : 0.0;
+                    cm |= (unsigned long long)(rc >= 0) << cc;
+                }
+                auto mac = [&](int r, int cc, int e) {
+                    if (((rm >> r) & (cm >> cc)) & 1ull) acc[r] += __ldcs(val + 32 * e) * xs[cc];
+                };
+#pragma unroll
+                for (int r = N; r < 2 * N; r++)
+#pragma unroll
+                    for (int cc = 0; cc < BS; cc++) mac(r, cc, L.cr(r, sl, cc));
+                mac(2 * N, 2 * N, L.w(sl, 2 * N));
+                mac(2 * N, 2 * N + 1, L.w(sl, 2 * N + 1));
+                if (sl == 0) {
+#pragma unroll
+                    for (int r = 0; r < N; r++)
+#pragma unroll
+                        for (int cc = 0; cc <= 2 * N; cc++) mac(r, cc, L.f(r, cc));
+#pragma unroll
+                    for (int r = 2 * N + 1; r < BS; r++)
+#pragma unroll
+                        for (int cc = 0; cc < BS; cc++) mac(r, cc, L.k(r, cc));
+                }
+                if ((sl == 3 || sl == 5) && ((rm >> (2 * N - 1)) & 1ull)) {
+                    // the shifted entries of the -y (slot 3) and -z (slot 5) faces: columns
+                    // counted from the row offset of the block after that neighbour
+                    // (osrj::entry_position)
+                    const long base = v.rowoff[tb + 1];
+                    const int nbase = lt ? -N : 0, reCol4 = lt ? 1 : 0, j0 = sl == 3 ? 0 : 4;
+#pragma unroll
+                    for (int t = 0; t < 4; t++) {
+                        const long gc = base + nbase + 2 * N + (t == 3 ? 3 - reCol4 : t);
+                        if (gc >= 0 && gc < v.rows) acc[2 * N - 1] += __ldcs(val + 32 * L.o(j0 + t)) * __ldg(x + gc);
+                    }
+                }
+            }
+        }
+        // sum the four slot lanes of each block row
+#pragma unroll
+        for (int r = 0; r < BS; r++) {
+            double t = acc[r];
+            t += __shfl_xor_sync(0xffffffffu, t, 8);
+            t += __shfl_xor_sync(0xffffffffu, t, 16);
+            acc[r] = t;
+        }
+        if (valid) {
+            const long off = v.rowoff[b];
+#pragma unroll
+            for (int r = 0; r < BS; r++) {
+                if ((r & 3) != g) continue;
+                const int rr = ref_row(N, lb, r);
+                if (rr >= 0) y[off + rr] = acc[r];
+            }
         }
     }
 }
@@ -336,29 +448,38 @@ __device__ __forceinline__ void block_sums(double (&v)[K], double *sm) {
         }
 }
 
-// Publish this CTA's K partials; returns true in the one thread of the last
-// CTA, with the totals in tot.
+// Publish this CTA's K partials (part[q][gridDim.x]); returns true in thread
+// 0 of the last CTA to finish, with the totals in tot.  The last CTA's
+// threads sum fixed strided subsets of the partials, then reduce them as one
+// block, so the order never depends on timing.
 template <int K>
 __device__ bool publish_partials(double (&v)[K], double *part, KspScal *s, double (&tot)[K]) {
     __shared__ double sm[K * 32];
     __shared__ bool last;
     block_sums<K>(v, sm);
+    const int nblk = (int)gridDim.x;
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < K; q++) part[q * kRedBlocks + blockIdx.x] = v[q];
+        for (int q = 0; q < K; q++) part[q * nblk + blockIdx.x] = v[q];
         __threadfence();
         const unsigned t = atomicAdd(&s->ticket, 1u);
         last = (t == gridDim.x - 1);
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return false;
+    if (!last) return false;
     __threadfence();
+    double w[K];
 #pragma unroll
     for (int q = 0; q < K; q++) {
         double t = 0;
-        for (int i = 0; i < (int)gridDim.x; i++) t += ((volatile double *)part)[q * kRedBlocks + i];
-        tot[q] = t;
+        for (int i = threadIdx.x; i < nblk; i += blockDim.x) t += ((volatile double *)part)[q * nblk + i];
+        w[q] = t;
     }
+    __syncthreads();
+    block_sums<K>(w, sm);
+    if (threadIdx.x != 0) return false;
+#pragma unroll
+    for (int q = 0; q < K; q++) tot[q] = w[q];
     s->ticket = 0;
     return true;
 }

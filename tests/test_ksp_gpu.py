@@ -128,3 +128,30 @@ def test_iteration_semantics_match_restatement(name, tmp_path, cuda_device):
     info = G.ksp_solve(J, torch.zeros_like(d_f), d_dx)
     assert (info["reason"], info["its"], info["rnorm0"]) == (linear.CONVERGED_ATOL, 0, 0.0)
     assert not d_dx.any()
+
+
+def test_matmult_large_grid_form(tmp_path, cuda_device):
+    """Grids of at least 148 x 2048 block rows use the one-thread-per-block-row
+    product: on 64x64x37 (303,104 block rows, the device start-up state of
+    the plain case) J v must match the host product of the same values placed
+    by the pattern, per row within 1e-12 of sum_j |J_ij v_j|."""
+    import torch
+    path = os.path.join(str(tmp_path), "large.dat")
+    deck.write_deck(path, deck.config_deck(nx=64, ny=64, nz=37, cdif=0.0))
+    G = osr.Grid(deck.parse_deck(path))
+    G.initialize(cuda_device)
+    n, _ = G.layout()
+    assert 2 * G.cells >= 148 * 2048
+    J = G.alloc_jacobian(cuda_device)
+    assert G.jacobian(J, T) == 0
+    v = np.random.default_rng(6).uniform(-1, 1, n)
+    y = torch.zeros(n, dtype=torch.float64, device=cuda_device)
+    G.jacobian_apply(J, torch.tensor(v, device=cuda_device), y)
+    torch.cuda.synchronize()
+    y = y.cpu().numpy()
+    r, c, vals = G.jacobian_coo(J)
+    prod = vals * v[c]
+    yr = np.bincount(r, weights=prod, minlength=n)
+    scale = np.bincount(r, weights=np.abs(prod), minlength=n)
+    bad = ~(np.abs(y - yr) <= 1e-12 * scale + 1e-300)
+    assert not bad.any(), (int(bad.sum()), [(int(i), y[i], yr[i]) for i in np.nonzero(bad)[0][:6]])
