@@ -187,6 +187,11 @@ osr_status osr_grid_dims(osr_grid *grid, int *dims /* [4]: nx, ny, nz, nc */);
 osr_status osr_grid_set_state(osr_grid *grid, int medium, const double *P_oil, const double *sat, const double *x,
                               const double *y, const double *z, const signed char *label, const double *rho);
 
+/* All three phase pressures of one continuum, HOST [3][cells] (water, oil,
+ * gas): what the reference's ReadRST restores (compsim/Do_Time_Step.cpp:
+ * 236-260); PhaseCtrl reads the gas pressure before the next update. */
+osr_status osr_grid_set_pressures(osr_grid *grid, int medium, const double *P);
+
 /* The property sweeps of UpdateDependencies (compsim/PetscAUX.cpp:530-548)
  * for both media: IFT, relative permeability and capillary pressure, phase
  * pressures, densities with d rho/dx and d rho/dP, LBC viscosities,
@@ -415,6 +420,15 @@ osr_status osr_sim_step(osr_sim *sim, const osr_ksp_opts *opts, osr_step_info *i
 
 /* Current simulation time and Dt (either may be null). */
 osr_status osr_sim_time(osr_sim *sim, double *sim_time, double *dt);
+
+/* Index of the next time marker (the reference's TSMCtrl, written to its
+ * restart file). */
+osr_status osr_sim_marker_index(osr_sim *sim, int *tsm_ctrl);
+
+/* Continue a run from a restart file (ReadRST, compsim/Do_Time_Step.cpp:
+ * 236-294): simulation time, Dt and marker index as read; the grid's
+ * current state (set from the file) becomes the backup. */
+osr_status osr_sim_restart(osr_sim *sim, double sim_time, double dt, int tsm_ctrl);
 
 osr_status osr_sim_destroy(osr_sim *sim);
 

@@ -405,6 +405,16 @@ class RefDeck:
         return float(self.lib.ref_time_rows(_p(rows), ctypes.c_long(len(rows)), _p(x), _p(f), ctypes.c_double(t),
                                             int(which)))
 
+    def write_rst(self, directory: str, t: float) -> str:
+        """The reference's WriteRST into directory/test.rst."""
+        cwd = os.getcwd()
+        try:
+            os.chdir(directory)
+            self.lib.ref_write_rst(ctypes.c_double(t))
+        finally:
+            os.chdir(cwd)
+        return os.path.join(directory, "test.rst")
+
     def create_backups(self, t: float):
         self.lib.ref_create_backups(ctypes.c_double(t))
 

@@ -205,6 +205,7 @@ double ref_scalar(const char *name) {
     if (s == "SigmaMF") return SigmaMF;
     if (s == "CDiffCoef") return CDiffCoef;
     if (s == "Dt") return Dt;
+    if (s == "SMethQ") return SMethQ;
     return 0.0 / 0.0;
 }
 
@@ -476,6 +477,13 @@ int ref_time_markers(double *out, int *ctrl) {
     for (int i = 0; i < TSMSize; i++) out[i] = TStepMarker[i];
     if (ctrl) *ctrl = TSMCtrl;
     return TSMSize;
+}
+
+/* WriteRST (compsim/Do_Time_Step.cpp:179-234): the restart file "test.rst"
+ * in the current directory, at simulation time t. */
+int ref_write_rst(double t) {
+    WriteRST(t);
+    return 0;
 }
 
 /* FormFunction(x) -> f (compsim/PetscAUX.cpp:59-104) at simulation time t. */

@@ -364,6 +364,11 @@ class Grid:
         self.refresh_layout(stream)
         self.update_dependencies(stream)
 
+    def set_pressures(self, medium: int, P):
+        """All three phase pressures of one continuum, [3][cells]."""
+        a = np.ascontiguousarray(P, np.float64)
+        _check(lib().osr_grid_set_pressures(self._h, int(medium), a.ctypes.data), "osr_grid_set_pressures")
+
     def update_dependencies(self, stream=None):
         _check(lib().osr_grid_update_dependencies(self._h, None if stream is None else _vp(stream)),
                "osr_grid_update_dependencies")
@@ -547,6 +552,15 @@ class Sim:
         _check(lib().osr_sim_step(self._h, ctypes.byref(o), ctypes.byref(info),
                                   None if stream is None else _vp(stream)), "osr_sim_step")
         return {k: getattr(info, k) for k, _ in StepInfo._fields_}
+
+    def marker_index(self) -> int:
+        k = ctypes.c_int()
+        _check(lib().osr_sim_marker_index(self._h, ctypes.byref(k)), "osr_sim_marker_index")
+        return k.value
+
+    def restart(self, sim_time: float, dt: float, tsm_ctrl: int):
+        _check(lib().osr_sim_restart(self._h, ctypes.c_double(sim_time), ctypes.c_double(dt), int(tsm_ctrl)),
+               "osr_sim_restart")
 
     def time(self):
         t, dt = ctypes.c_double(), ctypes.c_double()

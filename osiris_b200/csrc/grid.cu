@@ -287,6 +287,13 @@ osr_status osr_grid_destroy(osr_grid *g) {
     return OSR_OK;
 }
 
+osr_status osr_grid_set_pressures(osr_grid *g, int medium, const double *P) {
+    if (!g || (medium != 0 && medium != 1) || !P) return OSR_ERR_ARG;
+    if (cudaMemcpy(g->m[medium].P, P, 3 * g->cells * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        return OSR_ERR_CUDA;
+    return OSR_OK;
+}
+
 osr_status osr_grid_set_state(osr_grid *g, int medium, const double *P_oil, const double *sat, const double *x,
                               const double *y, const double *z, const signed char *label, const double *rho) {
     if (!g || (medium != 0 && medium != 1) || !P_oil || !sat || !x || !y || !z || !label) return OSR_ERR_ARG;

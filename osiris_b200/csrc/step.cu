@@ -191,6 +191,25 @@ osr_status osr_sim_time(osr_sim *s, double *sim_time, double *dt) {
     return OSR_OK;
 }
 
+osr_status osr_sim_marker_index(osr_sim *s, int *tsm_ctrl) {
+    if (!s || !tsm_ctrl) return OSR_ERR_ARG;
+    *tsm_ctrl = s->tsm_ctrl;
+    return OSR_OK;
+}
+
+osr_status osr_sim_restart(osr_sim *s, double sim_time, double dt, int tsm_ctrl) {
+    if (!s || !(dt > 0) || tsm_ctrl < 0 || tsm_ctrl > (int)s->markers.size()) return OSR_ERR_ARG;
+    s->sim_time = sim_time;
+    s->dt = dt;
+    s->tsm_ctrl = tsm_ctrl;
+    s->inc_count = 0;
+    // the restored state is the new backup (CreateBackups after ReadRST, compsim/PrimeSim.cpp:84-86)
+    osr_status rc = osr_grid_refresh_layout(s->g, nullptr);
+    if (rc == OSR_OK) rc = copy_state(*s, true, nullptr);
+    if (rc == OSR_OK && cudaStreamSynchronize(nullptr) != cudaSuccess) rc = OSR_ERR_CUDA;
+    return rc;
+}
+
 osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *info, void *stream) {
     if (!s) return OSR_ERR_ARG;
     osr_grid *g = s->g;
