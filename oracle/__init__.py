@@ -415,6 +415,11 @@ class RefDeck:
             os.chdir(cwd)
         return os.path.join(directory, "test.rst")
 
+    def print_all(self, path, t: float):
+        """The reference's PrintAll at time t appended to path (one stream
+        kept open across calls); path None closes it."""
+        self.lib.ref_print_all(None if path is None else path.encode(), ctypes.c_double(t))
+
     def create_backups(self, t: float):
         self.lib.ref_create_backups(ctypes.c_double(t))
 

@@ -10,6 +10,7 @@
  * library): per-cell scalars are [n]; per-component fields are
  * component-major [nc][n]. */
 #include <chrono>
+#include <fstream>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -483,6 +484,21 @@ int ref_time_markers(double *out, int *ctrl) {
  * in the current directory, at simulation time t. */
 int ref_write_rst(double t) {
     WriteRST(t);
+    return 0;
+}
+
+/* PrintAll (compsim/ViewAssist.Cpp:39-88) of the current state at time t,
+ * appended to one stream kept open across calls as the main program keeps
+ * its output file (path opens it, a null path closes it). */
+int ref_print_all(const char *path, double t) {
+    static std::ofstream out;
+    if (!path) {
+        if (out.is_open()) out.close();
+        return 0;
+    }
+    if (!out.is_open()) out.open(path, std::ios::out);
+    if (!out.is_open()) return -1;
+    PrintAll(out, t);
     return 0;
 }
 

@@ -58,3 +58,51 @@ def test_wrong_size_is_rejected(tmp_path):
     open(p, "wb").write(b"\0" * 100)
     with pytest.raises(ValueError):
         restart.read_rst(p, 2, 2, 2, 3)
+
+
+_LISTING_CHILD = r"""
+import ctypes, sys
+# the reference's C++ output streams must bind to its own runtime: load it
+# before numpy brings a second libstdc++ into the process
+ctypes.CDLL(sys.argv[1])
+import numpy as np
+import oracle
+from oracle import steps
+R = oracle.RefDeck(sys.argv[2])
+t = 0.0
+R.create_backups(t)
+for k in range(3):
+    if k:
+        t = steps.ref_pass(R, t)["sim_time"]
+    R.print_all(sys.argv[3], t)
+    np.savez(f"{sys.argv[4]}_{k}.npz", t=t, **{f"{m}.{q}": R.get(f"{m}.{q}") for m in "mf"
+                                                for q in ("P", "sat", "x", "y")})
+R.print_all(None, 0.0)
+"""
+
+
+@needs_ref
+def test_state_listing_matches_reference_print_all(tmp_path):
+    """The state listing from the reference's state is the reference's own
+    PrintAll output character for character, over a start-up call and two
+    calls after accepted passes on one stream (the reference runs in a child
+    process that loads it before numpy, see _LISTING_CHILD)."""
+    import subprocess
+    import sys
+    from osiris_b200 import output
+    td = str(tmp_path)
+    path = os.path.join(td, "deck.dat")
+    spec = deck.config_deck(nx=4, ny=3, nz=2, cdif=0.0, ipress=1e7, seed=3)
+    deck.write_deck(path, spec)
+    ref_out = os.path.join(td, "ref.txt")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    subprocess.run([sys.executable, "-c", _LISTING_CHILD, oracle.REF_LIB, path, ref_out, os.path.join(td, "st")],
+                   check=True, env=env, stdout=subprocess.DEVNULL)
+    d = deck.parse_deck(path)
+    mine = output.StateListing(os.path.join(td, "mine.txt"))
+    for k in range(3):
+        z = np.load(os.path.join(td, f"st_{k}.npz"))
+        mine.write(d.nx, d.ny, d.nz, d.nc, {q: z[q] for q in z.files if q != "t"}, float(z["t"]))
+    mine.close()
+    assert open(os.path.join(td, "mine.txt")).read() == open(ref_out).read()
