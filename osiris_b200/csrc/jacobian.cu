@@ -21,7 +21,7 @@ static osr_status jfail(cudaError_t) { return OSR_ERR_CUDA; }
 constexpr int kRowThreads = 128;
 // Resident CTAs per SM the row kernels are compiled for (bounds their registers).
 #ifndef OSR_JAC_MIN_BLOCKS
-#define OSR_JAC_MIN_BLOCKS 4
+#define OSR_JAC_MIN_BLOCKS 5
 #endif
 
 template <int N>

@@ -14,6 +14,14 @@ struct osr_ksp_work {
     double *part = nullptr;
     osrk::KspScal *scal = nullptr;   // device
     osrk::KspScal *host = nullptr;   // pinned
+    // one batch of iterations captured as a CUDA graph, replayed while the
+    // matrix values, solution vector, row count and batch size stay the same
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t batch = nullptr;
+    const double *g_vals = nullptr;
+    double *g_x = nullptr;
+    long g_rows = -1;
+    int g_every = 0;
 };
 
 namespace osr {
@@ -31,6 +39,8 @@ void ksp_free(osr_grid &g) {
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (k->host) cudaFreeHost(k->host);
+    if (k->batch) cudaGraphExecDestroy(k->batch);
+    if (k->cap) cudaStreamDestroy(k->cap);
     delete k;
     g.ksp = nullptr;
 }
@@ -146,19 +156,51 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     osrk::bcgs_setup_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.r0, k.p, k.v, x);
     KSP_CUDA(cudaGetLastError());
     const int every = o.check_every > 0 ? o.check_every : 8;
+    auto iterations = [&](cudaStream_t q_st, int count) {
+        for (int q = 0; q < count; q++) {
+            osrk::bcgs_p_kernel<<<vbk, 256, 0, q_st>>>(n, k.r, k.p, k.v, k.scal);
+            spmv_launch<N>(v, k.p, k.t, k.scal, q_st);
+            osrk::bjac_apply_kernel<N, 1><<<ab, atb, 0, q_st>>>(v, k.inv, k.t, k.v, k.r0, k.part, k.scal);
+            osrk::bcgs_s_kernel<<<vbk, 256, 0, q_st>>>(n, k.r, k.v, k.s, k.scal);
+            spmv_launch<N>(v, k.s, k.w, k.scal, q_st);
+            osrk::bjac_apply_kernel<N, 2><<<ab, atb, 0, q_st>>>(v, k.inv, k.w, k.t, k.s, k.part, k.scal);
+            osrk::bcgs_xr_kernel<<<xb, osrk::kRedThreads, 0, q_st>>>(n, x, k.p, k.s, k.t, k.r, k.r0, k.part,
+                                                                      k.scal);
+        }
+    };
+    // the batch graph: every kernel reads its scalars and the solve's status
+    // from device memory, so one capture serves every batch of this system
+    if (k.batch && (k.g_vals != vals || k.g_x != x || k.g_rows != n || k.g_every != every)) {
+        cudaGraphExecDestroy(k.batch);
+        k.batch = nullptr;
+    }
+    if (!k.batch && o.max_it >= every) {
+        if (!k.cap) KSP_CUDA(cudaStreamCreateWithFlags(&k.cap, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(k.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            iterations(k.cap, every);
+            if (cudaStreamEndCapture(k.cap, &graph) == cudaSuccess && graph) {
+                if (cudaGraphInstantiate(&k.batch, graph, 0) != cudaSuccess) k.batch = nullptr;
+                cudaGraphDestroy(graph);
+            }
+        }
+        cudaGetLastError();   // a failed capture falls back to direct launches
+        if (k.batch) {
+            k.g_vals = vals;
+            k.g_x = x;
+            k.g_rows = n;
+            k.g_every = every;
+        }
+    }
     int launched = 0;
     for (;;) {
-        for (int q = 0; q < every && launched < o.max_it; q++, launched++) {
-            osrk::bcgs_p_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.p, k.v, k.scal);
-            spmv_launch<N>(v, k.p, k.t, k.scal, st);
-            osrk::bjac_apply_kernel<N, 1><<<ab, atb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part,
-                                                                            k.scal);
-            osrk::bcgs_s_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.v, k.s, k.scal);
-            spmv_launch<N>(v, k.s, k.w, k.scal, st);
-            osrk::bjac_apply_kernel<N, 2><<<ab, atb, 0, st>>>(v, k.inv, k.w, k.t, k.s, k.part,
-                                                                            k.scal);
-            osrk::bcgs_xr_kernel<<<xb, osrk::kRedThreads, 0, st>>>(n, x, k.p, k.s, k.t, k.r, k.r0,
-                                                                                 k.part, k.scal);
+        if (k.batch && launched + every <= o.max_it) {
+            KSP_CUDA(cudaGraphLaunch(k.batch, st));
+            launched += every;
+        } else {
+            const int c = every < o.max_it - launched ? every : o.max_it - launched;
+            iterations(st, c);
+            launched += c;
         }
         KSP_CUDA(cudaGetLastError());
         KSP_CUDA(cudaMemcpyAsync(k.host, k.scal, sizeof(h), cudaMemcpyDeviceToHost, st));
