@@ -67,3 +67,39 @@ def test_slab_residual_rows_match_single_grid(name, world, tmp_path, cuda_device
             err = np.abs(fl[la:lb] - f[ga:gb])
             bad = err > 1e-12 * scale[ga:gb] + 1e-300
             assert not bad.any(), (z0, z1, m, int(bad.sum()), float((err / (scale[ga:gb] + 1e-300)).max()))
+
+
+def test_slab_wrapper_single_rank_nccl(tmp_path, cuda_device):
+    """The Slab wrapper on a one-rank NCCL group (no neighbours, PCoeff
+    through the all-reduce) gives the single grid's residual exactly."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    path = os.path.join(str(tmp_path), "d.dat")
+    deck.write_deck(path, CASES["twophase_10MPa_cdif0"]())
+    d = deck.parse_deck(path)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=cuda_device)
+    try:
+        G = osr.Grid(d)
+        G.initialize(cuda_device)
+        rows, _ = G.layout()
+        x = torch.zeros(rows, dtype=torch.float64, device=cuda_device)
+        G.init_guess(x)
+        f = torch.zeros_like(x)
+        S = slabs.Slab(d, 0, 1)
+        S.grid.initialize(cuda_device)
+        assert S.refresh_layout(cuda_device) == rows
+        fl = torch.zeros_like(x)
+        G.form_function(x.clone(), f, T)
+        S.form_function(x.clone(), fl, T)
+        torch.cuda.synchronize()
+        assert S.owned_rows()[0][0] == 0 and S.owned_rows()[1][1] == rows
+        assert torch.equal(f, fl)
+    finally:
+        dist.destroy_process_group()
