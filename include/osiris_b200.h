@@ -116,9 +116,13 @@ osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, cons
                                  const double *d_z, long n, const osr_flash_out *out, void *stream);
 
 /* End-to-end form for callers holding HOST arrays (same layouts; out fields
- * are host pointers): copies inputs to the device, runs osr_flash_batch,
- * copies results back, synchronises.  Device buffers come from the
- * stream-ordered pool and are released before return. */
+ * are host pointers): the cells go through in chunks of about 131,072
+ * (at most 16 chunks) pipelined over three internal streams -- inputs in,
+ * osr_flash_batch, results out -- so transfers overlap the flash (pinned
+ * host memory gives the overlap; pageable memory works, without it).
+ * Results are those of osr_flash_batch.  Waits for the caller's earlier
+ * work on `stream` and synchronises before return.  Device buffers come
+ * from the stream-ordered pool and are released before return. */
 osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const double *T, const double *z,
                                 long n, const osr_flash_out *out, void *stream);
 

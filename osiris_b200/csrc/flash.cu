@@ -412,6 +412,15 @@ osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, cons
     return flash_device(fluid, d_P, d_T, d_z, n, out, stream, Form::kPlain);
 }
 
+// Host form: the cells go through in chunks pipelined over three streams.
+// Chunk k's inputs in, its batched flash and its outputs out run on stream
+// k % 3 with that stream's device buffers, so the copies of the chunks before
+// and after it (both directions of PCIe at once) overlap its flash.  Every
+// cell's result is independent of how the cells are grouped.
+constexpr int kHostStreams = 3;
+constexpr long kHostChunkCells = 131072;
+constexpr int kHostMaxChunks = 16;
+
 osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const double *T, const double *z, long n,
                                 const osr_flash_out *out, void *stream) {
     osr_status st = check_fluid(fluid);
@@ -423,59 +432,102 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
     cudaStream_t s = (cudaStream_t)stream;
     const int nc = fluid->nc;
     const bool derivs = out->dlnphi_dx != nullptr;
-    // one device block: inputs, then outputs, 256-byte aligned pieces
-    size_t nd = (size_t)n;
+    long chunks = n / kHostChunkCells;
+    if (chunks < 1) chunks = 1;
+    if (chunks > kHostMaxChunks) chunks = kHostMaxChunks;
+    const long m = (n + chunks - 1) / chunks;   // cells per chunk (the last may hold fewer)
+    const int slots = chunks < kHostStreams ? (int)chunks : kHostStreams;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    size_t szP = al(nd * 8), szz = al(nd * nc * 8), szl = al(nd), szi = al(nd * 4);
-    size_t szdx = derivs ? al(nd * 2 * nc * nc * 8) : 0, szdp = derivs ? al(nd * 2 * nc * 8) : 0;
-    size_t total = 2 * szP + szz + szl + szP + 2 * szz + 2 * szP + 2 * szi + szdx + szdp;
-    char *base = nullptr;
-    OSR_CUDA(pool_alloc((void **)&base, total, s));
-    char *p = base;
-    auto take = [&](size_t sz) { char *r = p; p += sz; return r; };
-    double *dP = (double *)take(szP), *dT = (double *)take(szP), *dz = (double *)take(szz);
-    osr_flash_out d{};
-    d.label = (signed char *)take(szl);
-    d.L = (double *)take(szP);
-    d.x = (double *)take(szz);
-    d.y = (double *)take(szz);
-    d.Zl = (double *)take(szP);
-    d.Zg = (double *)take(szP);
-    int *di = (int *)take(szi), *dr = (int *)take(szi);
-    d.iters = out->iters ? di : nullptr;
-    d.rr_iters = out->rr_iters ? dr : nullptr;
-    if (derivs) {
-        d.dlnphi_dx = (double *)take(szdx);
-        d.dlnphi_dP = (double *)take(szdp);
+    const size_t md = (size_t)m;
+    const size_t szP = al(md * 8), szz = al(md * nc * 8), szl = al(md), szi = al(md * 4);
+    const size_t szdx = derivs ? al(md * 2 * nc * nc * 8) : 0, szdp = derivs ? al(md * 2 * nc * 8) : 0;
+    const size_t slot_bytes = 2 * szP + szz + szl + szP + 2 * szz + 2 * szP + 2 * szi + szdx + szdp;
+    cudaStream_t ss[kHostStreams] = {};
+    char *base[kHostStreams] = {};
+    cudaEvent_t ready = nullptr, done[kHostStreams] = {};
+    cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ready, s);   // caller's earlier work comes first
+    for (int k = 0; k < slots && e == cudaSuccess; k++) {
+        e = cudaStreamCreateWithFlags(&ss[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ss[k], ready, 0);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = pool_alloc((void **)&base[k], slot_bytes, ss[k]);
     }
-    cudaError_t e = cudaSuccess;
-    auto h2d = [&](void *dst, const void *src, size_t b) {
-        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, s);
-    };
-    auto d2h = [&](void *dst, const void *src, size_t b) {
-        if (e == cudaSuccess && dst) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, s);
-    };
-    h2d(dP, P, nd * 8);
-    h2d(dT, T, nd * 8);
-    h2d(dz, z, nd * nc * 8);
-    if (e == cudaSuccess) st = flash_device(fluid, dP, dT, dz, n, &d, stream, Form::kQueue);
-    d2h(out->label, d.label, nd);
-    d2h(out->L, d.L, nd * 8);
-    d2h(out->x, d.x, nd * nc * 8);
-    d2h(out->y, d.y, nd * nc * 8);
-    d2h(out->Zl, d.Zl, nd * 8);
-    d2h(out->Zg, d.Zg, nd * 8);
-    if (out->iters) d2h(out->iters, d.iters, nd * 4);
-    if (out->rr_iters) d2h(out->rr_iters, d.rr_iters, nd * 4);
-    if (derivs) {
-        d2h(out->dlnphi_dx, d.dlnphi_dx, nd * 2 * nc * nc * 8);
-        d2h(out->dlnphi_dP, d.dlnphi_dP, nd * 2 * nc * 8);
+    for (long c = 0; c < chunks && e == cudaSuccess && st == OSR_OK; c++) {
+        const long c0 = c * m;
+        const long len = c0 + m <= n ? m : n - c0;
+        if (len <= 0) break;
+        const int k = (int)(c % slots);
+        cudaStream_t q = ss[k];
+        char *p = base[k];
+        auto take = [&](size_t sz) { char *r = p; p += sz; return r; };
+        double *dP = (double *)take(szP), *dT = (double *)take(szP), *dz = (double *)take(szz);
+        osr_flash_out d{};
+        d.label = (signed char *)take(szl);
+        d.L = (double *)take(szP);
+        d.x = (double *)take(szz);
+        d.y = (double *)take(szz);
+        d.Zl = (double *)take(szP);
+        d.Zg = (double *)take(szP);
+        int *di = (int *)take(szi), *dr = (int *)take(szi);
+        d.iters = out->iters ? di : nullptr;
+        d.rr_iters = out->rr_iters ? dr : nullptr;
+        if (derivs) {
+            d.dlnphi_dx = (double *)take(szdx);
+            d.dlnphi_dP = (double *)take(szdp);
+        }
+        const size_t w = (size_t)len * 8, hp = (size_t)n * 8;
+        // planes of the host arrays are n apart, planes of the chunk len apart
+        auto in1 = [&](void *dst, const void *src, size_t b) {
+            if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, q);
+        };
+        auto out1 = [&](void *dst, const void *src, size_t b) {
+            if (e == cudaSuccess && dst) e = cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, q);
+        };
+        auto outp = [&](double *dst, const double *src, size_t planes) {
+            if (e == cudaSuccess && dst)
+                e = cudaMemcpy2DAsync(dst + c0, hp, src, w, w, planes, cudaMemcpyDeviceToHost, q);
+        };
+        in1(dP, P + c0, w);
+        in1(dT, T + c0, w);
+        if (e == cudaSuccess) e = cudaMemcpy2DAsync(dz, w, z + c0, hp, w, nc, cudaMemcpyHostToDevice, q);
+        if (e == cudaSuccess) st = flash_device(fluid, dP, dT, dz, len, &d, q, Form::kQueue);
+        out1(out->label ? out->label + c0 : nullptr, d.label, (size_t)len);
+        out1(out->L ? out->L + c0 : nullptr, d.L, w);
+        outp(out->x, d.x, nc);
+        outp(out->y, d.y, nc);
+        out1(out->Zl ? out->Zl + c0 : nullptr, d.Zl, w);
+        out1(out->Zg ? out->Zg + c0 : nullptr, d.Zg, w);
+        if (out->iters) out1(out->iters + c0, d.iters, (size_t)len * 4);
+        if (out->rr_iters) out1(out->rr_iters + c0, d.rr_iters, (size_t)len * 4);
+        if (derivs) {
+            outp(out->dlnphi_dx, d.dlnphi_dx, (size_t)2 * nc * nc);
+            outp(out->dlnphi_dP, d.dlnphi_dP, (size_t)2 * nc);
+        }
     }
-    cudaError_t ef = cudaFreeAsync(base, s);
+    for (int k = 0; k < slots; k++) {
+        if (base[k]) {
+            cudaError_t ef = cudaFreeAsync(base[k], ss[k]);
+            if (e == cudaSuccess) e = ef;
+        }
+        if (ss[k] && done[k]) {
+            cudaError_t er = cudaEventRecord(done[k], ss[k]);
+            if (e == cudaSuccess) e = er;
+            if (er == cudaSuccess) {
+                er = cudaStreamWaitEvent(s, done[k], 0);
+                if (e == cudaSuccess) e = er;
+            }
+        }
+    }
     cudaError_t es = cudaStreamSynchronize(s);
+    for (int k = 0; k < slots; k++) {
+        if (ss[k]) cudaStreamSynchronize(ss[k]);
+        if (done[k]) cudaEventDestroy(done[k]);
+        if (ss[k]) cudaStreamDestroy(ss[k]);
+    }
+    if (ready) cudaEventDestroy(ready);
     if (e != cudaSuccess) return cuda_fail(e);
     if (st != OSR_OK) return st;
-    if (ef != cudaSuccess) return cuda_fail(ef);
     if (es != cudaSuccess) return cuda_fail(es);
     return OSR_OK;
 }
