@@ -164,9 +164,57 @@ class Slab:
         return [(int(self._rowoff[m * nl + (self.z0 - self.lo) * nxy]),
                  int(self._rowoff[m * nl + (self.z1 - self.lo) * nxy])) for m in (0, 1)]
 
+    def frac_start(self) -> int:
+        """First local row of the fracture continuum."""
+        return int(self._rowoff[self.grid.cells])
+
+    def global_offsets(self, device=None):
+        """This rank's global row offsets per continuum (an all-gather of the
+        ranks' owned row counts)."""
+        import torch
+        import torch.distributed as dist
+        own = self.owned_rows()
+        mine = torch.tensor([own[0][1] - own[0][0], own[1][1] - own[1][0]], dtype=torch.int64, device=device)
+        every = [torch.zeros_like(mine) for _ in range(self.world)]
+        dist.all_gather(every, mine, group=self.group)
+        return global_offsets([tuple(t.tolist()) for t in every], self.rank)
+
+    def jacobian_coo_global(self, vals, offsets):
+        """(rows, cols, values) of the owned rows of the local Jacobian values
+        in the global numbering, the triplets a multi-rank PETSc matrix takes
+        (MatSetValuesCOO with global indices)."""
+        r, c, v = self.grid.jacobian_coo(vals)
+        own = self.owned_rows()
+        keep = ((r >= own[0][0]) & (r < own[0][1])) | ((r >= own[1][0]) & (r < own[1][1]))
+        fs = self.frac_start()
+        return (to_global(r[keep], fs, own, offsets), to_global(c[keep], fs, own, offsets), v[keep])
+
     def form_function(self, x_local, f_local, sim_time: float):
         """Exchange the ghost layers' unknowns, then UpdateAll + residual on
         the whole local grid; the owned rows of f_local are this rank's part."""
         exchange_ghost_unknowns(x_local, self._rowoff, self.deck.nx, self.deck.ny, self.hi - self.lo,
                                 self.z0 > 0, self.z1 < self.deck.nz, self.rank, self.group)
         self.grid.form_function(x_local, f_local, sim_time)
+
+
+def global_offsets(owned_counts, rank: int):
+    """Global row offset of a rank's first owned row in each continuum, from
+    every rank's owned row counts [(matrix, fracture)] in rank order: the
+    global numbering holds all matrix rows (rank by rank) before all fracture
+    rows."""
+    owned_counts = [tuple(int(v) for v in c) for c in owned_counts]
+    all_matrix = sum(c[0] for c in owned_counts)
+    before = [sum(c[m] for c in owned_counts[:rank]) for m in (0, 1)]
+    return before[0], all_matrix + before[1]
+
+
+def to_global(idx, frac_start: int, owned_local, offsets):
+    """Global row indices of local row indices idx.  Within one continuum a
+    slab's rows -- lower ghost layer, owned layers, upper ghost layer -- are
+    consecutive in the global numbering, so each continuum maps by one shift:
+    the distance between the rank's first owned row there, locally and
+    globally.  frac_start: the first local fracture row; owned_local: the
+    local owned row ranges (Slab.owned_rows); offsets: global_offsets."""
+    idx = np.asarray(idx)
+    return np.where(idx >= frac_start, idx + (offsets[1] - owned_local[1][0]),
+                    idx + (offsets[0] - owned_local[0][0]))

@@ -87,3 +87,16 @@ def test_ranges_and_sub_deck(tmp_path):
         path2 = os.path.join(str(tmp_path), "w.dat")
         deck.write_deck(path2, deck.config_deck(nx=3, ny=2, nz=5))
         slabs.sub_deck(deck.parse_deck(path2), 0, 2)
+
+
+def test_global_offsets_and_mapping():
+    counts = [(10, 6), (8, 4), (12, 9)]           # owned rows (matrix, fracture) per rank
+    assert slabs.global_offsets(counts, 0) == (0, 30)
+    assert slabs.global_offsets(counts, 1) == (10, 36)
+    assert slabs.global_offsets(counts, 2) == (18, 40)
+    # rank 1 with ghost layers: local matrix rows [0, 14) (4 ghost + 8 owned + 2 ghost),
+    # local fracture rows [14, 24) (3 ghost + 4 owned + 3 ghost)
+    own = [(4, 12), (17, 21)]
+    offs = slabs.global_offsets(counts, 1)
+    g = slabs.to_global(np.array([0, 4, 11, 13, 14, 17, 20, 23]), 14, own, offs)
+    assert g.tolist() == [6, 10, 17, 19, 33, 36, 39, 42]

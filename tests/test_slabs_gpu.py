@@ -101,5 +101,75 @@ def test_slab_wrapper_single_rank_nccl(tmp_path, cuda_device):
         torch.cuda.synchronize()
         assert S.owned_rows()[0][0] == 0 and S.owned_rows()[1][1] == rows
         assert torch.equal(f, fl)
+        offs = S.global_offsets(cuda_device)
+        assert offs == (0, S.frac_start())
+        J = G.alloc_jacobian(cuda_device)
+        assert G.jacobian(J, T) == 0
+        JS = S.grid.alloc_jacobian(cuda_device)
+        assert S.grid.jacobian(JS, T) == 0
+        r, c, v = S.jacobian_coo_global(JS, offs)
+        rg, cg, vg = G.jacobian_coo(J)
+        assert np.array_equal(r, rg) and np.array_equal(c, cg) and np.array_equal(v, vg)
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("name", list(CASES))
+def test_slab_jacobian_rows_match_single_grid(name, world, tmp_path, cuda_device):
+    """The owned rows of every slab's Jacobian, mapped to the global
+    numbering (slabs.global_offsets / to_global), rebuild the single grid's
+    Jacobian: every entry within 1e-12 of its row's largest."""
+    import scipy.sparse as sp
+    import torch
+    path = os.path.join(str(tmp_path), name + ".dat")
+    deck.write_deck(path, CASES[name]())
+    d = deck.parse_deck(path)
+    G = osr.Grid(d)
+    G.initialize(cuda_device)
+    rows, pcoeff = G.layout()
+    state = {f"{m}.{k}": G.get(f"{m}.{k}") for m in "mf" for k in FIELDS + ("P",)}
+    x0 = torch.zeros(rows, dtype=torch.float64, device=cuda_device)
+    G.init_guess(x0)
+    xp = x0.cpu().numpy() * (1 + 1e-3 * np.random.default_rng(2).uniform(-1, 1, rows))
+    f = torch.zeros(rows, dtype=torch.float64, device=cuda_device)
+    G.form_function(torch.tensor(xp, device=cuda_device), f, T)
+    J = G.alloc_jacobian(cuda_device)
+    assert G.jacobian(J, T) == 0
+    A = sp.csr_matrix((lambda r, c, v: (v, (r, c)))(*G.jacobian_coo(J)), shape=(rows, rows))
+    gro = G.row_offsets()
+    n, nxy = G.cells, d.nx * d.ny
+    parts = []
+    for z0, z1 in slabs.slab_ranges(d.nz, world):
+        lo, hi = slabs.ghost_range(d.nz, z0, z1)
+        S = osr.Grid(slabs.sub_deck(d, lo, hi))
+        a, b = lo * nxy, hi * nxy
+        for mi, m in enumerate("mf"):
+            cut = {k: state[f"{m}.{k}"][..., a:b] for k in FIELDS + ("P",)}
+            S.set_state(mi, cut["P"][1], cut["sat"], cut["x"], cut["y"], cut["z"], cut["label"], cut["rho"])
+            S.set_pressures(mi, cut["P"])
+        lrows, _ = S.refresh_layout()
+        S.set_controls(d.dt, pcoeff)
+        lro = S.row_offsets()
+        xl = np.concatenate([xp[gro[m * n + a]:gro[m * n + b]] for m in (0, 1)])
+        fl = torch.zeros(lrows, dtype=torch.float64, device=cuda_device)
+        S.form_function(torch.tensor(xl, device=cuda_device), fl, T)
+        JS = S.alloc_jacobian(cuda_device)
+        assert S.jacobian(JS, T) == 0
+        nl = S.cells
+        own = [(int(lro[m * nl + (z0 - lo) * nxy]), int(lro[m * nl + (z1 - lo) * nxy])) for m in (0, 1)]
+        parts.append((S, JS, own, int(lro[nl])))
+    counts = [(o[0][1] - o[0][0], o[1][1] - o[1][0]) for _, _, o, _ in parts]
+    R, C, V = [], [], []
+    for rank, (S, JS, own, fs) in enumerate(parts):
+        r, c, v = S.jacobian_coo(JS)
+        keep = ((r >= own[0][0]) & (r < own[0][1])) | ((r >= own[1][0]) & (r < own[1][1]))
+        offs = slabs.global_offsets(counts, rank)
+        R.append(slabs.to_global(r[keep], fs, own, offs))
+        C.append(slabs.to_global(c[keep], fs, own, offs))
+        V.append(v[keep])
+    B = sp.csr_matrix((np.concatenate(V), (np.concatenate(R), np.concatenate(C))), shape=(rows, rows))
+    D = abs(A - B)
+    scale = np.maximum(abs(A).max(axis=1).toarray().ravel(), 1e-300)
+    worst = (D.max(axis=1).toarray().ravel() / scale).max()
+    assert worst <= 1e-12, worst
