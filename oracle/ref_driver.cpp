@@ -182,6 +182,19 @@ int ref_deck_open(const char *path) {
     InitWells();
     WellCompSadeq_cum[0] = WellCompSadeq_cum[1] = WellCompSadeq_cum[2] = 0;
     SMethQ = 0;
+    /* UpdateDependencies(true) starts with PhaseCtrl, whose test for a
+     * gas-only cell reads the gas-phase pressure (compsim/Do_Cycle.cpp:1579)
+     * before anything has written it: the deck sets only the oil pressure.
+     * In a fresh process that memory reads zero; in a process that has
+     * allocated and freed memory before, it holds whatever was left there,
+     * and the start-up state changes from one opening to the next.  Pin it
+     * to the fresh-process value. */
+    for (int i = 0; i < Nx; i++)
+        for (int j = 0; j < Ny; j++)
+            for (int k = 0; k < Nz; k++) {
+                P[i + 1][j + 1][k + 1][0] = P[i + 1][j + 1][k + 1][2] = 0;
+                fP[i + 1][j + 1][k + 1][0] = fP[i + 1][j + 1][k + 1][2] = 0;
+            }
     UpdateDependencies(true);
     return 0;
 }
