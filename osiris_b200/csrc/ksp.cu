@@ -81,8 +81,8 @@ static osrk::KView kview(const osr_grid &g, const double *vals) {
     return v;
 }
 
-static unsigned spmv_blocks(long nb) {
-    const long per_cta = 8 * (osrk::kSpmvThreads / 32);   // block rows per CTA and sweep
+static unsigned spmv_blocks(long nb, int lanes) {
+    const long per_cta = (32 / lanes) * (osrk::kSpmvThreads / 32);   // block rows per CTA and sweep
     long b = (nb + per_cta - 1) / per_cta;
     if (b > 148L * 64) b = 148L * 64;
     return (unsigned)(b < 1 ? 1 : b);
@@ -108,19 +108,17 @@ static unsigned inv_blocks(long nb) {
     return (unsigned)(b < 1 ? 1 : b);
 }
 
-// y = A x: one thread per block row on large grids, four lanes per block
-// row below osrk::kSpmvRowForm block rows.
+// y = A x: two lanes per block row on large grids (128-byte runs per
+// slot), four below osrk::kSpmvRowForm block rows (shorter dependent chains
+// where the grid alone cannot fill the GPU).
 template <int N>
 static void spmv_launch(const osrk::KView &v, const double *x, double *y, const osrk::KspScal *sc,
                         cudaStream_t st) {
     const long nb = 2 * v.n;
-    if (nb >= osrk::kSpmvRowForm) {
-        long b = (nb + 127) / 128;
-        if (b > 148L * 64) b = 148L * 64;
-        osrk::spmv_row_kernel<N><<<(unsigned)b, 128, 0, st>>>(v, x, y, sc);
-    } else {
-        osrk::spmv_kernel<N><<<spmv_blocks(nb), osrk::kSpmvThreads, 0, st>>>(v, x, y, sc);
-    }
+    if (nb >= osrk::kSpmvRowForm)
+        osrk::spmv_kernel<N, 2><<<spmv_blocks(nb, 2), osrk::kSpmvThreads, 0, st>>>(v, x, y, sc);
+    else
+        osrk::spmv_kernel<N, 4><<<spmv_blocks(nb, 4), osrk::kSpmvThreads, 0, st>>>(v, x, y, sc);
 }
 
 template <int N>

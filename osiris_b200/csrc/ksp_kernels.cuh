@@ -21,7 +21,7 @@
 // Kernels, per iteration (each returns at once when the solve has ended,
 // so the host may enqueue iterations in batches and poll the status rarely):
 //   bcgs_p       p <- r + beta (p - omega_old v)
-//   spmv         t <- A p                  (four lanes per block row)
+//   spmv         t <- A p                  (two or four lanes per block row)
 //   bjac_apply   v <- B t, (v, r0)         (one thread per block row) -> alpha
 //   bcgs_s       s <- r - alpha v
 //   spmv         w <- A s
@@ -125,90 +125,12 @@ __device__ __forceinline__ int own_entry(const Layout &L, int r, int cc) {
 }
 
 // ---------------------------------------------------------------------------
-// y = A x, one thread per block row (the form for large grids, where the
-// grid alone fills the GPU and each entry a warp reads is one 256-byte run of
-// 32 block rows; spmv_kernel below serves smaller grids): the target
-// block's unknowns are gathered once per slot into canonical positions, the
-// block row's canonical rows accumulate in registers and are stored at the
-// reference-local rows of the block (no atomics: every entry of a block row
-// lies in that block row's rows).  Values whose row the block row does not
-// carry, or whose column the target block does not use (one-phase blocks),
-// are not fetched.
-// ---------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(128) spmv_row_kernel(const KView v, const double *__restrict__ x,
-                                                        double *__restrict__ y, const KspScal *s) {
-    if (s && s->reason != kItersRunning) return;
-    constexpr int BS = 2 * N + 4;
-    const Layout L(N);
-    const long nb = 2 * v.n;
-    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long)gridDim.x * blockDim.x) {
-        const int lb = label_of(v, b);
-        // canonical rows this block row carries (a one-phase block uses N+3 of 2N+4)
-        unsigned long long rm = 0;
-#pragma unroll
-        for (int r = 0; r < BS; r++) rm |= (unsigned long long)(ref_row(N, lb, r) >= 0) << r;
-        double acc[BS];
-#pragma unroll
-        for (int r = 0; r < BS; r++) acc[r] = 0;
-        const double *val = v.vals + ((b >> 5) * v.entries) * 32 + (b & 31);
-        // a value is fetched only where both its row and its target column are used
-        auto mac = [&](int r, int cc, int e, const double *xs, unsigned long long cm) {
-            if (((rm >> r) & (cm >> cc)) & 1ull) acc[r] += __ldcs(val + 32 * e) * xs[cc];
-        };
-#pragma unroll 1
-        for (int sl = 0; sl < 8; sl++) {
-            const long tb = slot_block(v, b, sl);
-            if (tb < 0) continue;
-            const int lt = label_of(v, tb);
-            const long toff = v.rowoff[tb];
-            double xs[BS];
-            unsigned long long cm = 0;
-#pragma unroll
-            for (int cc = 0; cc < BS; cc++) {
-                const int rc = ref_col(N, lt, cc);
-                xs[cc] = rc >= 0 ? __ldg(x + toff + rc) : 0.0;
-                cm |= (unsigned long long)(rc >= 0) << cc;
-            }
-            if (sl == 0) {
-#pragma unroll
-                for (int r = 0; r < N; r++)
-#pragma unroll
-                    for (int cc = 0; cc <= 2 * N; cc++) mac(r, cc, L.f(r, cc), xs, cm);
-            }
-#pragma unroll
-            for (int r = N; r < 2 * N; r++)
-#pragma unroll
-                for (int cc = 0; cc < BS; cc++) mac(r, cc, L.cr(r, sl, cc), xs, cm);
-            mac(2 * N, 2 * N, L.w(sl, 2 * N), xs, cm);
-            mac(2 * N, 2 * N + 1, L.w(sl, 2 * N + 1), xs, cm);
-            if (sl == 0) {
-#pragma unroll
-                for (int r = 2 * N + 1; r < BS; r++)
-#pragma unroll
-                    for (int cc = 0; cc < BS; cc++) mac(r, cc, L.k(r, cc), xs, cm);
-            }
-        }
-#pragma unroll 1
-        for (int j = 0; j < osrj::kOverflow; j++) {
-            const long g = overflow_col(v, b, j);
-            if (g >= 0) acc[2 * N - 1] += __ldcs(val + 32 * L.o(j)) * __ldg(x + g);
-        }
-        const long off = v.rowoff[b];
-#pragma unroll
-        for (int r = 0; r < BS; r++) {
-            const int rr = ref_row(N, lb, r);
-            if (rr >= 0) y[off + rr] = acc[r];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// y = A x on the compact layout.  Four lanes per block row and eight block
-// rows per warp: lane = 8 g + q serves block row base + q and target slots g
-// and g + 4 (slot 0 this cell, 1..6 the -x, +x, -y, +y, -z, +z neighbours,
-// 7 the other continuum).  Each entry a warp reads is then four runs of 64
-// contiguous bytes (eight block rows of one slot), whole DRAM access units.
+// y = A x on the compact layout.  LANES (2 or 4) lanes per block row and
+// 32 / LANES block rows per warp: lane = (32 / LANES) g + q serves block row
+// base + q and target slots g, g + LANES, ... (slot 0 this cell, 1..6 the
+// -x, +x, -y, +y, -z, +z neighbours, 7 the other continuum).  Each entry a
+// warp reads is then LANES runs of 256 / LANES contiguous bytes (the block
+// rows of one slot).
 // A lane gathers its target block's unknowns into canonical positions and
 // accumulates the block row's canonical rows in registers; the four partial
 // rows are summed by a butterfly over the lanes of the same q and stored at
@@ -219,21 +141,23 @@ __global__ void __launch_bounds__(128) spmv_row_kernel(const KView v, const doub
 // block does not use (one-phase blocks), are not fetched.
 // ---------------------------------------------------------------------------
 constexpr int kSpmvThreads = 128;
-// block rows from which the one-thread-per-block-row form is used
+// block rows from which the two-lane form is used
 constexpr long kSpmvRowForm = 148L * 2048;
 
-template <int N>
+template <int N, int LANES>
 __global__ void __launch_bounds__(kSpmvThreads) spmv_kernel(const KView v, const double *__restrict__ x,
                                                              double *__restrict__ y, const KspScal *s) {
     if (s && s->reason != kItersRunning) return;
+    static_assert(LANES == 2 || LANES == 4, "two or four lanes per block row");
     constexpr int BS = 2 * N + 4;
+    constexpr int ROWS = 32 / LANES;   // block rows per warp
     const Layout L(N);
     const long nb = 2 * v.n;
-    const int lane = threadIdx.x & 31, g = lane >> 3, q = lane & 7;
-    const long groups = (nb + 7) / 8;
+    const int lane = threadIdx.x & 31, g = lane / ROWS, q = lane % ROWS;
+    const long groups = (nb + ROWS - 1) / ROWS;
     const long gstride = (long)gridDim.x * (kSpmvThreads / 32);
     for (long grp = (long)blockIdx.x * (kSpmvThreads / 32) + (threadIdx.x >> 5); grp < groups; grp += gstride) {
-        const long b = grp * 8 + q;
+        const long b = grp * ROWS + q;
         const bool valid = b < nb;
         double acc[BS];
 #pragma unroll
@@ -246,8 +170,8 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_kernel(const KView v, const
             for (int r = 0; r < BS; r++) rm |= (unsigned long long)(ref_row(N, lb, r) >= 0) << r;
             const double *val = v.vals + ((b >> 5) * v.entries) * 32 + (b & 31);
 #pragma unroll 1
-            for (int h = 0; h < 2; h++) {
-                const int sl = g + 4 * h;
+            for (int h = 0; h < 8 / LANES; h++) {
+                const int sl = g + LANES * h;
                 const long tb = slot_block(v, b, sl);
                 if (tb < 0) continue;
                 const int lt = label_of(v, tb);
@@ -293,19 +217,19 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_kernel(const KView v, const
                 }
             }
         }
-        // sum the four slot lanes of each block row
+        // sum the slot lanes of each block row
 #pragma unroll
         for (int r = 0; r < BS; r++) {
             double t = acc[r];
-            t += __shfl_xor_sync(0xffffffffu, t, 8);
-            t += __shfl_xor_sync(0xffffffffu, t, 16);
+#pragma unroll
+            for (int o = ROWS; o < 32; o <<= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
             acc[r] = t;
         }
         if (valid) {
             const long off = v.rowoff[b];
 #pragma unroll
             for (int r = 0; r < BS; r++) {
-                if ((r & 3) != g) continue;
+                if ((r % LANES) != g) continue;
                 const int rr = ref_row(N, lb, r);
                 if (rr >= 0) y[off + rr] = acc[r];
             }

@@ -131,7 +131,7 @@ def test_iteration_semantics_match_restatement(name, tmp_path, cuda_device):
 
 
 def test_matmult_large_grid_form(tmp_path, cuda_device):
-    """Grids of at least 148 x 2048 block rows use the one-thread-per-block-row
+    """Grids of at least 148 x 2048 block rows use the two-lane-per-block-row
     product: on 64x64x37 (303,104 block rows, the device start-up state of
     the plain case) J v must match the host product of the same values placed
     by the pattern, per row within 1e-12 of sum_j |J_ij v_j|."""
