@@ -35,6 +35,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -44,6 +45,12 @@ METRIC = "flash+Jacobian cells/s on 1 B200, batched vs plain, at 1e-10 rel err"
 UNIT = "cells/s"
 WORKLOAD = "batched flash: 1,048,576 cells, SRK, 6 components, P~U(5,40) MPa, T~U(300,450) K, z~Dirichlet(1), " \
            "with fugacity derivatives of both phases"
+
+
+def flash_config(n: int, world: int) -> dict:
+    """The workload's config object, the same dict in both arms."""
+    return {"workload": WORKLOAD, "cells_per_gpu": n, "nc": 6, "eos": "SRK", "parallelism": f"replicas x{world}",
+            "l2": "GPU arm: flushed before every step (256 MiB write)"}
 
 
 def parse():
@@ -136,11 +143,12 @@ class CpuInstances:
             p.terminate()
 
 
-def _cpu_worker_run(_):
+def _cpu_worker_run(keep):
     import oracle
     t = time.perf_counter()
-    oracle.ref_flash_batch(_W["fl"], _W["P"], _W["T"], _W["z"])
-    return time.perf_counter() - t
+    out = oracle.ref_flash_batch(_W["fl"], _W["P"], _W["T"], _W["z"])
+    sec = time.perf_counter() - t
+    return (sec, out) if keep else sec
 
 
 ASM_CPU_GRID = (128, 128, 16)
@@ -198,14 +206,49 @@ class CpuReference:
 
     def step(self) -> float:
         t = time.perf_counter()
-        rs = [p.apply_async(_cpu_worker_run, (0,)) for p in self.pools]
+        rs = [p.apply_async(_cpu_worker_run, (False,)) for p in self.pools]
         for r in rs:
             r.get()
         return time.perf_counter() - t
 
+    def step_with_results(self):
+        """One timed step that also returns the reference's results for all
+        cells (label, x, y, sat_o, sat_g, rho_o, rho_g), shards in order."""
+        import numpy as np
+        t = time.perf_counter()
+        rs = [p.apply_async(_cpu_worker_run, (True,)) for p in self.pools]
+        parts = [r.get()[1] for r in rs]
+        sec = time.perf_counter() - t
+        out = {k: np.concatenate([q[k] for q in parts], axis=-1) for k in parts[0]}
+        return sec, out
+
     def close(self):
         for p in self.pools:
             p.terminate()
+
+
+def flash_parity_summary(got: dict, ref: dict, P, T) -> dict:
+    """Every benchmarked cell against the reference's own SuccFalsh results
+    (the CPU baseline's outputs): labels, present-phase compositions under
+    the flash bar (1e-10 relative + 1e-13), and the saturations and densities
+    the reference forms from L and Z."""
+    import numpy as np
+    import oracle
+    r = oracle.flash_parity(got, ref, fields=("x", "y"))
+    sat_o, sat_g, rho_o, rho_g = oracle.derived_sat_rho(got, P, T)
+    lab = ref["label"]
+    derived = {}
+    for k, v, pres in (("sat_o", sat_o, lab == 0), ("sat_g", sat_g, lab == 0), ("rho_o", rho_o, lab >= 0),
+                       ("rho_g", rho_g, lab <= 0)):
+        e = np.abs(v - ref[k]) / np.maximum(np.abs(ref[k]), 1e-300)
+        derived[k] = float(e[pres].max()) if pres.any() else 0.0
+    return {"against": "reference SuccFalsh (oracle/_ref), every cell of the workload",
+            "cells": int(lab.shape[0]), "labels_equal": r["labels_equal"],
+            "label_mismatches": int(np.count_nonzero(np.asarray(got["label"]) != lab)),
+            "frac_within_1e-10": r["frac_tight"], "margin_cells": int(len(r["margin"])),
+            "frac_within_1e-10_incipient": r["frac_tight_incipient"],
+            "max_scaled_err": r["max_scaled_err"], "bar_ok": bool(r["ok"]),
+            "max_rel_err_derived": derived}
 
 
 def run_reference_arm(args):
@@ -228,7 +271,7 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "cells": n, "nc": 6, "eos": "SRK"},
+            "config": flash_config(n, args.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.cores, "kind": "reference",
                              "sample": f"all {n} cells per step, sharded over {ref.cores} processes"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -246,9 +289,8 @@ class ClockSampler:
     def __init__(self, bus_id: str):
         self.proc = None
         self.bus = bus_id.lower()
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"osiris_clocks_{os.getpid()}_{id(self)}.csv")
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
@@ -265,7 +307,13 @@ class ClockSampler:
             self.proc.kill()
         self.fh.close()
         rows = []
-        for line in open(self.path):
+        with open(self.path) as fh:
+            lines = fh.readlines()
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
+        for line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9 and parts[0].lower().endswith(self.bus):
                 try:
@@ -291,18 +339,16 @@ def _gpu_id(torch, dev):
 
 # ----------------------------------------------------------------------------- GPU side
 
-def _traffic_from_profiles():
-    """dram bytes per launch of the flash kernel, from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "flash_queue_srk6.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+# DRAM bytes (read + write) per call of the flash iteration kernels, from one
+# ncu capture of the first pass at 262,144 cells (dram__bytes_read.sum +
+# dram__bytes_write.sum) scaled by 4 to the 1,048,576-cell call: the first
+# pass reads every cell's inputs and writes the outputs of the cells it
+# finishes and the parked state of the rest; later passes touch only the
+# parked lists.  Capture command:
+#   ncu --set full --clock-control none -k regex:flash_queue_kernel -c 1
+#       python bench.py --cells 262144 --steps 1 --warmup 1 --no-e2e
+#       --no-cpu-baseline --no-plain --no-assembly --no-instances --no-steps
+FLASH_TRAFFIC_BYTES = 214216704
 
 
 def instance_groups(args, rank):
@@ -819,6 +865,9 @@ def run_ours(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
+    # the benchmarked results, kept for the parity summary against the
+    # reference's own outputs (computed beside the CPU baseline)
+    got_host = {k: out[k].cpu().numpy() for k in ("label", "L", "x", "y", "Zl", "Zg")}
     iters = out["iters"].cpu().numpy()
     rr = out["rr_iters"].cpu().numpy()
     two_phase = float((out["label"] == 0).float().mean().item())
@@ -854,7 +903,7 @@ def run_ours(args):
     dflops = flop_model.deriv_kernel_flops(nc, n)
     # derivative pass: reads P, T once, x|y and Z per phase; writes both blocks
     deriv_bytes = n * (16 + 2 * (nc * 8 + 8) + 2 * (nc * nc + nc) * 8)
-    traffic = _traffic_from_profiles()
+    traffic = FLASH_TRAFFIC_BYTES if n == workloads.FLASH_CELLS else None
 
     # batched vs plain (same outputs; the plain form is the one-thread-per-cell kernel)
     plain = None
@@ -905,12 +954,14 @@ def run_ours(args):
                                       gpu_id, world, cpu_inst)
 
     cpu_line = None
+    parity = None
     if cpu is not None:
         cpu.step()  # warm the workers (library load, first-touch)
-        sec = cpu.step()
+        sec, ref_out = cpu.step_with_results()
         cpu.close()
         cpu_line = {"value": n / sec, "unit": UNIT, "cores": cpu.cores, "kind": "reference",
                     "sample": f"all {n} cells of the workload, reference SuccFalsh, one process per core"}
+        parity = flash_parity_summary(got_host, ref_out, Pn, Tn)
 
     if world > 1:
         dist.barrier()
@@ -921,11 +972,10 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, numpy default_rng)",
-        "config": {"workload": WORKLOAD, "cells_per_gpu": n, "nc": nc, "eos": "SRK", "form": "batched",
-                   "l2": "flushed before every step (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "two_phase_fraction": two_phase, "mean_ss_iters": float(iters.mean()),
-                   "mean_rr_iters": float(rr.mean()), "max_ss_iters": int(iters.max()),
-                   "max_rr_iters": int(rr.max())},
+        "config": flash_config(n, world),
+        "workload_stats": {"form": "batched", "two_phase_fraction": two_phase, "mean_ss_iters": float(iters.mean()),
+                           "mean_rr_iters": float(rr.mean()), "max_ss_iters": int(iters.max()),
+                           "max_rr_iters": int(rr.max())},
         "roofline": {"bound": "fp64", "kernel": f"flash_queue_kernel<6>, all {osr.flash_passes()} passes of one call",
                      "achieved": achieved,
                      "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
@@ -944,6 +994,8 @@ def run_ours(args):
         line["e2e"] = e2e
     if cpu_line is not None:
         line["cpu_baseline"] = cpu_line
+    if parity is not None:
+        line["parity"] = parity
     if assembly is not None:
         line["assembly"] = assembly
     if instances is not None:

@@ -89,8 +89,11 @@ osr_status osr_flash_batch(const osr_fluid *fluid, const double *d_P, const doub
  *     (about 466,000 cells at nc = 6, 220,000 at nc = 16); larger n returns
  *     OSR_ERR_SIZE before any device work.  Split larger batches.
  *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress, that device current) and caches it; make that
- *     first call before any stream capture.
+ *     (cudaGetSymbolAddress, that device current) and caches it per CUDA
+ *     context; make that first call before any stream capture.  After a
+ *     device reset (cudaDeviceReset) or with a new primary context the
+ *     next call looks the address up again.
+ *   - `stream` must belong to the current device (else OSR_ERR_ARG).
  *   - Every call shares the array: the call clears its header on `stream`,
  *     and calls that overlap on the GPU (other streams, other threads) race.
  *     Serialise them.
@@ -114,6 +117,19 @@ osr_status osr_flash_batch_instances(const osr_fluid *fluids, int n_inst, const 
  * baseline the batched form is measured against. */
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T,
                                  const double *d_z, long n, const osr_flash_out *out, void *stream);
+
+/* Fugacity-coefficient derivatives of both phases at given states (DEVICE
+ * pointers): d ln(phi_i)/d w_k into d_dlnphi_dx [2][nc][nc][n] and
+ * d ln(phi_i)/d P into d_dlnphi_dP [2][nc][n], phase 0 at (d_P, d_T, d_x
+ * [nc][n], d_Zl), phase 1 at (d_P, d_T, d_y [nc][n], d_Zg).  The pass the
+ * flash runs on its own outputs, for a caller whose compositions come from
+ * elsewhere (the reference renormalises them when it unpacks the unknowns,
+ * compsim/PetscAUX.cpp:176-498).  Replaces the mixing-rule and implicit-dZ
+ * part of the fugacity rows of IteratorJacobian
+ * (compsim/Petsc_Functions.cpp:30243-30372).  Asynchronous on `stream`. */
+osr_status osr_fugacity_derivs(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_x,
+                               const double *d_y, const double *d_Zl, const double *d_Zg, long n, double *d_dlnphi_dx,
+                               double *d_dlnphi_dP, void *stream);
 
 /* End-to-end form for callers holding HOST arrays (same layouts; out fields
  * are host pointers): the cells go through in chunks of about 131,072
@@ -441,9 +457,23 @@ osr_status osr_sim_destroy(osr_sim *sim);
  * denominator of the flash kernel's roofline.  No reference counterpart. */
 osr_status osr_probe_fp64_peak(double *tflops, void *stream);
 
+/* The flash kernels' branch-free quotient and reciprocal on n operand pairs
+ * (DEVICE pointers): d_q[i] = a_i / b_i, d_r[i] = 1 / b_i as the kernels
+ * compute them, and d_ok[i] = 1 where the operands are inside the range the
+ * kernels accept without their IEEE fallback.  A test hook for the
+ * quotients' accuracy against IEEE division; no reference counterpart. */
+osr_status osr_probe_quotients(const double *d_a, const double *d_b, long n, double *d_q, double *d_r,
+                               signed char *d_ok, void *stream);
+
 /* Error reporting. */
 const char *osr_status_string(osr_status s);
 int osr_last_cuda_error(void);
+
+/* Blocks the library has taken from its stream-ordered device pools since
+ * the process started (every allocating entry point counts here; the
+ * no-allocation entry point never does).  A diagnostic; no reference
+ * counterpart. */
+long osr_pool_alloc_count(void);
 int osr_version(void);
 
 #ifdef __cplusplus

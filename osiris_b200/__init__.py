@@ -21,7 +21,7 @@ import numpy as np
 
 from .build import INCLUDE, LIB
 
-__all__ = ["Fluid", "lib", "flash", "flash_host", "flash_instances", "set_shape", "get_shape", "header_symbols", "OsrError",
+__all__ = ["Fluid", "lib", "flash", "flash_host", "fugacity_derivs", "flash_instances", "set_shape", "get_shape", "header_symbols", "OsrError",
            "FLASH_OUTPUTS"]
 
 _vp = ctypes.c_void_p
@@ -194,9 +194,36 @@ def flash(fluid: Fluid, P, T, z, derivs: bool = True, form: str = "batched", out
     co = _out_struct(out, lambda t: t.data_ptr())
     fn = {"batched": lib().osr_flash_batch, "plain": lib().osr_flash_batch_plain,
           "noalloc": lib().osr_flash_batch_noalloc}[form]
-    rc = fn(fluid.cref, _vp(P.data_ptr()), _vp(T.data_ptr()), _vp(z.data_ptr()), ctypes.c_long(n),
-            ctypes.byref(co), _vp(stream.cuda_stream))
+    # the library takes its scratch on the current device: make it the tensors'
+    with torch.cuda.device(P.device):
+        rc = fn(fluid.cref, _vp(P.data_ptr()), _vp(T.data_ptr()), _vp(z.data_ptr()), ctypes.c_long(n),
+                ctypes.byref(co), _vp(stream.cuda_stream))
     _check(rc, f"osr_flash_batch ({form})")
+    return out
+
+
+def fugacity_derivs(fluid: Fluid, P, T, x, y, Zl, Zg, out: dict | None = None, stream=None):
+    """d ln(phi)/d w and d ln(phi)/d P of both phases at given device states
+    (``osr_fugacity_derivs``): P, T, Zl, Zg [n], x, y [nc, n] contiguous
+    float64 CUDA tensors.  Returns (or fills) {"dlnphi_dx": [2, nc, nc, n],
+    "dlnphi_dP": [2, nc, n]}."""
+    import torch
+    n, nc = int(P.shape[0]), fluid.nc
+    for t in (P, T, x, y, Zl, Zg):
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise OsrError("inputs must be contiguous float64 CUDA tensors")
+    if x.shape != (nc, n) or y.shape != (nc, n):
+        raise OsrError("x and y must be [nc, n]")
+    if out is None:
+        out = {"dlnphi_dx": torch.empty((2, nc, nc, n), dtype=torch.float64, device=P.device),
+               "dlnphi_dP": torch.empty((2, nc, n), dtype=torch.float64, device=P.device)}
+    if stream is None:
+        stream = torch.cuda.current_stream(P.device)
+    with torch.cuda.device(P.device):
+        _check(lib().osr_fugacity_derivs(fluid.cref, *(_vp(t.data_ptr()) for t in (P, T, x, y, Zl, Zg)),
+                                         ctypes.c_long(n), _vp(out["dlnphi_dx"].data_ptr()),
+                                         _vp(out["dlnphi_dP"].data_ptr()), _vp(stream.cuda_stream)),
+               "osr_fugacity_derivs")
     return out
 
 

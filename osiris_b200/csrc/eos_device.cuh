@@ -27,13 +27,18 @@ constexpr int kMaxNc = 16;
 // Branch-free FP64 reciprocal and quotient.  The IEEE operator is compiled
 // with an out-of-line slow path, and every such branch splits the code so
 // that independent divisions cannot overlap (a Rachford-Rice step measured
-// 4x its arithmetic latency).  Here the hardware reciprocal seed
-// (rcp.approx.ftz.f64) gets one Newton step and the quotient one residual
-// correction, q + r (a - b q): the result is within an ulp of the IEEE
-// quotient.  The callers gather qdiv_ok() over a whole step and redo that
-// step with IEEE division when any operand is out of range (zeros,
-// infinities, NaN, magnitudes beyond 2^+-1000), so special values follow the
-// reference exactly.
+// 4x its arithmetic latency).  Method: Newton-Raphson refinement of the
+// hardware reciprocal seed (rcp.approx.ftz.f64), r' = r + r (1 - b r), then a
+// residual-corrected quotient q' = q + r (a - b q) with the residual formed
+// by a fused multiply-add (P. Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).
+// qrcp takes two refinement steps, qdiv one step and the correction; both
+// are within one ulp of the IEEE result for operands inside qdiv_ok's range
+// (tests/test_quotients_gpu.py checks this on random and edge operands).
+// The callers gather qdiv_ok() over a whole step and redo that step with
+// IEEE division when any operand is out of range (zeros, infinities, NaN,
+// magnitudes beyond 2^+-1000), so special values follow the reference
+// exactly.
 __device__ __forceinline__ bool qdiv_ok(double a, double b) {
     double mb = fabs(b);
     return mb > 9.33e-302 && mb < 1.07e301 && fabs(a) < 1.07e301;

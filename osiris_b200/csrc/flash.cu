@@ -1,6 +1,7 @@
 // Host side of the flash hot path: component-table preparation, template
 // dispatch on the component count, launches, and the C-ABI entry points
 // declared in include/osiris_b200.h.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <atomic>
 #include <cmath>
@@ -69,42 +70,90 @@ static osr_status check_out(const osr_flash_out *o) {
     return OSR_OK;
 }
 
-// Library-private stream-ordered pool per device, keeping freed blocks for
-// reuse (release threshold = unlimited) so that repeated calls do not map and
-// unmap device memory; the process's default pool is left untouched.
+// Device a stream belongs to (the current device for the default streams).
+static cudaError_t stream_device(cudaStream_t s, int *dev) {
+    if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) return cudaGetDevice(dev);
+    return cudaStreamGetDevice(s, dev);
+}
+
+// Identifier of the calling thread's current CUDA context, read through the
+// driver entry points the runtime hands out (the library links no libcuda).
+// Per-device state cached by this file (memory pools, the no-allocation
+// scratch address) belongs to one context: a device reset or a new primary
+// context changes this id and the state is built again.  0 = unknown.
+static unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    using GetId = CUresult (*)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)f;
+    });
+    CUcontext c = nullptr;
+    if (!get_current || get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    unsigned long long id = 0;
+    if (get_id && get_id(c, &id) == CUDA_SUCCESS) return id + 1;
+    return (unsigned long long)(uintptr_t)c;
+}
+
+// Library-private stream-ordered pool per device (and context), keeping freed
+// blocks for reuse (release threshold = unlimited) so that repeated calls do
+// not map and unmap device memory; the process's default pool is left
+// untouched.  The pool lives on the device of the stream the block is taken
+// on, which must be the current device.
+static std::atomic<unsigned long long> g_pool_allocs{0};
+
 static cudaError_t pool_alloc(void **p, size_t bytes, cudaStream_t s) {
     static std::mutex mu;
     static cudaMemPool_t pools[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    static unsigned long long pool_ctx[64] = {};
+    int dev = 0, cur = 0;
+    cudaError_t e = stream_device(s, &dev);
     if (e != cudaSuccess) return e;
+    if ((e = cudaGetDevice(&cur)) != cudaSuccess) return e;
+    if (dev != cur) return cudaErrorInvalidResourceHandle;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
     {
         std::lock_guard<std::mutex> lk(mu);
-        if (!pools[dev]) {
+        const unsigned long long ctx = current_context_id();
+        if (!pools[dev] || (ctx != 0 && ctx != pool_ctx[dev])) {
             cudaMemPoolProps props = {};
             props.allocType = cudaMemAllocationTypePinned;
             props.location.type = cudaMemLocationTypeDevice;
             props.location.id = dev;
-            if ((e = cudaMemPoolCreate(&pools[dev], &props)) != cudaSuccess) return e;
+            cudaMemPool_t np = nullptr;
+            if ((e = cudaMemPoolCreate(&np, &props)) != cudaSuccess) return e;
             uint64_t keep = UINT64_MAX;
-            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            cudaMemPoolSetAttribute(np, cudaMemPoolAttrReleaseThreshold, &keep);
+            pools[dev] = np;
+            pool_ctx[dev] = ctx;
         }
+        pool = pools[dev];
     }
-    return cudaMallocFromPoolAsync(p, bytes, pools[dev], s);
+    g_pool_allocs.fetch_add(1);
+    return cudaMallocFromPoolAsync(p, bytes, pool, s);
 }
 
+// Multiprocessor count of the current device, cached per device.
 static int sm_count() {
-    static int cached = 0;
-    if (!cached) {
-        int dev = 0, n = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) ==
-                                                       cudaSuccess)
-            cached = n;
-        else
-            cached = 148;
-    }
-    return cached;
+    static std::atomic<int> cached[64] = {};
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    int c = cached[dev].load();
+    if (c > 0) return c;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached[dev].store(n);
+    return n;
 }
 
 enum class Form { kQueue, kPlain };
@@ -188,6 +237,34 @@ struct Instances {
     int n = 0;
 };
 
+// The derivative pass over given states: one thread per (cell, phase).
+template <int N>
+static osr_status launch_derivs(const FluidTable<N> &table, const Instances<N> &inst, const double *P, const double *T,
+                                const double *x, const double *y, const double *Zl, const double *Zg, long n,
+                                double *dlnphi_dx, double *dlnphi_dP, cudaStream_t s) {
+    DerivArgs<N> d;
+    d.f = table;
+    d.P = P;
+    d.T = T;
+    d.x = x;
+    d.y = y;
+    d.Zl = Zl;
+    d.Zg = Zg;
+    d.n = n;
+    d.dlnphi_dx = dlnphi_dx;
+    d.dlnphi_dP = dlnphi_dP;
+    d.tables = inst.tables;
+    d.inst_start = inst.start;
+    d.n_inst = inst.n;
+    long blocks = (n + 127) / 128;
+    long cap = (long)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    if (inst.tables) flash_deriv_kernel<N, true><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+    else flash_deriv_kernel<N, false><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
+    OSR_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
 template <int N>
 static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double *T, const double *z, long n,
                               const osr_flash_out &o, cudaStream_t s, Form form, char *scratch,
@@ -232,28 +309,7 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
             OSR_CUDA(cudaGetLastError());
         }
     }
-    if (o.dlnphi_dx) {
-        DerivArgs<N> d;
-        d.f = table;
-        d.P = P;
-        d.T = T;
-        d.x = o.x;
-        d.y = o.y;
-        d.Zl = o.Zl;
-        d.Zg = o.Zg;
-        d.n = n;
-        d.dlnphi_dx = o.dlnphi_dx;
-        d.dlnphi_dP = o.dlnphi_dP;
-        d.tables = inst.tables;
-        d.inst_start = inst.start;
-        d.n_inst = inst.n;
-        long blocks = (n + 127) / 128;
-        long cap = (long)sm_count() * 8;
-        if (blocks > cap) blocks = cap;
-        if (multi) flash_deriv_kernel<N, true><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
-        else flash_deriv_kernel<N, false><<<dim3((unsigned)blocks, 2), 128, 0, s>>>(d);
-        OSR_CUDA(cudaGetLastError());
-    }
+    if (o.dlnphi_dx) return launch_derivs<N>(table, inst, P, T, o.x, o.y, o.Zl, o.Zg, n, o.dlnphi_dx, o.dlnphi_dP, s);
     return OSR_OK;
 }
 
@@ -331,16 +387,21 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 static cudaError_t noalloc_scratch(char **out) {
     static std::mutex mu;
     static char *addr[64] = {};
+    static unsigned long long addr_ctx[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
+    // looked up again when the context changed (device reset, new primary
+    // context) or cannot be identified: the array may then sit elsewhere
+    const unsigned long long ctx = current_context_id();
+    if (!addr[dev] || ctx == 0 || ctx != addr_ctx[dev]) {
         void *a = nullptr;
         e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         addr[dev] = (char *)a;
+        addr_ctx[dev] = ctx;
     }
     *out = addr[dev];
     return cudaSuccess;
@@ -366,6 +427,11 @@ osr_status osr_flash_batch_noalloc(const osr_fluid *fluid, const double *d_P, co
     if ((st = check_out(out))) return st;
     if (!d_P || !d_T || !d_z) return OSR_ERR_ARG;
     if (queue_scratch_bytes(n, fluid->nc) > kNoAllocScratchBytes) return OSR_ERR_SIZE;
+    // the scratch address is the current device's: the stream must be on it
+    int sdev = 0, cur = 0;
+    OSR_CUDA(stream_device((cudaStream_t)stream, &sdev));
+    OSR_CUDA(cudaGetDevice(&cur));
+    if (sdev != cur) return OSR_ERR_ARG;
     char *scratch = nullptr;
     OSR_CUDA(noalloc_scratch(&scratch));
     // run_flash clears the scratch header (queue heads, parked counts) on
@@ -405,6 +471,31 @@ osr_status osr_flash_batch_instances(const osr_fluid *fluids, int n_inst, const 
     cudaError_t e = cudaFreeAsync(scratch, s);
     if (st == OSR_OK && e != cudaSuccess) return cuda_fail(e);
     return st;
+}
+
+osr_status osr_fugacity_derivs(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_x,
+                               const double *d_y, const double *d_Zl, const double *d_Zg, long n, double *d_dlnphi_dx,
+                               double *d_dlnphi_dP, void *stream) {
+    osr_status st = check_fluid(fluid);
+    if (st) return st;
+    if (n < 0) return OSR_ERR_ARG;
+    if (n == 0) return OSR_OK;
+    if (!d_P || !d_T || !d_x || !d_y || !d_Zl || !d_Zg || !d_dlnphi_dx || !d_dlnphi_dP) return OSR_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (fluid->nc) {
+#define OSR_NC_CASE(K)                                                                                        \
+    case K: {                                                                                                \
+        FluidTable<K> t;                                                                                     \
+        make_table<K>(*fluid, t);                                                                            \
+        return launch_derivs<K>(t, Instances<K>(), d_P, d_T, d_x, d_y, d_Zl, d_Zg, n, d_dlnphi_dx, d_dlnphi_dP, \
+                                s);                                                                          \
+    }
+        OSR_NC_CASE(1) OSR_NC_CASE(2) OSR_NC_CASE(3) OSR_NC_CASE(4) OSR_NC_CASE(5) OSR_NC_CASE(6)
+        OSR_NC_CASE(7) OSR_NC_CASE(8) OSR_NC_CASE(9) OSR_NC_CASE(10) OSR_NC_CASE(11) OSR_NC_CASE(12)
+        OSR_NC_CASE(13) OSR_NC_CASE(14) OSR_NC_CASE(15) OSR_NC_CASE(16)
+#undef OSR_NC_CASE
+        default: return OSR_ERR_NC;
+    }
 }
 
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
@@ -572,6 +663,7 @@ const char *osr_status_string(osr_status s) {
 }
 
 int osr_last_cuda_error(void) { return g_last_cuda.load(); }
+long osr_pool_alloc_count(void) { return (long)g_pool_allocs.load(); }
 int osr_version(void) { return OSR_VERSION; }
 
 }  // extern "C"

@@ -5,8 +5,21 @@
 // the grid fills every SM.  Result = 2 * FMAs / elapsed seconds.
 #include <cuda_runtime.h>
 #include "osiris_b200.h"
+#include "eos_device.cuh"
 
 namespace {
+
+// The branch-free quotient and reciprocal of the flash kernels on arrays of
+// operands, with the range predicate their callers gather.
+__global__ void __launch_bounds__(256) quotient_probe_kernel(const double *a, const double *b, long n, double *q,
+                                                             double *r, signed char *ok) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        q[i] = osr::qdiv(a[i], b[i]);
+        r[i] = osr::qrcp(b[i]);
+        ok[i] = osr::qdiv_ok(a[i], b[i]) ? 1 : 0;
+    }
+}
 
 constexpr int kChains = 8;
 constexpr int kIters = 4096;
@@ -28,6 +41,16 @@ __global__ void __launch_bounds__(256) dfma_probe_kernel(double seed, double *si
 }
 
 }  // namespace
+
+extern "C" osr_status osr_probe_quotients(const double *d_a, const double *d_b, long n, double *d_q, double *d_r,
+                                          signed char *d_ok, void *stream) {
+    if (n < 0 || (n > 0 && (!d_a || !d_b || !d_q || !d_r || !d_ok))) return OSR_ERR_ARG;
+    if (n == 0) return OSR_OK;
+    long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    quotient_probe_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(d_a, d_b, n, d_q, d_r, d_ok);
+    return cudaGetLastError() == cudaSuccess ? OSR_OK : OSR_ERR_CUDA;
+}
 
 extern "C" osr_status osr_probe_fp64_peak(double *tflops, void *stream) {
     if (!tflops) return OSR_ERR_ARG;

@@ -15,7 +15,7 @@ Counts are per cell and depend on the kernel-reported iteration numbers:
 with n_ss the successive-substitution steps and n_rr the Rachford-Rice
 Newton steps that cell took.  The roofline's achieved rate is the sum over
 all cells divided by the kernels' measured time; ncu's executed FP64
-instruction counts are the cross-check (profiles/).
+instruction counts are the cross-check.
 """
 from __future__ import annotations
 

@@ -56,8 +56,14 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda_device):
     ref = _host(osr.flash(fl, P, T, z, derivs=True, form="batched"))
     torch.cuda.synchronize()
     for _ in range(2):
-        got = osr.flash(fl, P, T, z, derivs=True, form="noalloc")
+        out = osr.alloc_flash_outputs(6, int(P.shape[0]), True, P.device)
         torch.cuda.synchronize()
+        taken = osr.lib().osr_pool_alloc_count()
+        got = osr.flash(fl, P, T, z, derivs=True, form="noalloc", out=out)
+        torch.cuda.synchronize()
+        # the property in the entry point's name: the call took no block from
+        # the library's device pools
+        assert osr.lib().osr_pool_alloc_count() == taken
         _check_same(_host(got), ref)
 
 
