@@ -33,7 +33,8 @@ typedef enum {
     OSR_ERR_CUDA = 3,      /* a CUDA runtime call failed (see osr_last_cuda_error) */
     OSR_ERR_NODEVICE = 4,  /* no sm_100 device is current */
     OSR_ERR_SIZE = 5,      /* request larger than the entry point supports */
-    OSR_ERR_UNSUPPORTED = 6  /* a cell state the entry point does not cover (see its description) */
+    OSR_ERR_UNSUPPORTED = 6, /* a cell state the entry point does not cover (see its description) */
+    OSR_ERR_DECK = 7         /* the deck cannot be read (see osr_deck_error) */
 } osr_status;
 
 typedef enum { OSR_EOS_PR = 0, OSR_EOS_SRK = 1 } osr_eos;
@@ -192,6 +193,43 @@ typedef struct osr_model {
 } osr_model;
 
 typedef struct osr_grid osr_grid;
+
+/* ---------------------------------------------------------------------------
+ * Decks: the reference's Data_Input keyword format read in C++
+ * (compsim/Data_Input.cpp:13-1349, compsim/MIfstream.cpp:8-47): GRID NC
+ * RESTEMP WATERPROPS DI DJ DK TOR POR CDIF SIGMA DTMAX FPOR Lf Re_f PERMI/J/K
+ * FPERMI/J/K REFP CPOR DCPOR MODEL SG TB MW AC PCRIT TCRIT VCRIT ZCRIT
+ * COMPNAME (the reference's component library) BIC SWT SGT INITCOND 0/1/3
+ * with IPRESS FIPRESS IWS FIWS IGC FIGC, WELLS, DT, TOTALT; CON/VAR/IVAR/KVAR
+ * arrays and k*v repeat groups.  Host memory only; no device work. */
+typedef struct osr_deck osr_deck;
+
+/* Parse a deck file.  OSR_ERR_DECK with the reason in osr_deck_error() when
+ * a required keyword is missing or malformed (the reference stops with TerM
+ * there, compsim/Data_Input.cpp). */
+osr_status osr_deck_open(const char *path, osr_deck **out);
+const char *osr_deck_error(void);
+/* The parsed values as an osr_model (pointers into the deck, valid until
+ * osr_deck_close), ready for osr_grid_create. */
+osr_status osr_deck_model(const osr_deck *deck, osr_model *out);
+/* The INITCOND state of one medium (0 matrix, 1 fracture): oil pressure
+ * [cells], water saturation [cells], feed composition [nc][cells]. */
+osr_status osr_deck_initial_state(const osr_deck *deck, int medium, const double **p0, const double **sw0,
+                                  const double **z0);
+/* DT and TOTALT in s, DTMAX, the INITCOND mode (any may be null). */
+osr_status osr_deck_times(const osr_deck *deck, double *dt, double *total_time, double *dtmax, int *initcond);
+osr_status osr_deck_close(osr_deck *deck);
+
+/* Open a deck and form the reference's start-up state on the current device
+ * (compsim/PrimeSim.cpp:68-85): the INITCOND pressures, water saturations
+ * and feed compositions, a flash of every cell-medium (AllFlash,
+ * compsim/Init_Calcs.cpp:949-962), then UpdateDependencies(true) (phase
+ * control, PCoeff, the row layout, the property sweeps;
+ * compsim/PetscAUX.cpp:500-545).  The grid is then ready for
+ * osr_grid_form_function / osr_grid_form_jacobian (FormFunction /
+ * FormJacobian) and osr_sim_create.  Synchronises `stream` before return;
+ * release with osr_grid_destroy. */
+osr_status osr_create(const char *deck_path, void *stream, osr_grid **out);
 
 /* Upload a model; geometric transmissibilities (IFK_Calc,
  * compsim/Init_Calcs.cpp:21-46) and block heights are formed here. */

@@ -314,6 +314,51 @@ class _CModel(ctypes.Structure):
                 ("nwells", ctypes.c_int), ("wells_i", _vp), ("wells_f", _vp), ("tor", _vp), ("dt", ctypes.c_double)]
 
 
+def read_deck(path: str) -> dict:
+    """The deck as the library's C++ reader parses it (osr_deck_open,
+    osr_deck_model, osr_deck_initial_state, osr_deck_times): a dict of
+    numpy copies keyed like ``deck.Deck``'s fields.  No device work."""
+    L = lib()
+    h = ctypes.c_void_p()
+    rc = L.osr_deck_open(path.encode(), ctypes.byref(h))
+    if rc:
+        raise OsrError(f"osr_deck_open: {L.osr_deck_error().decode()}")
+    try:
+        m = _CModel()
+        _check(L.osr_deck_model(h, ctypes.byref(m)), "osr_deck_model")
+        n, nc = m.nx * m.ny * m.nz, m.nc
+
+        def arr(ptr, count, ct=ctypes.c_double):
+            if not ptr:
+                return None
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)), shape=(count,)).copy()
+        out = dict(nx=m.nx, ny=m.ny, nz=m.nz, nc=nc, eos=m.eos, restemp=m.restemp, wat_ro=m.wat_ro,
+                   wat_mu=m.wat_mu, refp=m.refp, cpor=m.cpor, dcpor=m.dcpor, lf=m.lf, re_f=m.re_f, sigma=m.sigma,
+                   cdif=m.cdif if m.has_cdif else None, di=arr(m.di, m.nx), dj=arr(m.dj, m.ny), dk=arr(m.dk, m.nz),
+                   por=arr(m.por, n), fpor=arr(m.fpor, n), perm=arr(m.perm, 3 * n).reshape(3, n),
+                   fperm=arr(m.fperm, 3 * n).reshape(3, n), tor=arr(m.tor, n), dt=m.dt,
+                   swt=arr(m.swt, 4 * m.nswt).reshape(-1, 4), sgt=arr(m.sgt, 4 * m.nsgt).reshape(-1, 4),
+                   kij=arr(m.kij, nc * nc).reshape(nc, nc))
+        for k in ("mw", "tc", "pc", "vc", "acf", "parachor", "zc"):
+            out[k] = arr(getattr(m, k), nc)
+        nw = m.nwells
+        out["wells_i"] = (arr(m.wells_i, 5 * nw, ctypes.c_int).reshape(nw, 5) if nw else np.zeros((0, 5), np.int32))
+        out["wells_f"] = arr(m.wells_f, (nc + 6) * nw).reshape(nw, nc + 6) if nw else np.zeros((0, nc + 6))
+        for med, (kp, ks, kz) in enumerate((("p0", "sw0", "z0"), ("fp0", "fsw0", "fz0"))):
+            p0, sw0, z0 = (ctypes.c_void_p() for _ in range(3))
+            _check(L.osr_deck_initial_state(h, med, ctypes.byref(p0), ctypes.byref(sw0), ctypes.byref(z0)),
+                   "osr_deck_initial_state")
+            out[kp], out[ks] = arr(p0.value, n), arr(sw0.value, n)
+            out[kz] = arr(z0.value, nc * n).reshape(nc, n)
+        dt, tt, dtmax, ic = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(L.osr_deck_times(h, ctypes.byref(dt), ctypes.byref(tt), ctypes.byref(dtmax), ctypes.byref(ic)),
+               "osr_deck_times")
+        out.update(total_time=tt.value, dtmax=dtmax.value, initcond=ic.value)
+        return out
+    finally:
+        L.osr_deck_close(h)
+
+
 class Grid:
     """A dual-porosity model on the device, built from a parsed deck
     (``osiris_b200.deck.parse_deck``)."""
@@ -344,6 +389,23 @@ class Grid:
         L = lib()
         _check(L.osr_grid_create(ctypes.byref(m), ctypes.byref(h)), "osr_grid_create")
         self._h = h
+
+    @classmethod
+    def create(cls, path: str, stream=None) -> "Grid":
+        """osr_create: the deck read by the library's C++ reader and the
+        start-up state formed on the current device in one C call."""
+        from . import deck as _deck
+        h = ctypes.c_void_p()
+        L = lib()
+        rc = L.osr_create(path.encode(), None if stream is None else _vp(stream), ctypes.byref(h))
+        if rc == 7:
+            raise OsrError(f"osr_create: {L.osr_deck_error().decode()}")
+        _check(rc, "osr_create")
+        g = cls.__new__(cls)
+        g._h = h
+        g.deck = _deck.parse_deck(path)
+        g.nc, g.cells = g.deck.nc, g.deck.cells
+        return g
 
     def close(self):
         if self._h:

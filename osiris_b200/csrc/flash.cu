@@ -658,6 +658,7 @@ const char *osr_status_string(osr_status s) {
         case OSR_ERR_NODEVICE: return "no suitable CUDA device";
         case OSR_ERR_SIZE: return "request exceeds the entry point's size limit";
         case OSR_ERR_UNSUPPORTED: return "a cell state the entry point does not cover";
+        case OSR_ERR_DECK: return "the deck cannot be read (osr_deck_error has the reason)";
     }
     return "unknown status";
 }

@@ -57,3 +57,22 @@ def test_initialize_matches_reference_startup(name, tmp_path, cuda_device):
         for ph, present in ((0, lab >= 0), (1, lab <= 0)):
             e = np.abs(rho[ph] - rr[ph])[present] / np.abs(rr[ph][present]).max() if present.any() else np.zeros(1)
             assert e.max() <= 1e-9, (m, ph, e.max())
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_osr_create_equals_package_startup(name, tmp_path, cuda_device):
+    """osr_create (C++ deck reader + start-up in one C call) forms exactly
+    the state Grid.initialize forms from the package's reader."""
+    import torch
+    path = os.path.join(str(tmp_path), name + ".dat")
+    deck.write_deck(path, CASES[name]())
+    with torch.cuda.device(cuda_device):
+        C = osr.Grid.create(path)
+    G = osr.Grid(deck.parse_deck(path))
+    G.initialize(cuda_device)
+    assert C.layout() == G.layout()
+    assert np.array_equal(C.row_offsets(), G.row_offsets())
+    for m in "mf":
+        for f in osr.Grid.FIELD_PLANES:
+            a, b = C.get(f"{m}.{f}"), G.get(f"{m}.{f}")
+            assert np.array_equal(a, b, equal_nan=True), (m, f)
