@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=None)
+    ap.add_argument("--pair-from", type=int, default=None, help="first flash pass in pair form (12 = never)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -829,6 +830,8 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
 
+    if args.pair_from is not None:
+        osr.set_pair_from(args.pair_from)
     tc, pc, acf, kij, eos = workloads.flash_fluid_srk6()
     fl = osr.Fluid(tc, pc, acf, kij, eos)
     nc = fl.nc

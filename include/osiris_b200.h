@@ -154,6 +154,13 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
  * occupancy); park_after in 0..500.  Values outside the ranges are
  * rejected.  Process-wide. */
 osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, int park_after);
+
+/* First pass (0-based) of the batched flash that runs in pair form: two
+ * lanes per cell, one per phase, for the few long-running cells of the late
+ * passes (each substitution step's latency halves).  12 or more = never.
+ * Process-wide; the results agree to rounding either way. */
+osr_status osr_flash_set_pair_from(int pass);
+int osr_flash_get_pair_from(void);
 osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm, int *park_after);
 
 /* Age limit of the substitution-step batching: a warp runs the step for its

@@ -294,6 +294,16 @@ def set_shape(ss_batch: int, tail_batch: int, ctas_per_sm: int, park_after: int)
            "osr_flash_set_shape")
 
 
+def set_pair_from(pass_index: int):
+    """First pass of the batched flash in pair form (osr_flash_set_pair_from);
+    12 = never."""
+    _check(lib().osr_flash_set_pair_from(int(pass_index)), "osr_flash_set_pair_from")
+
+
+def get_pair_from() -> int:
+    return int(lib().osr_flash_get_pair_from())
+
+
 def get_shape():
     v = [ctypes.c_int() for _ in range(4)]
     _check(lib().osr_flash_get_shape(*[ctypes.byref(x) for x in v]), "osr_flash_get_shape")

@@ -14,12 +14,14 @@
 
 namespace osr {
 
+constexpr int kMaxPasses = 12;
 static std::atomic<int> g_last_cuda{0};
 static std::atomic<int> g_ss_batch{28};
 static std::atomic<int> g_tail_batch{32};
 static std::atomic<int> g_ctas_per_sm{3};
 static std::atomic<int> g_park_after{2};
 static std::atomic<int> g_max_wait{1000};
+static std::atomic<int> g_pair_from{kMaxPasses};   // first pass run by the pair form
 
 static osr_status cuda_fail(cudaError_t e) {
     g_last_cuda.store((int)e);
@@ -163,7 +165,6 @@ enum class Form { kQueue, kPlain };
 //                   [kMaxPasses] -- zeroed per call;
 //   two parked-cell lists (ping-pong between passes), each with room for
 //   every cell: cell, k, rr, Lb, K[nc].
-constexpr int kMaxPasses = 12;
 struct ScratchLayout {
     size_t heads = 0, counts = 8 * kMaxPasses, header = 256;
     size_t list[2], cell, k, rr, Lb, K, list_bytes, total;
@@ -215,12 +216,13 @@ static int pass_limits(int park_after, int *lim) {
 }
 
 template <int N, bool MULTI>
-static int queue_blocks(long n) {
-    long warps_needed = (n + 31) / 32;
+static int queue_blocks(long n, bool pair = false) {
+    long warps_needed = ((pair ? 2 : 1) * n + 31) / 32;
     int per_sm = g_ctas_per_sm.load(), fit = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N, MULTI>, 128, 0) == cudaSuccess &&
-        fit > 0 && per_sm > fit)
-        per_sm = fit;
+    const cudaError_t e =
+        pair ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_pair_kernel<N, MULTI>, 128, 0)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N, MULTI>, 128, 0);
+    if (e == cudaSuccess && fit > 0 && per_sm > fit) per_sm = fit;
     long blocks = (long)sm_count() * per_sm;
     long max_blocks = (warps_needed + 3) / 4;
     if (blocks > max_blocks) blocks = max_blocks;
@@ -295,6 +297,8 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
         q.inst_start = inst.start;
         q.n_inst = inst.n;
         const int blocks = multi ? queue_blocks<N, true>(n) : queue_blocks<N, false>(n);
+        const int pblocks = multi ? queue_blocks<N, true>(n, true) : queue_blocks<N, false>(n, true);
+        const int pair_from = g_pair_from.load();
         for (int p = 0; p < np; p++) {
             q.first = p == 0;
             q.src = park_view(scratch, n, N, (p + 1) & 1);
@@ -304,8 +308,15 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
             q.head = heads + p;
             q.park_at = lim[p];
             q.ss_batch = p == 0 ? g_ss_batch.load() : g_tail_batch.load();
-            if (multi) flash_queue_kernel<N, true><<<blocks, 128, 0, s>>>(q);
-            else flash_queue_kernel<N, false><<<blocks, 128, 0, s>>>(q);
+            if (p >= pair_from) {
+                // late passes: two lanes per cell (the cells left are few and long-running)
+                if (multi) flash_pair_kernel<N, true><<<pblocks, 128, 0, s>>>(q);
+                else flash_pair_kernel<N, false><<<pblocks, 128, 0, s>>>(q);
+            } else if (multi) {
+                flash_queue_kernel<N, true><<<blocks, 128, 0, s>>>(q);
+            } else {
+                flash_queue_kernel<N, false><<<blocks, 128, 0, s>>>(q);
+            }
             OSR_CUDA(cudaGetLastError());
         }
     }
@@ -633,6 +644,14 @@ osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, in
     g_park_after.store(park_after);
     return OSR_OK;
 }
+
+osr_status osr_flash_set_pair_from(int pass) {
+    if (pass < 0 || pass > kMaxPasses) return OSR_ERR_ARG;
+    g_pair_from.store(pass);
+    return OSR_OK;
+}
+
+int osr_flash_get_pair_from(void) { return g_pair_from.load(); }
 
 osr_status osr_flash_set_max_wait(int max_wait) {
     if (max_wait < 0 || max_wait > 1000) return OSR_ERR_ARG;

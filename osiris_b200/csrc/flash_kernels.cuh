@@ -460,6 +460,338 @@ __global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_queue_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pair form: two lanes per cell, one per phase.
+//
+// After the first passes only a few percent of the cells are still
+// iterating, and they run for tens to hundreds of substitution steps: the
+// late passes leave most of the GPU idle and last as long as the slowest
+// cells' steps take one after another.  There the two lanes of a pair
+// (lanes 2q and 2q+1 of a warp, `par` = lane & 1) split every step: the
+// Rachford-Rice sums and the K update by component parity, the phase work
+// (mixing rule, cubic root, logarithms, ln phi) by phase -- lane 0 the
+// liquid, lane 1 the vapour -- with xor-1 shuffles between the halves.  Both
+// lanes hold K, z and L, and every exchanged value comes out identical in
+// the two lanes, so a pair's control flow stays uniform.  The arithmetic is
+// the thread-per-cell form's operation for operation; only the order of the
+// Rachford-Rice sums differs (each lane sums its components, then the two
+// halves are added).
+
+constexpr unsigned kPairFull = 0xffffffffu;
+
+// (value of component 2k + par) for the half arrays of a lane; `pad` for the
+// odd lane's missing last component when N is odd.
+template <int N>
+__device__ __forceinline__ double half_pick(const double *a, int k, int par, double pad) {
+    const double e = a[2 * k];
+    const double o = (2 * k + 1 < N) ? a[2 * k + 1] : pad;
+    return par ? o : e;
+}
+
+template <int N>
+__device__ __forceinline__ void pair_halves(const double *K, const double *z, int par, double *Kh, double *zh) {
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; k++) {
+        Kh[k] = half_pick<N>(K, k, par, 1.0);
+        zh[k] = half_pick<N>(z, k, par, 0.0);
+    }
+}
+
+// One Rachford-Rice Newton step over this lane's components (K, z of the
+// components 2k + par; a pad component has K = 1, z = 0 and adds nothing),
+// the halves summed across the pair.  `mask` = the lanes taking the step.
+template <int N, bool Fast>
+__device__ __forceinline__ double rr_step_pair_impl(const double *Kh, const double *zh, double L, bool &ok,
+                                                    unsigned mask) {
+    constexpr int H = (N + 1) / 2;
+    double zt = 0, zq = 0;
+    const double omL = 1 - L;
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const bool pos = Kh[k] >= 0;
+        double num = pos ? 1 - Kh[k] : 1.0;
+        double den = pos ? L + omL * Kh[k] : L - 1;
+        double td;
+        if (Fast) {
+            ok &= qdiv_ok(num, den);
+            td = qdiv(num, den);
+        } else {
+            td = num / den;
+        }
+        const double a = zh[k] * td;
+        zt += a;
+        zq += a * td;
+    }
+    const double F = zt + __shfl_xor_sync(mask, zt, 1), dF = -(zq + __shfl_xor_sync(mask, zq, 1));
+    double t;
+    if (Fast) {
+        ok &= qdiv_ok(F, dF);
+        t = qdiv(F, dF);
+    } else {
+        t = F / dF;
+    }
+    return t;
+}
+
+template <int N>
+__device__ __forceinline__ double rr_step_pair(const double *Kh, const double *zh, double &L, unsigned mask) {
+    bool ok = true;
+    double t = rr_step_pair_impl<N, true>(Kh, zh, L, ok, mask);
+    ok = __shfl_xor_sync(mask, (int)ok, 1) && ok;
+    // pairs with an out-of-range operand redo the step with IEEE division
+    const unsigned redo = __ballot_sync(mask, !ok);
+    if (redo && !ok) {
+        bool ok2 = true;
+        t = rr_step_pair_impl<N, false>(Kh, zh, L, ok2, redo);
+    }
+    L -= t;
+    return t;
+}
+
+// One substitution step (as ss_update_impl), split across the pair.  x, y,
+// Zl, Zg and Kn come out identical in both lanes.  `mask` = the lanes taking
+// the step.
+template <int N, bool Fast>
+__device__ __forceinline__ double ss_update_pair_impl(const FluidTable<N> &f, const double *sa, double P, double T,
+                                                      const double *z, const double *K, double *Kn, double L0,
+                                                      double &L, double Lb, double *x, double *y, double &Zl,
+                                                      double &Zg, bool &ok, int par, unsigned mask) {
+    constexpr int H = (N + 1) / 2;
+    auto DIV = [&](double a, double b) -> double {
+        if (Fast) {
+            ok &= qdiv_ok(a, b);
+            return qdiv(a, b);
+        }
+        return a / b;
+    };
+    L = L0;
+    if (L > 1) L = 1;
+    else if (L < 0) L = 0;
+    const double es = fabs(Lb - L);
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        if (K[i] >= 0) {
+            x[i] = DIV(z[i], L + K[i] * (1 - L));
+            y[i] = K[i] * x[i];
+        } else {
+            x[i] = 0;
+            y[i] = DIV(z[i], 1 - L);
+        }
+    }
+    // this lane's phase
+    double u[N], v[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) u[i] = (par ? y[i] : x[i]) * sa[i];
+    double Ca = 0, Cb = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < N; j++) s += f.bic[i * N + j] * u[j];
+        v[i] = s;
+        Ca += u[i] * s;
+        Cb += (par ? y[i] : x[i]) * f.b[i];
+    }
+    const double pa = P / (kR * kR * T * T), pb = P / (kR * T);
+    const double A = Ca * pa, B = Cb * pb;
+    const bool srk = f.srk != 0;
+    const double Z = phase_z(A, B, srk, par != 0);
+    const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
+    const double DD = DIV(A, B * (d1 - d2));
+    const double FF = log(DIV(Z + d2 * B, Z + d1 * B));
+    const double cz = log(Z - B);
+    const double rCa = DIV(2.0, Ca), rCb = DIV(1.0, Cb);
+    const double DF = DD * FF;
+    double ln[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        const double t1 = f.b[i] * rCb;
+        ln[i] = t1 * (Z - 1) - cz + DF * (sa[i] * v[i] * rCa - t1);
+    }
+    const double Zo = __shfl_xor_sync(mask, Z, 1);
+    Zl = par ? Zo : Z;
+    Zg = par ? Z : Zo;
+    // K update: this lane takes the components 2k + par and needs the other
+    // phase's ln phi of exactly those components
+    double Kh[H];
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const int ie = 2 * k, io = 2 * k + 1 < N ? 2 * k + 1 : 2 * k;
+        const double send = par ? ln[ie] : ln[io];
+        const double recv = __shfl_xor_sync(mask, send, 1);
+        const double lnl = par ? recv : ln[ie];
+        const double lng = par ? ln[io] : recv;
+        const double Kk = par ? K[io] : K[ie], xk = par ? x[io] : x[ie], yk = par ? y[io] : y[ie];
+        const double zk = (par && 2 * k + 1 >= N) ? 0.0 : (par ? z[io] : z[ie]);
+        const double d = lnl - lng;
+        const bool fast = Kk > 0 && xk > 0 && yk > 0 && xk < 1e300 && yk < 1e300 && fabs(lnl) < 700 &&
+                          fabs(lng) < 700 && fabs(d) < 700;
+        const double e = exp(fast ? d : 0.0);
+        double kn = (zk != 0 && fast) ? e : Kk;
+        if (!(fast || zk == 0)) {
+            const double fL = xk * exp(lnl), fG = yk * exp(lng);
+            if (fG != 0) kn = Kk * (fL / fG);
+            else kn = -1;
+            if (fL != fL) kn = -1;
+            if (fG != fG) kn = 1;
+        }
+        Kh[k] = kn;
+    }
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const double other = __shfl_xor_sync(mask, Kh[k], 1);
+        Kn[2 * k] = par ? other : Kh[k];
+        if (2 * k + 1 < N) Kn[2 * k + 1] = par ? Kh[k] : other;
+    }
+    return es;
+}
+
+template <int N>
+__device__ __forceinline__ double ss_update_pair(const FluidTable<N> &f, const double *sa, double P, double T,
+                                                 const double *z, double *K, double &L, double &Lb, double *x,
+                                                 double *y, double &Zl, double &Zg, int par, unsigned mask) {
+    bool ok = true;
+    double Kn[N];
+    const double L0 = L;
+    double es = ss_update_pair_impl<N, true>(f, sa, P, T, z, K, Kn, L0, L, Lb, x, y, Zl, Zg, ok, par, mask);
+    ok = __shfl_xor_sync(mask, (int)ok, 1) && ok;
+    const unsigned redo = __ballot_sync(mask, !ok);
+    if (redo && !ok) {
+        bool ok2 = true;
+        es = ss_update_pair_impl<N, false>(f, sa, P, T, z, K, Kn, L0, L, Lb, x, y, Zl, Zg, ok2, par, redo);
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) K[i] = Kn[i];
+    Lb = L;
+    return es;
+}
+
+// Batched pair form: the queue kernel's passes with two lanes per cell
+// (used for the late passes, on the cells parked by the earlier ones).
+template <int N, bool MULTI>
+__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_pair_kernel(const __grid_constant__ QueueArgs<N> a) {
+    constexpr int H = (N + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    const int par = lane & 1;
+    const FlashIO &io = a.io;
+    const long total = a.first ? io.n : (long)*a.src_count;
+    int mode = kFetch;
+    long c = -1;
+    double P = 0, T = 0, L = 0, Lb = 10;
+    double z[N], K[N], sa[N], Kh[H], zh[H];
+    int j = 0, k = 0, rr = 0;
+    int waited = 0;
+    int inst = 0;
+    double big = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) z[i] = K[i] = sa[i] = 0;
+#pragma unroll
+    for (int q = 0; q < H; q++) Kh[q] = zh[q] = 0;
+    for (;;) {
+        // one slot per pair, claimed through its even lane
+        const unsigned need = __ballot_sync(kPairFull, mode == kFetch && par == 0);
+        if (need) {
+            const int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(a.head, (unsigned long long)__popc(need));
+            base = __shfl_sync(kPairFull, base, leader);
+            // both lanes of a pair count the even lanes below the pair: same slot
+            const long q = (long)base + __popc(need & ((1u << (lane & ~1)) - 1));
+            if (mode == kFetch) {
+                if (q < total) {
+                    if (a.first) {
+                        c = q;
+                        k = 0;
+                        rr = 0;
+                        Lb = 10;
+                    } else {
+                        c = a.src.cell[q];
+                        k = a.src.k[q];
+                        rr = a.src.rr[q];
+                        Lb = a.src.Lb[q];
+#pragma unroll
+                        for (int i = 0; i < N; i++) K[i] = a.src.K[(long)i * a.src.cap + q];
+                    }
+                    P = io.P[c];
+                    T = io.T[c];
+#pragma unroll
+                    for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
+                    if constexpr (MULTI) inst = find_instance(a.inst_start, a.n_inst, c);
+                    if (a.first) flash_init<N>(table_of<N, MULTI>(a, inst), P, T, K, sa);
+                    else sqrt_a<N>(table_of<N, MULTI>(a, inst), T, sa);
+                    pair_halves<N>(K, z, par, Kh, zh);
+                    L = 0.6;
+                    j = 0;
+                    big = rr_bound<N>(K);
+                    mode = kNewton;
+                } else {
+                    mode = kDone;
+                }
+            }
+        }
+        if (__ballot_sync(kPairFull, mode != kDone) == 0) break;
+        const unsigned newton = __ballot_sync(kPairFull, mode == kNewton);
+        if (mode == kNewton) {
+            const double t = rr_step_pair<N>(Kh, zh, L, newton);
+            j++;
+            if (fabs(L) > big) {
+                j = kRRMaxIt;  // provably divergent: the reference runs to its cap
+                mode = kReady;
+            } else if (!((t * t > kRRTol) && (j < kRRMaxIt))) {
+                mode = kReady;
+            }
+        }
+        const unsigned ready = __ballot_sync(kPairFull, mode == kReady);
+        const unsigned still = __ballot_sync(kPairFull, mode == kNewton);
+        if (ready != 0) waited++;
+        if (ready != 0 && (__popc(ready) >= a.ss_batch || still == 0 || waited > a.max_wait)) {
+            waited = 0;
+            if (mode == kReady) {
+                double x[N], y[N], Zl, Zg;
+                const double es = ss_update_pair<N>(table_of<N, MULTI>(a, inst), sa, P, T, z, K, L, Lb, x, y, Zl,
+                                                    Zg, par, ready);
+                rr += j;
+                k++;
+                if ((es > kSSTol) && (k < kSSMaxIt)) {
+                    if (k >= a.park_at) {
+                        if (par == 0) {
+                            const unsigned slot = atomicAdd(a.dst_count, 1u);
+                            a.dst.cell[slot] = c;
+                            a.dst.k[slot] = k;
+                            a.dst.rr[slot] = rr;
+                            a.dst.Lb[slot] = Lb;
+#pragma unroll
+                            for (int i = 0; i < N; i++) a.dst.K[(long)i * a.dst.cap + slot] = K[i];
+                        }
+                        mode = kFetch;
+                    } else {
+                        pair_halves<N>(K, z, par, Kh, zh);
+                        L = 0.6;
+                        j = 0;
+                        big = rr_bound<N>(K);
+                        mode = kNewton;
+                    }
+                } else {
+                    if (par == 0) {
+                        io.label[c] = flash_label(L);
+                        io.L[c] = L;
+#pragma unroll
+                        for (int i = 0; i < N; i++) io.x[(long)i * io.n + c] = x[i];
+                        io.Zl[c] = Zl;
+                        if (io.iters) io.iters[c] = k;
+                        if (io.rr_iters) io.rr_iters[c] = rr;
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < N; i++) io.y[(long)i * io.n + c] = y[i];
+                        io.Zg[c] = Zg;
+                    }
+                    mode = kFetch;
+                }
+            }
+        }
+    }
+}
+
 // Fugacity derivatives for both phases of every cell, following the
 // reference's fugacity rows of the analytic Jacobian
 // (compsim/Petsc_Functions.cpp:30243-30372) with dZ/dP, dZ/dw_k from the

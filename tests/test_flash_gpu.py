@@ -85,6 +85,27 @@ def test_flash_matches_oracle_random(eos, nc, seed, cuda_device):
     _assert_flash_parity(g, o, f"eos{eos}-nc{nc}")
 
 
+@pytest.mark.parametrize("pair_from", [0, 2])
+@pytest.mark.parametrize("eos,nc,seed", [(1, 6, 3), (0, 8, 4), (1, 3, 5), (0, 11, 6), (1, 16, 7), (0, 1, 8),
+                                         (1, 2, 9)])
+def test_pair_form_matches_oracle(pair_from, eos, nc, seed, cuda_device):
+    """The pair form (two lanes per cell) from the first pass (0) or from the
+    third (2, after the thread-per-cell form parked the cells), odd and even
+    component counts."""
+    tc, pc, acf, kij = workloads.flash_table(nc, 100 + seed)
+    fl = oracle.Fluid(tc, pc, acf, kij, eos)
+    P, T, z = workloads.flash_cells(6000, nc, seed=seed)
+    o = oracle.flash_batch(fl, P, T, z)
+    before = osr.get_pair_from()
+    osr.set_pair_from(pair_from)
+    try:
+        g = _run_gpu(fl, P, T, z)
+    finally:
+        osr.set_pair_from(before)
+    _assert_flash_parity(g, o, f"pair{pair_from}-eos{eos}-nc{nc}")
+    assert np.array_equal(g["iters"], o["iters"]) or (g["iters"] != o["iters"]).mean() < 0.005
+
+
 def test_derivatives_match_oracle(golden_srk6, cuda_device):
     gld = golden_srk6
     fl = oracle.Fluid(gld["tc"], gld["pc"], gld["acf"], gld["kij"], int(gld["eos"]))
