@@ -132,6 +132,30 @@ osr_status osr_fugacity_derivs(const osr_fluid *fluid, const double *d_P, const 
                                const double *d_y, const double *d_Zl, const double *d_Zg, long n, double *d_dlnphi_dx,
                                double *d_dlnphi_dP, void *stream);
 
+/* Adjoint of the flash (DEVICE pointers): sensitivities of a flash result
+ * to the binary-interaction coefficients, the feed and the pressure.  The
+ * reference has no adjoint; this differentiates the equilibrium its
+ * SuccFalsh converges to (compsim/Init_Calcs.cpp:571-738) by the implicit
+ * function theorem: for a two-phase cell the equal-fugacity, material-
+ * balance and Rachford-Rice equations in (x, y, L), an (nc+1) x (nc+1)
+ * solve per cell.  `state` holds the flash's outputs for these inputs
+ * (label, L, x, y, Zl, Zg; other fields unused); d_xbar, d_ybar [nc][n] and
+ * d_Lbar [n] are cotangents on x, y, L.  Outputs: d_kij_bar [nc*nc] =
+ * d(sum of cotangent . result)/d k_ij summed over the cells (overwritten;
+ * the sum is deterministic), optional d_z_bar [nc][n] and d_P_bar [n].
+ * One-phase cells: the present phase equals the feed, so its cotangent goes
+ * to z_bar and nothing else; the incipient phase's composition (the
+ * reference's unconverged two-step estimate) carries no sensitivity.  Cells
+ * whose system is singular (a critical point) contribute nothing and are
+ * counted in *singular (may be NULL; when given the call synchronises
+ * `stream`).  Two-phase cells that stopped at the 500-step cap are not at
+ * the equilibrium and get its sensitivity.  Scratch: blocks x nc^2 doubles
+ * from the library pool. */
+osr_status osr_flash_adjoint(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z, long n,
+                             const osr_flash_out *state, const double *d_xbar, const double *d_ybar,
+                             const double *d_Lbar, double *d_kij_bar, double *d_z_bar, double *d_P_bar,
+                             long *singular, void *stream);
+
 /* End-to-end form for callers holding HOST arrays (same layouts; out fields
  * are host pointers): the cells go through in chunks of about 131,072
  * (at most 16 chunks) pipelined over three internal streams -- inputs in,
@@ -161,6 +185,13 @@ osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, in
  * Process-wide; the results agree to rounding either way. */
 osr_status osr_flash_set_pair_from(int pass);
 int osr_flash_get_pair_from(void);
+
+/* First pass in group form: one lane per component (2, 4, 8 or 16 lanes per
+ * cell), for the last passes, whose few thousand cells run hundreds of
+ * steps each with most of the GPU idle.  Takes precedence over the pair
+ * form from that pass on.  12 or more = never.  Process-wide. */
+osr_status osr_flash_set_group_from(int pass);
+int osr_flash_get_group_from(void);
 osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm, int *park_after);
 
 /* Age limit of the substitution-step batching: a warp runs the step for its
@@ -319,6 +350,21 @@ osr_status osr_grid_residual(osr_grid *grid, double *d_f, double *d_scale, doubl
 /* FormFunction (compsim/PetscAUX.cpp:59-104): osr_grid_update_all then
  * osr_grid_residual. */
 osr_status osr_grid_form_function(osr_grid *grid, const double *d_x, double *d_f, double sim_time, void *stream);
+
+/* Residual adjoint with respect to the matrix continuum's per-cell
+ * log-permeability theta_c = ln k_c (k_x, k_y, k_z of matrix cell c scaled
+ * together): d_gk [cells] = sum_r lambda_r dF_r/d theta_c for a DEVICE
+ * vector d_lambda in the residual's row layout, at the grid's current state
+ * (call after osr_grid_form_function or osr_grid_update_all at the same
+ * unknowns).  The reference has no adjoint; this differentiates its
+ * residual (IteratorFunction, compsim/Petsc_Functions.cpp:10-6895) through
+ * the matrix faces' interface transmissibilities (IFK_Calc,
+ * compsim/Init_Calcs.cpp:21-46) and the convective matrix-fracture shape
+ * factor (compsim/Init_Calcs.cpp:970-983).  Well productivity indices are
+ * held fixed (their permeability dependence is not differentiated).
+ * Deterministic; asynchronous on `stream`. */
+osr_status osr_grid_residual_logk_vjp(osr_grid *grid, const double *d_lambda, double *d_gk, double sim_time,
+                                      void *stream);
 
 /* ---------------------------------------------------------------------------
  * Jacobian path: the PETSc FormJacobian callback on the device.

@@ -138,6 +138,37 @@ def flash_derivs(fl: Fluid, P, T, x, y, Zl, Zg):
     return dx, dp
 
 
+def flash_polish(fl: Fluid, P, T, z, out: dict) -> int:
+    """Two-phase cells of a flash result (dict of label, L, x, y, Zl, Zg;
+    modified in place) solved to rounding by Newton's method on the
+    equilibrium equations; returns the cells that did not settle."""
+    lib = oracle_lib()
+    n = P.shape[0]
+    for k in ("L", "x", "y", "Zl", "Zg"):
+        out[k] = np.ascontiguousarray(out[k], np.float64)
+    lab = np.ascontiguousarray(out["label"], np.int8)
+    return int(lib.orc_flash_polish(fl.cstruct, ctypes.c_long(n), _p(np.ascontiguousarray(P, np.float64)),
+                                    _p(np.ascontiguousarray(T, np.float64)), _p(np.ascontiguousarray(z, np.float64)),
+                                    _p(lab), _p(out["L"]), _p(out["x"]), _p(out["y"]), _p(out["Zl"]), _p(out["Zg"])))
+
+
+def flash_adjoint(fl: Fluid, P, T, z, st: dict, xbar, ybar, Lbar):
+    """Implicit-function adjoint of a flash result: (kij_bar [nc, nc],
+    z_bar [nc, n], P_bar [n], singular cells)."""
+    lib = oracle_lib()
+    n, nc = P.shape[0], fl.nc
+    kb = np.zeros(nc * nc)
+    zb = np.zeros((nc, n))
+    pb = np.zeros(n)
+    args = [np.ascontiguousarray(v, np.float64) for v in (P, T, z)]
+    lab = np.ascontiguousarray(st["label"], np.int8)
+    fs = [np.ascontiguousarray(st[k], np.float64) for k in ("L", "x", "y", "Zl", "Zg")]
+    bars = [np.ascontiguousarray(v, np.float64) for v in (xbar, ybar, Lbar)]
+    bad = lib.orc_flash_adjoint(fl.cstruct, ctypes.c_long(n), *[_p(v) for v in args], _p(lab), *[_p(v) for v in fs],
+                                *[_p(v) for v in bars], _p(kb), _p(zb), _p(pb))
+    return kb.reshape(nc, nc), zb, pb, int(bad)
+
+
 def fugacity(fl: Fluid, P: float, T: float, w, Z: float):
     """ln(phi), d ln(phi)/dw [nc, nc], d ln(phi)/dP for one phase."""
     lib = oracle_lib()

@@ -323,3 +323,235 @@ int orc_flash_derivs_batch(const orc_fluid *f, long n, const double *P, const do
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Converged flash sensitivities (test infrastructure for the device
+ * adjoint).  A two-phase cell's flash result u = (x, y, L) solves
+ *   G_i = ln x_i + ln phi_i^L(x) - ln y_i - ln phi_i^V(y) = 0   (equal fugacity)
+ *   H_i = z_i - L x_i - (1 - L) y_i = 0                        (material balance)
+ *   S   = sum_i (x_i - y_i) = 0                                (Rachford-Rice)
+ * to the reference's stopping tolerances (compsim/Init_Calcs.cpp:571-738).
+ * orc_flash_polish solves these equations to rounding by Newton's method
+ * from the flash's result, so that finite differences of its output are the
+ * derivatives of the exact solution; orc_flash_adjoint restates the
+ * implicit-function adjoint of the same equations. */
+
+/* Gaussian elimination with partial pivoting on a row-major n x n system;
+ * returns -1 when a pivot is exactly zero. */
+static int solve_dense(int n, double *A, double *b) {
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        for (int i = k + 1; i < n; i++)
+            if (fabs(A[i * n + k]) > fabs(A[p * n + k])) p = i;
+        if (A[p * n + k] == 0) return -1;
+        if (p != k) {
+            for (int j = 0; j < n; j++) { double t = A[k * n + j]; A[k * n + j] = A[p * n + j]; A[p * n + j] = t; }
+            double t = b[k]; b[k] = b[p]; b[p] = t;
+        }
+        for (int i = k + 1; i < n; i++) {
+            double l = A[i * n + k] / A[k * n + k];
+            if (l == 0) continue;
+            for (int j = k; j < n; j++) A[i * n + j] -= l * A[k * n + j];
+            b[i] -= l * b[k];
+        }
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double s = b[i];
+        for (int j = i + 1; j < n; j++) s -= A[i * n + j] * b[j];
+        b[i] = s / A[i * n + i];
+    }
+    return 0;
+}
+
+/* Compressibility of one phase composition (the flash's root choice). */
+static double phase_root(const orc_fluid *f, const double *b, const double *aij, double P, double T, const double *w,
+                         int gas) {
+    int nc = f->nc;
+    double Ca = 0, Cb = 0;
+    for (int i = 0; i < nc; i++) {
+        Cb += w[i] * b[i];
+        for (int j = 0; j < nc; j++) Ca += w[i] * w[j] * aij[i * nc + j];
+    }
+    double A = Ca * P / (R_GAS * R_GAS * T * T), B = Cb * P / (R_GAS * T);
+    double U, W, d1, d2;
+    eos_uw(f->eos, B, &U, &W, &d1, &d2);
+    return orc_solve_z(-(1 + B - U), A - B * U - U - W * W, -(A * B - B * W * W - W * W), gas);
+}
+
+int orc_flash_polish(const orc_fluid *f, long n, const double *P, const double *T, const double *z,
+                     const signed char *label, double *L, double *x, double *y, double *Zl, double *Zg) {
+    int nc = f->nc, m = 2 * nc + 1, failed = 0;
+    double a[ORC_MAX_NC], b[ORC_MAX_NC], aij[ORC_MAX_NC * ORC_MAX_NC];
+    double lastT = -1;
+    for (long c = 0; c < n; c++) {
+        if (label[c] != 0) continue;
+        if (T[c] != lastT) {
+            orc_eos_params(f, T[c], a, b);
+            mix_table(f, a, aij);
+            lastT = T[c];
+        }
+        double u[2 * ORC_MAX_NC + 1];
+        for (int i = 0; i < nc; i++) {
+            u[i] = x[(long)i * n + c];
+            u[nc + i] = y[(long)i * n + c];
+        }
+        u[2 * nc] = L[c];
+        int ok = 0, extra = -1;   /* once the step is small, two more steps settle the last bits */
+        for (int it = 0; it < 30 && !ok; it++) {
+            double J[(2 * ORC_MAX_NC + 1) * (2 * ORC_MAX_NC + 1)] = {0}, r[2 * ORC_MAX_NC + 1];
+            double lnl[ORC_MAX_NC], lng[ORC_MAX_NC], dxl[ORC_MAX_NC * ORC_MAX_NC], dxg[ORC_MAX_NC * ORC_MAX_NC];
+            double zl = phase_root(f, b, aij, P[c], T[c], u, 0), zg = phase_root(f, b, aij, P[c], T[c], u + nc, 1);
+            fugacity_core(f, b, aij, P[c], T[c], u, zl, lnl, dxl, NULL);
+            fugacity_core(f, b, aij, P[c], T[c], u + nc, zg, lng, dxg, NULL);
+            double Lc = u[2 * nc];
+            for (int i = 0; i < nc; i++) {
+                r[i] = -(log(u[i]) + lnl[i] - log(u[nc + i]) - lng[i]);
+                r[nc + i] = -(z[(long)i * n + c] - Lc * u[i] - (1 - Lc) * u[nc + i]);
+                for (int k = 0; k < nc; k++) {
+                    J[i * m + k] = (i == k ? 1 / u[i] : 0) + dxl[i * nc + k];
+                    J[i * m + nc + k] = -(i == k ? 1 / u[nc + i] : 0) - dxg[i * nc + k];
+                }
+                J[(nc + i) * m + i] = -Lc;
+                J[(nc + i) * m + nc + i] = -(1 - Lc);
+                J[(nc + i) * m + 2 * nc] = u[nc + i] - u[i];
+                J[2 * nc * m + i] = 1;
+                J[2 * nc * m + nc + i] = -1;
+            }
+            double s = 0;
+            for (int i = 0; i < nc; i++) s += u[i] - u[nc + i];
+            r[2 * nc] = -s;
+            if (solve_dense(m, J, r)) break;
+            double step = 0, size = 0;
+            for (int q = 0; q < m; q++) {
+                u[q] += r[q];
+                step = fmax(step, fabs(r[q]));
+                size = fmax(size, fabs(u[q]));
+            }
+            if (extra < 0 && step <= 1e-11 * fmax(size, 1e-300)) extra = 2;
+            else if (extra > 0 && --extra == 0) ok = 1;
+        }
+        if (!ok) { failed++; continue; }
+        for (int i = 0; i < nc; i++) {
+            x[(long)i * n + c] = u[i];
+            y[(long)i * n + c] = u[nc + i];
+        }
+        L[c] = u[2 * nc];
+        Zl[c] = phase_root(f, b, aij, P[c], T[c], u, 0);
+        Zg[c] = phase_root(f, b, aij, P[c], T[c], u + nc, 1);
+    }
+    return failed;
+}
+
+/* sum_i wt_i d ln(phi_i)/d k_mn for one phase, added into kbar[m nc + n]:
+ * k_mn enters through sqrt(a_m a_n)(1 - k_mn) in the mixing sum and in the
+ * i = m row of sum_j w_j a_ij, and Z follows A implicitly through the cubic. */
+static void lnphi_kij_vjp(const orc_fluid *f, const double *a, const double *b, const double *aij, double P,
+                          double T, const double *w, double Z, const double *wt, double *kbar) {
+    int nc = f->nc;
+    double Ca = 0, Cb = 0, t[ORC_MAX_NC];
+    for (int i = 0; i < nc; i++) {
+        Cb += w[i] * b[i];
+        t[i] = 0;
+        for (int j = 0; j < nc; j++) t[i] += w[j] * aij[i * nc + j];
+        Ca += w[i] * t[i];
+    }
+    double pa = P / (R_GAS * R_GAS * T * T), A = Ca * pa, B = Cb * P / (R_GAS * T);
+    double U, W, d1, d2;
+    eos_uw(f->eos, B, &U, &W, &d1, &d2);
+    double fp = 3 * Z * Z - 2 * Z * (1 + B - U) + A - B * U - U - W * W;
+    double dZdA = -(Z - B) / fp;
+    double DD = A / (B * (d1 - d2)), FF = log((Z + d2 * B) / (Z + d1 * B));
+    double dFF = 1 / (Z + d2 * B) - 1 / (Z + d1 * B);
+    double gZ = 0, gDD = 0, gCa = 0, gs[ORC_MAX_NC];
+    for (int i = 0; i < nc; i++) {
+        double t1 = b[i] / Cb, EE = 2 * t[i] / Ca - t1;
+        gZ += wt[i] * (t1 - 1 / (Z - B) + DD * EE * dFF);
+        gDD += wt[i] * FF * EE;
+        gCa += wt[i] * DD * FF * (-2 * t[i] / (Ca * Ca));
+        gs[i] = wt[i] * DD * FF * 2 / Ca;
+    }
+    gCa += gZ * dZdA * pa + gDD * DD / Ca;
+    for (int p = 0; p < nc; p++)
+        for (int q = 0; q < nc; q++) {
+            double sq = sqrt(a[p] * a[q]);
+            kbar[p * nc + q] -= gCa * w[p] * w[q] * sq + gs[p] * w[q] * sq;
+        }
+}
+
+int orc_flash_adjoint(const orc_fluid *f, long n, const double *P, const double *T, const double *z,
+                      const signed char *label, const double *L, const double *x, const double *y, const double *Zl,
+                      const double *Zg, const double *xbar, const double *ybar, const double *Lbar, double *kij_bar,
+                      double *z_bar, double *P_bar) {
+    int nc = f->nc, m = nc + 1, singular = 0;
+    double a[ORC_MAX_NC], b[ORC_MAX_NC], aij[ORC_MAX_NC * ORC_MAX_NC];
+    double lastT = -1;
+    for (int e = 0; e < nc * nc; e++) kij_bar[e] = 0;
+    for (long c = 0; c < n; c++) {
+        if (z_bar)
+            for (int i = 0; i < nc; i++) z_bar[(long)i * n + c] = 0;
+        if (P_bar) P_bar[c] = 0;
+        if (label[c] != 0) {
+            /* one phase: the present phase is the feed, nothing depends on k */
+            if (z_bar)
+                for (int i = 0; i < nc; i++)
+                    z_bar[(long)i * n + c] = label[c] > 0 ? xbar[(long)i * n + c] : ybar[(long)i * n + c];
+            continue;
+        }
+        if (T[c] != lastT) {
+            orc_eos_params(f, T[c], a, b);
+            mix_table(f, a, aij);
+            lastT = T[c];
+        }
+        double xs[ORC_MAX_NC], ys[ORC_MAX_NC], dxl[ORC_MAX_NC * ORC_MAX_NC], dxg[ORC_MAX_NC * ORC_MAX_NC];
+        double dpl[ORC_MAX_NC], dpg[ORC_MAX_NC], d[ORC_MAX_NC], xb[ORC_MAX_NC], yb[ORC_MAX_NC];
+        int live[ORC_MAX_NC];
+        for (int i = 0; i < nc; i++) {
+            xs[i] = x[(long)i * n + c];
+            ys[i] = y[(long)i * n + c];
+            xb[i] = xbar[(long)i * n + c];
+            yb[i] = ybar[(long)i * n + c];
+            d[i] = ys[i] - xs[i];
+            live[i] = xs[i] > 0 && ys[i] > 0;
+        }
+        double Lc = L[c];
+        fugacity_core(f, b, aij, P[c], T[c], xs, Zl[c], NULL, dxl, dpl);
+        fugacity_core(f, b, aij, P[c], T[c], ys, Zg[c], NULL, dxg, dpg);
+        double M[(ORC_MAX_NC + 1) * (ORC_MAX_NC + 1)], r[ORC_MAX_NC + 1];
+        double rN = Lbar[c];
+        for (int k = 0; k < nc; k++) {
+            double ck = 0;
+            for (int i = 0; i < nc; i++) {
+                double Ax = (i == k && live[i] ? 1 / xs[i] : 0) + dxl[k * nc + i];
+                double Ay = (i == k && live[i] ? 1 / ys[i] : 0) + dxg[k * nc + i];
+                M[i * m + k] = live[i] && live[k] ? (1 - Lc) * Ax + Lc * Ay : (i == k ? 1.0 : 0.0);
+                ck += live[i] ? d[i] * (Ax - Ay) : 0;
+            }
+            M[k * m + nc] = live[k] ? 1.0 : 0.0;
+            M[nc * m + k] = live[k] ? ck : 0.0;
+            r[k] = live[k] ? (1 - Lc) * xb[k] - Lc * yb[k] : 0.0;
+            rN += live[k] ? d[k] * (xb[k] + yb[k]) : 0;
+        }
+        M[nc * m + nc] = 0;
+        r[nc] = rN;
+        if (solve_dense(m, M, r)) { singular++; continue; }
+        double wl[ORC_MAX_NC], wg[ORC_MAX_NC];
+        double pb = 0;
+        for (int i = 0; i < nc; i++) {
+            double lg = live[i] ? r[i] : 0;
+            wl[i] = -lg;
+            wg[i] = lg;
+            pb -= lg * (dpl[i] - dpg[i]);
+            if (z_bar && live[i]) {
+                /* lambda_H = (Dx + Phi_x^T - Dy - Phi_y^T) lambda_G - xbar - ybar */
+                double lh = -xb[i] - yb[i] + r[i] / xs[i] - r[i] / ys[i];
+                for (int k = 0; k < nc; k++)
+                    if (live[k]) lh += (dxl[k * nc + i] - dxg[k * nc + i]) * r[k];
+                z_bar[(long)i * n + c] = -lh;
+            }
+        }
+        if (P_bar) P_bar[c] = pb;
+        lnphi_kij_vjp(f, a, b, aij, P[c], T[c], xs, Zl[c], wl, kij_bar);
+        lnphi_kij_vjp(f, a, b, aij, P[c], T[c], ys, Zg[c], wg, kij_bar);
+    }
+    return singular;
+}

@@ -46,6 +46,23 @@ int orc_flash_derivs_batch(const orc_fluid *f, long n, const double *P, const do
                            const double *y, const double *Zl, const double *Zg, double *dlnphi_dx,
                            double *dlnphi_dP);
 
+/* Two-phase cells (label 0) of a flash result polished in place: Newton's
+ * method on the equal-fugacity, material-balance and Rachford-Rice
+ * equations to rounding, Zl and Zg recomputed.  Returns the number of cells
+ * whose iteration did not settle (left unchanged). */
+int orc_flash_polish(const orc_fluid *f, long n, const double *P, const double *T, const double *z,
+                     const signed char *label, double *L, double *x, double *y, double *Zl, double *Zg);
+
+/* Implicit-function adjoint of the flash: given cotangents xbar, ybar
+ * [nc][n] and Lbar [n] on a flash result, kij_bar [nc*nc] (summed over the
+ * cells) and optionally z_bar [nc][n] and P_bar [n].  One-phase cells pass
+ * the present phase's cotangent to z and contribute nothing else.  Returns
+ * the number of two-phase cells whose system was singular (skipped). */
+int orc_flash_adjoint(const orc_fluid *f, long n, const double *P, const double *T, const double *z,
+                      const signed char *label, const double *L, const double *x, const double *y, const double *Zl,
+                      const double *Zg, const double *xbar, const double *ybar, const double *Lbar, double *kij_bar,
+                      double *z_bar, double *P_bar);
+
 #ifdef __cplusplus
 }
 #endif

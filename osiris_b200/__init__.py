@@ -21,7 +21,7 @@ import numpy as np
 
 from .build import INCLUDE, LIB
 
-__all__ = ["Fluid", "lib", "flash", "flash_host", "fugacity_derivs", "flash_instances", "set_shape", "get_shape", "header_symbols", "OsrError",
+__all__ = ["Fluid", "lib", "flash", "flash_host", "fugacity_derivs", "flash_adjoint", "flash_instances", "set_shape", "get_shape", "header_symbols", "OsrError",
            "FLASH_OUTPUTS"]
 
 _vp = ctypes.c_void_p
@@ -227,6 +227,35 @@ def fugacity_derivs(fluid: Fluid, P, T, x, y, Zl, Zg, out: dict | None = None, s
     return out
 
 
+def flash_adjoint(fluid: Fluid, P, T, z, state: dict, xbar, ybar, Lbar, want_z: bool = True, want_P: bool = True,
+                  stream=None) -> dict:
+    """Implicit-function adjoint of a flash result (osr_flash_adjoint):
+    device tensors P, T [n], z [nc, n], the flash's outputs ``state`` and
+    cotangents xbar, ybar [nc, n], Lbar [n].  Returns {"kij_bar": [nc, nc],
+    "z_bar": [nc, n] | None, "P_bar": [n] | None, "singular": count}."""
+    import torch
+    n, nc = int(P.shape[0]), fluid.nc
+    for t in (P, T, z, xbar, ybar, Lbar):
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise OsrError("inputs and cotangents must be contiguous float64 CUDA tensors")
+    dev = P.device
+    kb = torch.empty((nc, nc), dtype=torch.float64, device=dev)
+    zb = torch.empty((nc, n), dtype=torch.float64, device=dev) if want_z else None
+    pb = torch.empty(n, dtype=torch.float64, device=dev) if want_P else None
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    co = _out_struct(state, lambda t: t.data_ptr())
+    sing = ctypes.c_long()
+    with torch.cuda.device(dev):
+        _check(lib().osr_flash_adjoint(fluid.cref, _vp(P.data_ptr()), _vp(T.data_ptr()), _vp(z.data_ptr()),
+                                       ctypes.c_long(n), ctypes.byref(co), _vp(xbar.data_ptr()),
+                                       _vp(ybar.data_ptr()), _vp(Lbar.data_ptr()), _vp(kb.data_ptr()),
+                                       None if zb is None else _vp(zb.data_ptr()),
+                                       None if pb is None else _vp(pb.data_ptr()), ctypes.byref(sing),
+                                       _vp(stream.cuda_stream)), "osr_flash_adjoint")
+    return {"kij_bar": kb, "z_bar": zb, "P_bar": pb, "singular": int(sing.value)}
+
+
 def flash_host(fluid: Fluid, P, T, z, derivs: bool = True, out: dict | None = None, iters: bool = True):
     """End-to-end flash of host (numpy) arrays through osr_flash_batch_host.
     Inputs may be pinned torch CPU tensors or numpy arrays."""
@@ -302,6 +331,16 @@ def set_pair_from(pass_index: int):
 
 def get_pair_from() -> int:
     return int(lib().osr_flash_get_pair_from())
+
+
+def set_group_from(pass_index: int):
+    """First pass of the batched flash in group form (osr_flash_set_group_from);
+    12 = never."""
+    _check(lib().osr_flash_set_group_from(int(pass_index)), "osr_flash_set_group_from")
+
+
+def get_group_from() -> int:
+    return int(lib().osr_flash_get_group_from())
 
 
 def get_shape():
@@ -516,6 +555,13 @@ class Grid:
                                        None if d_scale is None else _vp(d_scale.data_ptr()),
                                        ctypes.c_double(sim_time), None if stream is None else _vp(stream)),
                "osr_grid_residual")
+
+    def residual_logk_vjp(self, d_lambda, d_gk, sim_time: float = 0.0, stream=None):
+        """sum_r lambda_r dF_r/d ln k_c for every matrix cell c at the current
+        state (osr_grid_residual_logk_vjp); d_lambda [rows], d_gk [cells]."""
+        _check(lib().osr_grid_residual_logk_vjp(self._h, _vp(d_lambda.data_ptr()), _vp(d_gk.data_ptr()),
+                                                ctypes.c_double(sim_time), None if stream is None else _vp(stream)),
+               "osr_grid_residual_logk_vjp")
 
     def form_function(self, d_x, d_f, sim_time: float = 0.0, stream=None):
         _check(lib().osr_grid_form_function(self._h, _vp(d_x.data_ptr()), _vp(d_f.data_ptr()),

@@ -324,6 +324,14 @@ static osr_status residual_n(osr_grid &g, double *f, double *fscale, double t, c
     return OSR_OK;
 }
 
+template <int N>
+static osr_status logk_vjp_n(osr_grid &g, const double *lam, double *gk, double t, cudaStream_t st) {
+    AsmArgs<N> A = asm_args<N>(g, nullptr, nullptr, t);
+    residual_logk_vjp_kernel<N><<<(unsigned)grid_blocks(g.cells), 128, 0, st>>>(A, lam, gk);
+    ASM_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
 #define ASM_SWITCH(call)                                                                                  \
     switch (g->nc) {                                                                                      \
         case 1: { constexpr int K = 1; return call; }                                                     \
@@ -433,6 +441,12 @@ osr_status osr_grid_update_all(osr_grid *g, const double *d_x, void *stream) {
 osr_status osr_grid_residual(osr_grid *g, double *d_f, double *d_scale, double sim_time, void *stream) {
     if (!g || !d_f) return OSR_ERR_ARG;
     ASM_SWITCH(residual_n<K>(*g, d_f, d_scale, sim_time, (cudaStream_t)stream))
+}
+
+osr_status osr_grid_residual_logk_vjp(osr_grid *g, const double *d_lambda, double *d_gk, double sim_time,
+                                      void *stream) {
+    if (!g || !d_lambda || !d_gk) return OSR_ERR_ARG;
+    ASM_SWITCH(logk_vjp_n<K>(*g, d_lambda, d_gk, sim_time, (cudaStream_t)stream))
 }
 
 osr_status osr_grid_form_function(osr_grid *g, const double *d_x, double *d_f, double sim_time, void *stream) {

@@ -888,4 +888,109 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Vector-Jacobian product of the residual with the matrix continuum's
+// per-cell log-permeability theta_c = ln k_c (k_x, k_y, k_z of matrix cell c
+// scaled together): gk[c] = sum_rows lambda_r dF_r/d theta_c at the current
+// state.  The reference has no adjoint; this differentiates its residual
+// (IteratorFunction, compsim/Petsc_Functions.cpp:10-6895) through the two
+// places the matrix permeability enters it:
+//  * the interface transmissibility of each matrix face, harmonic in the two
+//    cells' permeabilities (IFK_Calc, compsim/Init_Calcs.cpp:21-46), which
+//    multiplies every advective face term (Calc_Transes,
+//    compsim/Do_Cycle.cpp:800-1416): d ln T_f/d theta_a =
+//    (h_a/k_a)/(h_a/k_a + h_b/k_b);
+//  * the convective matrix-fracture shape factor 4 sigma sum_d k_d/L_d^2
+//    (compsim/Init_Calcs.cpp:970-983), linear in the cell's permeability.
+// The face terms are those residual_kernel forms for the matrix rows; a face
+// enters its two cells' rows with opposite signs, so a thread evaluates each
+// of its faces once and weights both cells' multipliers (no atomics; the
+// result is deterministic).  Well productivity indices (Peaceman, through
+// sqrt(k_x k_y)) are held fixed: this product is for the grid's flux and
+// transfer terms.
+template <int N>
+__global__ void __launch_bounds__(128) residual_logk_vjp_kernel(const __grid_constant__ AsmArgs<N> A,
+                                                                const double *lam, double *gk) {
+    const GridScalars &s = A.a.s;
+    const GridGeom &geo = A.a.geo;
+    const long n = s.cells;
+    const double wfac = s.wat_ro * kWatMRo;
+    const MediumFields &M = A.a.m[0], &Fr = A.a.m[1];
+    // lambda of block b's i-th component row, total row (i = N-1), water row (i = N)
+    auto lam_row = [&](long b, int i) -> double {
+        const signed char lb = b >= n ? Fr.label[b - n] : M.label[b];
+        return lam[A.rowoff[b] + (lb == 0 ? N : 0) + i];
+    };
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+        const int ix = (int)(c % s.nx), iy = (int)((c / s.nx) % s.ny), iz = (int)(c / ((long)s.nx * s.ny));
+        const bool act_c = M.por[c] >= kPorTiny;
+        double g = 0;
+        Face fc[6];
+        const int nf = cell_faces<N>(A, c, ix, iy, iz, fc);
+        for (int q = 0; q < nf; q++) {
+            const Face &e = fc[q];
+            const bool act_nb = M.por[e.nb] >= kPorTiny;
+            if (!act_c && !act_nb) continue;
+            const long plane = (long)e.d * n + e.tc;
+            const double dH = e.sgn > 0 ? geo.blockH[e.nb] - geo.blockH[c] : geo.blockH[c] - geo.blockH[e.nb];
+            double KPG[2];
+            long up[2];
+            for (int p = 0; p < 2; p++) {
+                const double Tp = M.trans[(long)(p * 3) * n + plane];
+                const double Tg = M.trans[(long)((2 + p) * 3) * n + plane];
+                const double Pc_ = M.P[(1 + p) * n + c], Pn_ = M.P[(1 + p) * n + e.nb];
+                const int tS = M.transS[(long)(p * 3) * n + plane];
+                if (e.sgn > 0) {
+                    KPG[p] = Tp * (Pn_ - Pc_) + Tg * dH;
+                    up[p] = tS ? e.nb : c;
+                } else {
+                    KPG[p] = -(Tp * (Pc_ - Pn_)) - Tg * dH;
+                    up[p] = tS ? c : e.nb;
+                }
+            }
+            const double Tw = M.wtran[plane];
+            const double dPw = e.sgn > 0 ? M.P[e.nb] - M.P[c] : M.P[c] - M.P[e.nb];
+            const double KW = e.sgn * (Tw * dPw + kGAcc * s.wat_ro * Tw * dH);
+            // this face's terms in c's rows; the neighbour's rows hold the negatives
+            double S = 0;
+            for (int i = 0; i < N - 1; i++) {
+                const double term = M.x[(long)i * n + up[0]] * KPG[0] + M.y[(long)i * n + up[1]] * KPG[1];
+                S += ((act_c ? lam_row(c, i) : 0.0) - (act_nb ? lam_row(e.nb, i) : 0.0)) * term;
+            }
+            S += ((act_c ? lam_row(c, N - 1) : 0.0) - (act_nb ? lam_row(e.nb, N - 1) : 0.0)) * (KPG[0] + KPG[1]);
+            S += ((act_c ? lam_row(c, N) : 0.0) - (act_nb ? lam_row(e.nb, N) : 0.0)) * KW;
+            const double hc = e.dl / M.perm[(long)e.d * n + c], hn = e.dn / M.perm[(long)e.d * n + e.nb];
+            g += hc / (hc + hn) * S;
+        }
+        // matrix-fracture convective transfer: +conv in the matrix rows, -conv in the fracture rows
+        const bool act_f = Fr.por[c] >= kPorTiny;
+        if (act_c || act_f) {
+            const double di = geo.di[ix], dj = geo.dj[iy], dk = geo.dk[iz];
+            const double Vb = di * dj * dk;
+            const double Mpor = porpor_at(M, s, c), Fpor = porpor_at(Fr, s, c);
+            const double SF2 = 4 * A.k.sigma *
+                               (M.perm[c] / (di * di) + M.perm[n + c] / (dj * dj) + M.perm[2 * n + c] / (dk * dk));
+            const double kr_o = M.P[n + c] >= Fr.P[n + c] ? M.kr[n + c] : Fr.kr[n + c];
+            const double kr_g = M.P[2 * n + c] >= Fr.P[2 * n + c] ? M.kr[2 * n + c] : Fr.kr[2 * n + c];
+            const double kr_w = M.P[c] >= Fr.P[c] ? M.kr[c] : Fr.kr[c];
+            const double mubar_o = (M.mu[c] * Mpor + Fr.mu[c] * Fpor) / (Mpor + Fpor);
+            const double mubar_g = (M.mu[n + c] * Mpor + Fr.mu[n + c] * Fpor) / (Mpor + Fpor);
+            const double conv_o = kSIC * M.rho[c] * SF2 * Vb * kr_o / mubar_o * (Fr.P[n + c] - M.P[n + c]);
+            const double conv_g = kSIC * M.rho[n + c] * SF2 * Vb * kr_g / mubar_g *
+                                  ((Fr.P[2 * n + c] - M.P[2 * n + c]) + (Fr.pc[n + c] - M.pc[n + c]));
+            const double conv_w =
+                kSIC * wfac * SF2 * kr_w / s.wat_mu * Vb * ((Fr.P[c] - M.P[c]) + (M.pc[c] - Fr.pc[c]));
+            double S = 0;
+            for (int i = 0; i < N - 1; i++) {
+                const double term = M.x[(long)i * n + c] * conv_o + M.y[(long)i * n + c] * conv_g;
+                S += ((act_c ? lam_row(c, i) : 0.0) - (act_f ? lam_row(n + c, i) : 0.0)) * term;
+            }
+            S += ((act_c ? lam_row(c, N - 1) : 0.0) - (act_f ? lam_row(n + c, N - 1) : 0.0)) * (conv_o + conv_g);
+            S += ((act_c ? lam_row(c, N) : 0.0) - (act_f ? lam_row(n + c, N) : 0.0)) * conv_w;
+            g += S;
+        }
+        gk[c] = -g;   // the residual is F = LSide - RSide with the flux terms in RSide
+    }
+}
+
 }  // namespace osr

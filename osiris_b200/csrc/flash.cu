@@ -11,6 +11,7 @@
 #include <vector>
 #include "osiris_b200.h"
 #include "flash_kernels.cuh"
+#include "adjoint_kernels.cuh"
 
 namespace osr {
 
@@ -22,6 +23,7 @@ static std::atomic<int> g_ctas_per_sm{3};
 static std::atomic<int> g_park_after{2};
 static std::atomic<int> g_max_wait{1000};
 static std::atomic<int> g_pair_from{kMaxPasses};   // first pass run by the pair form
+static std::atomic<int> g_group_from{kMaxPasses};  // first pass run by the group form
 
 static osr_status cuda_fail(cudaError_t e) {
     g_last_cuda.store((int)e);
@@ -215,13 +217,17 @@ static int pass_limits(int park_after, int *lim) {
     return np;
 }
 
+// lanes per cell: 1 thread-per-cell form, 2 pair form, group_lanes<N>() group form
 template <int N, bool MULTI>
-static int queue_blocks(long n, bool pair = false) {
-    long warps_needed = ((pair ? 2 : 1) * n + 31) / 32;
+static int queue_blocks(long n, int lanes = 1) {
+    long warps_needed = (lanes * n + 31) / 32;
     int per_sm = g_ctas_per_sm.load(), fit = 0;
     const cudaError_t e =
-        pair ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_pair_kernel<N, MULTI>, 128, 0)
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N, MULTI>, 128, 0);
+        lanes == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_pair_kernel<N, MULTI>, 128, 0)
+        : lanes > 2
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_group_kernel<N, group_lanes<N>(), MULTI>, 128,
+                                                            0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, flash_queue_kernel<N, MULTI>, 128, 0);
     if (e == cudaSuccess && fit > 0 && per_sm > fit) per_sm = fit;
     long blocks = (long)sm_count() * per_sm;
     long max_blocks = (warps_needed + 3) / 4;
@@ -297,8 +303,10 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
         q.inst_start = inst.start;
         q.n_inst = inst.n;
         const int blocks = multi ? queue_blocks<N, true>(n) : queue_blocks<N, false>(n);
-        const int pblocks = multi ? queue_blocks<N, true>(n, true) : queue_blocks<N, false>(n, true);
-        const int pair_from = g_pair_from.load();
+        const int pblocks = multi ? queue_blocks<N, true>(n, 2) : queue_blocks<N, false>(n, 2);
+        constexpr int G = group_lanes<N>();
+        const int gblocks = multi ? queue_blocks<N, true>(n, G) : queue_blocks<N, false>(n, G);
+        const int pair_from = g_pair_from.load(), group_from = g_group_from.load();
         for (int p = 0; p < np; p++) {
             q.first = p == 0;
             q.src = park_view(scratch, n, N, (p + 1) & 1);
@@ -308,7 +316,11 @@ static osr_status run_flash_n(const osr_fluid &fl, const double *P, const double
             q.head = heads + p;
             q.park_at = lim[p];
             q.ss_batch = p == 0 ? g_ss_batch.load() : g_tail_batch.load();
-            if (p >= pair_from) {
+            if (p >= group_from) {
+                // last passes: G lanes per cell, one per component
+                if (multi) flash_group_kernel<N, G, true><<<gblocks, 128, 0, s>>>(q);
+                else flash_group_kernel<N, G, false><<<gblocks, 128, 0, s>>>(q);
+            } else if (p >= pair_from) {
                 // late passes: two lanes per cell (the cells left are few and long-running)
                 if (multi) flash_pair_kernel<N, true><<<pblocks, 128, 0, s>>>(q);
                 else flash_pair_kernel<N, false><<<pblocks, 128, 0, s>>>(q);
@@ -509,6 +521,67 @@ osr_status osr_fugacity_derivs(const osr_fluid *fluid, const double *d_P, const 
     }
 }
 
+osr_status osr_flash_adjoint(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z, long n,
+                             const osr_flash_out *state, const double *d_xbar, const double *d_ybar,
+                             const double *d_Lbar, double *d_kij_bar, double *d_z_bar, double *d_P_bar,
+                             long *singular, void *stream) {
+    osr_status st = check_fluid(fluid);
+    if (st) return st;
+    if (n < 0 || !state || !d_kij_bar) return OSR_ERR_ARG;
+    const int nc = fluid->nc;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (singular) *singular = 0;
+    if (n == 0) {
+        OSR_CUDA(cudaMemsetAsync(d_kij_bar, 0, sizeof(double) * nc * nc, s));
+        return OSR_OK;
+    }
+    if (!d_P || !d_T || !d_z || !state->label || !state->L || !state->x || !state->y || !state->Zl ||
+        !state->Zg || !d_xbar || !d_ybar || !d_Lbar)
+        return OSR_ERR_ARG;
+    long blocks = (n + kAdjThreads - 1) / kAdjThreads;
+    const long cap = (long)sm_count() * 8;
+    if (blocks > cap) blocks = cap;
+    const size_t part_bytes = (size_t)blocks * nc * nc * sizeof(double);
+    char *scratch = nullptr;
+    OSR_CUDA(pool_alloc((void **)&scratch, part_bytes + 256, s));
+    unsigned *d_sing = (unsigned *)(scratch + part_bytes);
+    cudaError_t e = cudaMemsetAsync(d_sing, 0, sizeof(unsigned), s);
+    AdjointIO io{d_P, d_T, d_z, n, state->label, state->L, state->x, state->y, state->Zl, state->Zg,
+                 d_xbar, d_ybar, d_Lbar, d_z_bar, d_P_bar, (double *)scratch, d_sing};
+    if (e == cudaSuccess) {
+        switch (nc) {
+#define OSR_NC_CASE(K)                                                                         \
+    case K: {                                                                                 \
+        AdjointArgs<K> a;                                                                     \
+        make_table<K>(*fluid, a.f);                                                           \
+        a.io = io;                                                                            \
+        flash_adjoint_kernel<K><<<(unsigned)blocks, kAdjThreads, 0, s>>>(a);                  \
+        break;                                                                                \
+    }
+            OSR_NC_CASE(1) OSR_NC_CASE(2) OSR_NC_CASE(3) OSR_NC_CASE(4) OSR_NC_CASE(5) OSR_NC_CASE(6)
+            OSR_NC_CASE(7) OSR_NC_CASE(8) OSR_NC_CASE(9) OSR_NC_CASE(10) OSR_NC_CASE(11) OSR_NC_CASE(12)
+            OSR_NC_CASE(13) OSR_NC_CASE(14) OSR_NC_CASE(15) OSR_NC_CASE(16)
+#undef OSR_NC_CASE
+        }
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        adjoint_reduce_kernel<<<(nc * nc + 127) / 128, 128, 0, s>>>((const double *)scratch, (int)blocks, nc * nc,
+                                                                    d_kij_bar);
+        e = cudaGetLastError();
+    }
+    unsigned h_sing = 0;
+    if (e == cudaSuccess && singular) {
+        e = cudaMemcpyAsync(&h_sing, d_sing, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        *singular = (long)h_sing;
+    }
+    cudaError_t ef = cudaFreeAsync(scratch, s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (ef != cudaSuccess) return cuda_fail(ef);
+    return OSR_OK;
+}
+
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
                                  long n, const osr_flash_out *out, void *stream) {
     return flash_device(fluid, d_P, d_T, d_z, n, out, stream, Form::kPlain);
@@ -652,6 +725,14 @@ osr_status osr_flash_set_pair_from(int pass) {
 }
 
 int osr_flash_get_pair_from(void) { return g_pair_from.load(); }
+
+osr_status osr_flash_set_group_from(int pass) {
+    if (pass < 0 || pass > kMaxPasses) return OSR_ERR_ARG;
+    g_group_from.store(pass);
+    return OSR_OK;
+}
+
+int osr_flash_get_group_from(void) { return g_group_from.load(); }
 
 osr_status osr_flash_set_max_wait(int max_wait) {
     if (max_wait < 0 || max_wait > 1000) return OSR_ERR_ARG;

@@ -792,6 +792,282 @@ __global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_pair_kernel(c
     }
 }
 
+// ---------------------------------------------------------------------------
+// Group form: G lanes per cell (G = 4, 8 or 16 lanes, at least N), for the
+// last passes, where a few thousand cells run their last hundreds of
+// substitution steps with most of the GPU idle and each step's length is set
+// by the instructions one lane executes.  Lane r of a group owns component r
+// (lanes r >= N hold zero padding): its compositions, its row of the mixing
+// rule (the other components' w_j sqrt(a_j) come by shuffle), its ln phi in
+// both phases and its K update; the sums over components are butterfly
+// reductions, which leave the same value in every lane of the group; the
+// two phases' cubic roots, logarithms and quotients run on alternate lanes
+// and are exchanged.  The Rachford-Rice Newton run is replicated in every
+// lane (all K and z are kept in every lane), so it is the thread-per-cell
+// form's arithmetic exactly.  Only the order of the mixing and b sums
+// differs from the thread-per-cell form (a tree instead of a running sum).
+
+template <int G>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+// One substitution step of a group (as ss_update_impl).  Per lane: xi, yi,
+// Kn of its own component; Zl, Zg identical in the group.  `bic` = the
+// lane's row of 1 - k_ij, sai / bi its sqrt(a) and b (zero for pad lanes).
+template <int N, int G, bool Fast>
+__device__ __forceinline__ double ss_update_group_impl(const double *bic, double sai, double bi, bool srk, double P,
+                                                       double T, double zi, double Ki, double L0, double &L,
+                                                       double Lb, double &xi, double &yi, double &Zl, double &Zg,
+                                                       double &Kn, bool &ok, int r, int base, unsigned mask) {
+    auto DIV = [&](double a, double b) -> double {
+        if (Fast) {
+            ok &= qdiv_ok(a, b);
+            return qdiv(a, b);
+        }
+        return a / b;
+    };
+    L = L0;
+    if (L > 1) L = 1;
+    else if (L < 0) L = 0;
+    const double es = fabs(Lb - L);
+    const bool own = r < N;
+    xi = 0;
+    yi = 0;
+    if (own) {
+        if (Ki >= 0) {
+            xi = DIV(zi, L + Ki * (1 - L));
+            yi = Ki * xi;
+        } else {
+            yi = DIV(zi, 1 - L);
+        }
+    }
+    const double ul = xi * sai, ug = yi * sai;
+    double vl = 0, vg = 0;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        const double ulj = __shfl_sync(mask, ul, base + j), ugj = __shfl_sync(mask, ug, base + j);
+        vl += bic[j] * ulj;
+        vg += bic[j] * ugj;
+    }
+    const double Cal = group_sum<G>(ul * vl, mask), Cag = group_sum<G>(ug * vg, mask);
+    const double Cbl = group_sum<G>(xi * bi, mask), Cbg = group_sum<G>(yi * bi, mask);
+    // this lane's phase for the scalar work: even lanes liquid, odd vapour
+    const int p = r & 1;
+    const double pa = P / (kR * kR * T * T), pb = P / (kR * T);
+    const double Ca = p ? Cag : Cal, Cb = p ? Cbg : Cbl;
+    const double A = Ca * pa, B = Cb * pb;
+    const double Z = phase_z(A, B, srk, p != 0);
+    const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
+    const double DD = DIV(A, B * (d1 - d2));
+    const double FF = log(DIV(Z + d2 * B, Z + d1 * B));
+    const double cz = log(Z - B);
+    const double rCa = DIV(2.0, Ca), rCb = DIV(1.0, Cb);
+    const double DF = DD * FF;
+    const double Zo = __shfl_xor_sync(mask, Z, 1), DFo = __shfl_xor_sync(mask, DF, 1);
+    const double czo = __shfl_xor_sync(mask, cz, 1), rCao = __shfl_xor_sync(mask, rCa, 1);
+    const double rCbo = __shfl_xor_sync(mask, rCb, 1);
+    Zl = p ? Zo : Z;
+    Zg = p ? Z : Zo;
+    const double DFl = p ? DFo : DF, DFg = p ? DF : DFo, cl = p ? czo : cz, cg = p ? cz : czo;
+    const double rCal = p ? rCao : rCa, rCag = p ? rCa : rCao, rCbl = p ? rCbo : rCb, rCbg = p ? rCb : rCbo;
+    Kn = Ki;
+    if (own) {
+        const double t1l = bi * rCbl, t1g = bi * rCbg;
+        const double lnl = t1l * (Zl - 1) - cl + DFl * (sai * vl * rCal - t1l);
+        const double lng = t1g * (Zg - 1) - cg + DFg * (sai * vg * rCag - t1g);
+        const double d = lnl - lng;
+        const bool fast = Ki > 0 && xi > 0 && yi > 0 && xi < 1e300 && yi < 1e300 && fabs(lnl) < 700 &&
+                          fabs(lng) < 700 && fabs(d) < 700;
+        const double e = exp(fast ? d : 0.0);
+        Kn = (zi != 0 && fast) ? e : Ki;
+        if (!(fast || zi == 0)) {
+            const double fL = xi * exp(lnl), fG = yi * exp(lng);
+            if (fG != 0) Kn = Ki * (fL / fG);
+            else Kn = -1;
+            if (fL != fL) Kn = -1;
+            if (fG != fG) Kn = 1;
+        }
+    }
+    return es;
+}
+
+template <int N, int G>
+__device__ __forceinline__ double ss_update_group(const double *bic, double sai, double bi, bool srk, double P,
+                                                  double T, double zi, double &Ki, double *K, double &L, double &Lb,
+                                                  double &xi, double &yi, double &Zl, double &Zg, int r, int base,
+                                                  unsigned mask) {
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1)) << base;
+    bool ok = true;
+    double Kn;
+    const double L0 = L;
+    double es = ss_update_group_impl<N, G, true>(bic, sai, bi, srk, P, T, zi, Ki, L0, L, Lb, xi, yi, Zl, Zg, Kn, ok,
+                                                 r, base, mask);
+    // a group with an out-of-range operand in any lane redoes the step with
+    // IEEE division
+    const unsigned bad = __ballot_sync(mask, !ok);
+    const unsigned redo = __ballot_sync(mask, (bad & gmask) != 0);
+    if (redo && (bad & gmask)) {
+        bool ok2 = true;
+        es = ss_update_group_impl<N, G, false>(bic, sai, bi, srk, P, T, zi, Ki, L0, L, Lb, xi, yi, Zl, Zg, Kn, ok2,
+                                               r, base, redo);
+    }
+    Ki = Kn;
+#pragma unroll
+    for (int j = 0; j < N; j++) K[j] = __shfl_sync(mask, Kn, base + j);
+    Lb = L;
+    return es;
+}
+
+// Batched group form: the queue kernel's passes with G lanes per cell (used
+// for the last passes, on the cells parked by the earlier ones).
+template <int N, int G, bool MULTI>
+__global__ void __launch_bounds__(128) flash_group_kernel(const __grid_constant__ QueueArgs<N> a) {
+    static_assert(G >= N && G >= 2 && (G & (G - 1)) == 0 && G <= 32, "G lanes per cell, a power of two >= N");
+    const int lane = threadIdx.x & 31;
+    const int r = lane & (G - 1), base = lane & ~(G - 1);
+    const FlashIO &io = a.io;
+    const long total = a.first ? io.n : (long)*a.src_count;
+    int mode = kFetch;
+    long c = -1;
+    double P = 0, T = 0, L = 0, Lb = 10;
+    double z[N], K[N], bic[N];
+    double sai = 0, bi = 0, zi = 0, Ki = 0;
+    bool srk = false;
+    int j = 0, k = 0, rr = 0;
+    int waited = 0;
+    int inst = 0;
+    double big = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) z[i] = K[i] = bic[i] = 0;
+    for (;;) {
+        // one slot per group, claimed through its first lane
+        const unsigned need = __ballot_sync(kPairFull, mode == kFetch && r == 0);
+        if (need) {
+            const int leader = __ffs(need) - 1;
+            unsigned long long slot0 = 0;
+            if (lane == leader) slot0 = atomicAdd(a.head, (unsigned long long)__popc(need));
+            slot0 = __shfl_sync(kPairFull, slot0, leader);
+            const long q = (long)slot0 + __popc(need & ((1u << base) - 1));
+            if (mode == kFetch) {
+                if (q < total) {
+                    if (a.first) {
+                        c = q;
+                        k = 0;
+                        rr = 0;
+                        Lb = 10;
+                    } else {
+                        c = a.src.cell[q];
+                        k = a.src.k[q];
+                        rr = a.src.rr[q];
+                        Lb = a.src.Lb[q];
+#pragma unroll
+                        for (int i = 0; i < N; i++) K[i] = a.src.K[(long)i * a.src.cap + q];
+                    }
+                    P = io.P[c];
+                    T = io.T[c];
+#pragma unroll
+                    for (int i = 0; i < N; i++) z[i] = io.z[(long)i * io.n + c];
+                    if constexpr (MULTI) inst = find_instance(a.inst_start, a.n_inst, c);
+                    const FluidTable<N> &f = table_of<N, MULTI>(a, inst);
+                    double sa[N];
+                    if (a.first) flash_init<N>(f, P, T, K, sa);
+                    else sqrt_a<N>(f, T, sa);
+                    // this lane's component (zero padding past N)
+                    sai = bi = zi = 0;
+                    Ki = 1;
+#pragma unroll
+                    for (int i = 0; i < N; i++)
+                        if (i == r) {
+                            sai = sa[i];
+                            bi = f.b[i];
+                            zi = z[i];
+                            Ki = K[i];
+                        }
+#pragma unroll
+                    for (int jj = 0; jj < N; jj++) bic[jj] = r < N ? f.bic[(r < N ? r : 0) * N + jj] : 0.0;
+                    srk = f.srk != 0;
+                    L = 0.6;
+                    j = 0;
+                    big = rr_bound<N>(K);
+                    mode = kNewton;
+                } else {
+                    mode = kDone;
+                }
+            }
+        }
+        if (__ballot_sync(kPairFull, mode != kDone) == 0) break;
+        if (mode == kNewton) {
+            const double t = rr_step<N>(K, z, L);
+            j++;
+            if (fabs(L) > big) {
+                j = kRRMaxIt;  // provably divergent: the reference runs to its cap
+                mode = kReady;
+            } else if (!((t * t > kRRTol) && (j < kRRMaxIt))) {
+                mode = kReady;
+            }
+        }
+        const unsigned ready = __ballot_sync(kPairFull, mode == kReady);
+        const unsigned still = __ballot_sync(kPairFull, mode == kNewton);
+        if (ready != 0) waited++;
+        if (ready != 0 && (__popc(ready) >= a.ss_batch || still == 0 || waited > a.max_wait)) {
+            waited = 0;
+            if (mode == kReady) {
+                double xi, yi, Zl, Zg;
+                const double es = ss_update_group<N, G>(bic, sai, bi, srk, P, T, zi, Ki, K, L, Lb, xi, yi, Zl, Zg, r,
+                                                        base, ready);
+                rr += j;
+                k++;
+                // es and k are the same in every lane of a group
+                const bool go_on = (es > kSSTol) && (k < kSSMaxIt);
+                const unsigned parkers = __ballot_sync(ready, go_on && k >= a.park_at);
+                if (go_on) {
+                    if (k >= a.park_at) {
+                        unsigned slot = 0;
+                        if (r == 0) slot = atomicAdd(a.dst_count, 1u);
+                        slot = __shfl_sync(parkers, slot, base);
+                        if (r == 0) {
+                            a.dst.cell[slot] = c;
+                            a.dst.k[slot] = k;
+                            a.dst.rr[slot] = rr;
+                            a.dst.Lb[slot] = Lb;
+                        }
+                        if (r < N) a.dst.K[(long)r * a.dst.cap + slot] = Ki;
+                        mode = kFetch;
+                    } else {
+                        L = 0.6;
+                        j = 0;
+                        big = rr_bound<N>(K);
+                        mode = kNewton;
+                    }
+                } else {
+                    if (r < N) {
+                        io.x[(long)r * io.n + c] = xi;
+                        io.y[(long)r * io.n + c] = yi;
+                    }
+                    if (r == 0) {
+                        io.label[c] = flash_label(L);
+                        io.L[c] = L;
+                        io.Zl[c] = Zl;
+                        io.Zg[c] = Zg;
+                        if (io.iters) io.iters[c] = k;
+                        if (io.rr_iters) io.rr_iters[c] = rr;
+                    }
+                    mode = kFetch;
+                }
+            }
+        }
+    }
+}
+
+// Lanes per cell of the group form for N components.
+template <int N>
+constexpr int group_lanes() {
+    return N <= 2 ? 2 : N <= 4 ? 4 : N <= 8 ? 8 : 16;
+}
+
 // Fugacity derivatives for both phases of every cell, following the
 // reference's fugacity rows of the analytic Jacobian
 // (compsim/Petsc_Functions.cpp:30243-30372) with dZ/dP, dZ/dw_k from the
@@ -808,10 +1084,11 @@ struct DerivArgs {
     int n_inst;
 };
 
-template <int N>
-__device__ __forceinline__ void phase_derivs(const FluidTable<N> &f, const double *sa, double P, double T,
-                                             const double *w, double Z, double *out_dx, double *out_dp, long n,
-                                             long c) {
+// store_dx(i, k, value) receives d ln(phi_i)/d w_k, store_dp(i, value)
+// d ln(phi_i)/d P.
+template <int N, class SX, class SP>
+__device__ __forceinline__ void phase_derivs_into(const FluidTable<N> &f, const double *sa, double P, double T,
+                                                  const double *w, double Z, SX store_dx, SP store_dp) {
     double u[N], v[N];
 #pragma unroll
     for (int i = 0; i < N; i++) u[i] = w[i] * sa[i];
@@ -878,15 +1155,23 @@ __device__ __forceinline__ void phase_derivs(const FluidTable<N> &f, const doubl
         double ti = sai * vi;
         double t1 = bi * rCb;
         double EE = 2 * ti * rCa - t1;
-        out_dp[(long)i * n + c] = t1 * dZdp + dBBdp + EE * (dDDdp * FF + DD * dFFdp);
+        store_dp(i, t1 * dZdp + dBBdp + EE * (dDDdp * FF + DD * dFFdp));
         double g = 2 * ti * rCa * rCa * rpa;
         double hs = h * sai;
 #pragma unroll
         for (int k = 0; k < N; k++) {
-            out_dx[((long)i * N + k) * n + c] =
-                t1 * P1[k] + P2[k] + EE * P3[k] + hs * sa[k] * f.bic[i * N + k] - g * P4[k];
+            store_dx(i, k, t1 * P1[k] + P2[k] + EE * P3[k] + hs * sa[k] * f.bic[i * N + k] - g * P4[k]);
         }
     }
+}
+
+template <int N>
+__device__ __forceinline__ void phase_derivs(const FluidTable<N> &f, const double *sa, double P, double T,
+                                             const double *w, double Z, double *out_dx, double *out_dp, long n,
+                                             long c) {
+    phase_derivs_into<N>(
+        f, sa, P, T, w, Z, [&](int i, int k, double v) { out_dx[((long)i * N + k) * n + c] = v; },
+        [&](int i, double v) { out_dp[(long)i * n + c] = v; });
 }
 
 // One thread per (cell, phase); blockIdx.y selects the phase.

@@ -5,8 +5,8 @@
 // and libosiris_b200.so, and for each deck given on the command line:
 //   1. opens it with the reference's Data_Input + start-up (ref_deck_open) and
 //      with osr_create (the library's C++ reader + device start-up);
-//   2. checks the row layout and InitGuess2 (OsrInitGuess against the
-//      reference's) for equality;
+//   2. checks the row layout (equal) and InitGuess2 (OsrInitGuess against
+//      the reference's, within 1e-9: the two start-ups flash independently);
 //   3. perturbs the unknowns, then runs the reference's FormFunction and
 //      FormJacobian and the adapter's OsrFormFunction / OsrSetJacobianPattern /
 //      OsrFormJacobian (include/osiris_b200_petsc.hpp) on the same Vec and
@@ -27,6 +27,8 @@
 #include "petsc_cuda_lite.h"
 #include "shim_types.h"
 #include "osiris_b200_petsc.hpp"
+
+int CreateAllocationTable(void);   // the reference's own (compsim/PetscAUX.cpp:1081-1099)
 
 extern "C" {
 int ref_deck_open(const char *path);
@@ -78,8 +80,14 @@ static int check_deck(const char *path, double t) {
     ref_init_guess(x0.data());
     _p_Vec X{xg.data(), (int)n}, F{f.data(), (int)n};
     if (OsrInitGuess(nullptr, &X, &c) != 0) fail("OsrInitGuess status", (double)c.last, 0, -1);
-    for (long r = 0; r < n; r++)
-        if (!(xg[(size_t)r] == x0[(size_t)r])) fail("InitGuess2", xg[(size_t)r], x0[(size_t)r], r);
+    // the two start-ups flash the cells independently, so the unknowns agree
+    // to the flash's rounding, not bit for bit
+    double worst_x = 0;
+    for (long r = 0; r < n; r++) {
+        const double e = std::fabs(xg[(size_t)r] - x0[(size_t)r]) / std::fmax(1.0, std::fabs(x0[(size_t)r]));
+        if (!(e <= 1e-9)) fail("InitGuess2", xg[(size_t)r], x0[(size_t)r], r);
+        else if (e > worst_x) worst_x = e;
+    }
 
     // the same perturbed unknowns on both sides
     unsigned s = 12345u;
@@ -113,6 +121,7 @@ static int check_deck(const char *path, double t) {
     std::vector<double> rv((size_t)cap);
     xr = x0;
     g_last_blocks.clear();
+    CreateAllocationTable();   // SolveNonLinear's set-up of the rank's block sizes (compsim/PetscAUX.cpp:589)
     const long cnt = ref_form_jacobian(xr.data(), t, cap, rr.data(), rc.data(), rv.data());
     const std::vector<PetscInt> ref_blocks = g_last_blocks;
     _p_Mat B;
@@ -145,9 +154,9 @@ static int check_deck(const char *path, double t) {
     if (our_blocks != ref_blocks) fail("VPBJacobi block sizes", (double)our_blocks.size(), (double)ref_blocks.size(), -1);
     OsrSnesCtxRelease(&c);
     osr_grid_destroy(g);
-    std::printf("%s: %ld rows, %ld Jacobian entries; residual worst %.3e of the row's |terms|, Jacobian worst "
-                "%.3e of the row maximum, %zu block sizes equal: %s\n",
-                path, n, compared, worst_f, worst_j, our_blocks.size(), fails ? "FAIL" : "ok");
+    std::printf("%s: %ld rows, %ld Jacobian entries; unknowns worst %.3e, residual worst %.3e of the row's |terms|, "
+                "Jacobian worst %.3e of the row maximum, %zu block sizes equal: %s\n",
+                path, n, compared, worst_x, worst_f, worst_j, our_blocks.size(), fails ? "FAIL" : "ok");
     return fails ? 1 : 0;
 }
 

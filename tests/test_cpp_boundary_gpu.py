@@ -3,9 +3,10 @@ built by tests/cpp/Makefile): the reference's own Data_Input start-up,
 InitGuess2, FormFunction and FormJacobian against osr_create and the PETSc
 adapter of include/osiris_b200_petsc.hpp (OsrInitGuess, OsrFormFunction,
 OsrSetJacobianPattern, OsrFormJacobian) on the oracle's PETSc-lite Vec and
-Mat.  Residual rows within 1e-10 of the row's |terms|, Jacobian entries
-within 1e-9 of the reference row's largest entry, InitGuess2 and the
-VPBJacobi block sizes identical.  Decks: two-phase layers with diffusion and
+Mat.  Row layout and the VPBJacobi block sizes identical; unknowns from
+InitGuess2 within 1e-9 (the two start-ups flash independently); at the same
+perturbed unknowns, residual rows within 1e-10 of the row's |terms| and
+Jacobian entries within 1e-9 of the reference row's largest entry.  Decks: two-phase layers with diffusion and
 wells, every matrix/fracture state pairing, all nine well types, the
 reference's sample deck.
 """

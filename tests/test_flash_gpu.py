@@ -103,7 +103,25 @@ def test_pair_form_matches_oracle(pair_from, eos, nc, seed, cuda_device):
     finally:
         osr.set_pair_from(before)
     _assert_flash_parity(g, o, f"pair{pair_from}-eos{eos}-nc{nc}")
-    assert np.array_equal(g["iters"], o["iters"]) or (g["iters"] != o["iters"]).mean() < 0.005
+
+
+@pytest.mark.parametrize("group_from", [0, 3])
+@pytest.mark.parametrize("eos,nc,seed", [(1, 6, 3), (0, 8, 4), (1, 3, 5), (0, 11, 6), (1, 16, 7), (0, 1, 8),
+                                         (1, 2, 9), (0, 4, 10)])
+def test_group_form_matches_oracle(group_from, eos, nc, seed, cuda_device):
+    """The group form (one lane per component, 2-16 lanes per cell) from the
+    first pass (0) or after three thread-per-cell passes (3)."""
+    tc, pc, acf, kij = workloads.flash_table(nc, 100 + seed)
+    fl = oracle.Fluid(tc, pc, acf, kij, eos)
+    P, T, z = workloads.flash_cells(6000, nc, seed=seed)
+    o = oracle.flash_batch(fl, P, T, z)
+    before = osr.get_group_from()
+    osr.set_group_from(group_from)
+    try:
+        g = _run_gpu(fl, P, T, z)
+    finally:
+        osr.set_group_from(before)
+    _assert_flash_parity(g, o, f"group{group_from}-eos{eos}-nc{nc}")
 
 
 def test_derivatives_match_oracle(golden_srk6, cuda_device):
