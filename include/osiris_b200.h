@@ -39,6 +39,17 @@ typedef enum {
 
 typedef enum { OSR_EOS_PR = 0, OSR_EOS_SRK = 1 } osr_eos;
 
+/* Per-cell status codes (osr_flash_status, osr_grid_status).  The reference
+ * has none: a NaN reaches its acceptance test ((vnorm - vnorm) != 0,
+ * compsim/PetscAUX.cpp:703) or its fatal paths (TerM, compsim/Globals.cpp). */
+typedef enum {
+    OSR_CELL_OK = 0,
+    OSR_CELL_MAXIT = 1,   /* the flash's substitution stopped at its 500-step cap */
+    OSR_CELL_NAN = 2,     /* a value is not finite */
+    OSR_CELL_NOROOT = 3,  /* flash: a present phase's compressibility is not positive */
+    OSR_CELL_RANGE = 4    /* grid: oil pressure not positive */
+} osr_cell_status;
+
 /* Component table (HOST pointers, read during the call only).  Mirrors the
  * reference's fluidProp columns TCRIT, PCRIT, AC and its BIC matrix
  * (compsim/Functions.h:96-111, compsim/Data_Input.cpp:977-990), except that
@@ -156,6 +167,15 @@ osr_status osr_flash_adjoint(const osr_fluid *fluid, const double *d_P, const do
                              const double *d_Lbar, double *d_kij_bar, double *d_z_bar, double *d_P_bar,
                              long *singular, void *stream);
 
+/* Per-cell status of a flash result (DEVICE `out` of osr_flash_batch for n
+ * cells of nc components; iters optional -- without it MAXIT is not
+ * detected): d_status [n] (optional) receives an osr_cell_status per cell,
+ * counts [4] (HOST) the number of cells per code OK/MAXIT/NAN/NOROOT, and
+ * *first_bad (HOST) the lowest cell index whose code is not OK, or -1.
+ * Synchronises `stream`. */
+osr_status osr_flash_status(const osr_flash_out *out, int nc, long n, signed char *d_status, long *counts,
+                            long *first_bad, void *stream);
+
 /* End-to-end form for callers holding HOST arrays (same layouts; out fields
  * are host pointers): the cells go through in chunks of about 131,072
  * (at most 16 chunks) pipelined over three internal streams -- inputs in,
@@ -181,8 +201,9 @@ osr_status osr_flash_set_shape(int ss_batch, int tail_batch, int ctas_per_sm, in
 
 /* First pass (0-based) of the batched flash that runs in pair form: two
  * lanes per cell, one per phase, for the few long-running cells of the late
- * passes (each substitution step's latency halves).  12 or more = never.
- * Process-wide; the results agree to rounding either way. */
+ * passes (each substitution step's latency halves).  Default 6 (cells past
+ * 64 steps); 12 or more = never.  Process-wide; the results agree to
+ * rounding either way. */
 osr_status osr_flash_set_pair_from(int pass);
 int osr_flash_get_pair_from(void);
 
@@ -193,6 +214,27 @@ int osr_flash_get_pair_from(void);
 osr_status osr_flash_set_group_from(int pass);
 int osr_flash_get_group_from(void);
 osr_status osr_flash_get_shape(int *ss_batch, int *tail_batch, int *ctas_per_sm, int *park_after);
+
+/* The project's autotuner of the batched flash's launch shape.  Runs every
+ * candidate (substitution-step batch 24/28 ready lanes, park after 1/2/3
+ * steps, pair form from pass 4/5/6/never, 2/3 CTAs per SM: 48 shapes) on the
+ * caller's batch (DEVICE inputs and outputs as osr_flash_batch; the outputs
+ * are written), timed with CUDA events on `stream`; keeps the fastest for the
+ * batch's (component count, floor(log2 n)) bucket and makes it the current
+ * knobs.  No reference counterpart. */
+typedef struct osr_flash_tuning {
+    int ss_batch, tail_batch, ctas_per_sm, park_after, pair_from;
+    float ms;          /* the winner's time per call */
+    int candidates;    /* shapes timed */
+} osr_flash_tuning;
+osr_status osr_flash_autotune(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_z,
+                              long n, const osr_flash_out *out, void *stream, osr_flash_tuning *best);
+/* Use the tuned shape of a call's (component count, size bucket) when one is
+ * known (1), or the process-wide knobs always (0, the default). */
+osr_status osr_flash_use_tuned(int on);
+/* Persist / restore the tuned shapes (a text file, one line per bucket). */
+osr_status osr_flash_tuning_save(const char *path);
+osr_status osr_flash_tuning_load(const char *path);
 
 /* Age limit of the substitution-step batching: a warp runs the step for its
  * ready lanes once they have waited more than max_wait Newton trips, even if
@@ -301,6 +343,14 @@ osr_status osr_grid_update_dependencies(osr_grid *grid, void *stream);
  * osr_grid_field_size returns planes*cells (or -1 for an unknown name). */
 long osr_grid_field_size(osr_grid *grid, const char *field);
 osr_status osr_grid_get(osr_grid *grid, const char *field, double *out);
+
+/* State check: *code = OSR_CELL_NAN when any pressure, saturation or phase
+ * composition of either continuum is not finite, else OSR_CELL_RANGE when an
+ * oil pressure is not positive, else OSR_CELL_OK; *first_bad_block = the
+ * lowest such block (matrix blocks 0..cells-1, then fracture), or -1.  Where
+ * the reference would run on into its acceptance test or TerM(), a caller
+ * can stop first.  Synchronous. */
+osr_status osr_grid_status(osr_grid *grid, int *code, long *first_bad_block);
 
 /* ---------------------------------------------------------------------------
  * Residual path: the PETSc FormFunction callback on the device.

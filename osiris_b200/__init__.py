@@ -256,6 +256,27 @@ def flash_adjoint(fluid: Fluid, P, T, z, state: dict, xbar, ybar, Lbar, want_z: 
     return {"kij_bar": kb, "z_bar": zb, "P_bar": pb, "singular": int(sing.value)}
 
 
+CELL_STATUS = {0: "OK", 1: "MAXIT", 2: "NAN", 3: "NOROOT", 4: "RANGE"}
+
+
+def flash_status(out: dict, nc: int, stream=None) -> dict:
+    """Per-cell status of a device flash result (osr_flash_status): {"status":
+    int8 [n] device tensor, "counts": {OK, MAXIT, NAN, NOROOT}, "first_bad":
+    lowest non-OK cell or -1}."""
+    import torch
+    n = int(out["L"].shape[0])
+    st = torch.empty(n, dtype=torch.int8, device=out["L"].device)
+    counts = (ctypes.c_long * 4)()
+    first = ctypes.c_long()
+    if stream is None:
+        stream = torch.cuda.current_stream(out["L"].device)
+    co = _out_struct(out, lambda t: t.data_ptr())
+    with torch.cuda.device(out["L"].device):
+        _check(lib().osr_flash_status(ctypes.byref(co), int(nc), ctypes.c_long(n), _vp(st.data_ptr()), counts,
+                                      ctypes.byref(first), _vp(stream.cuda_stream)), "osr_flash_status")
+    return {"status": st, "counts": {CELL_STATUS[k]: int(counts[k]) for k in range(4)}, "first_bad": first.value}
+
+
 def flash_host(fluid: Fluid, P, T, z, derivs: bool = True, out: dict | None = None, iters: bool = True):
     """End-to-end flash of host (numpy) arrays through osr_flash_batch_host.
     Inputs may be pinned torch CPU tensors or numpy arrays."""
@@ -331,6 +352,44 @@ def set_pair_from(pass_index: int):
 
 def get_pair_from() -> int:
     return int(lib().osr_flash_get_pair_from())
+
+
+class FlashTuning(ctypes.Structure):
+    """osr_flash_tuning: the autotuner's winning launch shape."""
+    _fields_ = [("ss_batch", ctypes.c_int), ("tail_batch", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("park_after", ctypes.c_int), ("pair_from", ctypes.c_int), ("ms", ctypes.c_float),
+                ("candidates", ctypes.c_int)]
+
+
+def autotune(fluid: Fluid, P, T, z, out: dict | None = None, stream=None) -> dict:
+    """Time every candidate launch shape of the batched flash on this batch
+    (osr_flash_autotune); the winner becomes the current shape and the tuned
+    shape of the batch's (component count, size bucket)."""
+    import torch
+    n = int(P.shape[0])
+    if out is None:
+        out = alloc_flash_outputs(fluid.nc, n, False, P.device)
+    if stream is None:
+        stream = torch.cuda.current_stream(P.device)
+    co = _out_struct(out, lambda t: t.data_ptr())
+    best = FlashTuning()
+    with torch.cuda.device(P.device):
+        _check(lib().osr_flash_autotune(fluid.cref, _vp(P.data_ptr()), _vp(T.data_ptr()), _vp(z.data_ptr()),
+                                        ctypes.c_long(n), ctypes.byref(co), _vp(stream.cuda_stream),
+                                        ctypes.byref(best)), "osr_flash_autotune")
+    return {k: getattr(best, k) for k, _ in FlashTuning._fields_}
+
+
+def use_tuned(on: bool):
+    _check(lib().osr_flash_use_tuned(int(bool(on))), "osr_flash_use_tuned")
+
+
+def tuning_save(path: str):
+    _check(lib().osr_flash_tuning_save(path.encode()), "osr_flash_tuning_save")
+
+
+def tuning_load(path: str):
+    _check(lib().osr_flash_tuning_load(path.encode()), "osr_flash_tuning_load")
 
 
 def set_group_from(pass_index: int):
@@ -562,6 +621,13 @@ class Grid:
         _check(lib().osr_grid_residual_logk_vjp(self._h, _vp(d_lambda.data_ptr()), _vp(d_gk.data_ptr()),
                                                 ctypes.c_double(sim_time), None if stream is None else _vp(stream)),
                "osr_grid_residual_logk_vjp")
+
+    def status(self):
+        """(osr_cell_status code, first bad block or -1) of the current state
+        (osr_grid_status)."""
+        code, first = ctypes.c_int(), ctypes.c_long()
+        _check(lib().osr_grid_status(self._h, ctypes.byref(code), ctypes.byref(first)), "osr_grid_status")
+        return code.value, first.value
 
     def form_function(self, d_x, d_f, sim_time: float = 0.0, stream=None):
         _check(lib().osr_grid_form_function(self._h, _vp(d_x.data_ptr()), _vp(d_f.data_ptr()),

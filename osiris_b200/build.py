@@ -26,6 +26,9 @@ OBJDIR = os.path.join(PKG, "_build")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
+    # device code of a translation unit optimised in parallel (the flash unit
+    # instantiates its kernels for 16 component counts)
+    "--split-compile=8",
     "-Xcompiler", "-fPIC",
     "-I" + INCLUDE, "-I" + CSRC,
 ]

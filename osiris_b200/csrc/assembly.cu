@@ -220,7 +220,8 @@ osr_status grid_assembly_init(osr_grid &g, const osr_model *md) {
     ASM_CUDA(cudaMalloc((void **)&g.tor, n * 8));
     ASM_CUDA(cudaMemcpy(g.tor, tor.data(), n * 8, cudaMemcpyHostToDevice));
     ASM_CUDA(cudaMalloc((void **)&g.rowoff, (2 * n + 1) * 8));
-    ASM_CUDA(cudaMalloc((void **)&g.sizes, 2 * n * 8));
+    // block sizes, then the scan's chunk sums
+    ASM_CUDA(cudaMalloc((void **)&g.sizes, (2 * n + kScanBlocks) * 8));
     ASM_CUDA(cudaMalloc((void **)&g.pmax, 8));
     ASM_CUDA(cudaMemset(g.rowoff, 0, (2 * n + 1) * 8));
     const int nw = g.nwells > 0 ? g.nwells : 0;
@@ -365,7 +366,10 @@ osr_status osr_grid_refresh_layout(osr_grid *g, void *stream) {
     const long n = g->cells;
     block_size_kernel<<<(unsigned)grid_blocks(2 * n), 128, 0, st>>>(g->m[0].label, g->m[1].label, n, g->nc, g->sizes);
     ASM_CUDA(cudaGetLastError());
-    row_offset_kernel<<<1, 1024, 0, st>>>(g->sizes, 2 * n, g->rowoff);
+    long *part = g->sizes + 2 * n;
+    scan_sums_kernel<<<kScanBlocks, kScanThreads, 0, st>>>(g->sizes, 2 * n, part);
+    scan_bases_kernel<<<1, 32, 0, st>>>(part, 2 * n, g->rowoff);
+    scan_apply_kernel<<<kScanBlocks, kScanThreads, 0, st>>>(g->sizes, 2 * n, part, g->rowoff);
     ASM_CUDA(cudaGetLastError());
     ASM_CUDA(cudaMemsetAsync(g->pmax, 0, 8, st));
     pcoeff_kernel<<<(unsigned)grid_blocks(n), 128, 0, st>>>(g->m[0].P + n, g->m[1].P + n, n, g->pmax);

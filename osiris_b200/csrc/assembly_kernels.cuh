@@ -223,31 +223,85 @@ static __global__ void block_size_kernel(const signed char *lab_m, const signed 
     }
 }
 
-// Single-block exclusive scan of the block sizes (2 cells + 1 outputs), with
-// a per-thread serial segment so any cell count fits one launch.
-static __global__ void __launch_bounds__(1024) row_offset_kernel(const long *sizes, long nb, long *off) {
-    __shared__ long part[1024];
-    const int t = threadIdx.x;
-    const long per = (nb + blockDim.x - 1) / blockDim.x;
-    const long b0 = t * per, b1 = min(nb, b0 + per);
+// Exclusive scan of the block sizes into the row offsets (2 cells + 1
+// outputs), across the whole GPU in three launches: every CTA sums its
+// contiguous chunk of sizes (coalesced, strided by the CTA's threads); one
+// warp scans the kScanBlocks chunk sums into chunk bases (and the total);
+// every CTA then scans its chunk in tiles of kScanThreads with warp shuffles,
+// carrying the running sum from tile to tile.  Integer sums: exact and
+// independent of the launch shape.
+constexpr int kScanBlocks = 296;
+constexpr int kScanThreads = 256;
+
+__device__ __forceinline__ long scan_chunk_begin(long nb, int blk) {
+    const long chunk = (nb + kScanBlocks - 1) / kScanBlocks;
+    const long b = (long)blk * chunk;
+    return b < nb ? b : nb;
+}
+
+static __global__ void __launch_bounds__(kScanThreads) scan_sums_kernel(const long *sizes, long nb, long *part) {
+    __shared__ long warp_sum[kScanThreads / 32];
+    const long b0 = scan_chunk_begin(nb, blockIdx.x), b1 = scan_chunk_begin(nb, blockIdx.x + 1);
     long s = 0;
-    for (long b = b0; b < b1; b++) s += sizes[b];
-    part[t] = s;
+    for (long b = b0 + threadIdx.x; b < b1; b += kScanThreads) s += sizes[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5] = s;
     __syncthreads();
-    if (t == 0) {
-        long acc = 0;
-        for (int i = 0; i < (int)blockDim.x; i++) {
-            long v = part[i];
-            part[i] = acc;
-            acc += v;
-        }
-        off[nb] = acc;
+    if (threadIdx.x == 0) {
+        long t = 0;
+        for (int w = 0; w < kScanThreads / 32; w++) t += warp_sum[w];
+        part[blockIdx.x] = t;
     }
-    __syncthreads();
-    long acc = part[t];
-    for (long b = b0; b < b1; b++) {
-        off[b] = acc;
-        acc += sizes[b];
+}
+
+// one warp: exclusive scan of the chunk sums in place, total into off[nb]
+static __global__ void scan_bases_kernel(long *part, long nb, long *off) {
+    const int lane = threadIdx.x;
+    long carry = 0;
+    for (int i0 = 0; i0 < kScanBlocks; i0 += 32) {
+        const int i = i0 + lane;
+        const long v = i < kScanBlocks ? part[i] : 0;
+        long incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (i < kScanBlocks) part[i] = carry + incl - v;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) off[nb] = carry;
+}
+
+static __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const long *sizes, long nb, const long *base,
+                                                                       long *off) {
+    __shared__ long warp_tot[kScanThreads / 32];
+    __shared__ long tile_total;
+    const long b0 = scan_chunk_begin(nb, blockIdx.x), b1 = scan_chunk_begin(nb, blockIdx.x + 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long carry = base[blockIdx.x];
+    for (long t0 = b0; t0 < b1; t0 += kScanThreads) {
+        const long b = t0 + threadIdx.x;
+        const long v = b < b1 ? sizes[b] : 0;
+        long incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        long before = 0, total = 0;
+        for (int w = 0; w < kScanThreads / 32; w++) {
+            if (w < warp) before += warp_tot[w];
+            total += warp_tot[w];
+        }
+        if (b < b1) off[b] = carry + before + incl - v;
+        if (threadIdx.x == 0) tile_total = total;
+        __syncthreads();
+        carry += tile_total;
+        __syncthreads();
     }
 }
 

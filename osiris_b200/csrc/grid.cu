@@ -144,6 +144,33 @@ FieldRef find_field(osr_grid *g, const std::string &name) {
 }
 }  // namespace
 
+
+namespace osr {
+
+// Per cell-medium check of the primary state: every pressure, saturation
+// and phase composition finite, the oil pressure positive.  The first bad
+// block (matrix blocks 0..cells-1, then fracture) is kept by an atomic min.
+__global__ void grid_status_kernel(MediumFields m0, MediumFields m1, long n, int nc, unsigned long long *first,
+                                   unsigned *codes) {
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < 2 * n; b += (long)gridDim.x * blockDim.x) {
+        const MediumFields &F = b >= n ? m1 : m0;
+        const long c = b >= n ? b - n : b;
+        unsigned code = 0;
+        for (int p = 0; p < 3; p++) {
+            if (!isfinite(F.P[(long)p * n + c]) || !isfinite(F.sat[(long)p * n + c])) code |= 1u;
+        }
+        for (int i = 0; i < nc; i++)
+            if (!isfinite(F.x[(long)i * n + c]) || !isfinite(F.y[(long)i * n + c])) code |= 1u;
+        if (!(F.P[n + c] > 0)) code |= 2u;
+        if (code) {
+            atomicMin(first, (unsigned long long)b);
+            atomicOr(codes, code);
+        }
+    }
+}
+
+}  // namespace osr
+
 extern "C" {
 
 osr_status osr_grid_create(const osr_model *md, osr_grid **out) {
@@ -348,6 +375,28 @@ osr_status osr_grid_dims(osr_grid *g, int *dims) {
     dims[1] = g->ny;
     dims[2] = g->nz;
     dims[3] = g->nc;
+    return OSR_OK;
+}
+
+osr_status osr_grid_status(osr_grid *g, int *code, long *first_bad_block) {
+    if (!g || !code || !first_bad_block) return OSR_ERR_ARG;
+    unsigned long long *d = nullptr;
+    if (cudaMalloc((void **)&d, 16) != cudaSuccess) return osr::gfail(cudaGetLastError());
+    const unsigned long long init[2] = {~0ull, 0ull};
+    cudaError_t e = cudaMemcpy(d, init, 16, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        long blocks = (2 * g->cells + 255) / 256;
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        osr::grid_status_kernel<<<(unsigned)blocks, 256>>>(g->m[0], g->m[1], g->cells, g->nc, d, (unsigned *)(d + 1));
+        e = cudaGetLastError();
+    }
+    unsigned long long h[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, 16, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return osr::gfail(e);
+    const unsigned bits = (unsigned)h[1];
+    *code = (bits & 1u) ? OSR_CELL_NAN : (bits & 2u) ? OSR_CELL_RANGE : OSR_CELL_OK;
+    *first_bad_block = bits ? (long)h[0] : -1;
     return OSR_OK;
 }
 

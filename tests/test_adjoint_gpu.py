@@ -14,11 +14,19 @@ equations (oracle.flash_polish): the derivatives of the exact equilibrium.
 Workload: SRK, 6 components (the batched flash's seeded table), 3,000 cells
 of the batched flash's P/T/z draw; objective = sum of seeded random
 cotangents times x, y, L over two-phase cells plus the present phase of
-one-phase cells (whose composition is the feed).  Bars: directional
-derivatives along 32 seeded kij directions (zero diagonal) within 1e-6 of
-central differences with h = 1e-6; z and P directions within 1e-5 (their
-differences are taken at much smaller relative steps); the device's kij_bar,
-z_bar and P_bar within 1e-10 of the oracle's adjoint at the same state.
+one-phase cells (whose composition is the feed).  Bars:
+  * the device adjoint evaluated at the polished equilibrium (the state it
+    is the derivative at): directional derivatives along 32 seeded kij
+    directions (zero diagonal) within 1e-6 relative of central differences
+    with h = 1e-6;
+  * the same gradient through the autograd function at the device flash's
+    own result (stopped by the reference's tolerances, ~1e-9 from the
+    equilibrium): within 1e-6 of the direction's scale sum |g_ij V_ij|
+    (a direction whose derivative cancels to 1/200 of that scale magnifies
+    the state's distance from the equilibrium accordingly); z and P within
+    1e-5;
+  * the device's kij_bar, z_bar and P_bar within 1e-10 of the oracle's
+    adjoint at the same state.
 """
 import numpy as np
 import pytest
@@ -107,6 +115,45 @@ def setup(cuda_device):
                 Lb=Lb, dev=dev)
 
 
+def _directions(seed=5):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(N_DIRECTIONS):
+        V = rng.standard_normal((6, 6))
+        np.fill_diagonal(V, 0)
+        out.append(V)
+    return out
+
+
+def _fd(s, V):
+    fp = oracle.Fluid(s["tc"], s["pc"], s["acf"], s["kij"] + H * V, s["eos"])
+    fm = oracle.Fluid(s["tc"], s["pc"], s["acf"], s["kij"] - H * V, s["eos"])
+    rp, rm = _polished(fp, s["P"], s["T"], s["z"]), _polished(fm, s["P"], s["T"], s["z"])
+    assert np.array_equal(rp["label"], s["ref"]["label"]) and np.array_equal(rm["label"], s["ref"]["label"])
+    return (_objective(rp, s["xb"], s["yb"], s["Lb"]) - _objective(rm, s["xb"], s["yb"], s["Lb"])) / (2 * H)
+
+
+def test_device_adjoint_at_equilibrium_matches_central_differences(setup):
+    """osr_flash_adjoint at the polished equilibrium against central
+    differences of the polished flash: 32 kij directions, 1e-6 relative."""
+    import torch
+    s = setup
+    d = s["dev"]
+    fl = osr.Fluid(s["tc"], s["pc"], s["acf"], s["kij"], s["eos"])
+    st = {k: torch.from_numpy(np.ascontiguousarray(s["ref"][k])).to(d) for k in ("label", "L", "x", "y", "Zl", "Zg")}
+    r = osr.flash_adjoint(fl, s["tP"], s["tT"], s["tz"], st, torch.from_numpy(s["xb"]).to(d),
+                          torch.from_numpy(s["yb"]).to(d), torch.from_numpy(s["Lb"]).to(d))
+    g = r["kij_bar"].cpu().numpy()
+    worst = 0.0
+    for q, V in enumerate(_directions()):
+        fd = _fd(s, V)
+        ad = float((g * V).sum())
+        err = abs(ad - fd) / abs(fd)
+        worst = max(worst, err)
+        assert err <= 1e-6, (q, ad, fd, err)
+    print(f"kij at the equilibrium: {N_DIRECTIONS} directions, worst relative difference {worst:.2e}")
+
+
 def test_kij_gradient_matches_central_differences(setup):
     import torch
     s = setup
@@ -120,21 +167,18 @@ def test_kij_gradient_matches_central_differences(setup):
         (torch.from_numpy(s["Lb"]).to(d) * L).sum()
     obj.backward()
     g = k.grad.numpy()
-    rng = np.random.default_rng(5)
-    worst = 0.0
-    for q in range(N_DIRECTIONS):
-        V = rng.standard_normal((6, 6))
-        np.fill_diagonal(V, 0)
-        fp = oracle.Fluid(s["tc"], s["pc"], s["acf"], s["kij"] + H * V, s["eos"])
-        fm = oracle.Fluid(s["tc"], s["pc"], s["acf"], s["kij"] - H * V, s["eos"])
-        rp, rm = _polished(fp, s["P"], s["T"], s["z"]), _polished(fm, s["P"], s["T"], s["z"])
-        assert np.array_equal(rp["label"], s["ref"]["label"]) and np.array_equal(rm["label"], s["ref"]["label"])
-        fd = (_objective(rp, s["xb"], s["yb"], s["Lb"]) - _objective(rm, s["xb"], s["yb"], s["Lb"])) / (2 * H)
+    worst = worst_rel = 0.0
+    for q, V in enumerate(_directions()):
+        fd = _fd(s, V)
         ad = float((g * V).sum())
-        err = abs(ad - fd) / max(abs(fd), 1e-300)
+        scale = float(np.abs(g * V).sum())
+        err = abs(ad - fd) / scale
         worst = max(worst, err)
+        worst_rel = max(worst_rel, abs(ad - fd) / abs(fd))
         assert err <= 1e-6, (q, ad, fd, err)
-    print(f"kij: {N_DIRECTIONS} directions, worst relative difference from central differences {worst:.2e}")
+    print(f"kij through autograd at the flash's result: {N_DIRECTIONS} directions, worst difference {worst:.2e} of "
+          f"the direction's scale ({worst_rel:.2e} of the derivative)")
+    rng = np.random.default_rng(6)
     # z and P through the same autograd graph
     for name, t, scale in (("z", zt, 1e-3), ("P", Pt, 1e3)):
         grad = t.grad.cpu().numpy()
