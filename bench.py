@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cells", type=int, default=None)
     ap.add_argument("--pair-from", type=int, default=None, help="first flash pass in pair form (12 = never)")
+    ap.add_argument("--no-autotune", action="store_true", help="time the default launch shape")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -564,6 +565,7 @@ def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier,
     sv = structural_values(nx, ny, nz, nc)
     state_doubles = 4 * nc + 73
     jac_bytes = sv * 8 + cells * state_doubles * 8
+    res_bytes = cells * state_doubles * 8 + rows * 8
     peak, peak_src = hbm_peak()
     achieved = jac_bytes / (jac_max * 1e-3) / 1e9
     del J, G
@@ -579,6 +581,13 @@ def measure_assembly(osr, torch, dev, stream, flush, args, rank, world, barrier,
                                f"{nc} components, seeded properties, all cells two-phase (P0 {p0:.4g} Pa)",
                    "rows": rows, "two_phase_fraction": two_phase, "cdif": 0.0,
                    "l2": "flushed before every step (256 MiB write); values 12.6 GB per step exceed L2"},
+        "residual_roofline": {"bound": "hbm", "kernel": "residual_kernel (FormFunction rows)",
+                              "achieved": res_bytes / (res * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": (res_bytes / (res * 1e-3) / 1e9 / peak) if peak else None,
+                              "bytes_per_launch": res_bytes,
+                              "bytes_model": "state fields read once per cell-medium (4N + 73 doubles) + the "
+                                             "rows written (8 B each)",
+                              "ms_per_launch": res, "traffic": None},
         "roofline": {"bound": "hbm", "kernel": "Jacobian: well pass, derivative tables, five column/row kernels",
                      "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                      "frac": (achieved / peak) if peak else None,
@@ -864,6 +873,12 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         return [s.elapsed_time(e) for s, e in ev]
 
+    # the project's autotuner picks the launch shape on this batch before
+    # anything is timed (48 candidate shapes, CUDA events)
+    tuned = None
+    if not args.no_autotune:
+        tuned = osr.autotune(fl, P, T, z)
+        torch.cuda.synchronize(dev)
     step = lambda: osr.flash(fl, P, T, z, derivs=True, out=out)  # noqa: E731
     for _ in range(args.warmup):
         step()
@@ -976,6 +991,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, numpy default_rng)",
         "config": flash_config(n, world),
+        "launch_shape": {"tuned": tuned, "ss_batch_tail_batch_ctas_park": list(osr.get_shape()),
+                         "pair_from": osr.get_pair_from(), "group_from": osr.get_group_from()},
         "workload_stats": {"form": "batched", "two_phase_fraction": two_phase, "mean_ss_iters": float(iters.mean()),
                            "mean_rr_iters": float(rr.mean()), "max_ss_iters": int(iters.max()),
                            "max_rr_iters": int(rr.max())},
