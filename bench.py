@@ -342,15 +342,15 @@ def _gpu_id(torch, dev):
 # ----------------------------------------------------------------------------- GPU side
 
 # DRAM bytes (read + write) per call of the flash iteration kernels, from one
-# ncu capture of the first pass at 262,144 cells (dram__bytes_read.sum +
-# dram__bytes_write.sum) scaled by 4 to the 1,048,576-cell call: the first
-# pass reads every cell's inputs and writes the outputs of the cells it
-# finishes and the parked state of the rest; later passes touch only the
-# parked lists.  Capture command:
-#   ncu --set full --clock-control none -k regex:flash_queue_kernel -c 1
-#       python bench.py --cells 262144 --steps 1 --warmup 1 --no-e2e
+# ncu capture of all nine passes at 262,144 cells (dram__bytes_read.sum +
+# dram__bytes_write.sum summed over the passes: 199.9 MB) scaled by the cell
+# count (x4) to the 1,048,576-cell call.  Capture command:
+#   ncu --section SpeedOfLight --section Occupancy --section WarpStateStats
+#       --section LaunchStats --metrics dram__bytes_read.sum,dram__bytes_write.sum
+#       --clock-control none -k regex:flash_ -c 10
+#       python bench.py --no-autotune --cells 262144 --steps 1 --warmup 1 --no-e2e
 #       --no-cpu-baseline --no-plain --no-assembly --no-instances --no-steps
-FLASH_TRAFFIC_BYTES = 214216704
+FLASH_TRAFFIC_BYTES = 799618048
 
 
 def instance_groups(args, rank):

@@ -3,6 +3,7 @@
 // Jacobian, and the matrix-vector product alone (MatMult).
 #include <cuda_runtime.h>
 #include <cstring>
+#include <vector>
 #include "grid_internal.h"
 #include "ksp_kernels.cuh"
 
@@ -22,6 +23,14 @@ struct osr_ksp_work {
     double *g_x = nullptr;
     long g_rows = -1;
     int g_every = 0;
+    // the whole solve as one graph: the scalars in, block-Jacobi set-up, a
+    // device-side while loop over batches of iterations, the scalars out
+    cudaGraphExec_t whole = nullptr;
+    const double *w_vals = nullptr, *w_b = nullptr;
+    double *w_x = nullptr;
+    long w_rows = -1;
+    int w_every = 0, w_max = 0;
+    bool whole_failed = false;
 };
 
 namespace osr {
@@ -129,6 +138,18 @@ static osr_status spmv_n(const osr_grid &g, const double *vals, const double *x,
     return OSR_OK;
 }
 
+// Condition of the solve graph's while loop: another batch while the solve
+// is running, at most max_batches in all (KspScal.pad counts the batches; it
+// is zero when the scalars are copied in).  The bound holds whatever the
+// scalars say, so the loop always ends.
+__global__ void bcgs_continue_kernel(cudaGraphConditionalHandle h, osrk::KspScal *s, int max_batches) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const int done = ++s->pad;
+        const bool go = s->reason == osrk::kItersRunning && done < max_batches;
+        cudaGraphSetConditional(h, go ? 1u : 0u);
+    }
+}
+
 template <int N>
 static osr_status solve_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
                           osr_ksp_info *info, cudaStream_t st) {
@@ -144,15 +165,17 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     h.dtol = o.dtol;
     h.max_it = o.max_it;
     *k.host = h;
-    KSP_CUDA(cudaMemcpyAsync(k.scal, k.host, sizeof(h), cudaMemcpyHostToDevice, st));
     const unsigned vbk = vec_blocks(n), ib = inv_blocks(nb);
     const unsigned tpb = 32 * osrk::kInvWarps;
-    osrk::bjac_invert_kernel<N><<<ib, tpb, 0, st>>>(v, k.inv, k.scal);
     const unsigned atb = osrk::kApplyThreads;
     const unsigned ab = red_blocks(nb, osrk::kApplyThreads), xb = red_blocks(n, 4 * osrk::kRedThreads);
-    osrk::bjac_apply_kernel<N, 0><<<ab, atb, 0, st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
-    osrk::bcgs_setup_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.r0, k.p, k.v, x);
-    KSP_CUDA(cudaGetLastError());
+    // scalars in, block-Jacobi inverse, r = B b, the BiCGStab set-up
+    auto prologue = [&](cudaStream_t q_st) {
+        cudaMemcpyAsync(k.scal, k.host, sizeof(h), cudaMemcpyHostToDevice, q_st);
+        osrk::bjac_invert_kernel<N><<<ib, tpb, 0, q_st>>>(v, k.inv, k.scal);
+        osrk::bjac_apply_kernel<N, 0><<<ab, atb, 0, q_st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
+        osrk::bcgs_setup_kernel<<<vbk, 256, 0, q_st>>>(n, k.r, k.r0, k.p, k.v, x);
+    };
     const int every = o.check_every > 0 ? o.check_every : 8;
     auto iterations = [&](cudaStream_t q_st, int count) {
         for (int q = 0; q < count; q++) {
@@ -166,6 +189,97 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
                                                                       k.scal);
         }
     };
+    // The whole solve as one graph: prologue, a while node whose body is one
+    // batch of iterations and the continue test, the scalars back to the
+    // pinned host copy.  One launch and one synchronisation per solve.  Used
+    // when the iteration cap is a whole number of batches (so the graph
+    // stops exactly where the host loop would); kept while the system's
+    // buffers and size stay the same.
+    if (k.whole && (k.w_vals != vals || k.w_b != b || k.w_x != x || k.w_rows != n || k.w_every != every ||
+                    k.w_max != o.max_it)) {
+        cudaGraphExecDestroy(k.whole);
+        k.whole = nullptr;
+    }
+    if (!k.whole && !k.whole_failed && o.max_it >= every && o.max_it % every == 0) {
+        if (!k.cap) KSP_CUDA(cudaStreamCreateWithFlags(&k.cap, cudaStreamNonBlocking));
+        cudaGraph_t G = nullptr;
+        bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraphNode_t wnode = nullptr;
+        cudaGraphConditionalHandle handle;
+        if (ok) ok = cudaGraphConditionalHandleCreate(&handle, G, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        if (ok) ok = cudaStreamBeginCaptureToGraph(k.cap, G, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                     cudaSuccess;
+        if (ok) {
+            prologue(k.cap);
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t cg = nullptr;
+            ok = cudaStreamGetCaptureInfo(k.cap, &cs, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
+                 cs == cudaStreamCaptureStatusActive;
+            std::vector<cudaGraphNode_t> tail(deps, deps + (ok ? ndeps : 0));
+            cudaGraph_t out = nullptr;
+            ok = (cudaStreamEndCapture(k.cap, &out) == cudaSuccess) && ok;
+            if (ok) {
+                cudaGraphNodeParams cp = {};
+                cp.type = cudaGraphNodeTypeConditional;
+                cp.conditional.handle = handle;
+                cp.conditional.type = cudaGraphCondTypeWhile;
+                cp.conditional.size = 1;
+                ok = cudaGraphAddNode(&wnode, G, tail.data(), tail.size(), &cp) == cudaSuccess;
+                cudaGraph_t body = ok ? cp.conditional.phGraph_out[0] : nullptr;
+                if (ok)
+                    ok = cudaStreamBeginCaptureToGraph(k.cap, body, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    iterations(k.cap, every);
+                    bcgs_continue_kernel<<<1, 32, 0, k.cap>>>(handle, k.scal, o.max_it / every);
+                    cudaGraph_t bout = nullptr;
+                    ok = cudaStreamEndCapture(k.cap, &bout) == cudaSuccess;
+                    size_t body_nodes = 0;
+                    // the body must hold the continue test (else the loop could not end)
+                    if (ok) ok = cudaGraphGetNodes(body, nullptr, &body_nodes) == cudaSuccess &&
+                                 body_nodes == (size_t)(7 * every + 1);
+                }
+                if (ok)
+                    ok = cudaStreamBeginCaptureToGraph(k.cap, G, &wnode, nullptr, 1,
+                                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    cudaMemcpyAsync(k.host, k.scal, sizeof(h), cudaMemcpyDeviceToHost, k.cap);
+                    cudaGraph_t eout = nullptr;
+                    ok = cudaStreamEndCapture(k.cap, &eout) == cudaSuccess;
+                }
+            }
+        }
+        if (ok) ok = cudaGraphInstantiate(&k.whole, G, 0) == cudaSuccess;
+        if (!ok) {
+            k.whole = nullptr;
+            k.whole_failed = true;   // the host-driven batches below serve every later solve
+        }
+        if (G) cudaGraphDestroy(G);
+        cudaGetLastError();
+        if (k.whole) {
+            k.w_vals = vals;
+            k.w_b = b;
+            k.w_x = x;
+            k.w_rows = n;
+            k.w_every = every;
+            k.w_max = o.max_it;
+        }
+    }
+    if (k.whole) {
+        KSP_CUDA(cudaGraphLaunch(k.whole, st));
+        KSP_CUDA(cudaStreamSynchronize(st));
+        if (info) {
+            info->reason = k.host->reason == osrk::kItersRunning ? osrk::kDivergedIts : k.host->reason;
+            info->its = k.host->its;
+            info->rnorm0 = k.host->rnorm0;
+            info->rnorm = k.host->rnorm;
+        }
+        return OSR_OK;
+    }
+    prologue(st);
+    KSP_CUDA(cudaGetLastError());
     // the batch graph: every kernel reads its scalars and the solve's status
     // from device memory, so one capture serves every batch of this system
     if (k.batch && (k.g_vals != vals || k.g_x != x || k.g_rows != n || k.g_every != every)) {

@@ -124,6 +124,14 @@ def test_iteration_semantics_match_restatement(name, tmp_path, cuda_device):
         assert (info["reason"], info["its"]) == (reason, its) == (linear.DIVERGED_ITS, k)
         x = d_dx.cpu().numpy()
         assert np.abs(x - x_np).max() <= 1e-9 * np.abs(x_np).max(), k
+    # the whole solve as one graph (the cap a whole number of 8-iteration
+    # batches) and the host-driven batches (a cap that is not) run the same
+    # kernels in the same order: identical iterates
+    info_g = G.ksp_solve(J, d_f, d_dx, max_it=5000)
+    xg = d_dx.clone()
+    info_h = G.ksp_solve(J, d_f, d_dx, max_it=4999)
+    assert (info_g["reason"], info_g["its"]) == (info_h["reason"], info_h["its"])
+    assert torch.equal(xg, d_dx)
     # zero right-hand side
     info = G.ksp_solve(J, torch.zeros_like(d_f), d_dx)
     assert (info["reason"], info["its"], info["rnorm0"]) == (linear.CONVERGED_ATOL, 0, 0.0)
