@@ -485,6 +485,39 @@ osr_status osr_grid_form_jacobian(osr_grid *grid, const double *d_x, double sim_
  * DEVICE pointers; asynchronous on `stream`. */
 osr_status osr_grid_saturation_pressure(osr_grid *grid, int medium, double *d_psat, double *d_xm, void *stream);
 
+/* Saturation-pressure variants the reference keeps without live call sites
+ * (compsim/Do_Cycle.cpp:1576-1605, 1653-1682), on every cell of one
+ * continuum (0 matrix, 1 fracture; the reference's functions read the
+ * matrix):
+ *   kind 0 OSR_SATP_BUBBLE_NR  Bubl_NR (compsim/Minor_NR.cpp:33-266) on oil-only
+ *          cells: Newton on the fugacity equalities and the sum of the
+ *          incipient gas composition, from Wilson K-values at the oil pressure;
+ *   kind 1 OSR_SATP_DEW_NR     Dew_NR (compsim/Minor_NR.cpp:268-489) on gas-only
+ *          cells, from the gas pressure;
+ *   kind 2 OSR_SATP_LOWER_DEW  LowerDew_Succ (compsim/Minor_NR.cpp:2017-2136)
+ *          on gas-only cells: the lower dew point by substitution, 1e100 for a
+ *          trivial solution.
+ * d_psat [cells] the pressure (0 for cells of the other labels); d_xm
+ * [nc][cells] (optional) the incipient composition of the last iterate;
+ * d_status [cells] (optional) osr_cell_status: OSR_CELL_MAXIT where the
+ * Newton forms did not stop within 100 steps (the reference iterates without
+ * a cap), OSR_CELL_NAN for a non-finite pressure; d_iters [cells] (optional)
+ * the steps taken.  DEVICE pointers; asynchronous on `stream`. */
+enum { OSR_SATP_BUBBLE_NR = 0, OSR_SATP_DEW_NR = 1, OSR_SATP_LOWER_DEW = 2 };
+osr_status osr_grid_saturation_pressure_nr(osr_grid *grid, int medium, int kind, double *d_psat, double *d_xm,
+                                           int *d_status, int *d_iters, void *stream);
+
+/* critTest (compsim/Minor_NR.cpp:2138-2308): the successive-substitution
+ * stability test of every one-phase cell of one continuum at its oil
+ * pressure.  An oil-only cell whose flash gives L = 0 becomes gas-only (its
+ * oil composition and saturation move to the gas); a gas-only cell whose
+ * flash gives L = 1 becomes oil-only.  d_L [cells] (optional): the final L
+ * (-1 for two-phase cells); d_changed (optional, one int the caller zeroes):
+ * incremented by the number of relabelled cells.  A relabelled cell changes
+ * the row layout: follow with osr_grid_refresh_layout.  DEVICE pointers;
+ * asynchronous on `stream`. */
+osr_status osr_grid_crit_test(osr_grid *grid, int medium, double *d_L, int *d_changed, void *stream);
+
 /* PhaseCtrl and fPhaseCtrl (compsim/Do_Cycle.cpp:1558-1721) on the current
  * state: phase appearance at 0.95 of the saturation pressure with a new-phase
  * saturation of 1e-3 and the incipient composition, phase disappearance at

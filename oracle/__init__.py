@@ -335,6 +335,8 @@ class RefDeck:
         lib.ref_form_jacobian.restype = ctypes.c_long
         lib.ref_set.restype = ctypes.c_long
         lib.ref_sat_pressure.restype = ctypes.c_double
+        lib.ref_sat_pressure_nr.restype = ctypes.c_double
+        lib.ref_crit_test.restype = ctypes.c_int
         rc = lib.ref_deck_open(path.encode())
         if rc:
             raise RuntimeError(f"reference could not open {path}")
@@ -400,6 +402,19 @@ class RefDeck:
         xm = np.zeros(self.nc)
         p = self.lib.ref_sat_pressure(int(medium), ctypes.c_long(int(cell)), _p(xm))
         return float(p), xm
+
+    def sat_pressure_nr(self, kind: int, cell: int):
+        """(pressure, Xm) of matrix cell ``cell`` from Bubl_NR (kind 0),
+        Dew_NR (1) or LowerDew_Succ (2).  Bubl_NR and Dew_NR have no
+        iteration cap: call them only on cells whose restated iteration
+        stopped."""
+        xm = np.zeros(self.nc)
+        p = self.lib.ref_sat_pressure_nr(int(kind), ctypes.c_long(int(cell)), _p(xm))
+        return float(p), xm
+
+    def crit_test(self, cell: int) -> int:
+        """critTest on one-phase matrix cell ``cell``; its label afterwards."""
+        return int(self.lib.ref_crit_test(ctypes.c_long(int(cell))))
 
     def phase_ctrl(self):
         self.lib.ref_phase_ctrl()

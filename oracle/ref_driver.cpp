@@ -379,6 +379,26 @@ double ref_sat_pressure(int med, long c, double *xm) {
     return p;
 }
 
+/* Bubl_NR (kind 0, an oil-only cell), Dew_NR (kind 1) or LowerDew_Succ
+ * (kind 2, a gas-only cell) on matrix cell c (compsim/Minor_NR.cpp:33-489,
+ * 2017-2136); xm receives Xm[0..Nc-1].  Bubl_NR and Dew_NR iterate without a
+ * cap, so callers pass only cells whose restated iteration stopped. */
+double ref_sat_pressure_nr(int kind, long c, double *xm) {
+    const int Ix = (int)(c % Nx), Iy = (int)((c / Nx) % Ny), Iz = (int)(c / ((long)Nx * Ny));
+    double p = kind == 0 ? Bubl_NR(Ix, Iy, Iz) : kind == 1 ? Dew_NR(Ix, Iy, Iz) : LowerDew_Succ(Ix, Iy, Iz);
+    for (int i = 0; i < Nc; i++) xm[i] = Xm[i];
+    return p;
+}
+
+/* critTest on matrix cell c (compsim/Minor_NR.cpp:2138-2308), as its
+ * commented call site applies it to one-phase cells
+ * (compsim/Do_Cycle.cpp:1576); returns the cell's label afterwards. */
+int ref_crit_test(long c) {
+    const int Ix = (int)(c % Nx), Iy = (int)((c / Nx) % Ny), Iz = (int)(c / ((long)Nx * Ny));
+    if (phaseStat[Ix][Iy][Iz]) critTest(Ix, Iy, Iz);
+    return phaseStat[Ix][Iy][Iz];
+}
+
 /* PhaseCtrl and fPhaseCtrl (compsim/Do_Cycle.cpp:1558-1721). */
 int ref_phase_ctrl(void) {
     PhaseCtrl();

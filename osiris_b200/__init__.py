@@ -647,6 +647,35 @@ class Grid:
                "osr_grid_saturation_pressure")
         return p, xm
 
+    SATP_KINDS = {"bubble_nr": 0, "dew_nr": 1, "lower_dew": 2}
+
+    def saturation_pressure_nr(self, medium: int, kind: str, device, stream=None):
+        """Bubl_NR ("bubble_nr", oil-only cells), Dew_NR ("dew_nr") or
+        LowerDew_Succ ("lower_dew", gas-only cells) on one continuum:
+        (pressure [cells], incipient composition [nc, cells], status [cells],
+        steps [cells]) device tensors; 0 for cells of the other labels."""
+        import torch
+        p = torch.empty(self.cells, dtype=torch.float64, device=device)
+        xm = torch.empty((self.nc, self.cells), dtype=torch.float64, device=device)
+        st = torch.empty(self.cells, dtype=torch.int32, device=device)
+        it = torch.empty(self.cells, dtype=torch.int32, device=device)
+        _check(lib().osr_grid_saturation_pressure_nr(self._h, int(medium), self.SATP_KINDS[kind], _vp(p.data_ptr()),
+                                                     _vp(xm.data_ptr()), _vp(st.data_ptr()), _vp(it.data_ptr()),
+                                                     None if stream is None else _vp(stream)),
+               "osr_grid_saturation_pressure_nr")
+        return p, xm, st, it
+
+    def crit_test(self, medium: int, device, stream=None):
+        """critTest on every one-phase cell of one continuum (relabels the
+        cells found in the other phase): (final L [cells] device tensor,
+        number of relabelled cells)."""
+        import torch
+        L = torch.empty(self.cells, dtype=torch.float64, device=device)
+        changed = torch.zeros(1, dtype=torch.int32, device=device)
+        _check(lib().osr_grid_crit_test(self._h, int(medium), _vp(L.data_ptr()), _vp(changed.data_ptr()),
+                                        None if stream is None else _vp(stream)), "osr_grid_crit_test")
+        return L, int(changed.item())
+
     def phase_ctrl(self, stream=None):
         _check(lib().osr_grid_phase_ctrl(self._h, None if stream is None else _vp(stream)), "osr_grid_phase_ctrl")
 

@@ -44,6 +44,21 @@ static osr_status phase_ctrl_n(osr_grid &g, cudaStream_t st) {
     return OSR_OK;
 }
 
+template <int N>
+static osr_status sat_pressure_nr_n(osr_grid &g, int med, int kind, double *psat, double *xm, int *status, int *iters,
+                                    cudaStream_t st) {
+    sat_pressure_nr_kernel<N><<<phase_blocks(g.cells), 128, 0, st>>>(phase_args<N>(g), med, kind, psat, xm, status, iters);
+    PH_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
+template <int N>
+static osr_status crit_test_n(osr_grid &g, int med, double *lout, int *changed, cudaStream_t st) {
+    crit_test_kernel<N><<<phase_blocks(g.cells), 128, 0, st>>>(phase_args<N>(g), med, lout, changed);
+    PH_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
 #define PH_SWITCH(call)                                                                                   \
     switch (g->nc) {                                                                                      \
         case 1: { constexpr int K = 1; return call; }                                                     \
@@ -74,6 +89,17 @@ extern "C" {
 osr_status osr_grid_saturation_pressure(osr_grid *g, int medium, double *d_psat, double *d_xm, void *stream) {
     if (!g || !d_psat || (medium != 0 && medium != 1)) return OSR_ERR_ARG;
     PH_SWITCH(sat_pressure_n<K>(*g, medium, d_psat, d_xm, (cudaStream_t)stream))
+}
+
+osr_status osr_grid_saturation_pressure_nr(osr_grid *g, int medium, int kind, double *d_psat, double *d_xm,
+                                           int *d_status, int *d_iters, void *stream) {
+    if (!g || !d_psat || (medium != 0 && medium != 1) || kind < 0 || kind > 2) return OSR_ERR_ARG;
+    PH_SWITCH(sat_pressure_nr_n<K>(*g, medium, kind, d_psat, d_xm, d_status, d_iters, (cudaStream_t)stream))
+}
+
+osr_status osr_grid_crit_test(osr_grid *g, int medium, double *d_L, int *d_changed, void *stream) {
+    if (!g || (medium != 0 && medium != 1)) return OSR_ERR_ARG;
+    PH_SWITCH(crit_test_n<K>(*g, medium, d_L, d_changed, (cudaStream_t)stream))
 }
 
 osr_status osr_grid_phase_ctrl(osr_grid *g, void *stream) {
