@@ -383,6 +383,22 @@ osr_status osr_grid_set_well_condition(osr_grid *grid, int well, int latched);
  * compsim/Minor_NR.cpp:2700-3249), formed once per well at create. */
 osr_status osr_grid_well_radius(osr_grid *grid, int well, double *re);
 
+/* Sums over a well's completed layers, both continua, that split the rate of
+ * a rate-controlled well (or a latched one) over its completions inside the
+ * well regions of IteratorFunction (compsim/Petsc_Functions.cpp:164-702,
+ * 3505-4044), taken over this grid's layers [layer0, layer1) at the current
+ * state: d_sums DEVICE [nwells][2 completion continua][5].  A z-slab run
+ * takes them over each rank's owned layers, adds them over the ranks and
+ * hands the totals to osr_grid_set_well_sums, so that a well crossing slabs
+ * sees the same sums as on one grid.  Asynchronous. */
+osr_status osr_grid_well_sums(osr_grid *grid, int layer0, int layer1, double *d_sums, void *stream);
+
+/* Residual and Jacobian take the wells' layer sums from d_sums (DEVICE, the
+ * layout of osr_grid_well_sums; the pointer is kept and read at every
+ * evaluation) instead of summing the grid's own layers; NULL restores the
+ * grid's own sums. */
+osr_status osr_grid_set_well_sums(osr_grid *grid, const double *d_sums);
+
 /* State -> unknowns (InitGuess2, compsim/PetscAUX.cpp:878-964); d_x DEVICE
  * [n_rows]. */
 osr_status osr_grid_init_guess(osr_grid *grid, double *d_x, void *stream);
@@ -571,6 +587,43 @@ osr_status osr_grid_jacobian_apply(osr_grid *grid, const double *d_vals, const d
  * OSR_OK with a negative info->reason, as KSPSolve does. */
 osr_status osr_grid_ksp_solve(osr_grid *grid, const double *d_vals, const double *d_rhs, double *d_sol,
                               const osr_ksp_opts *opts, osr_ksp_info *info, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Distributed linear solve over z-slabs (the multi-rank KSPSolve of the
+ * reference: PETSc's KSPBCGS + PCVPBJACOBI over CreateAllocationTable's row
+ * ownership, compsim/PetscAUX.cpp:1081-1099, with VecDot / VecNorm summed over
+ * the ranks).  Each rank holds one slab grid (its owned layers plus one ghost
+ * layer towards each neighbour) and the slab's compact Jacobian.  The
+ * iteration above is split at its dot products into stages: every stage's
+ * partial sums over the slab's OWNED rows land in d_dots, which the caller
+ * sums over the ranks (an all-reduce on `stream`) before the next stage, and
+ * the caller refills the ghost rows of d_p (after stage 1) and d_s (after
+ * stage 3) from the neighbouring ranks.  Protocol:
+ *   osr_dksp_begin  (dots[0]: sum)   osr_dksp_stage 0
+ *   per iteration:  stage 1 (ghosts of p), 2 (dots[0]: sum), 3 (ghosts of s),
+ *                   4 (dots[0..2]: sum), 5 (dots[0..1]: sum), 6
+ *   osr_dksp_info every few iterations; stop once info.reason != 0.
+ * Every rank takes the same scalar steps from the same sums, so all ranks
+ * stop at the same iteration.  With one rank owning every row the stages
+ * perform the single-grid solve's arithmetic exactly.  The handle shares the
+ * grid's solve workspace: a distributed solve and osr_grid_ksp_solve on the
+ * same grid do not interleave.
+ * ------------------------------------------------------------------------- */
+typedef struct osr_dksp osr_dksp;
+osr_status osr_dksp_create(osr_grid *grid, osr_dksp **out);
+void osr_dksp_destroy(osr_dksp *dksp);
+/* Start solving J x = b from x = 0.  owned[4]: the owned block rows
+ * [owned[0], owned[1]) of the matrix continuum and [owned[2], owned[3]) of
+ * the fracture continuum (cell-medium indices, fracture from `cells`).
+ * d_x, d_p, d_s: the caller's DEVICE vectors of the grid's row count (the
+ * solution, and the two search vectors whose ghost rows the caller fills);
+ * d_dots: at least 3 doubles.  Asynchronous on `stream`. */
+osr_status osr_dksp_begin(osr_dksp *dksp, const double *d_vals, const double *d_b, double *d_x, double *d_p,
+                          double *d_s, const long *owned, const osr_ksp_opts *opts, double *d_dots, void *stream);
+/* One stage (0..6; see above).  Asynchronous on `stream`. */
+osr_status osr_dksp_stage(osr_dksp *dksp, int stage, void *stream);
+/* The solve's state (reason 0 while running).  Synchronises `stream`. */
+osr_status osr_dksp_info(osr_dksp *dksp, osr_ksp_info *info, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Time stepping: one osr_sim_step is one pass of the reference's main loop

@@ -605,6 +605,19 @@ class Grid:
         _check(lib().osr_grid_init_guess(self._h, _vp(d_x.data_ptr()), None if stream is None else _vp(stream)),
                "osr_grid_init_guess")
 
+    def well_sums(self, layer0: int, layer1: int, d_sums, stream=None):
+        """Layer sums of the wells' rate split over layers [layer0, layer1)
+        into d_sums [nwells, 2, 5] (osr_grid_well_sums)."""
+        _check(lib().osr_grid_well_sums(self._h, int(layer0), int(layer1), _vp(d_sums.data_ptr()),
+                                        None if stream is None else _vp(stream)), "osr_grid_well_sums")
+
+    def set_well_sums(self, d_sums):
+        """Take the wells' layer sums from d_sums (kept alive by the caller);
+        None: the grid's own layers."""
+        self._well_sums = d_sums
+        _check(lib().osr_grid_set_well_sums(self._h, None if d_sums is None else _vp(d_sums.data_ptr())),
+               "osr_grid_set_well_sums")
+
     def update_all(self, d_x, stream=None):
         _check(lib().osr_grid_update_all(self._h, _vp(d_x.data_ptr()), None if stream is None else _vp(stream)),
                "osr_grid_update_all")

@@ -293,7 +293,7 @@ static AsmArgs<N> asm_args(const osr_grid &g, double *f, double *fscale, double 
     A.k.re_f = g.re_f;
     A.k.diff_off = (g.const_dif && g.cdif == 0) ? 1 : 0;
     A.k.sf1 = A.k.sf3 = 0;
-    A.w = WellSet{g.nwells > 0 ? g.nwells : 0, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws};
+    A.w = WellSet{g.nwells > 0 ? g.nwells : 0, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws, g.well_sums_ext};
     A.tor = g.tor;
     A.rowoff = g.rowoff;
     A.f = f;
@@ -329,6 +329,14 @@ template <int N>
 static osr_status logk_vjp_n(osr_grid &g, const double *lam, double *gk, double t, cudaStream_t st) {
     AsmArgs<N> A = asm_args<N>(g, nullptr, nullptr, t);
     residual_logk_vjp_kernel<N><<<(unsigned)grid_blocks(g.cells), 128, 0, st>>>(A, lam, gk);
+    ASM_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
+template <int N>
+static osr_status well_sums_n(osr_grid &g, int l0, int l1, double *sums, cudaStream_t st) {
+    if (g.nwells <= 0) return OSR_OK;
+    well_sums_kernel<N><<<(2 * g.nwells + 63) / 64, 64, 0, st>>>(asm_args<N>(g, nullptr, nullptr, 0.0), l0, l1, sums);
     ASM_CUDA(cudaGetLastError());
     return OSR_OK;
 }
@@ -410,6 +418,17 @@ osr_status osr_grid_set_well_condition(osr_grid *g, int well, int latched) {
     if (!g || well < 0 || well >= g->nwells) return OSR_ERR_ARG;
     g->cond_host[well] = latched ? 1 : 0;
     ASM_CUDA(cudaMemcpy(g->d_cond + well, &g->cond_host[well], 1, cudaMemcpyHostToDevice));
+    return OSR_OK;
+}
+
+osr_status osr_grid_well_sums(osr_grid *g, int layer0, int layer1, double *d_sums, void *stream) {
+    if (!g || !d_sums || layer0 < 0 || layer1 < layer0 || layer1 > g->nz) return OSR_ERR_ARG;
+    ASM_SWITCH(well_sums_n<K>(*g, layer0, layer1, d_sums, (cudaStream_t)stream))
+}
+
+osr_status osr_grid_set_well_sums(osr_grid *g, const double *d_sums) {
+    if (!g) return OSR_ERR_ARG;
+    g->well_sums_ext = d_sums;
     return OSR_OK;
 }
 

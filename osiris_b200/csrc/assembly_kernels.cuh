@@ -51,7 +51,15 @@ struct WellSet {
     const double *re;     // [n] Peaceman radius of the matrix completion (Calc_Re)
     const unsigned char *cond;  // [n] WellCondition latch
     const WellStream *ws; // [n]
+    // [n][2][kWellSums] layer sums of the rate split given by the caller (a
+    // z-slab run: the sums over the whole reservoir); null: summed here
+    const double *sums = nullptr;
 };
+
+// Layer sums per well and completion continuum (well_sums_kernel): the sums
+// over the own continuum's and the other continuum's completed layers, then
+// type 6's mobility-fraction sums SSw, SSo, SSg.
+constexpr int kWellSums = 5;
 
 struct AsmScalars {
     double dt, sim_time, pcoeff;
@@ -482,6 +490,8 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
             }
             return acc;
         };
+        // the caller's layer sums of this well and completion continuum, if any
+        const double *wsum = A.w.sums ? A.w.sums + ((long)i * 2 + med) * kWellSums : nullptr;
         auto S1_2pi = [&]() { return 2 * kSIC * kPi * dk[iz] * sqk / own_log(Re); };
         auto S1_plain = [&]() { return dk[iz] * sqrt(O.perm[c] * O.perm[n + c]) / own_log(Re); };
         auto all_pi = [&](double S1) {
@@ -514,9 +524,10 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
             all_pi(S1_2pi());
             producer_signs();
             if (cond) {
-                double SS = layer_sum([&](const MediumFields &M, long cj, double S2) {
-                    return M.rho[n + cj] * S2 * M.kr[2 * n + cj] / M.mu[n + c];
-                });
+                double SS = wsum ? wsum[0] / O.mu[n + c] + wsum[1] / X.mu[n + c]
+                                 : layer_sum([&](const MediumFields &M, long cj, double S2) {
+                                       return M.rho[n + cj] * S2 * M.kr[2 * n + cj] / M.mu[n + c];
+                                   });
                 double S1 = S1_plain();
                 if (SS != 0) r.Qg = -S1 * wf[1] * rho_g * krg / (mu_g * SS);
                 r.Qw = r.Qg * krw * wfac * mu_g / (krg * rho_g * watMu);
@@ -528,7 +539,7 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
             r.Qw = r.PIw * (wf[0] - Pw);
             if (r.Qw < 0 || (r.Qw - r.Qw) != 0) { r.Qw = 0; r.PIw = 0; }
             if (cond) {
-                double SS = layer_sum([&](const MediumFields &M, long cj, double S2) {
+                double SS = wsum ? wsum[0] + wsum[1] : layer_sum([&](const MediumFields &M, long cj, double S2) {
                     return watRo * S2 * M.kr[cj] / watMu;
                 });
                 S1 = S1_plain();
@@ -546,14 +557,19 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
             if (r.Qg < 0 || (r.Qg - r.Qg) != 0) { r.Qg = 0; r.PIg = 0; }
             r.iwell = i;
             if (cond) {
-                double SS = layer_sum([&](const MediumFields &, long, double S2) { return S2; });
+                double SS = wsum ? wsum[0] + wsum[1]
+                                 : layer_sum([&](const MediumFields &, long, double S2) { return S2; });
                 S1 = S1_plain();
                 if (SS != 0) r.Qg = S1 * wf[1] / SS;
                 if (SS != 0) r.Qo = r.Qg * ws.of / ws.gf;
             }
         } else if (type == 4 || type == 5 || type == 6) {  // constant oil / gas / total rate
             double SS, S1 = S1_plain();
-            if (type == 6) {
+            if (type == 6 && wsum) {
+                SS = wsum[0] / O.mu[c] + wsum[1] / X.mu[c];
+                const double QoP = wsum[3] * wf[0] / (wsum[2] + wsum[3] + wsum[4]);
+                if (SS != 0) r.Qo = -S1 * QoP * rho_o * kro / (mu_o * SS);
+            } else if (type == 6) {
                 double SSw = 0, SSo = 0, SSg = 0;
                 SS = 0;
                 for (int j = wi[3]; j <= wi[4]; j++) {
@@ -571,14 +587,16 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
                 const double QoP = SSo * wf[0] / (SSw + SSo + SSg);
                 if (SS != 0) r.Qo = -S1 * QoP * rho_o * kro / (mu_o * SS);
             } else if (type == 4) {
-                SS = layer_sum([&](const MediumFields &M, long cj, double S2) {
-                    return M.rho[cj] * S2 * M.kr[n + cj] / M.mu[c];
-                });
+                SS = wsum ? wsum[0] / O.mu[c] + wsum[1] / X.mu[c]
+                          : layer_sum([&](const MediumFields &M, long cj, double S2) {
+                                return M.rho[cj] * S2 * M.kr[n + cj] / M.mu[c];
+                            });
                 if (SS != 0) r.Qo = -S1 * wf[0] * rho_o * kro / (mu_o * SS);
             } else {
-                SS = layer_sum([&](const MediumFields &M, long cj, double S2) {
-                    return M.rho[n + cj] * S2 * M.kr[2 * n + cj] / M.mu[n + c];
-                });
+                SS = wsum ? wsum[0] / O.mu[n + c] + wsum[1] / X.mu[n + c]
+                          : layer_sum([&](const MediumFields &M, long cj, double S2) {
+                                return M.rho[n + cj] * S2 * M.kr[2 * n + cj] / M.mu[n + c];
+                            });
                 if (SS != 0) r.Qg = -S1 * wf[1] * rho_g * krg / (mu_g * SS);
             }
             if (type == 5) {
@@ -606,7 +624,8 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
         } else if (type == 8) {  // constant gas injection rate
             const WellStream &ws = A.w.ws[i];
             if (med == 0 && Re <= rw) Re += rw;
-            double SS = layer_sum([&](const MediumFields &, long, double S2) { return S2; });
+            double SS = wsum ? wsum[0] + wsum[1]
+                             : layer_sum([&](const MediumFields &, long, double S2) { return S2; });
             double S1 = S1_plain();
             if (SS != 0) r.Qg = S1 * wf[0] / SS;
             if (SS != 0) r.Qo = r.Qg * ws.of / ws.gf;
@@ -626,6 +645,53 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
             r.iwell = i;
         }
     }
+}
+
+// Layer sums of the rate split of every well and completion continuum over
+// the layers [l0, l1) of this grid (the layer_sum terms of well_rates without
+// the completion cell's viscosity, which well_rates divides by; the own and
+// the other continuum summed apart): sums[w][med][kWellSums].  A z-slab run
+// takes them over each rank's owned layers and adds them over the ranks.
+template <int N>
+__global__ void well_sums_kernel(const __grid_constant__ AsmArgs<N> A, int l0, int l1, double *sums) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * A.w.n) return;
+    const int i = t >> 1, med = t & 1;
+    const GridScalars &s = A.a.s;
+    const MediumFields &O = A.a.m[med], &X = A.a.m[1 - med];
+    const long n = s.cells;
+    const double *dk = A.a.geo.dk;
+    const int *wi = A.w.wi + 5 * i;
+    const double *wf = A.w.wf + (long)i * (N + 6);
+    const int type = wi[0], ix = wi[1], iy = wi[2];
+    const double rw = wf[3], skin = wf[2];
+    double Re = med == 0 ? A.w.re[i] : A.k.re_f;
+    if ((type == 3 || type == 8) && med == 0 && Re <= rw) Re += rw;
+    const double own_l = med == 0 ? log(Re / rw) + skin : log((rw + A.k.re_f) / rw) + skin;
+    const double oth_l = med == 0 ? log((rw + A.k.re_f) / rw) + skin : log(Re / rw) + skin;
+    const double watRo = s.wat_ro, watMu = s.wat_mu;
+    double acc[kWellSums] = {0, 0, 0, 0, 0};
+    const int j0 = wi[3] > l0 ? wi[3] : l0, j1 = wi[4] < l1 - 1 ? wi[4] : l1 - 1;
+    for (int j = j0; j <= j1; j++) {
+        const long cj = ix + (long)s.nx * (iy + (long)s.ny * j);
+        for (int pass = 0; pass < 2; pass++) {
+            const MediumFields &M = pass ? X : O;
+            const double S2 = dk[j] * sqrt(M.perm[cj] * M.perm[n + cj]) / (pass ? oth_l : own_l);
+            double term = 0;
+            if (type == 1 || type == 5) term = M.rho[n + cj] * S2 * M.kr[2 * n + cj];
+            else if (type == 2) term = watRo * S2 * M.kr[cj] / watMu;
+            else if (type == 3 || type == 8) term = S2;
+            else if (type == 4 || type == 6) term = M.rho[cj] * S2 * M.kr[n + cj];
+            acc[pass] += term;
+            if (type == 6) {
+                const double mob = (M.kr[cj] / watMu) + (M.kr[n + cj] / M.mu[cj]) + (M.kr[2 * n + cj] / M.mu[n + cj]);
+                acc[2] += (M.kr[cj] / watMu) / mob;
+                acc[3] += (M.kr[n + cj] / M.mu[cj]) / mob;
+                acc[4] += (M.kr[2 * n + cj] / M.mu[n + cj]) / mob;
+            }
+        }
+    }
+    for (int q = 0; q < kWellSums; q++) sums[(long)t * kWellSums + q] = acc[q];
 }
 
 // Well rates and productivity indices of every cell-medium at the current

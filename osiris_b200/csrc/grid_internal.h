@@ -38,6 +38,7 @@ struct osr_grid {
     osr::WellStream *d_ws = nullptr;
     std::vector<double> re_host;
     std::vector<unsigned char> cond_host;
+    const double *well_sums_ext = nullptr;   // caller's layer sums of the rate split (osr_grid_set_well_sums)
     // Jacobian scratch: per cell-medium well rates / productivity indices,
     // injection-well index, injected gas compositions, unsupported-cell count
     double *jw_q = nullptr, *jw_pi = nullptr, *j_stream_y = nullptr;

@@ -180,7 +180,7 @@ static osr_status well_pass(osr_grid &g, double sim_time, cudaStream_t st) {
     A.k.re_f = g.re_f;
     A.k.diff_off = (g.const_dif && g.cdif == 0) ? 1 : 0;
     A.k.sf1 = A.k.sf3 = 0;
-    A.w = WellSet{g.nwells, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws};
+    A.w = WellSet{g.nwells, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws, g.well_sums_ext};
     A.tor = g.tor;
     A.rowoff = g.rowoff;
     A.f = nullptr;

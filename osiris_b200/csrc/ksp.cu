@@ -33,6 +33,19 @@ struct osr_ksp_work {
     bool whole_failed = false;
 };
 
+// One slab's part of a distributed solve (osr_dksp_*): its scalars and the
+// caller's vectors; the other vectors, the block inverses and the partial
+// sums are the grid's solve workspace.
+struct osr_dksp {
+    osr_grid *g = nullptr;
+    osrk::KspScal *scal = nullptr;   // device
+    osrk::KspScal *host = nullptr;   // pinned
+    const double *vals = nullptr, *b = nullptr;
+    double *x = nullptr, *p = nullptr, *s = nullptr, *dots = nullptr;
+    osrk::Owned own;
+    long rows = 0;
+};
+
 namespace osr {
 
 #define KSP_CUDA(call)                                     \
@@ -328,6 +341,59 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     return OSR_OK;
 }
 
+// The set-up (stage -1) or stage 1..6 of one slab's distributed solve (the
+// stage list in ksp_kernels.cuh); stage 0 is the set-up's scalar step.
+template <int N>
+static osr_status dksp_stage_n(osr_dksp &d, int stage, cudaStream_t st) {
+    osr_grid &g = *d.g;
+    osr_ksp_work &k = *g.ksp;
+    const osrk::KView v = kview(g, d.vals);
+    const long n = d.rows, nb = 2 * g.cells;
+    const unsigned vbk = vec_blocks(n), ab = red_blocks(nb, osrk::kApplyThreads);
+    const unsigned xb = red_blocks(n, 4 * osrk::kRedThreads), atb = osrk::kApplyThreads;
+    switch (stage) {
+        case -1:
+            KSP_CUDA(cudaMemcpyAsync(d.scal, d.host, sizeof(osrk::KspScal), cudaMemcpyHostToDevice, st));
+            osrk::bjac_invert_kernel<N><<<inv_blocks(nb), 32 * osrk::kInvWarps, 0, st>>>(v, k.inv, d.scal);
+            osrk::bjac_apply_kernel<N, 0, true><<<ab, atb, 0, st>>>(v, k.inv, d.b, k.r, nullptr, k.part, d.scal,
+                                                                    d.own, d.dots);
+            osrk::bcgs_setup_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.r0, d.p, k.v, d.x);
+            break;
+        case 0:
+            osrk::dksp_scalar_kernel<<<1, 32, 0, st>>>(d.scal, d.dots, 0);
+            break;
+        case 1:
+            osrk::bcgs_p_kernel<<<vbk, 256, 0, st>>>(n, k.r, d.p, k.v, d.scal);
+            break;
+        case 2:
+            spmv_launch<N>(v, d.p, k.t, d.scal, st);
+            osrk::bjac_apply_kernel<N, 1, true><<<ab, atb, 0, st>>>(v, k.inv, k.t, k.v, k.r0, k.part, d.scal,
+                                                                    d.own, d.dots);
+            break;
+        case 3:
+            osrk::dksp_scalar_kernel<<<1, 32, 0, st>>>(d.scal, d.dots, 3);
+            osrk::bcgs_s_kernel<<<vbk, 256, 0, st>>>(n, k.r, k.v, d.s, d.scal);
+            break;
+        case 4:
+            spmv_launch<N>(v, d.s, k.w, d.scal, st);
+            osrk::bjac_apply_kernel<N, 2, true><<<ab, atb, 0, st>>>(v, k.inv, k.w, k.t, d.s, k.part, d.scal,
+                                                                    d.own, d.dots);
+            break;
+        case 5:
+            osrk::dksp_scalar_kernel<<<1, 32, 0, st>>>(d.scal, d.dots, 5);
+            osrk::dbcgs_xr_kernel<<<xb, osrk::kRedThreads, 0, st>>>(n, d.x, d.p, d.s, k.t, k.r, k.r0, g.rowoff,
+                                                                    d.own, k.part, d.dots, d.scal);
+            break;
+        case 6:
+            osrk::dksp_scalar_kernel<<<1, 32, 0, st>>>(d.scal, d.dots, 6);
+            break;
+        default:
+            return OSR_ERR_ARG;
+    }
+    KSP_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
 #define KSP_SWITCH(call)                                                                                  \
     switch (g->nc) {                                                                                      \
         case 1: { constexpr int K = 1; return call; }                                                     \
@@ -365,6 +431,80 @@ void osr_ksp_default_opts(osr_ksp_opts *o) {
 osr_status osr_grid_jacobian_apply(osr_grid *g, const double *d_vals, const double *d_x, double *d_y, void *stream) {
     if (!g || !d_vals || !d_x || !d_y || !g->rowoff || g->n_rows <= 0) return OSR_ERR_ARG;
     KSP_SWITCH(osr::spmv_n<K>(*g, d_vals, d_x, d_y, (cudaStream_t)stream))
+}
+
+osr_status osr_dksp_create(osr_grid *g, osr_dksp **out) {
+    if (!g || !out) return OSR_ERR_ARG;
+    osr_status rc = osr::ksp_ensure(*g);
+    if (rc != OSR_OK) return rc;
+    osr_dksp *d = new osr_dksp();
+    d->g = g;
+    if (cudaMalloc((void **)&d->scal, sizeof(osrk::KspScal)) != cudaSuccess ||
+        cudaMallocHost((void **)&d->host, sizeof(osrk::KspScal)) != cudaSuccess) {
+        osr_dksp_destroy(d);
+        return OSR_ERR_CUDA;
+    }
+    *out = d;
+    return OSR_OK;
+}
+
+void osr_dksp_destroy(osr_dksp *d) {
+    if (!d) return;
+    if (d->scal) cudaFree(d->scal);
+    if (d->host) cudaFreeHost(d->host);
+    delete d;
+}
+
+osr_status osr_dksp_begin(osr_dksp *d, const double *d_vals, const double *d_b, double *d_x, double *d_p,
+                          double *d_s, const long *owned, const osr_ksp_opts *opts, double *d_dots, void *stream) {
+    if (!d || !d_vals || !d_b || !d_x || !d_p || !d_s || !owned || !d_dots) return OSR_ERR_ARG;
+    osr_grid *g = d->g;
+    if (!g->rowoff || g->n_rows <= 0 || !g->ksp) return OSR_ERR_ARG;
+    const long nb = 2 * g->cells;
+    if (!(0 <= owned[0] && owned[0] <= owned[1] && owned[1] <= g->cells && g->cells <= owned[2] &&
+          owned[2] <= owned[3] && owned[3] <= nb))
+        return OSR_ERR_ARG;
+    osr_ksp_opts o;
+    osr_ksp_default_opts(&o);
+    if (opts) o = *opts;
+    if (o.max_it < 0 || !(o.rtol >= 0) || !(o.atol >= 0)) return OSR_ERR_ARG;
+    d->vals = d_vals;
+    d->b = d_b;
+    d->x = d_x;
+    d->p = d_p;
+    d->s = d_s;
+    d->dots = d_dots;
+    d->own.b0 = owned[0];
+    d->own.b1 = owned[1];
+    d->own.b2 = owned[2];
+    d->own.b3 = owned[3];
+    d->rows = g->n_rows;
+    std::memset(d->host, 0, sizeof(osrk::KspScal));
+    d->host->rtol = o.rtol;
+    d->host->atol = o.atol;
+    d->host->dtol = o.dtol;
+    d->host->max_it = o.max_it;
+    KSP_SWITCH(osr::dksp_stage_n<K>(*d, -1, (cudaStream_t)stream))
+}
+
+osr_status osr_dksp_stage(osr_dksp *d, int stage, void *stream) {
+    if (!d || !d->vals || stage < 0 || stage > 6) return OSR_ERR_ARG;
+    osr_grid *g = d->g;
+    if (g->n_rows != d->rows) return OSR_ERR_ARG;   // the layout changed since osr_dksp_begin
+    KSP_SWITCH(osr::dksp_stage_n<K>(*d, stage, (cudaStream_t)stream))
+}
+
+osr_status osr_dksp_info(osr_dksp *d, osr_ksp_info *info, void *stream) {
+    if (!d || !info) return OSR_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(d->host, d->scal, sizeof(osrk::KspScal), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return OSR_ERR_CUDA;
+    info->reason = d->host->reason;
+    info->its = d->host->its;
+    info->rnorm0 = d->host->rnorm0;
+    info->rnorm = d->host->rnorm;
+    return OSR_OK;
 }
 
 osr_status osr_grid_ksp_solve(osr_grid *g, const double *d_vals, const double *d_rhs, double *d_sol,

@@ -434,12 +434,23 @@ __device__ __forceinline__ void converged_test(KspScal *s, double rnorm) {
 // ---------------------------------------------------------------------------
 constexpr int kApplyThreads = 128;
 
-template <int N, int MODE>
+// Owned block rows of one slab in a z-slab decomposition: [b0, b1) in the
+// matrix continuum, [b2, b3) in the fracture continuum (local numbering).
+struct Owned {
+    long b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+    __device__ __forceinline__ bool block(long b) const { return (b >= b0 && b < b1) || (b >= b2 && b < b3); }
+};
+
+// DIST: the distributed form (one slab): the dot products are summed over
+// the owned block rows only and written to dots[] for the host to sum over
+// the slabs; the scalar step is left to dksp_scalar_kernel.
+template <int N, int MODE, bool DIST = false>
 __global__ void __launch_bounds__(kApplyThreads) bjac_apply_kernel(const KView v, const double *__restrict__ inv,
                                                                     const double *__restrict__ r,
                                                                     double *__restrict__ z,
                                                                     const double *__restrict__ a, double *part,
-                                                                    KspScal *s) {
+                                                                    KspScal *s, Owned own = Owned(),
+                                                                    double *dots = nullptr) {
     if (s->reason != kItersRunning) return;
     constexpr int BS = 2 * N + 4;
     const long nb = 2 * v.n;
@@ -461,11 +472,13 @@ __global__ void __launch_bounds__(kApplyThreads) bjac_apply_kernel(const KView v
             for (int i = 0; i < BS; i++)
                 if (i < bs) zv[i] += __ldg(ib + 32 * (j * BS + i)) * rv[j];
         }
+        const bool count = !DIST || own.block(b);
 #pragma unroll
         for (int i = 0; i < BS; i++) {
             if (i >= bs) break;
             const double t = zv[i];
             z[off + i] = t;
+            if (!count) continue;
             if (MODE == 0) {
                 acc[0] += t * t;
             } else if (MODE == 1) {
@@ -480,6 +493,11 @@ __global__ void __launch_bounds__(kApplyThreads) bjac_apply_kernel(const KView v
     }
     double tot[kParts];
     if (!publish_partials<kParts>(acc, part, s, tot)) return;
+    if (DIST) {
+#pragma unroll
+        for (int q = 0; q < kParts; q++) dots[q] = tot[q];
+        return;
+    }
     if (MODE == 0) {
         // set-up of KSPSolve_BCGS: |r_0| and the convergence test at iteration 0
         const double rn = sqrt(tot[0]);
@@ -588,6 +606,120 @@ __global__ void __launch_bounds__(256) bcgs_setup_kernel(long n, const double *_
         p[i] = 0;
         v[i] = 0;
         x[i] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Distributed form: one slab of a z-slab decomposition runs the iteration
+// above split at its dot products (PETSc runs KSPBCGS the same way over MPI
+// ranks, with VecDot / VecNorm reductions across the ranks).  Each stage's
+// dot products are summed over the slab's owned rows into dots[]; the host
+// sums dots[] over the slabs (an all-reduce, stream-ordered) and the next
+// stage's dksp_scalar_kernel takes the scalar step from the sums.  Vector
+// updates run over every local row; the host refills the ghost rows of p and
+// s from the neighbouring slabs before each product.  Stages of one
+// iteration:
+//   1  p <- r + beta (p - omega_old v)                     [ghost rows of p]
+//   2  t <- A p, v <- B t, dots = (v, r0)                  [sum]
+//   3  alpha; s <- r - alpha v                             [ghost rows of s]
+//   4  w <- A s, t <- B w, dots = (s, t) (t, t) (s, s)     [sum]
+//   5  omega; x += alpha p + omega s, r <- s - omega t, dots = |r|^2 (r, r0)
+//                                                          [sum]
+//   6  convergence test, rho, beta
+// The set-up (r <- B b, dots = |r|^2 [sum]) is followed by stage 0, the
+// set-up's scalar step.  Every slab takes the same scalar steps from the
+// same sums, so all slabs stop at the same iteration.
+// ---------------------------------------------------------------------------
+
+// x += alpha p + omega s; r <- s - omega t; |r|^2 and (r, r0) over the owned
+// rows ([rowoff[b0], rowoff[b1]) and [rowoff[b2], rowoff[b3])) into dots.
+__global__ void __launch_bounds__(kRedThreads) dbcgs_xr_kernel(long n, double *__restrict__ x,
+                                                                const double *__restrict__ p,
+                                                                const double *__restrict__ sv,
+                                                                const double *__restrict__ t,
+                                                                double *__restrict__ r,
+                                                                const double *__restrict__ r0,
+                                                                const long *__restrict__ rowoff, Owned own,
+                                                                double *part, double *dots, KspScal *s) {
+    const int reason = s->reason;
+    if (reason != kItersRunning && reason != kFinishWithP) return;
+    const long m0 = rowoff[own.b0], m1 = rowoff[own.b1], f0 = rowoff[own.b2], f1 = rowoff[own.b3];
+    const double alpha = s->alpha, omega = s->omega;
+    double acc[2] = {0, 0};
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        if (reason == kFinishWithP) {
+            x[i] += alpha * p[i];
+            continue;
+        }
+        const double si = sv[i];
+        x[i] += alpha * p[i] + omega * si;
+        const double ri = si - omega * t[i];
+        r[i] = ri;
+        if ((i >= m0 && i < m1) || (i >= f0 && i < f1)) {
+            acc[0] += ri * ri;
+            acc[1] += ri * r0[i];
+        }
+    }
+    double tot[2];
+    if (!publish_partials<2>(acc, part, s, tot)) return;
+    dots[0] = tot[0];
+    dots[1] = tot[1];
+}
+
+// The scalar step of a stage from the summed dot products (the tails of
+// bjac_apply_kernel MODE 0 / 1 / 2 and bcgs_xr_kernel above).
+__global__ void dksp_scalar_kernel(KspScal *s, const double *dots, int stage) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (stage == 0) {
+        const double rn = sqrt(dots[0]);
+        s->rnorm0 = rn;
+        s->rnorm = rn;
+        s->ttol = fmax(s->rtol * rn, s->atol);
+        s->its = 0;
+        converged_test(s, rn);
+        s->rho = dots[0];
+        s->rhoold = 1.0;
+        s->alpha = 1.0;
+        s->omegaold = 1.0;
+        s->beta = (s->rho / s->rhoold) * (s->alpha / s->omegaold);
+    } else if (stage == 3) {
+        if (s->reason != kItersRunning) return;
+        const double d1 = dots[0];
+        if (!isfinite(d1)) s->reason = kDivergedNanOrInf;
+        else if (d1 == 0.0) s->reason = kDivergedBreakdown;
+        else s->alpha = s->rho / d1;
+    } else if (stage == 5) {
+        if (s->reason != kItersRunning) return;
+        const double d1 = dots[0], d2 = dots[1], ss = dots[2];
+        if (d2 == 0.0) {
+            if (ss != 0.0) {
+                s->reason = kDivergedBreakdown;
+            } else {
+                s->omega = 0.0;
+                s->its += 1;
+                s->rnorm = 0.0;
+                s->reason = kFinishWithP;
+            }
+        } else {
+            s->omega = d1 / d2;
+        }
+    } else if (stage == 6) {
+        if (s->reason == kFinishWithP) {
+            s->reason = kConvergedRtol;
+            return;
+        }
+        if (s->reason != kItersRunning) return;
+        const double dp = sqrt(dots[0]);
+        const double rho = s->rho, omega = s->omega;
+        s->rhoold = rho;
+        s->omegaold = omega;
+        s->its += 1;
+        s->rnorm = dp;
+        converged_test(s, dp);
+        if (s->reason == kItersRunning && rho == 0.0) s->reason = kDivergedBreakdown;
+        if (s->reason == kItersRunning && s->its >= s->max_it) s->reason = kDivergedIts;
+        s->rho = dots[1];
+        s->beta = (s->rho / s->rhoold) * (s->alpha / s->omegaold);
     }
 }
 

@@ -20,10 +20,20 @@ grid:
   (``torch.distributed.all_reduce`` with MAX);
 * the rows of the owned layers are the rank's part of the global residual
   (``owned_blocks``); ghost rows are discarded (their outer faces are
-  missing).
+  missing);
+* the linear solve is distributed the way PETSc distributes KSPBCGS +
+  PCVPBJACOBI over MPI ranks: every rank iterates on its slab's Jacobian,
+  the dot products are summed over the ranks, and the search vectors' ghost
+  layers are refreshed from the neighbours before each matrix-vector product
+  (``SlabSolve``, ``solve_slabs``; the device stages are osr_dksp_* of the C
+  library, the sums an all-reduce on the launching stream).
 
-Decks with wells are not split: a rate-controlled well distributes its rate
-over all its completions, which would couple slabs.
+Wells go to every slab with their completions cut to the slab's layers. A
+rate-controlled (or latched) well splits its rate over all its completions
+by sums over its completed layers; each rank takes those sums over its owned
+layers (osr_grid_well_sums), the ranks add them (all-reduce) and every slab
+evaluates its completions with the totals (osr_grid_set_well_sums), so a
+well crossing slabs sees the sums of the whole reservoir.
 """
 from __future__ import annotations
 
@@ -48,10 +58,18 @@ def ghost_range(nz: int, z0: int, z1: int):
 
 
 def sub_deck(d, lo: int, hi: int):
-    """The deck restricted to layers [lo, hi)."""
-    if d.wells_i is not None and len(d.wells_i):
-        raise ValueError("decks with wells are not split into slabs")
+    """The deck restricted to layers [lo, hi).  Every well is kept (the
+    ranks hold the same well list), its completed layers cut to [lo, hi) and
+    renumbered; a well with none there keeps an empty range (first layer
+    after the last)."""
     s = copy.copy(d)
+    if d.wells_i is not None and len(d.wells_i):
+        wi = np.array(d.wells_i, dtype=np.int64)
+        k0, k1 = np.maximum(wi[:, 3], lo) - lo, np.minimum(wi[:, 4], hi - 1) - lo
+        empty = k0 > k1
+        wi[:, 3] = np.where(empty, 1, k0)
+        wi[:, 4] = np.where(empty, 0, k1)
+        s.wells_i = wi
     nxy = d.nx * d.ny
     a, b = lo * nxy, hi * nxy
     s.nz = hi - lo
@@ -189,12 +207,41 @@ class Slab:
         fs = self.frac_start()
         return (to_global(r[keep], fs, own, offsets), to_global(c[keep], fs, own, offsets), v[keep])
 
+    def ksp_solve(self, vals, b, x, check_every: int = 8, **opts) -> dict:
+        """Distributed solve of the global Newton system: this rank's slab
+        Jacobian vals, right-hand side b and solution x in the local row
+        layout (ghost rows of x are not set)."""
+        part = SlabSolve(self.grid, self.deck.nx, self.deck.ny, self.z0, self.z1, self.lo, self.hi)
+        try:
+            part.begin(vals, b, x, **opts)
+            return solve_slabs([part], RankComm(self.rank, self.group), check_every)
+        finally:
+            part.close()
+
     def form_function(self, x_local, f_local, sim_time: float):
         """Exchange the ghost layers' unknowns, then UpdateAll + residual on
-        the whole local grid; the owned rows of f_local are this rank's part."""
+        the whole local grid (with the wells' layer sums added over the
+        ranks); the owned rows of f_local are this rank's part.  The grid's
+        Jacobian evaluated next uses the same sums."""
         exchange_ghost_unknowns(x_local, self._rowoff, self.deck.nx, self.deck.ny, self.hi - self.lo,
                                 self.z0 > 0, self.z1 < self.deck.nz, self.rank, self.group)
-        self.grid.form_function(x_local, f_local, sim_time)
+        self.grid.update_all(x_local)
+        self.sum_wells(x_local.device)
+        self.grid.residual(f_local, None, sim_time)
+
+    def sum_wells(self, device=None):
+        """The wells' layer sums over the owned layers, added over the ranks
+        and handed to the grid (no-op without wells)."""
+        import torch
+        import torch.distributed as dist
+        nw = 0 if self.deck.wells_i is None else len(self.deck.wells_i)
+        if nw == 0:
+            return
+        if getattr(self, "_wsums", None) is None or self._wsums.device != torch.device(device):
+            self._wsums = torch.zeros((nw, 2, 5), dtype=torch.float64, device=device)
+        self.grid.well_sums(self.z0 - self.lo, self.z1 - self.lo, self._wsums)
+        dist.all_reduce(self._wsums, op=dist.ReduceOp.SUM, group=self.group)
+        self.grid.set_well_sums(self._wsums)
 
 
 def global_offsets(owned_counts, rank: int):
@@ -218,3 +265,118 @@ def to_global(idx, frac_start: int, owned_local, offsets):
     idx = np.asarray(idx)
     return np.where(idx >= frac_start, idx + (offsets[1] - owned_local[1][0]),
                     idx + (offsets[0] - owned_local[0][0]))
+
+
+class SlabSolve:
+    """One slab's part of the distributed linear solve (osr_dksp_*): the
+    handle, the search vectors p and s whose ghost rows ``solve_slabs``
+    refreshes, and the partial sums ``dots`` it sums over the slabs."""
+
+    def __init__(self, grid, nx: int, ny: int, z0: int, z1: int, lo: int, hi: int):
+        import ctypes
+
+        from . import _check, lib
+        self.grid, self.nx, self.ny = grid, nx, ny
+        self.nz_local = hi - lo
+        self.has_lower, self.has_upper = z0 > lo, z1 < hi
+        nxy, nl = nx * ny, grid.cells
+        self.owned = [(z0 - lo) * nxy, (z1 - lo) * nxy, nl + (z0 - lo) * nxy, nl + (z1 - lo) * nxy]
+        h = ctypes.c_void_p()
+        _check(lib().osr_dksp_create(grid._h, ctypes.byref(h)), "osr_dksp_create")
+        self._h = h
+        self.rowoff = None
+        self.p = self.s = self.dots = None
+
+    def close(self):
+        from . import lib
+        if self._h:
+            lib().osr_dksp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _stream(self, device):
+        import torch
+        return torch.cuda.current_stream(device).cuda_stream
+
+    def begin(self, vals, b, x, **opts):
+        """Set-up of J x = b on this slab from x = 0 (vectors in the slab's
+        local row layout, on the device)."""
+        import ctypes
+
+        import torch
+
+        from . import _check, _vp, ksp_opts, lib
+        self.rowoff = self.grid.row_offsets()
+        rows = int(self.rowoff[-1])
+        self.p = torch.zeros(rows, dtype=torch.float64, device=x.device)
+        self.s = torch.zeros_like(self.p)
+        self.dots = torch.zeros(4, dtype=torch.float64, device=x.device)
+        self._dev = x.device
+        o = ksp_opts(**opts)
+        owned = (ctypes.c_long * 4)(*self.owned)
+        self._keep = (vals, b, x)
+        _check(lib().osr_dksp_begin(self._h, _vp(vals.data_ptr()), _vp(b.data_ptr()), _vp(x.data_ptr()),
+                                    _vp(self.p.data_ptr()), _vp(self.s.data_ptr()), owned, ctypes.byref(o),
+                                    _vp(self.dots.data_ptr()), _vp(self._stream(self._dev))), "osr_dksp_begin")
+
+    def stage(self, k: int):
+        from . import _check, _vp, lib
+        _check(lib().osr_dksp_stage(self._h, int(k), _vp(self._stream(self._dev))), "osr_dksp_stage")
+
+    def info(self) -> dict:
+        import ctypes
+
+        from . import KspInfo, _check, _vp, lib
+        i = KspInfo()
+        _check(lib().osr_dksp_info(self._h, ctypes.byref(i), _vp(self._stream(self._dev))), "osr_dksp_info")
+        return {"reason": i.reason, "its": i.its, "rnorm0": i.rnorm0, "rnorm": i.rnorm}
+
+
+class RankComm:
+    """The sums and ghost exchanges of ``solve_slabs`` between ranks, over
+    ``torch.distributed`` (NCCL between GPUs, gloo between CPU processes);
+    each rank passes its one part."""
+
+    def __init__(self, rank: int, group=None):
+        self.rank, self.group = rank, group
+
+    def sum(self, parts, k: int):
+        import torch.distributed as dist
+        dist.all_reduce(parts[0].dots[:k], op=dist.ReduceOp.SUM, group=self.group)
+
+    def exchange(self, parts, name: str):
+        q = parts[0]
+        exchange_ghost_unknowns(getattr(q, name), q.rowoff, q.nx, q.ny, q.nz_local, q.has_lower, q.has_upper,
+                                self.rank, self.group)
+
+
+# the collective after each stage of one iteration: a sum of k partial sums,
+# or a ghost refresh of a search vector
+_STAGES = ((1, ("exchange", "p")), (2, ("sum", 1)), (3, ("exchange", "s")), (4, ("sum", 3)), (5, ("sum", 2)),
+           (6, None))
+
+
+def solve_slabs(parts, comm, check_every: int = 8) -> dict:
+    """Run the distributed iteration to its end on parts whose ``begin`` was
+    called: every stage on every part, then the stage's collective through
+    ``comm`` (``sum(parts, k)``, ``exchange(parts, name)``); the state is
+    read back every ``check_every`` iterations.  Every rank takes the same
+    steps in the same order, so the collectives match across ranks."""
+    comm.sum(parts, 1)
+    for q in parts:
+        q.stage(0)
+    while True:
+        info = parts[0].info()
+        if info["reason"] != 0:
+            return info
+        for _ in range(max(1, check_every)):
+            for k, after in _STAGES:
+                for q in parts:
+                    q.stage(k)
+                if after is not None:
+                    getattr(comm, after[0])(parts, after[1])

@@ -83,10 +83,19 @@ def test_ranges_and_sub_deck(tmp_path):
     assert s.nz == 3 and np.array_equal(s.dk, d.dk[1:4])
     assert np.array_equal(s.perm, d.perm[:, nxy:4 * nxy]) and np.array_equal(s.z0, d.z0[:, nxy:4 * nxy])
     assert np.array_equal(s.por, d.por[nxy:4 * nxy])
-    with pytest.raises(ValueError):
-        path2 = os.path.join(str(tmp_path), "w.dat")
-        deck.write_deck(path2, deck.config_deck(nx=3, ny=2, nz=5))
-        slabs.sub_deck(deck.parse_deck(path2), 0, 2)
+    # wells are kept with their completed layers cut to the slab and renumbered
+    path2 = os.path.join(str(tmp_path), "w.dat")
+    spec = deck.config_deck(nx=3, ny=2, nz=5)
+    spec["wells"][1][3:5] = [4, 5]                  # producer completed in layers 4..5 (1-based)
+    deck.write_deck(path2, spec)
+    dw = deck.parse_deck(path2)
+    assert dw.wells_i[:, 3:5].tolist() == [[0, 4], [3, 4]]
+    sw = slabs.sub_deck(dw, 1, 4)
+    assert sw.wells_i[:, 3:5].tolist() == [[0, 2], [2, 2]]
+    assert np.array_equal(sw.wells_i[:, :3], dw.wells_i[:, :3]) and np.array_equal(sw.wells_f, dw.wells_f)
+    s0 = slabs.sub_deck(dw, 0, 2)
+    assert s0.wells_i[:, 3:5].tolist() == [[0, 1], [1, 0]]   # no producer layer here: an empty range
+    assert dw.wells_i[:, 3:5].tolist() == [[0, 4], [3, 4]]   # the deck itself is unchanged
 
 
 def test_global_offsets_and_mapping():
