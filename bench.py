@@ -376,8 +376,11 @@ def cpu_instance_sample(groups, k: int = 64):
 
 
 def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max_over_ranks, gpu_id, world, cpu):
-    """The uneven-instance flash: one osr_flash_batch_instances call per
-    component count, the calls on separate streams inside one timed step."""
+    """The uneven-instance flash.  A step is one launch of the flash plan's
+    CUDA graph (osr_flash_plan_run: every component count's passes and
+    derivative passes, each on its own branch); the same work as one
+    osr_flash_batch_instances call per component count on separate streams
+    is timed beside it."""
     import numpy as np
     G = []
     for g in groups:
@@ -390,7 +393,7 @@ def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max
     n_total = sum(t["n"] for t in G)
     n_inst = sum(len(t["fluids"]) for t in G)
 
-    def step():
+    def step_streams():
         ev = torch.cuda.Event()
         ev.record(stream)
         ends = []
@@ -404,22 +407,45 @@ def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max
         for e in ends:
             stream.wait_event(e)
 
-    for _ in range(max(args.warmup, 1)):
-        step()
-    torch.cuda.synchronize(dev)
+    # the project's autotuner picks each component count's launch shape on
+    # its group (first member's table) before the graph is captured
+    tuned = {}
+    if not args.no_autotune:
+        for t in G:
+            tuned[str(t["nc"])] = osr.autotune(t["fluids"][0], t["P"], t["T"], t["z"])
+        osr.use_tuned(True)
+        torch.cuda.synchronize(dev)
+    plan = osr.FlashPlan([dict(fluids=t["fluids"], start=t["start"], P=t["P"], T=t["T"], z=t["z"], out=t["out"])
+                          for t in G])
+
+    def step():
+        plan.run(stream)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize(dev)
+        out = []
+        for _ in range(args.steps):
+            flush.zero_()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            fn()
+            s1.record(stream)
+            torch.cuda.synchronize(dev)
+            out.append(s0.elapsed_time(s1))
+        return out
+
+    ms_streams = timed(step_streams)
     barrier()
     clocks = ClockSampler(gpu_id)
-    ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        step()
-        s1.record(stream)
-        torch.cuda.synchronize(dev)
-        ms.append(s0.elapsed_time(s1))
+    ms = timed(step)
     clk = clocks.stop()
     barrier()
+    m_streams = max_over_ranks(sum(ms_streams) / len(ms_streams))
+    plan.close()
+    if tuned:
+        osr.use_tuned(False)
     m = max_over_ranks(sum(ms) / len(ms))
     two_phase = float(sum(float((t["out"]["label"] == 0).sum().item()) for t in G) / n_total)
     # one instance per launch (plain kernel; batched kernel), on every 16th instance
@@ -462,8 +488,12 @@ def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max
         "config": {"workload": f"{n_inst} instances, log-uniform 1,000-64,000 cells, 3-12 components, PR or SRK, "
                                "seeded tables; P~U(5,40) MPa, T~U(300,450) K, z~Dirichlet(1); with fugacity "
                                "derivatives", "cells": n_total, "instances": n_inst,
-                   "calls_per_step": len(G), "streams": len(G), "two_phase_fraction": two_phase,
+                   "launches_per_step": 1, "launch": "one CUDA graph (osr_flash_plan_run)",
+                   "tuned_shapes": tuned or None,
+                   "graph_branches": len(G), "two_phase_fraction": two_phase,
                    "l2": "flushed before every step (256 MiB write)"},
+        "streams_form": {"value": world * n_total / (m_streams * 1e-3), "ms_per_step": m_streams,
+                         "calls_per_step": len(G), "streams": len(G)},
         "one_instance_per_launch": forms,
         "batched_over_plain": (world * n_total / (m * 1e-3)) / forms["plain"]["value"],
         "cpu_baseline": cpu_line,

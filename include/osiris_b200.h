@@ -125,6 +125,29 @@ osr_status osr_flash_batch_instances(const osr_fluid *fluids, int n_inst, const 
                                      const double *d_T, const double *d_z, long n, const osr_flash_out *out,
                                      void *stream);
 
+/* A fixed batch of instance groups flashed as one CUDA graph (the batched
+ * step of many uneven instances): each group is one osr_flash_batch_instances
+ * call's worth (instances of one component count, their cells contiguous).
+ * osr_flash_plan_create uploads every group's tables, allocates its scratch
+ * and captures all groups' passes and derivative passes, each group on its
+ * own branch, into one graph; osr_flash_plan_run is then one graph launch
+ * that gives every cell exactly osr_flash_batch_instances's result (the same
+ * kernels and launch shapes).  The groups' device pointers (inputs, outputs)
+ * are kept by the plan: refill the inputs in place between runs.  Host
+ * arrays are read during create only. */
+typedef struct {
+    const osr_fluid *fluids;    /* HOST [n_inst], one component count */
+    int n_inst;
+    const long *inst_start;     /* HOST [n_inst + 1], cells of each instance */
+    const double *d_P, *d_T, *d_z;
+    long n;                     /* cells of the group */
+    const osr_flash_out *out;   /* HOST struct of DEVICE outputs */
+} osr_flash_group;
+typedef struct osr_flash_plan osr_flash_plan;
+osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, osr_flash_plan **out);
+osr_status osr_flash_plan_run(osr_flash_plan *plan, void *stream);
+void osr_flash_plan_destroy(osr_flash_plan *plan);
+
 /* Same results, plain form: one thread per cell, no work queue.  Kept as the
  * baseline the batched form is measured against. */
 osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, const double *d_T,

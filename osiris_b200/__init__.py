@@ -339,6 +339,53 @@ def flash_instances(fluids, start, P, T, z, derivs: bool = True, out: dict | Non
     return out
 
 
+class _CFlashGroup(ctypes.Structure):
+    _fields_ = [("fluids", _vp), ("n_inst", ctypes.c_int), ("inst_start", _vp), ("d_P", _vp), ("d_T", _vp),
+                ("d_z", _vp), ("n", ctypes.c_long), ("out", _vp)]
+
+
+class FlashPlan:
+    """Instance groups of several component counts flashed as one CUDA graph
+    (osr_flash_plan_*): ``groups`` a list of dicts with ``fluids`` (list of
+    Fluid, one component count), ``start`` (host int64 cell offsets), device
+    tensors ``P``, ``T``, ``z`` and an output dict ``out``.  ``run`` is one
+    graph launch; refill the input tensors in place between runs."""
+
+    def __init__(self, groups):
+        self.groups = groups       # keeps the device tensors alive
+        keep, cg = [], []
+        for g in groups:
+            fl = g["fluids"]
+            arr = (_CFluid * len(fl))(*[f._c for f in fl])
+            start = np.ascontiguousarray(g["start"], dtype=np.int64)
+            co = _out_struct(g["out"], lambda t: _vp(t.data_ptr()))
+            keep += [arr, start, co]
+            cg.append(_CFlashGroup(ctypes.cast(arr, _vp), len(fl), _vp(start.ctypes.data), _vp(g["P"].data_ptr()),
+                                   _vp(g["T"].data_ptr()), _vp(g["z"].data_ptr()), int(g["P"].shape[0]),
+                                   ctypes.cast(ctypes.pointer(co), _vp)))
+        garr = (_CFlashGroup * len(cg))(*cg)
+        h = _vp()
+        _check(lib().osr_flash_plan_create(garr, len(cg), ctypes.byref(h)), "osr_flash_plan_create")
+        self._h = h
+
+    def run(self, stream=None):
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(self.groups[0]["P"].device)
+        _check(lib().osr_flash_plan_run(self._h, _vp(stream.cuda_stream)), "osr_flash_plan_run")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().osr_flash_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def set_shape(ss_batch: int, tail_batch: int, ctas_per_sm: int, park_after: int):
     _check(lib().osr_flash_set_shape(int(ss_batch), int(tail_batch), int(ctas_per_sm), int(park_after)),
            "osr_flash_set_shape")

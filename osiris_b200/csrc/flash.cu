@@ -457,6 +457,43 @@ static osr_status run_instances_n(const osr_fluid *fluids, int n_inst, const lon
 }
 
 // ---------------------------------------------------------------------------
+// Flash plan: a fixed set of instance groups (one component count each) whose
+// tables and scratch are uploaded and allocated once, and whose passes and
+// derivative passes, every group on its own branch, are captured into one
+// CUDA graph; a step is then one graph launch.
+
+struct PlanGroup {
+    void *tables = nullptr;
+    long *start = nullptr;
+    char *scratch = nullptr;
+};
+
+template <int N>
+static osr_status plan_prepare_n(const osr_flash_group &gr, PlanGroup &pg, std::vector<void *> &bufs) {
+    std::vector<FluidTable<N>> tabs((size_t)gr.n_inst);
+    for (int i = 0; i < gr.n_inst; i++) make_table<N>(gr.fluids[i], tabs[i]);
+    const size_t tb = tabs.size() * sizeof(FluidTable<N>), sb = (size_t)(gr.n_inst + 1) * sizeof(long);
+    OSR_CUDA(cudaMalloc(&pg.tables, tb));
+    bufs.push_back(pg.tables);
+    OSR_CUDA(cudaMalloc((void **)&pg.start, sb));
+    bufs.push_back(pg.start);
+    OSR_CUDA(cudaMalloc((void **)&pg.scratch, queue_scratch_bytes(gr.n, N)));
+    bufs.push_back(pg.scratch);
+    OSR_CUDA(cudaMemcpy(pg.tables, tabs.data(), tb, cudaMemcpyHostToDevice));
+    OSR_CUDA(cudaMemcpy(pg.start, gr.inst_start, sb, cudaMemcpyHostToDevice));
+    return OSR_OK;
+}
+
+template <int N>
+static osr_status plan_launch_n(const osr_flash_group &gr, const PlanGroup &pg, cudaStream_t s) {
+    Instances<N> inst;
+    inst.tables = (const FluidTable<N> *)pg.tables;
+    inst.start = pg.start;
+    inst.n = gr.n_inst;
+    return run_flash_n<N>(gr.fluids[0], gr.d_P, gr.d_T, gr.d_z, gr.n, *gr.out, s, Form::kQueue, pg.scratch, inst);
+}
+
+// ---------------------------------------------------------------------------
 // No-allocation variant of the batched flash.
 //
 // Its scratch (queue heads, parked counts, the two parked-cell lists) lives in
@@ -554,6 +591,129 @@ osr_status osr_flash_batch_instances(const osr_fluid *fluids, int n_inst, const 
     cudaError_t e = cudaFreeAsync(scratch, s);
     if (st == OSR_OK && e != cudaSuccess) return cuda_fail(e);
     return st;
+}
+
+}  // extern "C"
+
+struct osr_flash_plan {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<void *> bufs;
+    int groups = 0;
+    long cells = 0;
+};
+
+namespace {
+
+void plan_free(osr_flash_plan *p) {
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    for (void *b : p->bufs) cudaFree(b);
+    delete p;
+}
+
+#define OSR_PLAN_SWITCH(nc, call)                                                                        \
+    switch (nc) {                                                                                         \
+        case 1: { constexpr int K = 1; st = call; break; }                                                \
+        case 2: { constexpr int K = 2; st = call; break; }                                                \
+        case 3: { constexpr int K = 3; st = call; break; }                                                \
+        case 4: { constexpr int K = 4; st = call; break; }                                                \
+        case 5: { constexpr int K = 5; st = call; break; }                                                \
+        case 6: { constexpr int K = 6; st = call; break; }                                                \
+        case 7: { constexpr int K = 7; st = call; break; }                                                \
+        case 8: { constexpr int K = 8; st = call; break; }                                                \
+        case 9: { constexpr int K = 9; st = call; break; }                                                \
+        case 10: { constexpr int K = 10; st = call; break; }                                              \
+        case 11: { constexpr int K = 11; st = call; break; }                                              \
+        case 12: { constexpr int K = 12; st = call; break; }                                              \
+        case 13: { constexpr int K = 13; st = call; break; }                                              \
+        case 14: { constexpr int K = 14; st = call; break; }                                              \
+        case 15: { constexpr int K = 15; st = call; break; }                                              \
+        case 16: { constexpr int K = 16; st = call; break; }                                              \
+        default: st = OSR_ERR_NC;                                                                         \
+    }
+
+}  // namespace
+
+extern "C" {
+
+osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, osr_flash_plan **out) {
+    if (!groups || n_groups < 1 || n_groups > 64 || !out) return OSR_ERR_ARG;
+    *out = nullptr;
+    for (int g = 0; g < n_groups; g++) {
+        const osr_flash_group &gr = groups[g];
+        if (!gr.fluids || gr.n_inst < 1 || !gr.inst_start || !gr.out || gr.n <= 0) return OSR_ERR_ARG;
+        const int nc = gr.fluids[0].nc;
+        for (int i = 0; i < gr.n_inst; i++) {
+            osr_status st = check_fluid(&gr.fluids[i]);
+            if (st) return st;
+            if (gr.fluids[i].nc != nc || gr.inst_start[i + 1] < gr.inst_start[i]) return OSR_ERR_ARG;
+        }
+        if (gr.inst_start[0] != 0 || gr.inst_start[gr.n_inst] != gr.n) return OSR_ERR_ARG;
+        osr_status st = check_out(gr.out);
+        if (st) return st;
+        if (!gr.d_P || !gr.d_T || !gr.d_z) return OSR_ERR_ARG;
+    }
+    osr_flash_plan *p = new osr_flash_plan();
+    p->groups = n_groups;
+    std::vector<PlanGroup> pg((size_t)n_groups);
+    osr_status st = OSR_OK;
+    for (int g = 0; g < n_groups && st == OSR_OK; g++) {
+        const osr_flash_group &gr = groups[g];
+        p->cells += gr.n;
+        OSR_PLAN_SWITCH(gr.fluids[0].nc, plan_prepare_n<K>(gr, pg[(size_t)g], p->bufs))
+    }
+    // capture: fork one branch per group from a private stream, join back
+    cudaStream_t cs = nullptr;
+    std::vector<cudaStream_t> bs((size_t)n_groups, nullptr);
+    std::vector<cudaEvent_t> ev((size_t)n_groups + 1, nullptr);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = st == OSR_OK ? cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) : cudaSuccess;
+    for (int g = 0; g < n_groups && e == cudaSuccess && st == OSR_OK; g++)
+        e = cudaStreamCreateWithFlags(&bs[(size_t)g], cudaStreamNonBlocking);
+    for (size_t i = 0; i < ev.size() && e == cudaSuccess && st == OSR_OK; i++)
+        e = cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming);
+    bool capturing = false;
+    if (e == cudaSuccess && st == OSR_OK) {
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+        capturing = e == cudaSuccess;
+    }
+    if (capturing) {
+        e = cudaEventRecord(ev[0], cs);
+        for (int g = 0; g < n_groups && e == cudaSuccess && st == OSR_OK; g++) {
+            const size_t k = (size_t)g;
+            e = cudaStreamWaitEvent(bs[k], ev[0], 0);
+            if (e != cudaSuccess) break;
+            OSR_PLAN_SWITCH(groups[g].fluids[0].nc, plan_launch_n<K>(groups[g], pg[k], bs[k]))
+            if (st != OSR_OK) break;
+            e = cudaEventRecord(ev[k + 1], bs[k]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev[k + 1], 0);
+        }
+        const cudaError_t ee = cudaStreamEndCapture(cs, &graph);
+        if (e == cudaSuccess) e = ee;
+    }
+    if (e == cudaSuccess && st == OSR_OK) e = cudaGraphInstantiate(&p->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    for (cudaStream_t x : bs)
+        if (x) cudaStreamDestroy(x);
+    if (cs) cudaStreamDestroy(cs);
+    if (st == OSR_OK && e != cudaSuccess) st = cuda_fail(e);
+    if (st != OSR_OK) {
+        plan_free(p);
+        return st;
+    }
+    *out = p;
+    return OSR_OK;
+}
+
+osr_status osr_flash_plan_run(osr_flash_plan *plan, void *stream) {
+    if (!plan || !plan->exec) return OSR_ERR_ARG;
+    OSR_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));
+    return OSR_OK;
+}
+
+void osr_flash_plan_destroy(osr_flash_plan *plan) {
+    if (plan) plan_free(plan);
 }
 
 osr_status osr_fugacity_derivs(const osr_fluid *fluid, const double *d_P, const double *d_T, const double *d_x,

@@ -77,3 +77,50 @@ def test_instance_offsets_are_validated(cuda_device):
     bad[-1] += 1
     with pytest.raises(osr.OsrError):
         osr.flash_instances(fluids, bad, tP, tT, tz)
+
+
+def test_plan_graph_equals_per_group_calls(cuda_device):
+    """osr_flash_plan: instance groups of every component count 3..12 as one
+    CUDA graph.  Every output of every group equals the group's own
+    osr_flash_batch_instances call bit for bit (the same kernels and launch
+    shapes), on the first run, on a repeat, and after the inputs are
+    refilled in place with another seed."""
+    import torch
+    insts = workloads.batched_instances(n_inst=120, seed=13, cells_lo=20, cells_hi=3000)
+    dev = cuda_device
+    groups, refs = [], []
+    for nc in sorted({d["nc"] for d in insts}):
+        members, start, P, T, z = workloads.instance_group([d for d in insts if d["nc"] == nc], nc, seed=5)
+        fluids = [osr.Fluid(d["tc"], d["pc"], d["acf"], d["kij"], d["eos"]) for d in members]
+        g = dict(fluids=fluids, start=start, P=torch.from_numpy(P).to(dev), T=torch.from_numpy(T).to(dev),
+                 z=torch.from_numpy(z).to(dev))
+        g["out"] = osr.alloc_flash_outputs(nc, int(P.shape[0]), True, dev)
+        groups.append(g)
+    assert len(groups) == 10
+    plan = osr.FlashPlan(groups)
+
+    def check():
+        torch.cuda.synchronize()
+        for g in groups:
+            ref = osr.flash_instances(g["fluids"], g["start"], g["P"], g["T"], g["z"], derivs=True)
+            torch.cuda.synchronize()
+            for k, v in ref.items():
+                a, b = g["out"][k], v
+                assert torch.equal(torch.nan_to_num(a, nan=7.0), torch.nan_to_num(b, nan=7.0)), k
+
+    plan.run()
+    check()
+    for g in groups:
+        for k in g["out"]:
+            g["out"][k].zero_()
+    plan.run()
+    check()
+    for i, g in enumerate(groups):
+        _, _, P, T, z = workloads.instance_group([d for d in insts if d["nc"] == g["fluids"][0].nc],
+                                                 g["fluids"][0].nc, seed=40 + i)
+        g["P"].copy_(torch.from_numpy(P))
+        g["T"].copy_(torch.from_numpy(T))
+        g["z"].copy_(torch.from_numpy(z))
+    plan.run()
+    check()
+    plan.close()
