@@ -72,8 +72,10 @@ def parse():
     ap.add_argument("--steps-grids", default=None, help="NX,NY,NZ[;...] of the scaled time-stepping runs")
     ap.add_argument("--steps-passes", type=int, default=None, help="passes timed per scaled grid (3)")
     ap.add_argument("--steps-scaled-only", action="store_true", help="skip the small plain case (profiling)")
-    ap.add_argument("--part", choices=["all", "assembly", "steps"], default="all",
-                    help="assembly: only the Newton-step assembly object (profiling)")
+    ap.add_argument("--part", choices=["all", "assembly", "steps", "slabs"], default="all",
+                    help="assembly: only the Newton-step assembly object (profiling); slabs: the z-slab Newton "
+                         "step over the ranks (one grid split across the GPUs)")
+    ap.add_argument("--slab-ksp-its", type=int, default=100, help="BiCGStab iterations per slab Newton step")
     ap.add_argument("--assembly-grid", default=None, help="NX,NY,NZ of the assembly grid (default 128,128,32)")
     return ap.parse_args()
 
@@ -818,6 +820,80 @@ def _small_plain_run(osr, torch, dev, cpu_sample):
     return out
 
 
+def measure_slabs(osr, torch, dev, args, rank, world):
+    """One Newton step of the z-slab decomposition over the ranks (one grid
+    split across the GPUs, strong scaling): the assembly workload's grid cut
+    into `world` slabs of layers; every rank evaluates its slab's residual
+    (ghost layers of the unknowns from the neighbours), its Jacobian, and its
+    part of the distributed BiCGStab + block-Jacobi solve (osr_dksp_* stages;
+    dot products all-reduced, the search vectors' ghost layers refreshed
+    before each product) for a fixed number of iterations.  CUDA events on
+    the launching stream, max over ranks."""
+    import torch.distributed as dist
+    from osiris_b200 import slabs, workloads
+    nx, ny, nz = (tuple(int(v) for v in args.assembly_grid.split(",")) if args.assembly_grid
+                  else workloads.ASSEMBLY_GRID)
+    d = workloads.assembly_deck(nx, ny, nz)
+    S = slabs.Slab(d, rank, world)
+    workloads.assembly_state(S.grid, S.grid.deck, dev, noise=0.0)
+    rows = S.refresh_layout(dev)
+    x0 = torch.zeros(rows, dtype=torch.float64, device=dev)
+    S.grid.init_guess(x0)
+    x = x0.clone()
+    f = torch.zeros_like(x0)
+    J = S.grid.alloc_jacobian(dev)
+    dx = torch.zeros_like(x0)
+    t = 3600.0
+    its = max(1, args.slab_ksp_its)
+    opts = dict(rtol=0.0, atol=0.0, dtol=1e300, max_it=its, check_every=its)
+
+    def step():
+        x.copy_(x0)
+        S.form_function(x, f, t)
+        if S.grid.jacobian(J, t) != 0:
+            raise osr.OsrError("osr_grid_jacobian failed")
+        return S.ksp_solve(J, f, dx, check_every=its, **{k: v for k, v in opts.items() if k != "check_every"})
+
+    for _ in range(max(args.warmup, 1)):
+        info = step()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    clocks = ClockSampler(_gpu_id(torch, dev))
+    ms, parts = [], []
+    for _ in range(args.steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        x.copy_(x0)
+        torch.cuda.synchronize(dev)
+        e[0].record()
+        S.form_function(x, f, t)
+        e[1].record()
+        S.grid.jacobian(J, t)
+        e[2].record()
+        info = S.ksp_solve(J, f, dx, check_every=its, **{k: v for k, v in opts.items() if k != "check_every"})
+        e[3].record()
+        torch.cuda.synchronize(dev)
+        ms.append(e[0].elapsed_time(e[3]))
+        parts.append([e[k].elapsed_time(e[k + 1]) for k in range(3)])
+    clk = clocks.stop()
+    m = torch.tensor([sum(ms) / len(ms)], dtype=torch.float64, device=dev)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    m = float(m.item())
+    cells = 2 * nx * ny * nz
+    return {"part": "slabs", "metric": "z-slab Newton step cell-media/s (residual + Jacobian + distributed solve)",
+            "value": cells / (m * 1e-3), "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m, "higher_is_better": True, "scaling": "strong",
+            "dtype": "f64", "data": "synthetic",
+            "phases_ms_rank0": {k: sum(p[i] for p in parts) / len(parts)
+                                for i, k in enumerate(("form_function", "jacobian", "solve"))},
+            "ksp": {"iterations": info["its"], "reason": info["reason"], "rnorm0": info["rnorm0"],
+                    "rnorm": info["rnorm"]},
+            "config": {"workload": f"{nx}x{ny}x{nz} dual-porosity grid, PR, 8 components, all cells two-phase, "
+                                   f"cut into {world} z-slabs (one per rank), {its} BiCGStab iterations per step",
+                       "cell_media": cells, "rows_rank0": rows, "layers_rank0": [S.z0, S.z1],
+                       "parallelism": f"z-slabs x{world}"},
+            "clocks": clk}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -836,6 +912,28 @@ def run_ours(args):
         st = measure_steps(osr, torch, dev, args, cpu_sample=rank == 0 and world == 1 and not args.no_cpu_baseline)
         if rank == 0:
             print(json.dumps(st), flush=True)
+        return 0
+
+    if args.part == "slabs":
+        dev = torch.device("cuda", local)
+        torch.cuda.set_device(dev)
+        from datetime import timedelta
+        if world > 1:
+            dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
+        else:
+            import socket
+            sk = socket.socket()
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+            sk.close()
+            dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                    device_id=dev, timeout=timedelta(seconds=300))
+        try:
+            o = measure_slabs(osr, torch, dev, args, rank, world)
+            if rank == 0:
+                print(json.dumps(o), flush=True)
+        finally:
+            dist.destroy_process_group()
         return 0
 
     if args.part == "assembly":
