@@ -688,6 +688,15 @@ osr_status osr_sim_create(osr_grid *grid, const double *markers, int n_markers, 
  * finished. */
 osr_status osr_sim_step(osr_sim *sim, const osr_ksp_opts *opts, osr_step_info *info, void *stream);
 
+/* Whether osr_sim_step runs a pass's InitGuess2, FormFunction, FormJacobian,
+ * linear solve and x - dx as one CUDA graph (default on).  The graph reads
+ * the pass's Dt, time and PCoeff from device memory, so one capture serves
+ * every pass of a row layout; it is captured again after a layout change and
+ * gives exactly the direct launches' results.  Off: direct launches. */
+osr_status osr_sim_set_graph(osr_sim *sim, int on);
+/* Passes run through the step graph so far. */
+osr_status osr_sim_graph_launches(osr_sim *sim, long *launches);
+
 /* Current simulation time and Dt (either may be null). */
 osr_status osr_sim_time(osr_sim *sim, double *sim_time, double *dt);
 

@@ -853,6 +853,16 @@ class Sim:
                                   None if stream is None else _vp(stream)), "osr_sim_step")
         return {k: getattr(info, k) for k, _ in StepInfo._fields_}
 
+    def set_graph(self, on: bool):
+        """Run each pass's linearisation and solve as one CUDA graph (the
+        default) or as direct launches (osr_sim_set_graph)."""
+        _check(lib().osr_sim_set_graph(self._h, int(bool(on))), "osr_sim_set_graph")
+
+    def graph_launches(self) -> int:
+        n = ctypes.c_long()
+        _check(lib().osr_sim_graph_launches(self._h, ctypes.byref(n)), "osr_sim_graph_launches")
+        return n.value
+
     def marker_index(self) -> int:
         k = ctypes.c_int()
         _check(lib().osr_sim_marker_index(self._h, ctypes.byref(k)), "osr_sim_marker_index")

@@ -293,6 +293,7 @@ static AsmArgs<N> asm_args(const osr_grid &g, double *f, double *fscale, double 
     A.k.re_f = g.re_f;
     A.k.diff_off = (g.const_dif && g.cdif == 0) ? 1 : 0;
     A.k.sf1 = A.k.sf3 = 0;
+    A.k.ctl = g.d_ctl;
     A.w = WellSet{g.nwells > 0 ? g.nwells : 0, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws, g.well_sums_ext};
     A.tor = g.tor;
     A.rowoff = g.rowoff;
@@ -304,7 +305,7 @@ static AsmArgs<N> asm_args(const osr_grid &g, double *f, double *fscale, double 
 template <int N>
 static osr_status init_guess_n(osr_grid &g, double *x, cudaStream_t st) {
     GridArgs<N> a = grid_args<N>(g);
-    init_guess_kernel<N><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(a, g.rowoff, g.pcoeff, x);
+    init_guess_kernel<N><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(a, g.rowoff, g.pcoeff, g.d_ctl, x);
     ASM_CUDA(cudaGetLastError());
     return OSR_OK;
 }
@@ -312,7 +313,7 @@ static osr_status init_guess_n(osr_grid &g, double *x, cudaStream_t st) {
 template <int N>
 static osr_status update_all_n(osr_grid &g, const double *x, cudaStream_t st) {
     GridArgs<N> a = grid_args<N>(g);
-    update_all_kernel<N><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(a, g.rowoff, g.pcoeff, x);
+    update_all_kernel<N><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(a, g.rowoff, g.pcoeff, g.d_ctl, x);
     ASM_CUDA(cudaGetLastError());
     return OSR_OK;
 }

@@ -63,6 +63,9 @@ constexpr int kWellSums = 5;
 
 struct AsmScalars {
     double dt, sim_time, pcoeff;
+    // per-pass controls in device memory ([dt, time, PCoeff]) read in place
+    // of the three values above when set (a Newton step replayed as a graph)
+    const double *ctl;
     double sf1, sf3;      // ShapeFactor_1 / _3 without the geometric sums' zero gate applied
     double sigma, lf, re_f;
     int diff_off;         // CDIF present with a zero value: both diffusive shape factors vanish
@@ -335,7 +338,9 @@ static __global__ void pcoeff_kernel(const double *Pm, const double *Pf, long ce
 
 // State -> unknowns (InitGuess2).
 template <int N>
-__global__ void init_guess_kernel(const __grid_constant__ GridArgs<N> a, const long *rowoff, double pcoeff, double *x) {
+__global__ void init_guess_kernel(const __grid_constant__ GridArgs<N> a, const long *rowoff, double pcoeff_arg,
+                                  const double *ctl, double *x) {
+    const double pcoeff = ctl ? ctl[2] : pcoeff_arg;
     const long n = a.s.cells;
     for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < 2 * n; b += (long)gridDim.x * blockDim.x) {
         const int med = b >= n;
@@ -366,8 +371,9 @@ __global__ void init_guess_kernel(const __grid_constant__ GridArgs<N> a, const l
 // by the reference's step rule and floored at MINPPP, saturations clamped
 // and renormalised.
 template <int N>
-__global__ void update_all_kernel(const __grid_constant__ GridArgs<N> a, const long *rowoff, double pcoeff,
-                                  const double *x) {
+__global__ void update_all_kernel(const __grid_constant__ GridArgs<N> a, const long *rowoff, double pcoeff_arg,
+                                  const double *ctl, const double *x) {
+    const double pcoeff = ctl ? ctl[2] : pcoeff_arg;
     const long n = a.s.cells;
     for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < 2 * n; b += (long)gridDim.x * blockDim.x) {
         const int med = b >= n;
@@ -456,7 +462,7 @@ __device__ void well_rates(const AsmArgs<N> &A, int med, long c, int ix, int iy,
     const double watRo = s.wat_ro, watMu = s.wat_mu;
     const double wfac = watRo * kWatMRo;
     r = WellRates{0, 0, 0, 0, 0, 0, -1};
-    const double t = A.k.sim_time;
+    const double t = A.k.ctl ? A.k.ctl[1] : A.k.sim_time;
     // own-cell quantities
     const double Pw = O.P[c], Po = O.P[n + c], Pg = O.P[2 * n + c];
     const double krw = O.kr[c], kro = O.kr[n + c], krg = O.kr[2 * n + c];

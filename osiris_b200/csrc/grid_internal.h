@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <vector>
 #include "osiris_b200.h"
 #include "assembly_kernels.cuh"
@@ -31,6 +32,9 @@ struct osr_grid {
     long n_rows = 0;
     double pcoeff = 0;
     double dt = 0;
+    // per-pass controls [dt, time, PCoeff] in device memory, read by the
+    // kernels in place of dt / time / pcoeff when set (osr_sim's step graph)
+    const double *d_ctl = nullptr;
     // wells
     int *d_wi = nullptr;
     double *d_wf = nullptr, *d_re = nullptr;
@@ -57,6 +61,16 @@ double peaceman_re(const double *di, const double *dj, int nx, int ny, int ix, i
 osr_status grid_assembly_init(osr_grid &g, const osr_model *md);
 void grid_assembly_free(osr_grid &g);
 void ksp_free(osr_grid &g);
+// The sim's step graph: `pre` (captured ahead), the whole linear solve of
+// vals x = b (the reference's KSP options o), the solve's scalars to the
+// grid's pinned copy, then `post`, as one instantiated graph.
+osr_status ksp_step_graph(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
+                          const std::function<void(cudaStream_t)> &pre, const std::function<void(cudaStream_t)> &post,
+                          cudaGraphExec_t *out);
+// The scalars the step graph's solve starts from (set before each launch)
+// and its outcome (read after the launch has completed).
+void ksp_step_set_host(osr_grid &g, const osr_ksp_opts &o);
+void ksp_step_read_host(const osr_grid &g, osr_ksp_info *info);
 // Per-component constants at the reservoir temperature, formed with the
 // reference's expressions: EOS_Init (compsim/Init_Calcs.cpp:66-97), Tr_Mu
 // (:48-64) and the pair factors of CalcDiffusion (compsim/Mass_Tran.cpp:43-46).

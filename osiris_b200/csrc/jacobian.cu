@@ -21,7 +21,7 @@ static osr_status jfail(cudaError_t) { return OSR_ERR_CUDA; }
 constexpr int kRowThreads = 128;
 // Resident CTAs per SM the row kernels are compiled for (bounds their registers).
 #ifndef OSR_JAC_MIN_BLOCKS
-#define OSR_JAC_MIN_BLOCKS 5
+#define OSR_JAC_MIN_BLOCKS 4
 #endif
 
 template <int N>
@@ -128,6 +128,7 @@ static void make_view(const osr_grid &g, osrj::JacView &v) {
     v.lf = g.lf;
     v.pcoeff = g.pcoeff;
     v.dt = g.dt;
+    v.ctl = g.d_ctl;
     v.diff_off = (g.const_dif && g.cdif == 0) ? 1 : 0;
     v.const_dif = g.const_dif;
     for (int m = 0; m < 2; m++) {
@@ -180,6 +181,7 @@ static osr_status well_pass(osr_grid &g, double sim_time, cudaStream_t st) {
     A.k.re_f = g.re_f;
     A.k.diff_off = (g.const_dif && g.cdif == 0) ? 1 : 0;
     A.k.sf1 = A.k.sf3 = 0;
+    A.k.ctl = g.d_ctl;
     A.w = WellSet{g.nwells, g.d_wi, g.d_wf, g.d_re, g.d_cond, g.d_ws, g.well_sums_ext};
     A.tor = g.tor;
     A.rowoff = g.rowoff;

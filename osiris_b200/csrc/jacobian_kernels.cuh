@@ -97,6 +97,9 @@ struct JacView {
     int srk;
     // scalars
     double cpor, dcpor, refp, wat_ro, wat_mu, sigma, lf, pcoeff, dt;
+    // per-pass controls in device memory ([dt, time, PCoeff]), read in place
+    // of dt and pcoeff when set (a Newton step replayed as one CUDA graph)
+    const double *ctl;
     int diff_off;   // CDIF present and zero: diffusive shape factors vanish
     int const_dif;  // CDIF present: diffusion-coefficient derivatives vanish
     JMed m[2];
@@ -113,6 +116,9 @@ struct JacView {
     double *vals;  // [chunks of 32 block rows][entries][32]
     int entries;   // values per block row
 };
+
+OSR_HD inline double jdt(const JacView &v) { return v.ctl ? v.ctl[0] : v.dt; }
+OSR_HD inline double jpc(const JacView &v) { return v.ctl ? v.ctl[2] : v.pcoeff; }
 
 // Entry indices of the compact block row (see the file comment).
 struct Layout {
@@ -919,22 +925,22 @@ OSR_HD inline void column_task(const JacView &v, int med, long c, int k, const O
         if (total) {
             const double po_ = med ? pf : pm;
             const double dEq0 = med ? dEkF[0] : dEkM[0], dEq1 = med ? dEkF[1] : dEkM[1];
-            X = (Vb / v.dt) * po_ * q.S(1) * dEq0 - accX[i];
-            Y = (Vb / v.dt) * po_ * q.S(2) * dEq1 - accY[i];
+            X = (Vb / jdt(v)) * po_ * q.S(1) * dEq0 - accX[i];
+            Y = (Vb / jdt(v)) * po_ * q.S(2) * dEq1 - accY[i];
         } else {
             const double dQxl = (diag && W.iwell < 0) ? W.Qo : 0.0, dQxg = (diag && W.iwell < 0) ? W.Qg : 0.0;
             if (med == 0) {
                 const double xi = M.w(0, i), yi = M.w(1, i);
                 const double dLxl = diag ? ro + xi * dEkM[0] : xi * dEkM[0];
                 const double dLxg = diag ? rg + yi * dEkM[1] : yi * dEkM[1];
-                X = (Vb / v.dt) * pm * M.S(1) * dLxl - dQxl - accX[i];
-                Y = (Vb / v.dt) * pm * M.S(2) * dLxg - dQxg - accY[i];
+                X = (Vb / jdt(v)) * pm * M.S(1) * dLxl - dQxl - accX[i];
+                Y = (Vb / jdt(v)) * pm * M.S(2) * dLxg - dQxg - accY[i];
             } else {
                 const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
                 const double dLxl = diag ? Fr.rho(0) + fxi * dEkF[0] : fxi * dEkF[0];
                 const double dLxg = diag ? Fr.rho(1) + fyi * dEkF[1] : fyi * dEkF[1];
-                X = (Vb / v.dt) * pf * Fr.S(1) * dLxl - dQxl - accX[i];
-                Y = (Vb / v.dt) * pf * Fr.S(2) * dLxg - dQxg - accY[i];
+                X = (Vb / jdt(v)) * pf * Fr.S(1) * dLxl - dQxl - accX[i];
+                Y = (Vb / jdt(v)) * pf * Fr.S(2) * dLxg - dQxg - accY[i];
             }
         }
         out.st(L.cr(row, 0, k), O.x ? X : 0.0);
@@ -1119,7 +1125,7 @@ OSR_HD inline void ps_task(const JacView &v, int med, long c, const Out &out, Sm
         dSw[i] = a_dSw;
         dSo[i] = a_dSo;
         dSg[i] = a_dSg;
-        store_other_ps(N, out, row, lo, v.pcoeff * oP, oSw, oSo, oSg);
+        store_other_ps(N, out, row, lo, jpc(v) * oP, oSw, oSo, oSg);
     }
     // 2) faces
     JFace fc[6];
@@ -1243,7 +1249,7 @@ OSR_HD inline void ps_task(const JacView &v, int med, long c, const Out &out, Sm
                     dB += NNd * DX * (MMd[ph] * dDdp2 + Dup * dMM2[ph]);
                 }
             }
-            put(0, 0, v.pcoeff * (-xo * fd.T[0] - yg * fd.T[1] - dB));
+            put(0, 0, jpc(v) * (-xo * fd.T[0] - yg * fd.T[1] - dB));
             for (int tt = 0; tt < 4; tt++) out.st(L.cr(row, e.slot, 2 * N + tt), ps[tt]);
             if (total && qk.shifted_block)
                 for (int tt = 0; tt < 4; tt++) ov[(e.d == 1 ? 0 : 4) + tt] = ovl[tt];
@@ -1260,27 +1266,27 @@ OSR_HD inline void ps_task(const JacView &v, int med, long c, const Out &out, Sm
         double dLdp, dLdSo, dLdSg, well;
         if (i == N - 1) {
             const double po_ = med ? pf : pm, dpo_ = med ? dpf : dpm;
-            dLdp = (Vb / v.dt) * (q.S(1) * (q.rho(0) * dpo_ + q.dE(N, 0) * po_) + q.S(2) * (q.rho(1) * dpo_ + q.dE(N, 1) * po_));
-            dLdSo = (Vb / v.dt) * (po_ * q.rho(0));
-            dLdSg = (Vb / v.dt) * (po_ * q.rho(1));
+            dLdp = (Vb / jdt(v)) * (q.S(1) * (q.rho(0) * dpo_ + q.dE(N, 0) * po_) + q.S(2) * (q.rho(1) * dpo_ + q.dE(N, 1) * po_));
+            dLdSo = (Vb / jdt(v)) * (po_ * q.rho(0));
+            dLdSg = (Vb / jdt(v)) * (po_ * q.rho(1));
             const WellAt W = well_at(v, med, c, 0, 0.0);
             well = W.PIo + W.PIg;
         } else if (med == 0) {
             const double xi = M.w(0, i), yi = M.w(1, i);
-            dLdp = (Vb / v.dt) * (xi * M.S(1) * (ro * dpm + M.dE(N, 0) * pm) + yi * M.S(2) * (rg * dpm + M.dE(N, 1) * pm));
-            dLdSo = (Vb / v.dt) * (xi * pm * ro);
-            dLdSg = (Vb / v.dt) * (yi * pm * rg);
+            dLdp = (Vb / jdt(v)) * (xi * M.S(1) * (ro * dpm + M.dE(N, 0) * pm) + yi * M.S(2) * (rg * dpm + M.dE(N, 1) * pm));
+            dLdSo = (Vb / jdt(v)) * (xi * pm * ro);
+            dLdSg = (Vb / jdt(v)) * (yi * pm * rg);
             const WellAt W = well_at(v, 0, c, i, yi);
             well = xi * W.PIo + W.gcomp * W.PIg;
         } else {
             const double fxi = Fr.w(0, i), fyi = Fr.w(1, i);
-            dLdp = (Vb / v.dt) * (fxi * Fr.S(1) * (Fr.rho(0) * dpf + Fr.dE(N, 0) * pf) + fyi * Fr.S(2) * (Fr.rho(1) * dpf + Fr.dE(N, 1) * pf));
-            dLdSo = (Vb / v.dt) * (fxi * pf * Fr.rho(0));
-            dLdSg = (Vb / v.dt) * (fyi * pf * Fr.rho(1));
+            dLdp = (Vb / jdt(v)) * (fxi * Fr.S(1) * (Fr.rho(0) * dpf + Fr.dE(N, 0) * pf) + fyi * Fr.S(2) * (Fr.rho(1) * dpf + Fr.dE(N, 1) * pf));
+            dLdSo = (Vb / jdt(v)) * (fxi * pf * Fr.rho(0));
+            dLdSg = (Vb / jdt(v)) * (fyi * pf * Fr.rho(1));
             const WellAt W = well_at(v, 1, c, i, fyi);
             well = fxi * W.PIo + W.gcomp * W.PIg;
         }
-        store_own_ps(N, out, row, lq, v.pcoeff * (dLdp + dp[i] + well), -dSw[i], dLdSo - dSo[i], dLdSg - dSg[i]);
+        store_own_ps(N, out, row, lq, jpc(v) * (dLdp + dp[i] + well), -dSw[i], dLdSo - dSo[i], dLdSg - dSg[i]);
     }
 }
 
@@ -1333,8 +1339,8 @@ OSR_HD inline void water_row(const JacView &v, int med, long c, const Out &out) 
     const double wr = v.wat_ro * kWatMRo;
     const double po_ = med ? t.pf : t.pm, dpo_ = med ? t.dpf : t.dpm;
     const double sg = med ? -1.0 : 1.0;
-    const double dLdp = (t.Vb / v.dt) * wr * O.S(0) * dpo_;
-    const double dLdSw = (t.Vb / v.dt) * (po_ * wr);
+    const double dLdp = (t.Vb / jdt(v)) * wr * O.S(0) * dpo_;
+    const double dLdSw = (t.Vb / jdt(v)) * (po_ * wr);
     const double tr = kSIC * v.wat_ro * kWatMRo * t.SF2 * t.krw / v.wat_mu * t.Vb;
     // both continua's water rows take -tr for their own pressure, +tr for the other's
     double dRdp = -tr;
@@ -1344,7 +1350,7 @@ OSR_HD inline void water_row(const JacView &v, int med, long c, const Out &out) 
     const long n = v.n;
     for (int q = 0; q < nf; q++) dRdp += ld(F.wtran + (long)fc[q].d * n + fc[q].tc);
     const WellAt W = well_at(v, med, c, 0, 0.0);
-    out.st(L.w(0, 2 * N), v.pcoeff * (dLdp + dRdp + W.PIw));
+    out.st(L.w(0, 2 * N), jpc(v) * (dLdp + dRdp + W.PIw));
     const double smw = kSIC * kWatMRo * t.dkm[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
     const double sfw = kSIC * kWatMRo * t.dkf[0] * v.wat_ro * t.SF2 / v.wat_mu * t.Vb * t.dPw;
     double dRdSw = sg * (med ? sfw : smw);
@@ -1355,7 +1361,7 @@ OSR_HD inline void water_row(const JacView &v, int med, long c, const Out &out) 
         present |= 1u << e.slot;
         const FaceData fd = face_data(v, F, c, e);
         const double Tw = ld(F.wtran + (long)e.d * n + e.tc), dTw = ld(F.dwtran + (long)e.d * n + e.tc);
-        out.st(L.w(e.slot, 2 * N), v.pcoeff * (-Tw));
+        out.st(L.w(e.slot, 2 * N), jpc(v) * (-Tw));
         const double dsw = e.sgn * (dTw * fd.dP[0] + kGAcc * v.wat_ro * dTw * fd.dH);
         const bool up_nb = upstream(e, fd, c, 2) == e.nb;
         out.st(L.w(e.slot, 2 * N + 1), up_nb ? dsw : 0.0);
@@ -1367,7 +1373,7 @@ OSR_HD inline void water_row(const JacView &v, int med, long c, const Out &out) 
             out.st(L.w(s, 2 * N + 1), 0.0);
         }
     out.st(L.w(0, 2 * N + 1), dLdSw - dRdSw);
-    out.st(L.w(7, 2 * N), v.pcoeff * dROdp);
+    out.st(L.w(7, 2 * N), jpc(v) * dROdp);
     out.st(L.w(7, 2 * N + 1), dROSw);
 }
 
@@ -1432,7 +1438,7 @@ OSR_HD inline void fugacity_rows(const JacView &v, const Cell &q, const Out &out
         const double dPhil = phiL * (dAAl + dBBl + EEl * (dDDl * FFl + DDl * dFFl));
         const double dPhig = phiG * (dAAg + dBBg + EEg * (dDDg * FFg + DDg * dFFg));
         const double xi = xl[i], yi = yg[i];
-        out.st(L.f(i, 2 * N), v.pcoeff * (xi * (phiL + Pl * dPhil) - yi * (phiG + Pg * dPhig)));
+        out.st(L.f(i, 2 * N), jpc(v) * (xi * (phiL + Pl * dPhil) - yi * (phiG + Pg * dPhig)));
         for (int k = 0; k < N; k++) {
             const double dAl = tl[k] * (2 * Pl / (RT * RT)), dAg = tg[k] * (2 * Pg / (RT * RT));
             const double dBl = v.b[k] * Pl / RT, dBg = v.b[k] * Pg / RT;

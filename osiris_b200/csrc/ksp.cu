@@ -3,6 +3,7 @@
 // Jacobian, and the matrix-vector product alone (MatMult).
 #include <cuda_runtime.h>
 #include <cstring>
+#include <functional>
 #include <vector>
 #include "grid_internal.h"
 #include "ksp_kernels.cuh"
@@ -163,14 +164,123 @@ __global__ void bcgs_continue_kernel(cudaGraphConditionalHandle h, osrk::KspScal
     }
 }
 
+// Launch shapes and operands of one system.
 template <int N>
-static osr_status solve_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
-                          osr_ksp_info *info, cudaStream_t st) {
-    osr_status rc = ksp_ensure(g);
-    if (rc != OSR_OK) return rc;
-    osr_ksp_work &k = *g.ksp;
-    const osrk::KView v = kview(g, vals);
-    const long n = g.n_rows, nb = 2 * g.cells;
+struct SolvePlan {
+    osrk::KView v;
+    long n, nb;
+    unsigned vbk, ib, tpb, atb, ab, xb;
+    const double *b;
+    double *x;
+};
+
+template <int N>
+static SolvePlan<N> solve_plan(const osr_grid &g, const double *vals, const double *b, double *x) {
+    SolvePlan<N> p;
+    p.v = kview(g, vals);
+    p.n = g.n_rows;
+    p.nb = 2 * g.cells;
+    p.vbk = vec_blocks(p.n);
+    p.ib = inv_blocks(p.nb);
+    p.tpb = 32 * osrk::kInvWarps;
+    p.atb = osrk::kApplyThreads;
+    p.ab = red_blocks(p.nb, osrk::kApplyThreads);
+    p.xb = red_blocks(p.n, 4 * osrk::kRedThreads);
+    p.b = b;
+    p.x = x;
+    return p;
+}
+
+// scalars in (from the pinned host copy), block-Jacobi inverse, r = B b,
+// the BiCGStab set-up
+template <int N>
+static void solve_prologue(osr_ksp_work &k, const SolvePlan<N> &p, cudaStream_t st) {
+    cudaMemcpyAsync(k.scal, k.host, sizeof(osrk::KspScal), cudaMemcpyHostToDevice, st);
+    osrk::bjac_invert_kernel<N><<<p.ib, p.tpb, 0, st>>>(p.v, k.inv, k.scal);
+    osrk::bjac_apply_kernel<N, 0><<<p.ab, p.atb, 0, st>>>(p.v, k.inv, p.b, k.r, nullptr, k.part, k.scal);
+    osrk::bcgs_setup_kernel<<<p.vbk, 256, 0, st>>>(p.n, k.r, k.r0, k.p, k.v, p.x);
+}
+
+template <int N>
+static void solve_iterations(osr_ksp_work &k, const SolvePlan<N> &p, cudaStream_t st, int count) {
+    for (int q = 0; q < count; q++) {
+        osrk::bcgs_p_kernel<<<p.vbk, 256, 0, st>>>(p.n, k.r, k.p, k.v, k.scal);
+        spmv_launch<N>(p.v, k.p, k.t, k.scal, st);
+        osrk::bjac_apply_kernel<N, 1><<<p.ab, p.atb, 0, st>>>(p.v, k.inv, k.t, k.v, k.r0, k.part, k.scal);
+        osrk::bcgs_s_kernel<<<p.vbk, 256, 0, st>>>(p.n, k.r, k.v, k.s, k.scal);
+        spmv_launch<N>(p.v, k.s, k.w, k.scal, st);
+        osrk::bjac_apply_kernel<N, 2><<<p.ab, p.atb, 0, st>>>(p.v, k.inv, k.w, k.t, k.s, k.part, k.scal);
+        osrk::bcgs_xr_kernel<<<p.xb, osrk::kRedThreads, 0, st>>>(p.n, p.x, k.p, k.s, k.t, k.r, k.r0, k.part,
+                                                                  k.scal);
+    }
+}
+
+// The whole solve as one graph: `pre` (work captured ahead of it, or null),
+// the prologue, a while node whose body is one batch of `every` iterations
+// and the continue test (at most max_it / every batches), the scalars back
+// to the pinned host copy, then `post` (or null).  False when any part of
+// the capture fails (nothing is left instantiated).
+template <int N>
+static bool build_solve_graph(osr_ksp_work &k, const SolvePlan<N> &p, int every, int max_it,
+                              const std::function<void(cudaStream_t)> *pre,
+                              const std::function<void(cudaStream_t)> *post, cudaGraphExec_t *out) {
+    *out = nullptr;
+    if (!k.cap && cudaStreamCreateWithFlags(&k.cap, cudaStreamNonBlocking) != cudaSuccess) return false;
+    const cudaStreamCaptureMode mode = pre || post ? cudaStreamCaptureModeRelaxed : cudaStreamCaptureModeThreadLocal;
+    cudaGraph_t G = nullptr;
+    bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphNode_t wnode = nullptr;
+    cudaGraphConditionalHandle handle;
+    if (ok) ok = cudaGraphConditionalHandleCreate(&handle, G, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) ok = cudaStreamBeginCaptureToGraph(k.cap, G, nullptr, nullptr, 0, mode) == cudaSuccess;
+    if (ok) {
+        if (pre) (*pre)(k.cap);
+        solve_prologue<N>(k, p, k.cap);
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        ok = cudaStreamGetCaptureInfo(k.cap, &cs, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
+             cs == cudaStreamCaptureStatusActive;
+        std::vector<cudaGraphNode_t> tail(deps, deps + (ok ? ndeps : 0));
+        cudaGraph_t og = nullptr;
+        ok = (cudaStreamEndCapture(k.cap, &og) == cudaSuccess) && ok;
+        if (ok) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&wnode, G, tail.data(), tail.size(), &cp) == cudaSuccess;
+            cudaGraph_t body = ok ? cp.conditional.phGraph_out[0] : nullptr;
+            if (ok) ok = cudaStreamBeginCaptureToGraph(k.cap, body, nullptr, nullptr, 0, mode) == cudaSuccess;
+            if (ok) {
+                solve_iterations<N>(k, p, k.cap, every);
+                bcgs_continue_kernel<<<1, 32, 0, k.cap>>>(handle, k.scal, max_it / every);
+                cudaGraph_t bout = nullptr;
+                ok = cudaStreamEndCapture(k.cap, &bout) == cudaSuccess;
+                size_t body_nodes = 0;
+                // the body must hold the continue test (else the loop could not end)
+                if (ok) ok = cudaGraphGetNodes(body, nullptr, &body_nodes) == cudaSuccess &&
+                             body_nodes == (size_t)(7 * every + 1);
+            }
+            if (ok) ok = cudaStreamBeginCaptureToGraph(k.cap, G, &wnode, nullptr, 1, mode) == cudaSuccess;
+            if (ok) {
+                cudaMemcpyAsync(k.host, k.scal, sizeof(osrk::KspScal), cudaMemcpyDeviceToHost, k.cap);
+                if (post) (*post)(k.cap);
+                cudaGraph_t eout = nullptr;
+                ok = cudaStreamEndCapture(k.cap, &eout) == cudaSuccess;
+            }
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(out, G, 0) == cudaSuccess;
+    if (!ok) *out = nullptr;
+    if (G) cudaGraphDestroy(G);
+    cudaGetLastError();
+    return ok;
+}
+
+static void ksp_set_host(osr_ksp_work &k, const osr_ksp_opts &o) {
     osrk::KspScal h;
     std::memset(&h, 0, sizeof(h));
     h.rtol = o.rtol;
@@ -178,99 +288,38 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     h.dtol = o.dtol;
     h.max_it = o.max_it;
     *k.host = h;
-    const unsigned vbk = vec_blocks(n), ib = inv_blocks(nb);
-    const unsigned tpb = 32 * osrk::kInvWarps;
-    const unsigned atb = osrk::kApplyThreads;
-    const unsigned ab = red_blocks(nb, osrk::kApplyThreads), xb = red_blocks(n, 4 * osrk::kRedThreads);
-    // scalars in, block-Jacobi inverse, r = B b, the BiCGStab set-up
-    auto prologue = [&](cudaStream_t q_st) {
-        cudaMemcpyAsync(k.scal, k.host, sizeof(h), cudaMemcpyHostToDevice, q_st);
-        osrk::bjac_invert_kernel<N><<<ib, tpb, 0, q_st>>>(v, k.inv, k.scal);
-        osrk::bjac_apply_kernel<N, 0><<<ab, atb, 0, q_st>>>(v, k.inv, b, k.r, nullptr, k.part, k.scal);
-        osrk::bcgs_setup_kernel<<<vbk, 256, 0, q_st>>>(n, k.r, k.r0, k.p, k.v, x);
-    };
+}
+
+static void ksp_read_host(const osr_ksp_work &k, osr_ksp_info *info) {
+    if (!info) return;
+    info->reason = k.host->reason == osrk::kItersRunning ? osrk::kDivergedIts : k.host->reason;
+    info->its = k.host->its;
+    info->rnorm0 = k.host->rnorm0;
+    info->rnorm = k.host->rnorm;
+}
+
+template <int N>
+static osr_status solve_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
+                          osr_ksp_info *info, cudaStream_t st) {
+    osr_status rc = ksp_ensure(g);
+    if (rc != OSR_OK) return rc;
+    osr_ksp_work &k = *g.ksp;
+    const SolvePlan<N> p = solve_plan<N>(g, vals, b, x);
+    const long n = p.n;
+    ksp_set_host(k, o);
     const int every = o.check_every > 0 ? o.check_every : 8;
-    auto iterations = [&](cudaStream_t q_st, int count) {
-        for (int q = 0; q < count; q++) {
-            osrk::bcgs_p_kernel<<<vbk, 256, 0, q_st>>>(n, k.r, k.p, k.v, k.scal);
-            spmv_launch<N>(v, k.p, k.t, k.scal, q_st);
-            osrk::bjac_apply_kernel<N, 1><<<ab, atb, 0, q_st>>>(v, k.inv, k.t, k.v, k.r0, k.part, k.scal);
-            osrk::bcgs_s_kernel<<<vbk, 256, 0, q_st>>>(n, k.r, k.v, k.s, k.scal);
-            spmv_launch<N>(v, k.s, k.w, k.scal, q_st);
-            osrk::bjac_apply_kernel<N, 2><<<ab, atb, 0, q_st>>>(v, k.inv, k.w, k.t, k.s, k.part, k.scal);
-            osrk::bcgs_xr_kernel<<<xb, osrk::kRedThreads, 0, q_st>>>(n, x, k.p, k.s, k.t, k.r, k.r0, k.part,
-                                                                      k.scal);
-        }
-    };
-    // The whole solve as one graph: prologue, a while node whose body is one
-    // batch of iterations and the continue test, the scalars back to the
-    // pinned host copy.  One launch and one synchronisation per solve.  Used
-    // when the iteration cap is a whole number of batches (so the graph
-    // stops exactly where the host loop would); kept while the system's
-    // buffers and size stay the same.
+    // The whole solve as one graph: one launch and one synchronisation per
+    // solve.  Used when the iteration cap is a whole number of batches (so
+    // the graph stops exactly where the host loop would); kept while the
+    // system's buffers and size stay the same.
     if (k.whole && (k.w_vals != vals || k.w_b != b || k.w_x != x || k.w_rows != n || k.w_every != every ||
                     k.w_max != o.max_it)) {
         cudaGraphExecDestroy(k.whole);
         k.whole = nullptr;
     }
     if (!k.whole && !k.whole_failed && o.max_it >= every && o.max_it % every == 0) {
-        if (!k.cap) KSP_CUDA(cudaStreamCreateWithFlags(&k.cap, cudaStreamNonBlocking));
-        cudaGraph_t G = nullptr;
-        bool ok = cudaGraphCreate(&G, 0) == cudaSuccess;
-        const cudaGraphNode_t *deps = nullptr;
-        size_t ndeps = 0;
-        cudaGraphNode_t wnode = nullptr;
-        cudaGraphConditionalHandle handle;
-        if (ok) ok = cudaGraphConditionalHandleCreate(&handle, G, 1, cudaGraphCondAssignDefault) == cudaSuccess;
-        if (ok) ok = cudaStreamBeginCaptureToGraph(k.cap, G, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
-                     cudaSuccess;
-        if (ok) {
-            prologue(k.cap);
-            cudaStreamCaptureStatus cs;
-            cudaGraph_t cg = nullptr;
-            ok = cudaStreamGetCaptureInfo(k.cap, &cs, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
-                 cs == cudaStreamCaptureStatusActive;
-            std::vector<cudaGraphNode_t> tail(deps, deps + (ok ? ndeps : 0));
-            cudaGraph_t out = nullptr;
-            ok = (cudaStreamEndCapture(k.cap, &out) == cudaSuccess) && ok;
-            if (ok) {
-                cudaGraphNodeParams cp = {};
-                cp.type = cudaGraphNodeTypeConditional;
-                cp.conditional.handle = handle;
-                cp.conditional.type = cudaGraphCondTypeWhile;
-                cp.conditional.size = 1;
-                ok = cudaGraphAddNode(&wnode, G, tail.data(), tail.size(), &cp) == cudaSuccess;
-                cudaGraph_t body = ok ? cp.conditional.phGraph_out[0] : nullptr;
-                if (ok)
-                    ok = cudaStreamBeginCaptureToGraph(k.cap, body, nullptr, nullptr, 0,
-                                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-                if (ok) {
-                    iterations(k.cap, every);
-                    bcgs_continue_kernel<<<1, 32, 0, k.cap>>>(handle, k.scal, o.max_it / every);
-                    cudaGraph_t bout = nullptr;
-                    ok = cudaStreamEndCapture(k.cap, &bout) == cudaSuccess;
-                    size_t body_nodes = 0;
-                    // the body must hold the continue test (else the loop could not end)
-                    if (ok) ok = cudaGraphGetNodes(body, nullptr, &body_nodes) == cudaSuccess &&
-                                 body_nodes == (size_t)(7 * every + 1);
-                }
-                if (ok)
-                    ok = cudaStreamBeginCaptureToGraph(k.cap, G, &wnode, nullptr, 1,
-                                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-                if (ok) {
-                    cudaMemcpyAsync(k.host, k.scal, sizeof(h), cudaMemcpyDeviceToHost, k.cap);
-                    cudaGraph_t eout = nullptr;
-                    ok = cudaStreamEndCapture(k.cap, &eout) == cudaSuccess;
-                }
-            }
-        }
-        if (ok) ok = cudaGraphInstantiate(&k.whole, G, 0) == cudaSuccess;
-        if (!ok) {
-            k.whole = nullptr;
+        if (!build_solve_graph<N>(k, p, every, o.max_it, nullptr, nullptr, &k.whole))
             k.whole_failed = true;   // the host-driven batches below serve every later solve
-        }
-        if (G) cudaGraphDestroy(G);
-        cudaGetLastError();
         if (k.whole) {
             k.w_vals = vals;
             k.w_b = b;
@@ -283,15 +332,10 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     if (k.whole) {
         KSP_CUDA(cudaGraphLaunch(k.whole, st));
         KSP_CUDA(cudaStreamSynchronize(st));
-        if (info) {
-            info->reason = k.host->reason == osrk::kItersRunning ? osrk::kDivergedIts : k.host->reason;
-            info->its = k.host->its;
-            info->rnorm0 = k.host->rnorm0;
-            info->rnorm = k.host->rnorm;
-        }
+        ksp_read_host(k, info);
         return OSR_OK;
     }
-    prologue(st);
+    solve_prologue<N>(k, p, st);
     KSP_CUDA(cudaGetLastError());
     // the batch graph: every kernel reads its scalars and the solve's status
     // from device memory, so one capture serves every batch of this system
@@ -303,7 +347,7 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
         if (!k.cap) KSP_CUDA(cudaStreamCreateWithFlags(&k.cap, cudaStreamNonBlocking));
         cudaGraph_t graph = nullptr;
         if (cudaStreamBeginCapture(k.cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-            iterations(k.cap, every);
+            solve_iterations<N>(k, p, k.cap, every);
             if (cudaStreamEndCapture(k.cap, &graph) == cudaSuccess && graph) {
                 if (cudaGraphInstantiate(&k.batch, graph, 0) != cudaSuccess) k.batch = nullptr;
                 cudaGraphDestroy(graph);
@@ -324,21 +368,28 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
             launched += every;
         } else {
             const int c = every < o.max_it - launched ? every : o.max_it - launched;
-            iterations(st, c);
+            solve_iterations<N>(k, p, st, c);
             launched += c;
         }
         KSP_CUDA(cudaGetLastError());
-        KSP_CUDA(cudaMemcpyAsync(k.host, k.scal, sizeof(h), cudaMemcpyDeviceToHost, st));
+        KSP_CUDA(cudaMemcpyAsync(k.host, k.scal, sizeof(osrk::KspScal), cudaMemcpyDeviceToHost, st));
         KSP_CUDA(cudaStreamSynchronize(st));
         if (k.host->reason != osrk::kItersRunning || launched >= o.max_it) break;
     }
-    if (info) {
-        info->reason = k.host->reason == osrk::kItersRunning ? osrk::kDivergedIts : k.host->reason;
-        info->its = k.host->its;
-        info->rnorm0 = k.host->rnorm0;
-        info->rnorm = k.host->rnorm;
-    }
+    ksp_read_host(k, info);
     return OSR_OK;
+}
+
+template <int N>
+static osr_status step_graph_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
+                               const std::function<void(cudaStream_t)> &pre,
+                               const std::function<void(cudaStream_t)> &post, cudaGraphExec_t *out) {
+    osr_status rc = ksp_ensure(g);
+    if (rc != OSR_OK) return rc;
+    const int every = o.check_every > 0 ? o.check_every : 8;
+    if (!(o.max_it >= every && o.max_it % every == 0)) return OSR_ERR_UNSUPPORTED;
+    const SolvePlan<N> p = solve_plan<N>(g, vals, b, x);
+    return build_solve_graph<N>(*g.ksp, p, every, o.max_it, &pre, &post, out) ? OSR_OK : OSR_ERR_CUDA;
 }
 
 // The set-up (stage -1) or stage 1..6 of one slab's distributed solve (the
@@ -414,6 +465,21 @@ static osr_status dksp_stage_n(osr_dksp &d, int stage, cudaStream_t st) {
         case 16: { constexpr int K = 16; return call; }                                                   \
         default: return OSR_ERR_NC;                                                                       \
     }
+
+osr_status ksp_step_graph(osr_grid &grid, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
+                          const std::function<void(cudaStream_t)> &pre, const std::function<void(cudaStream_t)> &post,
+                          cudaGraphExec_t *out) {
+    osr_grid *g = &grid;
+    KSP_SWITCH(step_graph_n<K>(grid, vals, b, x, o, pre, post, out))
+}
+
+void ksp_step_set_host(osr_grid &g, const osr_ksp_opts &o) {
+    if (g.ksp) ksp_set_host(*g.ksp, o);
+}
+
+void ksp_step_read_host(const osr_grid &g, osr_ksp_info *info) {
+    if (g.ksp) ksp_read_host(*g.ksp, info);
+}
 
 }  // namespace osr
 

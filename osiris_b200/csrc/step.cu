@@ -18,6 +18,13 @@
 //   saturations, phase compositions, labels, well latches) is restored and
 //   the row layout rebuilt (RestoreBackups, PJac).  A Dt below MINDT (1e-10 s)
 //   ends the run with an error, where the reference terminates.
+//
+// From the second pass on, InitGuess2 through x1 = x0 - dx and |dx|_1 run as
+// one CUDA graph (the linear solve's iterations inside it as a device-side
+// while loop); the kernels read Dt, the time and PCoeff from a 3-double
+// device array the graph fills first, so one capture serves every pass until
+// the row layout changes.  The acceptance test, UpdateAll(x, true) and
+// TimeStepCtrl stay on the host: they decide what runs next.
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstring>
@@ -77,6 +84,17 @@ struct osr_sim {
     signed char *blab[2] = {nullptr, nullptr};
     std::vector<unsigned char> bcond;
     double *h_sum = nullptr;   // pinned
+    // The step graph: InitGuess2, FormFunction, FormJacobian, the whole
+    // linear solve and x - dx with |dx|_1, one launch per pass.  Its kernels
+    // read the pass's controls [dt, time, PCoeff] from d_ctl, which the graph
+    // fills from the pinned h_ctl first; it is captured again when the row
+    // layout or the solver options change.
+    double *d_ctl = nullptr, *h_ctl = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    long graph_rows = -1;
+    osr_ksp_opts graph_opts{};
+    bool use_graph = true, graph_failed = false;
+    long graph_launches = 0;
 };
 
 namespace {
@@ -89,11 +107,58 @@ namespace {
 
 void sim_free(osr_sim *s) {
     void *ptrs[] = {s->x, s->f, s->dx, s->vals, s->part, s->bP[0], s->bP[1], s->bsat[0], s->bsat[1],
-                    s->bx[0], s->bx[1], s->by[0], s->by[1], s->blab[0], s->blab[1]};
+                    s->bx[0], s->bx[1], s->by[0], s->by[1], s->blab[0], s->blab[1], s->d_ctl};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s->h_sum) cudaFreeHost(s->h_sum);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
     delete s;
+}
+
+bool same_opts(const osr_ksp_opts &a, const osr_ksp_opts &b) {
+    return a.rtol == b.rtol && a.atol == b.atol && a.dtol == b.dtol && a.max_it == b.max_it &&
+           a.check_every == b.check_every;
+}
+
+unsigned norm_blocks(long rows) {
+    long nb = (rows + 255) / 256;
+    if (nb > kSumBlocks) nb = kSumBlocks;
+    if (nb < 1) nb = 1;
+    return (unsigned)nb;
+}
+
+// Capture the step graph for the current row layout and options.  The
+// kernels captured here take the controls from d_ctl (the grid's pointer is
+// set for the capture only); false leaves the sim on direct launches.
+bool build_step_graph(osr_sim &s, const osr_ksp_opts &o) {
+    osr_grid *g = s.g;
+    const long rows = g->n_rows;
+    const unsigned nb = norm_blocks(rows);
+    bool fine = true;
+    auto pre = [&](cudaStream_t cs) {
+        fine = fine && cudaMemcpyAsync(s.d_ctl, s.h_ctl, 3 * sizeof(double), cudaMemcpyHostToDevice, cs) == cudaSuccess;
+        fine = fine && osr_grid_init_guess(g, s.x, cs) == OSR_OK;
+        fine = fine && osr_grid_form_function(g, s.x, s.f, s.sim_time, cs) == OSR_OK;
+        fine = fine && osr_grid_jacobian(g, s.sim_time, s.vals, cs) == OSR_OK;
+    };
+    auto post = [&](cudaStream_t cs) {
+        update_norm1_kernel<<<nb, 256, 0, cs>>>(rows, s.x, s.dx, s.part);
+        sum_parts_kernel<<<1, 32, 0, cs>>>(s.part, (int)nb, s.part + kSumBlocks);
+        fine = fine && cudaMemcpyAsync(s.h_sum, s.part + kSumBlocks, 8, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
+    };
+    g->d_ctl = s.d_ctl;
+    osr_status rc = osr::ksp_step_graph(*g, s.vals, s.f, s.dx, o, pre, post, &s.graph);
+    g->d_ctl = nullptr;
+    if (rc != OSR_OK || !fine) {
+        if (s.graph) cudaGraphExecDestroy(s.graph);
+        s.graph = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    s.graph_rows = rows;
+    s.graph_opts = o;
+    return true;
 }
 
 // CreateBackups / RestoreBackups: the primary state of both continua.
@@ -160,6 +225,8 @@ osr_status osr_sim_create(osr_grid *g, const double *markers, int n_markers, dou
         A((void **)&s->blab[m], n);
     }
     if (e == cudaSuccess) e = cudaMallocHost((void **)&s->h_sum, 8);
+    A((void **)&s->d_ctl, 3 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&s->h_ctl, 3 * sizeof(double));
     if (e != cudaSuccess) {
         sim_free(s);
         return OSR_ERR_CUDA;
@@ -210,6 +277,21 @@ osr_status osr_sim_restart(osr_sim *s, double sim_time, double dt, int tsm_ctrl)
     return rc;
 }
 
+osr_status osr_sim_set_graph(osr_sim *s, int on) {
+    if (!s) return OSR_ERR_ARG;
+    s->use_graph = on != 0;
+    s->graph_failed = false;
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    return OSR_OK;
+}
+
+osr_status osr_sim_graph_launches(osr_sim *s, long *launches) {
+    if (!s || !launches) return OSR_ERR_ARG;
+    *launches = s->graph_launches;
+    return OSR_OK;
+}
+
 osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *info, void *stream) {
     if (!s) return OSR_ERR_ARG;
     osr_grid *g = s->g;
@@ -228,21 +310,44 @@ osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *inf
     if ((rc = osr_grid_set_controls(g, s->dt, 0.0)) != OSR_OK) return rc;
     const long rows = g->n_rows;
     inf.rows = rows;
-    if ((rc = osr_grid_init_guess(g, s->x, stream)) != OSR_OK) return rc;
-    if ((rc = osr_grid_form_function(g, s->x, s->f, s->sim_time, stream)) != OSR_OK) return rc;
-    if ((rc = osr_grid_jacobian(g, s->sim_time, s->vals, stream)) != OSR_OK) return rc;
+    osr_ksp_opts o;
+    osr_ksp_default_opts(&o);
+    if (opts) o = *opts;
     osr_ksp_info ki;
-    if ((rc = osr_grid_ksp_solve(g, s->vals, s->f, s->dx, opts, &ki, stream)) != OSR_OK) return rc;
+    bool graphed = false;
+    if (s->use_graph && !s->graph_failed) {
+        if (s->graph && (s->graph_rows != rows || !same_opts(s->graph_opts, o))) {
+            cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+        }
+        // the Jacobian's scratch is allocated by its first direct call
+        if (!s->graph && g->jw_q && !build_step_graph(*s, o)) s->graph_failed = true;
+        if (s->graph) {
+            s->h_ctl[0] = s->dt;
+            s->h_ctl[1] = s->sim_time;
+            s->h_ctl[2] = g->pcoeff;
+            osr::ksp_step_set_host(*g, o);
+            SIM_CUDA(cudaGraphLaunch(s->graph, st));
+            SIM_CUDA(cudaStreamSynchronize(st));
+            osr::ksp_step_read_host(*g, &ki);
+            s->graph_launches++;
+            graphed = true;
+        }
+    }
+    if (!graphed) {
+        if ((rc = osr_grid_init_guess(g, s->x, stream)) != OSR_OK) return rc;
+        if ((rc = osr_grid_form_function(g, s->x, s->f, s->sim_time, stream)) != OSR_OK) return rc;
+        if ((rc = osr_grid_jacobian(g, s->sim_time, s->vals, stream)) != OSR_OK) return rc;
+        if ((rc = osr_grid_ksp_solve(g, s->vals, s->f, s->dx, &o, &ki, stream)) != OSR_OK) return rc;
+        const unsigned nb = norm_blocks(rows);
+        update_norm1_kernel<<<nb, 256, 0, st>>>(rows, s->x, s->dx, s->part);
+        sum_parts_kernel<<<1, 32, 0, st>>>(s->part, (int)nb, s->part + kSumBlocks);
+        SIM_CUDA(cudaGetLastError());
+        SIM_CUDA(cudaMemcpyAsync(s->h_sum, s->part + kSumBlocks, 8, cudaMemcpyDeviceToHost, st));
+        SIM_CUDA(cudaStreamSynchronize(st));
+    }
     inf.ksp_reason = ki.reason;
     inf.ksp_its = ki.its;
-    long nb = (rows + 255) / 256;
-    if (nb > kSumBlocks) nb = kSumBlocks;
-    if (nb < 1) nb = 1;
-    update_norm1_kernel<<<(unsigned)nb, 256, 0, st>>>(rows, s->x, s->dx, s->part);
-    sum_parts_kernel<<<1, 32, 0, st>>>(s->part, (int)nb, s->part + kSumBlocks);
-    SIM_CUDA(cudaGetLastError());
-    SIM_CUDA(cudaMemcpyAsync(s->h_sum, s->part + kSumBlocks, 8, cudaMemcpyDeviceToHost, st));
-    SIM_CUDA(cudaStreamSynchronize(st));
     const double vnorm = *s->h_sum / (double)rows;
     inf.vnorm = vnorm;
     const bool accepted = ki.reason > 0 && !(vnorm > kTolMain) && vnorm == vnorm;
