@@ -688,14 +688,19 @@ osr_status osr_sim_create(osr_grid *grid, const double *markers, int n_markers, 
  * finished. */
 osr_status osr_sim_step(osr_sim *sim, const osr_ksp_opts *opts, osr_step_info *info, void *stream);
 
-/* Whether osr_sim_step runs a pass's InitGuess2, FormFunction, FormJacobian,
- * linear solve and x - dx as one CUDA graph (default on).  The graph reads
+/* Whether osr_sim_step runs a pass as one CUDA graph (default on): InitGuess2,
+ * FormFunction, FormJacobian, the linear solve, x - dx, the acceptance test
+ * and, by a device-side if / else, UpdateAll(x, true) + CreateBackups or
+ * RestoreBackups + PJac; TimeStepCtrl follows on the host.  The graph reads
  * the pass's Dt, time and PCoeff from device memory, so one capture serves
- * every pass of a row layout; it is captured again after a layout change and
- * gives exactly the direct launches' results.  Off: direct launches. */
+ * every pass until the row count changes, and it gives exactly the direct
+ * launches' results.  Off: direct launches. */
 osr_status osr_sim_set_graph(osr_sim *sim, int on);
 /* Passes run through the step graph so far. */
 osr_status osr_sim_graph_launches(osr_sim *sim, long *launches);
+/* The current step graph: 0 none, 1 linearisation and solve only (the
+ * acceptance and UpdateAll by direct launches), 2 the whole pass. */
+osr_status osr_sim_graph_form(osr_sim *sim, int *form);
 
 /* Current simulation time and Dt (either may be null). */
 osr_status osr_sim_time(osr_sim *sim, double *sim_time, double *dt);

@@ -863,6 +863,12 @@ class Sim:
         _check(lib().osr_sim_graph_launches(self._h, ctypes.byref(n)), "osr_sim_graph_launches")
         return n.value
 
+    def graph_form(self) -> int:
+        """0 no step graph, 1 linearisation and solve, 2 the whole pass."""
+        f = ctypes.c_int()
+        _check(lib().osr_sim_graph_form(self._h, ctypes.byref(f)), "osr_sim_graph_form")
+        return f.value
+
     def marker_index(self) -> int:
         k = ctypes.c_int()
         _check(lib().osr_sim_marker_index(self._h, ctypes.byref(k)), "osr_sim_marker_index")

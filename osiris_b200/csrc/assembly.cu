@@ -334,6 +334,24 @@ static osr_status logk_vjp_n(osr_grid &g, const double *lam, double *gk, double 
     return OSR_OK;
 }
 
+// PJac and CalcPCoeff on the device: block sizes of the current labels, the
+// row offsets (multi-CTA scan), the PCoeff maximum into g.pmax.  Row count
+// and PCoeff stay on the device (osr_grid_refresh_layout reads them back).
+osr_status relayout_launch(osr_grid &g, cudaStream_t st) {
+    const long n = g.cells;
+    block_size_kernel<<<(unsigned)grid_blocks(2 * n), 128, 0, st>>>(g.m[0].label, g.m[1].label, n, g.nc, g.sizes);
+    ASM_CUDA(cudaGetLastError());
+    long *part = g.sizes + 2 * n;
+    scan_sums_kernel<<<kScanBlocks, kScanThreads, 0, st>>>(g.sizes, 2 * n, part);
+    scan_bases_kernel<<<1, 32, 0, st>>>(part, 2 * n, g.rowoff);
+    scan_apply_kernel<<<kScanBlocks, kScanThreads, 0, st>>>(g.sizes, 2 * n, part, g.rowoff);
+    ASM_CUDA(cudaGetLastError());
+    ASM_CUDA(cudaMemsetAsync(g.pmax, 0, 8, st));
+    pcoeff_kernel<<<(unsigned)grid_blocks(n), 128, 0, st>>>(g.m[0].P + n, g.m[1].P + n, n, g.pmax);
+    ASM_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
 template <int N>
 static osr_status well_sums_n(osr_grid &g, int l0, int l1, double *sums, cudaStream_t st) {
     if (g.nwells <= 0) return OSR_OK;
@@ -372,21 +390,12 @@ extern "C" {
 osr_status osr_grid_refresh_layout(osr_grid *g, void *stream) {
     if (!g) return OSR_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    const long n = g->cells;
-    block_size_kernel<<<(unsigned)grid_blocks(2 * n), 128, 0, st>>>(g->m[0].label, g->m[1].label, n, g->nc, g->sizes);
-    ASM_CUDA(cudaGetLastError());
-    long *part = g->sizes + 2 * n;
-    scan_sums_kernel<<<kScanBlocks, kScanThreads, 0, st>>>(g->sizes, 2 * n, part);
-    scan_bases_kernel<<<1, 32, 0, st>>>(part, 2 * n, g->rowoff);
-    scan_apply_kernel<<<kScanBlocks, kScanThreads, 0, st>>>(g->sizes, 2 * n, part, g->rowoff);
-    ASM_CUDA(cudaGetLastError());
-    ASM_CUDA(cudaMemsetAsync(g->pmax, 0, 8, st));
-    pcoeff_kernel<<<(unsigned)grid_blocks(n), 128, 0, st>>>(g->m[0].P + n, g->m[1].P + n, n, g->pmax);
-    ASM_CUDA(cudaGetLastError());
+    osr_status rc = osr::relayout_launch(*g, st);
+    if (rc != OSR_OK) return rc;
     unsigned long long pm = 0;
     long rows = 0;
     ASM_CUDA(cudaMemcpyAsync(&pm, g->pmax, 8, cudaMemcpyDeviceToHost, st));
-    ASM_CUDA(cudaMemcpyAsync(&rows, g->rowoff + 2 * n, 8, cudaMemcpyDeviceToHost, st));
+    ASM_CUDA(cudaMemcpyAsync(&rows, g->rowoff + 2 * g->cells, 8, cudaMemcpyDeviceToHost, st));
     ASM_CUDA(cudaStreamSynchronize(st));
     double p;
     std::memcpy(&p, &pm, 8);

@@ -61,16 +61,25 @@ double peaceman_re(const double *di, const double *dj, int nx, int ny, int ix, i
 osr_status grid_assembly_init(osr_grid &g, const osr_model *md);
 void grid_assembly_free(osr_grid &g);
 void ksp_free(osr_grid &g);
+// PJac / CalcPCoeff launched on `st` without reading the row count and PCoeff
+// back (they stay in rowoff[2 cells] and pmax).
+osr_status relayout_launch(osr_grid &g, cudaStream_t st);
 // The sim's step graph: `pre` (captured ahead), the whole linear solve of
 // vals x = b (the reference's KSP options o), the solve's scalars to the
 // grid's pinned copy, then `post`, as one instantiated graph.
+// `extend` (optional) adds nodes after `post`: it receives the graph, the
+// capture stream and the leaf nodes, and returns false on failure.
+using GraphExtend = std::function<bool(cudaGraph_t, cudaStream_t, const std::vector<cudaGraphNode_t> &)>;
 osr_status ksp_step_graph(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
                           const std::function<void(cudaStream_t)> &pre, const std::function<void(cudaStream_t)> &post,
-                          cudaGraphExec_t *out);
+                          const GraphExtend *extend, cudaGraphExec_t *out);
 // The scalars the step graph's solve starts from (set before each launch)
 // and its outcome (read after the launch has completed).
 void ksp_step_set_host(osr_grid &g, const osr_ksp_opts &o);
 void ksp_step_read_host(const osr_grid &g, osr_ksp_info *info);
+// Device address of the solve's outcome (PETSc KSPConvergedReason; 0 while
+// running), valid once the grid's solve workspace exists.
+const int *ksp_reason_device(const osr_grid &g);
 // Per-component constants at the reservoir temperature, formed with the
 // reference's expressions: EOS_Init (compsim/Init_Calcs.cpp:66-97), Tr_Mu
 // (:48-64) and the pair factors of CalcDiffusion (compsim/Mass_Tran.cpp:43-46).

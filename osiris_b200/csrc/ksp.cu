@@ -2,6 +2,7 @@
 // SolveNonLinear (compsim/PetscAUX.cpp:631-646, 672-698) on the compact
 // Jacobian, and the matrix-vector product alone (MatMult).
 #include <cuda_runtime.h>
+#include <cstddef>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -223,7 +224,8 @@ static void solve_iterations(osr_ksp_work &k, const SolvePlan<N> &p, cudaStream_
 template <int N>
 static bool build_solve_graph(osr_ksp_work &k, const SolvePlan<N> &p, int every, int max_it,
                               const std::function<void(cudaStream_t)> *pre,
-                              const std::function<void(cudaStream_t)> *post, cudaGraphExec_t *out) {
+                              const std::function<void(cudaStream_t)> *post, const GraphExtend *extend,
+                              cudaGraphExec_t *out) {
     *out = nullptr;
     if (!k.cap && cudaStreamCreateWithFlags(&k.cap, cudaStreamNonBlocking) != cudaSuccess) return false;
     const cudaStreamCaptureMode mode = pre || post ? cudaStreamCaptureModeRelaxed : cudaStreamCaptureModeThreadLocal;
@@ -268,8 +270,18 @@ static bool build_solve_graph(osr_ksp_work &k, const SolvePlan<N> &p, int every,
             if (ok) {
                 cudaMemcpyAsync(k.host, k.scal, sizeof(osrk::KspScal), cudaMemcpyDeviceToHost, k.cap);
                 if (post) (*post)(k.cap);
+                std::vector<cudaGraphNode_t> leaves;
+                if (extend) {
+                    cudaStreamCaptureStatus cs2;
+                    const cudaGraphNode_t *d2 = nullptr;
+                    size_t n2 = 0;
+                    ok = cudaStreamGetCaptureInfo(k.cap, &cs2, nullptr, nullptr, &d2, &n2) == cudaSuccess &&
+                         cs2 == cudaStreamCaptureStatusActive;
+                    if (ok) leaves.assign(d2, d2 + n2);
+                }
                 cudaGraph_t eout = nullptr;
-                ok = cudaStreamEndCapture(k.cap, &eout) == cudaSuccess;
+                ok = (cudaStreamEndCapture(k.cap, &eout) == cudaSuccess) && ok;
+                if (ok && extend) ok = (*extend)(G, k.cap, leaves);
             }
         }
     }
@@ -318,7 +330,7 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
         k.whole = nullptr;
     }
     if (!k.whole && !k.whole_failed && o.max_it >= every && o.max_it % every == 0) {
-        if (!build_solve_graph<N>(k, p, every, o.max_it, nullptr, nullptr, &k.whole))
+        if (!build_solve_graph<N>(k, p, every, o.max_it, nullptr, nullptr, nullptr, &k.whole))
             k.whole_failed = true;   // the host-driven batches below serve every later solve
         if (k.whole) {
             k.w_vals = vals;
@@ -383,13 +395,14 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
 template <int N>
 static osr_status step_graph_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
                                const std::function<void(cudaStream_t)> &pre,
-                               const std::function<void(cudaStream_t)> &post, cudaGraphExec_t *out) {
+                               const std::function<void(cudaStream_t)> &post, const GraphExtend *extend,
+                               cudaGraphExec_t *out) {
     osr_status rc = ksp_ensure(g);
     if (rc != OSR_OK) return rc;
     const int every = o.check_every > 0 ? o.check_every : 8;
     if (!(o.max_it >= every && o.max_it % every == 0)) return OSR_ERR_UNSUPPORTED;
     const SolvePlan<N> p = solve_plan<N>(g, vals, b, x);
-    return build_solve_graph<N>(*g.ksp, p, every, o.max_it, &pre, &post, out) ? OSR_OK : OSR_ERR_CUDA;
+    return build_solve_graph<N>(*g.ksp, p, every, o.max_it, &pre, &post, extend, out) ? OSR_OK : OSR_ERR_CUDA;
 }
 
 // The set-up (stage -1) or stage 1..6 of one slab's distributed solve (the
@@ -468,9 +481,13 @@ static osr_status dksp_stage_n(osr_dksp &d, int stage, cudaStream_t st) {
 
 osr_status ksp_step_graph(osr_grid &grid, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
                           const std::function<void(cudaStream_t)> &pre, const std::function<void(cudaStream_t)> &post,
-                          cudaGraphExec_t *out) {
+                          const GraphExtend *extend, cudaGraphExec_t *out) {
     osr_grid *g = &grid;
-    KSP_SWITCH(step_graph_n<K>(grid, vals, b, x, o, pre, post, out))
+    KSP_SWITCH(step_graph_n<K>(grid, vals, b, x, o, pre, post, extend, out))
+}
+
+const int *ksp_reason_device(const osr_grid &g) {
+    return g.ksp ? (const int *)((const char *)g.ksp->scal + offsetof(osrk::KspScal, reason)) : nullptr;
 }
 
 void ksp_step_set_host(osr_grid &g, const osr_ksp_opts &o) {

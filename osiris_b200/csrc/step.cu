@@ -19,12 +19,14 @@
 //   the row layout rebuilt (RestoreBackups, PJac).  A Dt below MINDT (1e-10 s)
 //   ends the run with an error, where the reference terminates.
 //
-// From the second pass on, InitGuess2 through x1 = x0 - dx and |dx|_1 run as
-// one CUDA graph (the linear solve's iterations inside it as a device-side
-// while loop); the kernels read Dt, the time and PCoeff from a 3-double
-// device array the graph fills first, so one capture serves every pass until
-// the row layout changes.  The acceptance test, UpdateAll(x, true) and
-// TimeStepCtrl stay on the host: they decide what runs next.
+// From the second pass on, the whole pass but TimeStepCtrl runs as one CUDA
+// graph: InitGuess2, FormFunction, FormJacobian, the linear solve (its
+// iterations a device-side while loop), x1 = x0 - dx and |dx|_1, the
+// acceptance test, then a device-side if / else: UpdateAll(x1, true) and
+// CreateBackups, or RestoreBackups and PJac.  The kernels read Dt, the time
+// and PCoeff from a 3-double device array the graph fills first, so one
+// capture serves every pass until the row count changes.  TimeStepCtrl (a
+// few host scalars) follows on the host.
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstring>
@@ -70,6 +72,19 @@ __global__ void sum_parts_kernel(const double *part, int n, double *out) {
     }
 }
 
+// The acceptance test of SolveNonLinear (compsim/PetscAUX.cpp:703): the solve
+// converged and |dx|_1 / rows <= TOLMAIN is a number; selects the branch of
+// the full step graph (UpdateAll(x, true) + CreateBackups, or RestoreBackups).
+__global__ void accept_kernel(cudaGraphConditionalHandle h, const int *reason, const double *sum, double rows,
+                              int *flag) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const double vnorm = *sum / rows;
+        const bool ok = *reason > 0 && !(vnorm > kTolMain) && vnorm == vnorm;
+        *flag = ok ? 1 : 0;
+        cudaGraphSetConditional(h, ok ? 1u : 0u);
+    }
+}
+
 }  // namespace
 
 struct osr_sim {
@@ -94,7 +109,16 @@ struct osr_sim {
     long graph_rows = -1;
     osr_ksp_opts graph_opts{};
     bool use_graph = true, graph_failed = false;
+    bool graph_full = false;   // the graph also takes the acceptance and UpdateAll / RestoreBackups
     long graph_launches = 0;
+    // what the full graph hands back: PCoeff (bits), row count, acceptance
+    struct PassOut {
+        unsigned long long pmax;
+        long rows;
+        int accepted, pad;
+    };
+    PassOut *h_out = nullptr;   // pinned
+    int *d_flag = nullptr;
 };
 
 namespace {
@@ -107,11 +131,12 @@ namespace {
 
 void sim_free(osr_sim *s) {
     void *ptrs[] = {s->x, s->f, s->dx, s->vals, s->part, s->bP[0], s->bP[1], s->bsat[0], s->bsat[1],
-                    s->bx[0], s->bx[1], s->by[0], s->by[1], s->blab[0], s->blab[1], s->d_ctl};
+                    s->bx[0], s->bx[1], s->by[0], s->by[1], s->blab[0], s->blab[1], s->d_ctl, s->d_flag};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s->h_sum) cudaFreeHost(s->h_sum);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
+    if (s->h_out) cudaFreeHost(s->h_out);
     if (s->graph) cudaGraphExecDestroy(s->graph);
     delete s;
 }
@@ -128,41 +153,10 @@ unsigned norm_blocks(long rows) {
     return (unsigned)nb;
 }
 
-// Capture the step graph for the current row layout and options.  The
-// kernels captured here take the controls from d_ctl (the grid's pointer is
-// set for the capture only); false leaves the sim on direct launches.
-bool build_step_graph(osr_sim &s, const osr_ksp_opts &o) {
-    osr_grid *g = s.g;
-    const long rows = g->n_rows;
-    const unsigned nb = norm_blocks(rows);
-    bool fine = true;
-    auto pre = [&](cudaStream_t cs) {
-        fine = fine && cudaMemcpyAsync(s.d_ctl, s.h_ctl, 3 * sizeof(double), cudaMemcpyHostToDevice, cs) == cudaSuccess;
-        fine = fine && osr_grid_init_guess(g, s.x, cs) == OSR_OK;
-        fine = fine && osr_grid_form_function(g, s.x, s.f, s.sim_time, cs) == OSR_OK;
-        fine = fine && osr_grid_jacobian(g, s.sim_time, s.vals, cs) == OSR_OK;
-    };
-    auto post = [&](cudaStream_t cs) {
-        update_norm1_kernel<<<nb, 256, 0, cs>>>(rows, s.x, s.dx, s.part);
-        sum_parts_kernel<<<1, 32, 0, cs>>>(s.part, (int)nb, s.part + kSumBlocks);
-        fine = fine && cudaMemcpyAsync(s.h_sum, s.part + kSumBlocks, 8, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
-    };
-    g->d_ctl = s.d_ctl;
-    osr_status rc = osr::ksp_step_graph(*g, s.vals, s.f, s.dx, o, pre, post, &s.graph);
-    g->d_ctl = nullptr;
-    if (rc != OSR_OK || !fine) {
-        if (s.graph) cudaGraphExecDestroy(s.graph);
-        s.graph = nullptr;
-        cudaGetLastError();
-        return false;
-    }
-    s.graph_rows = rows;
-    s.graph_opts = o;
-    return true;
-}
 
-// CreateBackups / RestoreBackups: the primary state of both continua.
-osr_status copy_state(osr_sim &s, bool to_backup, cudaStream_t st) {
+// CreateBackups / RestoreBackups: the primary state of both continua (device
+// copies; capturable).
+osr_status copy_state_device(osr_sim &s, bool to_backup, cudaStream_t st) {
     osr_grid &g = *s.g;
     const long n = g.cells, nc = g.nc;
     for (int m = 0; m < 2; m++) {
@@ -179,6 +173,12 @@ osr_status copy_state(osr_sim &s, bool to_backup, cudaStream_t st) {
             SIM_CUDA(cudaMemcpyAsync(to_backup ? it.bak : it.live, to_backup ? it.live : it.bak, it.bytes,
                                      cudaMemcpyDeviceToDevice, st));
     }
+    return OSR_OK;
+}
+
+// The well latches of the backup (host side of CreateBackups / RestoreBackups).
+osr_status copy_conds(osr_sim &s, bool to_backup) {
+    osr_grid &g = *s.g;
     if (to_backup) {
         s.bcond = g.cond_host;
     } else {
@@ -189,6 +189,99 @@ osr_status copy_state(osr_sim &s, bool to_backup, cudaStream_t st) {
             }
     }
     return OSR_OK;
+}
+
+osr_status copy_state(osr_sim &s, bool to_backup, cudaStream_t st) {
+    osr_status rc = copy_state_device(s, to_backup, st);
+    return rc != OSR_OK ? rc : copy_conds(s, to_backup);
+}
+
+// Capture the step graph for the current row layout and options.  The
+// kernels captured here take the controls from d_ctl (the grid's pointer is
+// set for the capture only).  full: the graph also runs the acceptance test
+// and, by a device-side if / else, UpdateAll(x, true) + CreateBackups or
+// RestoreBackups + PJac, handing PCoeff, the row count and the decision back
+// to pinned memory.  False leaves the sim on the shorter graph or on direct
+// launches.
+bool build_step_graph(osr_sim &s, const osr_ksp_opts &o, bool full) {
+    osr_grid *g = s.g;
+    const long rows = g->n_rows;
+    const unsigned nb = norm_blocks(rows);
+    bool fine = true;
+    auto pre = [&](cudaStream_t cs) {
+        fine = fine && cudaMemcpyAsync(s.d_ctl, s.h_ctl, 3 * sizeof(double), cudaMemcpyHostToDevice, cs) == cudaSuccess;
+        fine = fine && osr_grid_init_guess(g, s.x, cs) == OSR_OK;
+        fine = fine && osr_grid_form_function(g, s.x, s.f, s.sim_time, cs) == OSR_OK;
+        fine = fine && osr_grid_jacobian(g, s.sim_time, s.vals, cs) == OSR_OK;
+    };
+    auto post = [&](cudaStream_t cs) {
+        update_norm1_kernel<<<nb, 256, 0, cs>>>(rows, s.x, s.dx, s.part);
+        sum_parts_kernel<<<1, 32, 0, cs>>>(s.part, (int)nb, s.part + kSumBlocks);
+        fine = fine && cudaMemcpyAsync(s.h_sum, s.part + kSumBlocks, 8, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
+    };
+    osr::GraphExtend ext = [&](cudaGraph_t G, cudaStream_t cs, const std::vector<cudaGraphNode_t> &leaves) -> bool {
+        const cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, G, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+        if (cudaStreamBeginCaptureToGraph(cs, G, leaves.data(), nullptr, leaves.size(), mode) != cudaSuccess)
+            return false;
+        accept_kernel<<<1, 32, 0, cs>>>(h, osr::ksp_reason_device(*g), s.part + kSumBlocks, (double)rows, s.d_flag);
+        cudaStreamCaptureStatus st2;
+        const cudaGraphNode_t *d2 = nullptr;
+        size_t n2 = 0;
+        bool ok = cudaStreamGetCaptureInfo(cs, &st2, nullptr, nullptr, &d2, &n2) == cudaSuccess &&
+                  st2 == cudaStreamCaptureStatusActive;
+        std::vector<cudaGraphNode_t> tail(d2, d2 + (ok ? n2 : 0));
+        cudaGraph_t tmp = nullptr;
+        ok = (cudaStreamEndCapture(cs, &tmp) == cudaSuccess) && ok;
+        if (!ok) return false;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 2;   // if: accepted; else: rejected
+        cudaGraphNode_t ifnode = nullptr;
+        if (cudaGraphAddNode(&ifnode, G, tail.data(), tail.size(), &cp) != cudaSuccess) return false;
+        cudaGraph_t acc = cp.conditional.phGraph_out[0], rej = cp.conditional.phGraph_out[1];
+        // accepted: UpdateAll(x, true) (unpack, PhaseCtrl, PJac, properties) and CreateBackups
+        if (cudaStreamBeginCaptureToGraph(cs, acc, nullptr, nullptr, 0, mode) != cudaSuccess) return false;
+        fine = fine && osr::grid_unpack(*g, s.x, cs) == OSR_OK;
+        fine = fine && osr_grid_phase_ctrl(g, cs) == OSR_OK;
+        fine = fine && osr::relayout_launch(*g, cs) == OSR_OK;
+        fine = fine && osr::grid_update(*g, cs) == OSR_OK;
+        fine = fine && copy_state_device(s, true, cs) == OSR_OK;
+        ok = cudaStreamEndCapture(cs, &tmp) == cudaSuccess;
+        // rejected: RestoreBackups and PJac of the restored labels
+        if (ok) ok = cudaStreamBeginCaptureToGraph(cs, rej, nullptr, nullptr, 0, mode) == cudaSuccess;
+        if (ok) {
+            fine = fine && copy_state_device(s, false, cs) == OSR_OK;
+            fine = fine && osr::relayout_launch(*g, cs) == OSR_OK;
+            ok = cudaStreamEndCapture(cs, &tmp) == cudaSuccess;
+        }
+        // PCoeff, the row count and the decision back to the host
+        if (ok) ok = cudaStreamBeginCaptureToGraph(cs, G, &ifnode, nullptr, 1, mode) == cudaSuccess;
+        if (ok) {
+            fine = fine && cudaMemcpyAsync(&s.h_out->pmax, g->pmax, 8, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
+            fine = fine && cudaMemcpyAsync(&s.h_out->rows, g->rowoff + 2 * g->cells, 8, cudaMemcpyDeviceToHost,
+                                           cs) == cudaSuccess;
+            fine = fine && cudaMemcpyAsync(&s.h_out->accepted, s.d_flag, 4, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
+            ok = cudaStreamEndCapture(cs, &tmp) == cudaSuccess;
+        }
+        return ok;
+    };
+    g->d_ctl = s.d_ctl;
+    osr_status rc = osr::ksp_step_graph(*g, s.vals, s.f, s.dx, o, pre, post, full ? &ext : nullptr, &s.graph);
+    g->d_ctl = nullptr;
+    if (rc != OSR_OK || !fine) {
+        if (s.graph) cudaGraphExecDestroy(s.graph);
+        s.graph = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    s.graph_rows = rows;
+    s.graph_opts = o;
+    s.graph_full = full;
+    return true;
 }
 
 }  // namespace
@@ -226,7 +319,9 @@ osr_status osr_sim_create(osr_grid *g, const double *markers, int n_markers, dou
     }
     if (e == cudaSuccess) e = cudaMallocHost((void **)&s->h_sum, 8);
     A((void **)&s->d_ctl, 3 * sizeof(double));
+    A((void **)&s->d_flag, sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&s->h_ctl, 3 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&s->h_out, sizeof(osr_sim::PassOut));
     if (e != cudaSuccess) {
         sim_free(s);
         return OSR_ERR_CUDA;
@@ -292,6 +387,12 @@ osr_status osr_sim_graph_launches(osr_sim *s, long *launches) {
     return OSR_OK;
 }
 
+osr_status osr_sim_graph_form(osr_sim *s, int *form) {
+    if (!s || !form) return OSR_ERR_ARG;
+    *form = !s->graph ? 0 : s->graph_full ? 2 : 1;
+    return OSR_OK;
+}
+
 osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *info, void *stream) {
     if (!s) return OSR_ERR_ARG;
     osr_grid *g = s->g;
@@ -314,14 +415,16 @@ osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *inf
     osr_ksp_default_opts(&o);
     if (opts) o = *opts;
     osr_ksp_info ki;
-    bool graphed = false;
+    bool graphed = false, full = false;
     if (s->use_graph && !s->graph_failed) {
         if (s->graph && (s->graph_rows != rows || !same_opts(s->graph_opts, o))) {
             cudaGraphExecDestroy(s->graph);
             s->graph = nullptr;
         }
-        // the Jacobian's scratch is allocated by its first direct call
-        if (!s->graph && g->jw_q && !build_step_graph(*s, o)) s->graph_failed = true;
+        // the Jacobian's scratch is allocated by its first direct call; the
+        // full graph first, the linearisation-and-solve graph if it fails
+        if (!s->graph && g->jw_q && !build_step_graph(*s, o, true) && !build_step_graph(*s, o, false))
+            s->graph_failed = true;
         if (s->graph) {
             s->h_ctl[0] = s->dt;
             s->h_ctl[1] = s->sim_time;
@@ -332,6 +435,7 @@ osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *inf
             osr::ksp_step_read_host(*g, &ki);
             s->graph_launches++;
             graphed = true;
+            full = s->graph_full;
         }
     }
     if (!graphed) {
@@ -350,9 +454,16 @@ osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *inf
     inf.ksp_its = ki.its;
     const double vnorm = *s->h_sum / (double)rows;
     inf.vnorm = vnorm;
-    const bool accepted = ki.reason > 0 && !(vnorm > kTolMain) && vnorm == vnorm;
+    const bool accepted = full ? s->h_out->accepted != 0 : (ki.reason > 0 && !(vnorm > kTolMain) && vnorm == vnorm);
     inf.accepted = accepted ? 1 : 0;
-    if (accepted) {
+    if (full) {
+        // the graph ran UpdateAll(x, true) + CreateBackups or RestoreBackups + PJac
+        double p;
+        std::memcpy(&p, &s->h_out->pmax, 8);
+        g->pcoeff = p;
+        g->n_rows = s->h_out->rows;
+        if ((rc = copy_conds(*s, accepted)) != OSR_OK) return rc;
+    } else if (accepted) {
         if ((rc = osr_grid_update_all_full(g, s->x, stream)) != OSR_OK) return rc;
         if ((rc = copy_state(*s, true, st)) != OSR_OK) return rc;
     }
@@ -375,8 +486,10 @@ osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *inf
         s->inc_count = 0;
         s->dt /= kStepDec;
         if (s->dt < kMinDt) return OSR_ERR_UNSUPPORTED;
-        if ((rc = copy_state(*s, false, st)) != OSR_OK) return rc;
-        if ((rc = osr_grid_refresh_layout(g, stream)) != OSR_OK) return rc;
+        if (!full) {
+            if ((rc = copy_state(*s, false, st)) != OSR_OK) return rc;
+            if ((rc = osr_grid_refresh_layout(g, stream)) != OSR_OK) return rc;
+        }
     }
     SIM_CUDA(cudaStreamSynchronize(st));
     inf.sim_time = s->sim_time;

@@ -1,7 +1,8 @@
 """The time step's CUDA graph (osr_sim_set_graph): from the second pass on,
-InitGuess2, FormFunction, FormJacobian, the whole linear solve and
-x1 = x0 - dx run as one graph launch whose kernels read Dt, the time and
-PCoeff from device memory.  Two runs of the same deck, one through the graph
+InitGuess2, FormFunction, FormJacobian, the whole linear solve,
+x1 = x0 - dx, the acceptance test and the device-side branch (UpdateAll(x1,
+true) + CreateBackups, or RestoreBackups + PJac) run as one graph launch
+whose kernels read Dt, the time and PCoeff from device memory.  Two runs of the same deck, one through the graph
 and one through direct launches, must take identical passes (accepted or
 not, Dt, time, row count, solver iterations and reason, |dx|_1 / rows) and
 hold bit-identical states after every pass, through rejections, phase
@@ -62,6 +63,7 @@ def test_graph_passes_equal_direct_launches(name, tmp_path, cuda_device):
     assert accepted > 0
     launches = runs[0][1].graph_launches()
     assert launches == passes - 1, (launches, passes)      # every pass after the first
+    assert runs[0][1].graph_form() == 2                    # the whole pass, acceptance and UpdateAll included
     assert runs[1][1].graph_launches() == 0
     if name in LAYOUT_CHANGES:
         assert len(layouts) > 1, layouts
