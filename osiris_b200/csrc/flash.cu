@@ -844,9 +844,27 @@ osr_status osr_flash_batch_plain(const osr_fluid *fluid, const double *d_P, cons
 // k % 3 with that stream's device buffers, so the copies of the chunks before
 // and after it (both directions of PCIe at once) overlap its flash.  Every
 // cell's result is independent of how the cells are grouped.
-constexpr int kHostStreams = 3;
-constexpr long kHostChunkCells = 131072;
-constexpr int kHostMaxChunks = 16;
+// Host pipeline of osr_flash_batch_host: chunks of g_host_chunk cells, each
+// copied in, flashed and copied out on one of g_host_streams streams in turn
+// (osr_flash_set_host_pipeline).
+constexpr int kHostStreams = 8;   // most streams
+constexpr int kHostMaxChunks = 64;
+static std::atomic<int> g_host_streams{4};
+static std::atomic<long> g_host_chunk{131072};
+
+osr_status osr_flash_set_host_pipeline(int streams, long chunk_cells) {
+    if (streams < 1 || streams > kHostStreams || chunk_cells < 1024) return OSR_ERR_ARG;
+    g_host_streams.store(streams);
+    g_host_chunk.store(chunk_cells);
+    return OSR_OK;
+}
+
+osr_status osr_flash_get_host_pipeline(int *streams, long *chunk_cells) {
+    if (!streams || !chunk_cells) return OSR_ERR_ARG;
+    *streams = g_host_streams.load();
+    *chunk_cells = g_host_chunk.load();
+    return OSR_OK;
+}
 
 osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const double *T, const double *z, long n,
                                 const osr_flash_out *out, void *stream) {
@@ -859,11 +877,12 @@ osr_status osr_flash_batch_host(const osr_fluid *fluid, const double *P, const d
     cudaStream_t s = (cudaStream_t)stream;
     const int nc = fluid->nc;
     const bool derivs = out->dlnphi_dx != nullptr;
-    long chunks = n / kHostChunkCells;
+    long chunks = n / g_host_chunk.load();
     if (chunks < 1) chunks = 1;
     if (chunks > kHostMaxChunks) chunks = kHostMaxChunks;
     const long m = (n + chunks - 1) / chunks;   // cells per chunk (the last may hold fewer)
-    const int slots = chunks < kHostStreams ? (int)chunks : kHostStreams;
+    const int nstreams = g_host_streams.load();
+    const int slots = chunks < nstreams ? (int)chunks : nstreams;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t md = (size_t)m;
     const size_t szP = al(md * 8), szz = al(md * nc * 8), szl = al(md), szi = al(md * 4);
