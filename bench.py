@@ -72,6 +72,10 @@ def parse():
     ap.add_argument("--steps-grids", default=None, help="NX,NY,NZ[;...] of the scaled time-stepping runs")
     ap.add_argument("--steps-passes", type=int, default=None, help="passes timed per scaled grid (3)")
     ap.add_argument("--steps-scaled-only", action="store_true", help="skip the small plain case (profiling)")
+    ap.add_argument("--ksp-check-every", type=int, default=None,
+                    help="BiCGStab iterations between host status reads in the scaled runs; one that does not "
+                         "divide MAXITERS keeps the solve on host-driven batches (profiling: ncu does not see "
+                         "kernels inside graphs with conditional nodes)")
     ap.add_argument("--part", choices=["all", "assembly", "steps", "slabs"], default="all",
                     help="assembly: only the Newton-step assembly object (profiling); slabs: the z-slab Newton "
                          "step over the ranks (one grid split across the GPUs)")
@@ -760,8 +764,11 @@ def measure_steps(osr, torch, dev, args, cpu_sample=False):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(passes + 1)]
         rec = []
         ev[0].record()
+        ksp = {} if args.ksp_check_every is None else {"check_every": args.ksp_check_every}
+        if ksp:
+            sim.set_graph(False)
         for k in range(passes):
-            rec.append(sim.step())
+            rec.append(sim.step(**ksp))
             ev[k + 1].record()
         torch.cuda.synchronize(dev)
         ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(passes)]

@@ -611,6 +611,16 @@ void osr_ksp_default_opts(osr_ksp_opts *opts);
 osr_status osr_grid_jacobian_apply(osr_grid *grid, const double *d_vals, const double *d_x, double *d_y,
                                    void *stream);
 
+/* y = J^T lambda (MatMultTranspose) on the compact Jacobian d_vals: the
+ * vector-Jacobian product of the residual in the unknowns at the state the
+ * Jacobian was formed at (the step an adjoint of the Newton system takes).
+ * Every stored value adds value * lambda[row] into y[column] of its reference
+ * (row, column); values that are exactly zero are skipped.  Atomic additions:
+ * the last bits may differ between runs.  DEVICE vectors of the layout's row
+ * count; asynchronous. */
+osr_status osr_grid_jacobian_apply_transpose(osr_grid *grid, const double *d_vals, const double *d_lambda,
+                                            double *d_y, void *stream);
+
 /* Solve J d_sol = d_rhs from a zero initial guess with left-preconditioned
  * BiCGStab and the inverse diagonal blocks of J (one block per cell-medium)
  * as preconditioner, PETSc's KSPBCGS + PCVPBJACOBI.  opts may be null (the

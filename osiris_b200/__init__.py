@@ -800,6 +800,13 @@ class Grid:
                                              _vp(d_y.data_ptr()), None if stream is None else _vp(stream)),
                "osr_grid_jacobian_apply")
 
+    def jacobian_apply_transpose(self, vals, d_lambda, d_y, stream=None):
+        """d_y = J^T d_lambda (MatMultTranspose; the residual's product with
+        an adjoint vector in the unknowns)."""
+        _check(lib().osr_grid_jacobian_apply_transpose(self._h, _vp(vals.data_ptr()), _vp(d_lambda.data_ptr()),
+                                                       _vp(d_y.data_ptr()), None if stream is None else _vp(stream)),
+               "osr_grid_jacobian_apply_transpose")
+
     def ksp_solve(self, vals, d_rhs, d_sol, stream=None, **opts) -> dict:
         """Solve J d_sol = d_rhs (KSPBCGS + PCVPBJACOBI, zero initial guess);
         keyword overrides of the reference's tolerances: rtol, atol, dtol,

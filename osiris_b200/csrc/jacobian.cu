@@ -217,6 +217,28 @@ static osr_status jacobian_n(osr_grid &g, double sim_time, double *vals, cudaStr
     return launch_rows<4>(v, 0, chunks, st);
 }
 
+// y += J^T lambda (MatMultTranspose): every stored value adds value x
+// lambda[row] into y[column] of its reference (row, column).  Values that are
+// exactly zero are skipped, as a sparse product skips absent entries.  The
+// additions into one y entry come from several block rows (atomic adds), so
+// the last bits may differ between runs.
+__global__ void jacobian_transpose_kernel(int N, int nx, int ny, int nz, long n, const long *rowoff,
+                                          const signed char *lab_m, const signed char *lab_f, int entries,
+                                          const double *vals, const double *lam, double *y) {
+    const long nb = 2 * n, total = (nb + 31) / 32 * 32 * entries;
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+        const long chunk = idx / (32L * entries);
+        const int e = (int)((idx / 32) % entries);
+        const long b = chunk * 32 + (idx & 31);
+        if (b >= nb) continue;
+        const double v = vals[idx];
+        if (v == 0.0) continue;
+        long r = -1, c = -1;
+        osrj::entry_position(N, nx, ny, nz, n, rowoff, lab_m, lab_f, b, e, &r, &c);
+        if (r >= 0 && c >= 0) atomicAdd(y + c, v * lam[r]);
+    }
+}
+
 static osr_status ensure_jacobian_scratch(osr_grid &g) {
     if (g.jw_q) return OSR_OK;
     const long nb = 2 * g.cells;
@@ -265,6 +287,22 @@ osr_status osr_grid_block_columns(osr_grid *g, long *out) {
         o[6] = iz < g->nz - 1 ? b + (long)g->nx * g->ny : -1;
         o[7] = med ? c : n + c;
     }
+    return OSR_OK;
+}
+
+osr_status osr_grid_jacobian_apply_transpose(osr_grid *g, const double *d_vals, const double *d_lambda, double *d_y,
+                                            void *stream) {
+    if (!g || !d_vals || !d_lambda || !d_y || !g->rowoff || g->n_rows <= 0) return OSR_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    const osrj::Layout L(g->nc);
+    JAC_CUDA(cudaMemsetAsync(d_y, 0, (size_t)g->n_rows * 8, st));
+    const long total = (2 * g->cells + 31) / 32 * 32 * L.ET;
+    long blocks = (total + 255) / 256;
+    if (blocks > 148L * 32) blocks = 148L * 32;
+    jacobian_transpose_kernel<<<(unsigned)blocks, 256, 0, st>>>(g->nc, g->nx, g->ny, g->nz, g->cells, g->rowoff,
+                                                                g->m[0].label, g->m[1].label, L.ET, d_vals, d_lambda,
+                                                                d_y);
+    JAC_CUDA(cudaGetLastError());
     return OSR_OK;
 }
 

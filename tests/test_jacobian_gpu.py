@@ -129,3 +129,35 @@ def test_pattern_covers_every_reference_entry(tmp_path, cuda_device):
     mine = set(zip(r[keep].tolist(), c[keep].tolist()))
     missing = set(zip(rr.tolist(), rc.tolist())) - mine
     assert not missing, sorted(missing)[:10]
+
+
+@pytest.mark.parametrize("name", ["state_pairs_diffusion", "sample_12MPa", "all_well_types_9MPa_latched"])
+def test_transpose_product_matches_reference(name, tmp_path, cuda_device):
+    """J^T lambda (osr_grid_jacobian_apply_transpose) against the reference's
+    own matrix transposed: within 1e-9 of sum_r |J_ref[r, c]| |lambda_r| per
+    entry (the row bar of the matrix test carried through the sum), and
+    within 1e-12 of the same scale against the device values' own COO
+    product (rounding of the atomic sums only)."""
+    import torch
+    R, G = open_pair(tmp_path, name)
+    t = CASES[name][1]
+    n, _ = G.refresh_layout()
+    x0 = R.init_guess()
+    rng = np.random.default_rng(6)
+    xp = x0 * (1 + 1e-2 * rng.uniform(-1, 1, x0.shape))
+    Jr = np.nan_to_num(dense(*R.form_jacobian(xp, t), n))
+    Jb = G.alloc_jacobian(cuda_device)
+    assert G.form_jacobian(torch.tensor(xp, device=cuda_device), Jb, t) == 0
+    lam = rng.standard_normal(n)
+    y = torch.zeros(n, dtype=torch.float64, device=cuda_device)
+    G.jacobian_apply_transpose(Jb, torch.tensor(lam, device=cuda_device), y)
+    torch.cuda.synchronize()
+    y = y.cpu().numpy()
+    Jg = dense(*G.jacobian_coo(Jb), n)
+    finite = np.isfinite(Jg).all(axis=0)
+    scale = np.abs(Jr).T @ np.abs(lam) + 1e-300
+    mine = np.nan_to_num(Jg).T @ lam
+    assert np.all(np.abs(y - mine)[finite] <= 1e-12 * scale[finite])
+    err = (np.abs(y - Jr.T @ lam) / scale)[finite]
+    print(f"{name}: {int(finite.sum())} of {n} columns finite, worst scaled error {err.max():.2e}")
+    assert err.max() <= 1e-9
