@@ -443,12 +443,21 @@ def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max
         return out
 
     ms_streams = timed(step_streams)
+    # the same step as one persistent cooperative kernel launch (device work table)
+    ms_persist = None
+    try:
+        ms_persist = timed(lambda: plan.run_persistent(stream))
+        if plan.persistent_error(stream) != 0:
+            ms_persist = None
+    except osr.OsrError:
+        ms_persist = None
     barrier()
     clocks = ClockSampler(gpu_id)
     ms = timed(step)
     clk = clocks.stop()
     barrier()
     m_streams = max_over_ranks(sum(ms_streams) / len(ms_streams))
+    m_persist = max_over_ranks(sum(ms_persist) / len(ms_persist)) if ms_persist else None
     plan.close()
     if tuned:
         osr.use_tuned(False)
@@ -500,6 +509,10 @@ def measure_instances(osr, torch, dev, stream, flush, args, groups, barrier, max
                    "l2": "flushed before every step (256 MiB write)"},
         "streams_form": {"value": world * n_total / (m_streams * 1e-3), "ms_per_step": m_streams,
                          "calls_per_step": len(G), "streams": len(G)},
+        "persistent_form": None if m_persist is None else {
+            "value": world * n_total / (m_persist * 1e-3), "ms_per_step": m_persist, "launches_per_step": 1,
+            "launch": "one cooperative kernel over every (component count, pass) work item "
+                      "(osr_flash_plan_run_persistent)"},
         "one_instance_per_launch": forms,
         "batched_over_plain": (world * n_total / (m * 1e-3)) / forms["plain"]["value"],
         "cpu_baseline": cpu_line,

@@ -146,6 +146,19 @@ typedef struct {
 typedef struct osr_flash_plan osr_flash_plan;
 osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, osr_flash_plan **out);
 osr_status osr_flash_plan_run(osr_flash_plan *plan, void *stream);
+/* The same step as ONE persistent cooperative kernel launch: every group's
+ * passes and derivative pass are work items of a device-side work table
+ * (pass p + 1 of a group opens when pass p has no cell left and no CTA in
+ * it), taken by whichever CTA is free; each item runs the same pass body as
+ * the separate launches, so the results equal osr_flash_plan_run's bit for
+ * bit.  Waits for an item are bounded: past the bound the launch records
+ * an error (osr_flash_plan_persistent_error) and ends.  OSR_ERR_UNSUPPORTED
+ * when the plan has more than 16 groups or the group form is enabled
+ * (osr_flash_set_group_from) for a pass the plan runs. */
+osr_status osr_flash_plan_run_persistent(osr_flash_plan *plan, void *stream);
+/* 1 when a persistent run's wait for a work item ran past its bound
+ * (synchronises `stream`). */
+osr_status osr_flash_plan_persistent_error(osr_flash_plan *plan, int *error, void *stream);
 void osr_flash_plan_destroy(osr_flash_plan *plan);
 
 /* Same results, plain form: one thread per cell, no work queue.  Kept as the

@@ -374,6 +374,23 @@ class FlashPlan:
             stream = torch.cuda.current_stream(self.groups[0]["P"].device)
         _check(lib().osr_flash_plan_run(self._h, _vp(stream.cuda_stream)), "osr_flash_plan_run")
 
+    def run_persistent(self, stream=None):
+        """The same step as one persistent cooperative kernel launch
+        (osr_flash_plan_run_persistent)."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(self.groups[0]["P"].device)
+        _check(lib().osr_flash_plan_run_persistent(self._h, _vp(stream.cuda_stream)), "osr_flash_plan_run_persistent")
+
+    def persistent_error(self, stream=None) -> int:
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(self.groups[0]["P"].device)
+        e = ctypes.c_int()
+        _check(lib().osr_flash_plan_persistent_error(self._h, ctypes.byref(e), _vp(stream.cuda_stream)),
+               "osr_flash_plan_persistent_error")
+        return e.value
+
     def close(self):
         if getattr(self, "_h", None):
             lib().osr_flash_plan_destroy(self._h)

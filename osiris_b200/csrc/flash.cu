@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <atomic>
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <cstdio>
@@ -494,6 +495,235 @@ static osr_status plan_launch_n(const osr_flash_group &gr, const PlanGroup &pg, 
 }
 
 // ---------------------------------------------------------------------------
+// Persistent form of a flash plan: one cooperative launch runs every group's
+// passes and derivative pass.  Each (group, stage) is a work item -- stage p
+// < passes is pass p of that group's multi-pass work queue, the last stage
+// its derivative pass -- and stage p + 1 of a group opens when stage p has
+// no cell left and no CTA working in it.  A CTA with nothing to do takes the
+// first open item that still has cells (groups scanned in one fixed
+// order), runs the same pass body the separate kernels run (queue or pair
+// form, by the group's pair_from), and on leaving the last CTA of an item
+// opens the next stage.  All CTAs are resident (cooperative launch), so an
+// item's workers always finish; a CTA waiting for an item sleeps in bounded
+// rounds and, past the bound, records an error and leaves.  The parked
+// lists and the iteration results that a later stage reads are loaded
+// through L2 (written by other CTAs of the same launch).
+
+constexpr int kPersistMaxGroups = 16;
+constexpr long kDerivUnit = 2048;   // cells (both phases) per derivative work unit
+
+struct PersistGroup {
+    int nc, passes, pair_from, stages;
+    long cells;
+    const void *pass_args[kMaxPasses];          // device QueueArgs<nc> of each pass
+    const void *deriv_args;                     // device DerivArgs<nc>, or null
+    const unsigned long long *head[kMaxPasses]; // queue head of each pass
+    const unsigned *src_count[kMaxPasses];      // cells of pass p (p > 0)
+};
+
+struct PersistState {
+    unsigned stage[kPersistMaxGroups];                    // open stage of each group
+    unsigned active[kPersistMaxGroups][kMaxPasses + 1];   // CTAs working in each item
+    unsigned long long deriv_next[kPersistMaxGroups];     // next derivative unit
+    int error;                                            // a wait ran past its bound
+};
+
+__device__ __forceinline__ bool persist_has_work(const PersistGroup &G, int st, const PersistState *s, int g) {
+    if (st < G.passes) {
+        const long total = st == 0 ? G.cells : (long)__ldcg(G.src_count[st]);
+        return (long)__ldcg(G.head[st]) < total;
+    }
+    const long units = (G.cells + kDerivUnit - 1) / kDerivUnit;
+    return (long)__ldcg(&s->deriv_next[g]) < units;
+}
+
+// The stage's arguments are copied into shared memory first: the pass bodies
+// read them in their inner loops, and from shared memory the compiler can
+// keep them across the bodies' global stores (a global copy could alias
+// those stores and would be re-read).
+constexpr size_t kPersistArgBytes = sizeof(QueueArgs<16>) > sizeof(DerivArgs<16>) ? sizeof(QueueArgs<16>)
+                                                                                   : sizeof(DerivArgs<16>);
+
+__device__ __forceinline__ void persist_load_args(void *dst, const void *src, size_t bytes) {
+    const unsigned long long *sv = (const unsigned long long *)src;
+    unsigned long long *dv = (unsigned long long *)dst;
+    for (size_t i = threadIdx.x; i < bytes / 8; i += blockDim.x) dv[i] = sv[i];
+    __syncthreads();
+}
+
+template <int N>
+__device__ void persist_stage(const PersistGroup &G, int st, PersistState *s, int g, unsigned long long *s_args,
+                              long *s_unit_p) {
+    long &s_unit = *s_unit_p;
+    if (st < G.passes) {
+        persist_load_args(s_args, G.pass_args[st], sizeof(QueueArgs<N>));
+        const QueueArgs<N> &a = *(const QueueArgs<N> *)s_args;
+        if (st >= G.pair_from) pair_pass<N, true>(a);
+        else queue_pass<N, true>(a);
+        __syncthreads();   // s_args is reloaded by the next stage
+        return;
+    }
+    persist_load_args(s_args, G.deriv_args, sizeof(DerivArgs<N>));
+    const DerivArgs<N> &d = *(const DerivArgs<N> *)s_args;
+    const long units = (G.cells + kDerivUnit - 1) / kDerivUnit;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = (long)atomicAdd(&s->deriv_next[g], 1ull);
+        __syncthreads();
+        const long u = s_unit;
+        __syncthreads();
+        if (u >= units) break;
+        const long c0 = u * kDerivUnit, c1 = c0 + kDerivUnit < G.cells ? c0 + kDerivUnit : G.cells;
+        for (int ph = 0; ph < 2; ph++) deriv_cells<N, true>(d, ph, c0 + threadIdx.x, c1, blockDim.x);
+    }
+}
+
+__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS)
+    flash_persist_kernel(const PersistGroup *groups, int ngroups, PersistState *s, long spin_limit) {
+    __shared__ int s_g, s_st;
+    __shared__ long s_unit;
+    __shared__ __align__(16) unsigned long long s_args[(kPersistArgBytes + 7) / 8];
+    long spins = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int pick = -1, pst = -1;
+            bool done = true;
+            // every CTA scans the groups in the same order, so the GPU works through
+            // the groups' first passes one group at a time (one code body per SM)
+            // while the long passes of earlier groups run beside them
+            for (int g = 0; g < ngroups; g++) {
+                const PersistGroup &G = groups[g];
+                const int st = (int)__ldcg(&s->stage[g]);
+                if (st >= G.stages) continue;
+                done = false;
+                if (!persist_has_work(G, st, s, g)) {
+                    // an item without cells left and without workers is complete (one that
+                    // never had cells, e.g. a pass nothing was parked for, is opened and
+                    // closed here)
+                    if (__ldcg(&s->active[g][st]) == 0u) atomicCAS(&s->stage[g], (unsigned)st, (unsigned)st + 1);
+                    continue;
+                }
+                atomicAdd(&s->active[g][st], 1u);
+                __threadfence();
+                if ((int)__ldcg(&s->stage[g]) != st) {   // the item closed meanwhile
+                    atomicSub(&s->active[g][st], 1u);
+                    continue;
+                }
+                pick = g;
+                pst = st;
+                break;
+            }
+            if (pick < 0 && !done) {
+                if (++spins > spin_limit) {
+                    atomicExch(&s->error, 1);
+                    done = true;
+                } else {
+                    __nanosleep(256);
+                }
+            }
+            if (pick >= 0) spins = 0;
+            s_g = pick;
+            s_st = done ? -2 : pst;
+        }
+        __syncthreads();
+        const int g = s_g, st = s_st;
+        __syncthreads();
+        if (st == -2) break;
+        if (g < 0) continue;
+        const PersistGroup &G = groups[g];
+        switch (G.nc) {
+#define OSR_PERSIST_CASE(K) \
+    case K: persist_stage<K>(G, st, s, g, s_args, &s_unit); break;
+            OSR_PERSIST_CASE(1) OSR_PERSIST_CASE(2) OSR_PERSIST_CASE(3) OSR_PERSIST_CASE(4) OSR_PERSIST_CASE(5)
+            OSR_PERSIST_CASE(6) OSR_PERSIST_CASE(7) OSR_PERSIST_CASE(8) OSR_PERSIST_CASE(9) OSR_PERSIST_CASE(10)
+            OSR_PERSIST_CASE(11) OSR_PERSIST_CASE(12) OSR_PERSIST_CASE(13) OSR_PERSIST_CASE(14)
+            OSR_PERSIST_CASE(15) OSR_PERSIST_CASE(16)
+#undef OSR_PERSIST_CASE
+            default: break;
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned left = atomicSub(&s->active[g][st], 1u) - 1u;
+            if (left == 0 && !persist_has_work(G, st, s, g)) atomicCAS(&s->stage[g], (unsigned)st, (unsigned)st + 1);
+        }
+        __syncthreads();
+    }
+}
+
+// Device copies of one group's per-pass arguments (the passes and shapes
+// run_flash_n would use), with the queue heads and counts in hdr.
+template <int N>
+static osr_status persist_group_n(const osr_flash_group &gr, const PlanGroup &pg, char *hdr, PersistGroup &G,
+                                  std::vector<void *> &bufs) {
+    FluidTable<N> table;
+    make_table<N>(gr.fluids[0], table);
+    const osr_flash_out &o = *gr.out;
+    FlashIO io{gr.d_P, gr.d_T, gr.d_z, gr.n, o.label, o.L, o.x, o.y, o.Zl, o.Zg, o.iters, o.rr_iters};
+    int lim[kMaxPasses];
+    const Shape sh = shape_for(N, gr.n);
+    const int np = pass_limits(sh.park_after, lim);
+    if (g_group_from.load() < np) return OSR_ERR_UNSUPPORTED;   // the group form has no persistent body
+    unsigned long long *heads = (unsigned long long *)hdr;
+    unsigned *counts = (unsigned *)(hdr + 8 * kMaxPasses);
+    std::vector<QueueArgs<N>> qa((size_t)np);
+    for (int p = 0; p < np; p++) {
+        QueueArgs<N> &q = qa[(size_t)p];
+        q.f = table;
+        q.io = io;
+        q.max_wait = g_max_wait.load();
+        q.tables = (const FluidTable<N> *)pg.tables;
+        q.inst_start = pg.start;
+        q.n_inst = gr.n_inst;
+        q.first = p == 0;
+        q.src = park_view(pg.scratch, gr.n, N, (p + 1) & 1);
+        q.dst = park_view(pg.scratch, gr.n, N, p & 1);
+        q.src_count = p > 0 ? counts + (p - 1) : nullptr;
+        q.dst_count = counts + p;
+        q.head = heads + p;
+        q.park_at = lim[p];
+        q.ss_batch = p == 0 ? sh.ss_batch : sh.tail_batch;
+    }
+    QueueArgs<N> *dq = nullptr;
+    OSR_CUDA(cudaMalloc((void **)&dq, qa.size() * sizeof(QueueArgs<N>)));
+    bufs.push_back(dq);
+    OSR_CUDA(cudaMemcpy(dq, qa.data(), qa.size() * sizeof(QueueArgs<N>), cudaMemcpyHostToDevice));
+    G = PersistGroup{};
+    G.nc = N;
+    G.passes = np;
+    G.pair_from = sh.pair_from;
+    G.cells = gr.n;
+    for (int p = 0; p < np; p++) {
+        G.pass_args[p] = dq + p;
+        G.head[p] = heads + p;
+        G.src_count[p] = p > 0 ? counts + (p - 1) : nullptr;
+    }
+    G.stages = np;
+    if (o.dlnphi_dx) {
+        DerivArgs<N> d;
+        d.f = table;
+        d.P = gr.d_P;
+        d.T = gr.d_T;
+        d.x = o.x;
+        d.y = o.y;
+        d.Zl = o.Zl;
+        d.Zg = o.Zg;
+        d.n = gr.n;
+        d.dlnphi_dx = o.dlnphi_dx;
+        d.dlnphi_dP = o.dlnphi_dP;
+        d.tables = (const FluidTable<N> *)pg.tables;
+        d.inst_start = pg.start;
+        d.n_inst = gr.n_inst;
+        DerivArgs<N> *dd = nullptr;
+        OSR_CUDA(cudaMalloc((void **)&dd, sizeof(DerivArgs<N>)));
+        bufs.push_back(dd);
+        OSR_CUDA(cudaMemcpy(dd, &d, sizeof(d), cudaMemcpyHostToDevice));
+        G.deriv_args = dd;
+        G.stages = np + 1;
+    }
+    return OSR_OK;
+}
+
+// ---------------------------------------------------------------------------
 // No-allocation variant of the batched flash.
 //
 // Its scratch (queue heads, parked counts, the two parked-cell lists) lives in
@@ -600,6 +830,15 @@ struct osr_flash_plan {
     std::vector<void *> bufs;
     int groups = 0;
     long cells = 0;
+    // the persistent form (built on its first run)
+    std::vector<osr_flash_group> grp;          // the groups as given at create (host structs)
+    std::vector<osr_flash_out> outs;           // copies of their output structs
+    std::vector<osr::PlanGroup> pg;            // tables, starts, scratch of each group
+    char *p_hdr = nullptr;                     // PersistState + each group's queue heads and counts
+    size_t p_hdr_bytes = 0;
+    osr::PersistGroup *p_groups = nullptr;
+    int p_grid = 0;
+    bool p_ready = false;
 };
 
 namespace {
@@ -608,6 +847,44 @@ void plan_free(osr_flash_plan *p) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     for (void *b : p->bufs) cudaFree(b);
     delete p;
+}
+
+
+// The persistent form's device tables (called at create, while the caller's
+// host arrays are valid): false leaves the plan without it.
+bool persist_build(osr_flash_plan *p) {
+    using namespace osr;
+    if (p->groups > kPersistMaxGroups) return false;
+    const size_t state_bytes = (sizeof(PersistState) + 255) & ~(size_t)255;
+    p->p_hdr_bytes = state_bytes + (size_t)p->groups * 256;
+    if (cudaMalloc((void **)&p->p_hdr, p->p_hdr_bytes) != cudaSuccess) return false;
+    p->bufs.push_back(p->p_hdr);
+    std::vector<PersistGroup> hg((size_t)p->groups);
+    for (int g = 0; g < p->groups; g++) {
+        osr_status rc = OSR_OK;
+        const osr_flash_group &gr = p->grp[(size_t)g];
+        char *hdr = p->p_hdr + state_bytes + (size_t)g * 256;
+        switch (gr.fluids[0].nc) {
+#define OSR_PG_CASE(K) \
+    case K: rc = persist_group_n<K>(gr, p->pg[(size_t)g], hdr, hg[(size_t)g], p->bufs); break;
+            OSR_PG_CASE(1) OSR_PG_CASE(2) OSR_PG_CASE(3) OSR_PG_CASE(4) OSR_PG_CASE(5) OSR_PG_CASE(6)
+            OSR_PG_CASE(7) OSR_PG_CASE(8) OSR_PG_CASE(9) OSR_PG_CASE(10) OSR_PG_CASE(11) OSR_PG_CASE(12)
+            OSR_PG_CASE(13) OSR_PG_CASE(14) OSR_PG_CASE(15) OSR_PG_CASE(16)
+#undef OSR_PG_CASE
+            default: rc = OSR_ERR_NC;
+        }
+        if (rc != OSR_OK) return false;
+    }
+    if (cudaMalloc((void **)&p->p_groups, hg.size() * sizeof(PersistGroup)) != cudaSuccess) return false;
+    p->bufs.push_back(p->p_groups);
+    if (cudaMemcpy(p->p_groups, hg.data(), hg.size() * sizeof(PersistGroup), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, flash_persist_kernel, 128, 0) != cudaSuccess ||
+        per_sm < 1)
+        return false;
+    p->p_grid = per_sm * sm_count();
+    return true;
 }
 
 #define OSR_PLAN_SWITCH(nc, call)                                                                        \
@@ -654,7 +931,12 @@ osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, os
     }
     osr_flash_plan *p = new osr_flash_plan();
     p->groups = n_groups;
-    std::vector<PlanGroup> pg((size_t)n_groups);
+    p->pg.assign((size_t)n_groups, PlanGroup());
+    std::vector<PlanGroup> &pg = p->pg;
+    p->outs.reserve((size_t)n_groups);
+    for (int g = 0; g < n_groups; g++) p->outs.push_back(*groups[g].out);
+    p->grp.assign(groups, groups + n_groups);
+    for (int g = 0; g < n_groups; g++) p->grp[(size_t)g].out = &p->outs[(size_t)g];
     osr_status st = OSR_OK;
     for (int g = 0; g < n_groups && st == OSR_OK; g++) {
         const osr_flash_group &gr = groups[g];
@@ -702,6 +984,8 @@ osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, os
         plan_free(p);
         return st;
     }
+    p->p_ready = persist_build(p);
+    cudaGetLastError();
     *out = p;
     return OSR_OK;
 }
@@ -709,6 +993,33 @@ osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, os
 osr_status osr_flash_plan_run(osr_flash_plan *plan, void *stream) {
     if (!plan || !plan->exec) return OSR_ERR_ARG;
     OSR_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));
+    return OSR_OK;
+}
+
+osr_status osr_flash_plan_run_persistent(osr_flash_plan *p, void *stream) {
+    if (!p) return OSR_ERR_ARG;
+    if (!p->p_ready) return OSR_ERR_UNSUPPORTED;
+    cudaStream_t st = (cudaStream_t)stream;
+    OSR_CUDA(cudaMemsetAsync(p->p_hdr, 0, p->p_hdr_bytes, st));
+    const PersistGroup *gptr = p->p_groups;
+    int ng = p->groups;
+    PersistState *sptr = (PersistState *)p->p_hdr;
+    long limit = 40000000;   // sleeps of about 256 ns: about 10 s of waiting for an item
+    void *args[] = {(void *)&gptr, (void *)&ng, (void *)&sptr, (void *)&limit};
+    OSR_CUDA(cudaLaunchCooperativeKernel((const void *)flash_persist_kernel, dim3((unsigned)p->p_grid), dim3(128), args,
+                                         0, st));
+    return OSR_OK;
+}
+
+osr_status osr_flash_plan_persistent_error(osr_flash_plan *p, int *error, void *stream) {
+    if (!p || !error) return OSR_ERR_ARG;
+    *error = 0;
+    if (!p->p_ready) return OSR_OK;
+    int e = 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    OSR_CUDA(cudaMemcpyAsync(&e, p->p_hdr + offsetof(PersistState, error), sizeof(int), cudaMemcpyDeviceToHost, st));
+    OSR_CUDA(cudaStreamSynchronize(st));
+    *error = e;
     return OSR_OK;
 }
 

@@ -360,11 +360,11 @@ __device__ __forceinline__ const FluidTable<N> &table_of(const Args &a, int inst
 // every pass starts with fully populated warps instead of draining a few
 // long cells through mostly idle warps.
 template <int N, bool MULTI>
-__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_queue_kernel(const __grid_constant__ QueueArgs<N> a) {
+__device__ __forceinline__ void queue_pass(const QueueArgs<N> &a) {
     constexpr unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const FlashIO &io = a.io;
-    const long total = a.first ? io.n : (long)*a.src_count;
+    const long total = a.first ? io.n : (long)__ldcg(a.src_count);
     int mode = kFetch;
     long c = -1;
     double P = 0, T = 0, L = 0, Lb = 10;
@@ -391,12 +391,12 @@ __global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_queue_kernel(
                         rr = 0;
                         Lb = 10;
                     } else {
-                        c = a.src.cell[q];
-                        k = a.src.k[q];
-                        rr = a.src.rr[q];
-                        Lb = a.src.Lb[q];
+                        c = __ldcg(a.src.cell + q);
+                        k = __ldcg(a.src.k + q);
+                        rr = __ldcg(a.src.rr + q);
+                        Lb = __ldcg(a.src.Lb + q);
 #pragma unroll
-                        for (int i = 0; i < N; i++) K[i] = a.src.K[(long)i * a.src.cap + q];
+                        for (int i = 0; i < N; i++) K[i] = __ldcg(a.src.K + (long)i * a.src.cap + q);
                     }
                     P = io.P[c];
                     T = io.T[c];
@@ -458,6 +458,11 @@ __global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_queue_kernel(
             }
         }
     }
+}
+
+template <int N, bool MULTI>
+__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_queue_kernel(const __grid_constant__ QueueArgs<N> a) {
+    queue_pass<N, MULTI>(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -669,12 +674,12 @@ __device__ __forceinline__ double ss_update_pair(const FluidTable<N> &f, const d
 // Batched pair form: the queue kernel's passes with two lanes per cell
 // (used for the late passes, on the cells parked by the earlier ones).
 template <int N, bool MULTI>
-__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_pair_kernel(const __grid_constant__ QueueArgs<N> a) {
+__device__ __forceinline__ void pair_pass(const QueueArgs<N> &a) {
     constexpr int H = (N + 1) / 2;
     const int lane = threadIdx.x & 31;
     const int par = lane & 1;
     const FlashIO &io = a.io;
-    const long total = a.first ? io.n : (long)*a.src_count;
+    const long total = a.first ? io.n : (long)__ldcg(a.src_count);
     int mode = kFetch;
     long c = -1;
     double P = 0, T = 0, L = 0, Lb = 10;
@@ -705,12 +710,12 @@ __global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_pair_kernel(c
                         rr = 0;
                         Lb = 10;
                     } else {
-                        c = a.src.cell[q];
-                        k = a.src.k[q];
-                        rr = a.src.rr[q];
-                        Lb = a.src.Lb[q];
+                        c = __ldcg(a.src.cell + q);
+                        k = __ldcg(a.src.k + q);
+                        rr = __ldcg(a.src.rr + q);
+                        Lb = __ldcg(a.src.Lb + q);
 #pragma unroll
-                        for (int i = 0; i < N; i++) K[i] = a.src.K[(long)i * a.src.cap + q];
+                        for (int i = 0; i < N; i++) K[i] = __ldcg(a.src.K + (long)i * a.src.cap + q);
                     }
                     P = io.P[c];
                     T = io.T[c];
@@ -790,6 +795,11 @@ __global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_pair_kernel(c
             }
         }
     }
+}
+
+template <int N, bool MULTI>
+__global__ void __launch_bounds__(128, OSR_FLASH_MIN_BLOCKS) flash_pair_kernel(const __grid_constant__ QueueArgs<N> a) {
+    pair_pass<N, MULTI>(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -929,7 +939,7 @@ __global__ void __launch_bounds__(128) flash_group_kernel(const __grid_constant_
     const int lane = threadIdx.x & 31;
     const int r = lane & (G - 1), base = lane & ~(G - 1);
     const FlashIO &io = a.io;
-    const long total = a.first ? io.n : (long)*a.src_count;
+    const long total = a.first ? io.n : (long)__ldcg(a.src_count);
     int mode = kFetch;
     long c = -1;
     double P = 0, T = 0, L = 0, Lb = 10;
@@ -959,12 +969,12 @@ __global__ void __launch_bounds__(128) flash_group_kernel(const __grid_constant_
                         rr = 0;
                         Lb = 10;
                     } else {
-                        c = a.src.cell[q];
-                        k = a.src.k[q];
-                        rr = a.src.rr[q];
-                        Lb = a.src.Lb[q];
+                        c = __ldcg(a.src.cell + q);
+                        k = __ldcg(a.src.k + q);
+                        rr = __ldcg(a.src.rr + q);
+                        Lb = __ldcg(a.src.Lb + q);
 #pragma unroll
-                        for (int i = 0; i < N; i++) K[i] = a.src.K[(long)i * a.src.cap + q];
+                        for (int i = 0; i < N; i++) K[i] = __ldcg(a.src.K + (long)i * a.src.cap + q);
                     }
                     P = io.P[c];
                     T = io.T[c];
@@ -1175,15 +1185,16 @@ __device__ __forceinline__ void phase_derivs(const FluidTable<N> &f, const doubl
 }
 
 // One thread per (cell, phase); blockIdx.y selects the phase.
+// Cells c0, c0 + stride, ... below c1 of phase ph.  The phase compositions
+// and Z factors are read through L2 (a persistent launch reads what other
+// CTAs wrote earlier in the same launch).
 template <int N, bool MULTI>
-__global__ void __launch_bounds__(128) flash_deriv_kernel(const __grid_constant__ DerivArgs<N> a) {
-    const int ph = blockIdx.y;
+__device__ __forceinline__ void deriv_cells(const DerivArgs<N> &a, int ph, long c0, long c1, long stride) {
     const double *comp = ph ? a.y : a.x;
     const double *Zp = ph ? a.Zg : a.Zl;
     double *odx = a.dlnphi_dx + (long)ph * N * N * a.n;
     double *odp = a.dlnphi_dP + (long)ph * N * a.n;
-    long stride = (long)gridDim.x * blockDim.x;
-    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < a.n; c += stride) {
+    for (long c = c0; c < c1; c += stride) {
         double sa[N], w[N];
         double T = a.T[c];
         int inst = 0;
@@ -1191,9 +1202,15 @@ __global__ void __launch_bounds__(128) flash_deriv_kernel(const __grid_constant_
         const FluidTable<N> &f = table_of<N, MULTI>(a, inst);
         sqrt_a<N>(f, T, sa);
 #pragma unroll
-        for (int i = 0; i < N; i++) w[i] = comp[(long)i * a.n + c];
-        phase_derivs<N>(f, sa, a.P[c], T, w, Zp[c], odx, odp, a.n, c);
+        for (int i = 0; i < N; i++) w[i] = __ldcg(comp + (long)i * a.n + c);
+        phase_derivs<N>(f, sa, a.P[c], T, w, __ldcg(Zp + c), odx, odp, a.n, c);
     }
+}
+
+template <int N, bool MULTI>
+__global__ void __launch_bounds__(128) flash_deriv_kernel(const __grid_constant__ DerivArgs<N> a) {
+    deriv_cells<N, MULTI>(a, blockIdx.y, (long)blockIdx.x * blockDim.x + threadIdx.x, a.n,
+                          (long)gridDim.x * blockDim.x);
 }
 
 }  // namespace osr

@@ -124,3 +124,39 @@ def test_plan_graph_equals_per_group_calls(cuda_device):
     plan.run()
     check()
     plan.close()
+
+
+def test_persistent_launch_equals_graph(cuda_device):
+    """osr_flash_plan_run_persistent: the same groups as ONE cooperative
+    kernel launch with the device work table.  Every output equals the
+    graph form's bit for bit, on repeated runs and on a plan whose groups
+    include very small ones (passes that park no cell open and close without
+    work), and no wait runs past its bound."""
+    import torch
+    dev = cuda_device
+    for seed, lo, hi in ((13, 20, 3000), (17, 1, 40)):
+        insts = workloads.batched_instances(n_inst=120, seed=seed, cells_lo=lo, cells_hi=hi)
+        groups = []
+        for nc in sorted({d["nc"] for d in insts}):
+            members, start, P, T, z = workloads.instance_group([d for d in insts if d["nc"] == nc], nc, seed=5)
+            fluids = [osr.Fluid(d["tc"], d["pc"], d["acf"], d["kij"], d["eos"]) for d in members]
+            g = dict(fluids=fluids, start=start, P=torch.from_numpy(P).to(dev), T=torch.from_numpy(T).to(dev),
+                     z=torch.from_numpy(z).to(dev))
+            g["out"] = osr.alloc_flash_outputs(nc, int(P.shape[0]), True, dev)
+            groups.append(g)
+        plan = osr.FlashPlan(groups)
+        plan.run()
+        torch.cuda.synchronize()
+        ref = [{k: v.clone() for k, v in g["out"].items()} for g in groups]
+        for rep in range(3):
+            for g in groups:
+                for k in g["out"]:
+                    g["out"][k].fill_(-7 if g["out"][k].dtype in (torch.int8, torch.int32) else float("nan"))
+            plan.run_persistent()
+            torch.cuda.synchronize()
+            assert plan.persistent_error() == 0
+            for g, r in zip(groups, ref):
+                for k, v in r.items():
+                    assert torch.equal(torch.nan_to_num(g["out"][k], nan=7.0), torch.nan_to_num(v, nan=7.0)), \
+                        (seed, rep, g["fluids"][0].nc, k)
+        plan.close()
