@@ -831,7 +831,7 @@ struct osr_flash_plan {
     int groups = 0;
     long cells = 0;
     // the persistent form (built on its first run)
-    std::vector<osr_flash_group> grp;          // the groups as given at create (host structs)
+    std::vector<osr_flash_group> grp;          // the groups as given at create (host arrays cleared after it)
     std::vector<osr_flash_out> outs;           // copies of their output structs
     std::vector<osr::PlanGroup> pg;            // tables, starts, scratch of each group
     char *p_hdr = nullptr;                     // PersistState + each group's queue heads and counts
@@ -986,6 +986,11 @@ osr_status osr_flash_plan_create(const osr_flash_group *groups, int n_groups, os
     }
     p->p_ready = persist_build(p);
     cudaGetLastError();
+    // the caller's host arrays are read during create only
+    for (osr_flash_group &gr : p->grp) {
+        gr.fluids = nullptr;
+        gr.inst_start = nullptr;
+    }
     *out = p;
     return OSR_OK;
 }
