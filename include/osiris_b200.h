@@ -746,6 +746,27 @@ osr_status osr_sim_marker_index(osr_sim *sim, int *tsm_ctrl);
  * current state (set from the file) becomes the backup. */
 osr_status osr_sim_restart(osr_sim *sim, double sim_time, double dt, int tsm_ctrl);
 
+/* The reference's restart file for a C++ host (WriteRST / ReadRST,
+ * compsim/Do_Time_Step.cpp:179-294): both continua's phase pressures with the
+ * one-cell halo (written as zeros), per cell the saturations, the liquid and
+ * vapour compositions and the label, then simTime, Dt, TSMCtrl and SMethQ
+ * (the main loop's cumulative producer methane, which the device run does
+ * not track: the caller passes it).  Reading restores the state, then
+ * PhaseCtrl, the row layout, the property sweeps and the run's time, Dt and
+ * marker (ReadRST + UpdateDependencies(true) + CreateBackups,
+ * compsim/PrimeSim.cpp:84-86); a file of another grid or component count is
+ * OSR_ERR_ARG.  HOST paths; synchronous. */
+osr_status osr_sim_write_restart(osr_sim *sim, const char *path, double smethq);
+osr_status osr_sim_read_restart(osr_sim *sim, const char *path, double *smethq);
+
+/* The reference's state listing (PrintAll, compsim/ViewAssist.Cpp:39-88)
+ * appended to `path`: 80 dashes, the time in hours (%g on the stream's first
+ * call, first_call != 0, then %.20g), the header, then per matrix and per
+ * fracture cell (z outermost, x fastest) the indices, oil pressure,
+ * saturations and both phase compositions at 20 significant digits.
+ * Synchronous. */
+osr_status osr_grid_write_listing(osr_grid *grid, const char *path, double sim_time, int first_call);
+
 osr_status osr_sim_destroy(osr_sim *sim);
 
 /* Measured FP64 FMA-pipe throughput of the current device in TFLOP/s (an FMA

@@ -756,6 +756,11 @@ class Grid:
     def phase_ctrl(self, stream=None):
         _check(lib().osr_grid_phase_ctrl(self._h, None if stream is None else _vp(stream)), "osr_grid_phase_ctrl")
 
+    def write_listing(self, path: str, sim_time: float, first_call: bool):
+        """Append the reference's state listing (PrintAll) through the C ABI."""
+        _check(lib().osr_grid_write_listing(self._h, path.encode(), ctypes.c_double(sim_time), int(bool(first_call))),
+               "osr_grid_write_listing")
+
     def update_all_full(self, d_x, stream=None):
         _check(lib().osr_grid_update_all_full(self._h, _vp(d_x.data_ptr()), None if stream is None else _vp(stream)),
                "osr_grid_update_all_full")
@@ -876,6 +881,17 @@ class Sim:
         _check(lib().osr_sim_step(self._h, ctypes.byref(o), ctypes.byref(info),
                                   None if stream is None else _vp(stream)), "osr_sim_step")
         return {k: getattr(info, k) for k, _ in StepInfo._fields_}
+
+    def write_restart(self, path: str, smethq: float = 0.0):
+        """The reference's restart file through the C ABI (osr_sim_write_restart)."""
+        _check(lib().osr_sim_write_restart(self._h, path.encode(), ctypes.c_double(smethq)), "osr_sim_write_restart")
+
+    def read_restart(self, path: str) -> float:
+        """Load a restart file into the run's grid and clock (osr_sim_read_restart);
+        returns SMethQ."""
+        sm = ctypes.c_double()
+        _check(lib().osr_sim_read_restart(self._h, path.encode(), ctypes.byref(sm)), "osr_sim_read_restart")
+        return sm.value
 
     def set_graph(self, on: bool):
         """Run each pass's linearisation and solve as one CUDA graph (the

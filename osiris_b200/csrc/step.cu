@@ -29,7 +29,9 @@
 // few host scalars) follows on the host.
 #include <cuda_runtime.h>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 #include "grid_internal.h"
 #include "jacobian_kernels.cuh"
@@ -496,6 +498,217 @@ osr_status osr_sim_step(osr_sim *s, const osr_ksp_opts *opts, osr_step_info *inf
     inf.dt = s->dt;
     if (info) *info = inf;
     return OSR_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// On-disk formats for a C++ host: the restart file (WriteRST / ReadRST,
+// compsim/Do_Time_Step.cpp:179-294) and the state listing (PrintAll,
+// compsim/ViewAssist.Cpp:39-88).
+//
+// Restart layout (native little-endian, packed, no header): per continuum
+// (matrix, then fracture) the three phase pressures P[Nx+2][Ny+2][Nz+2][3]
+// with the one-cell halo (x outermost, the phase innermost; the halo is
+// written as zeros -- the reference never writes its edges and corners);
+// per continuum, per cell (x outermost, then y, then z) sat[3], then x_i, y_i
+// for every component, then the label as one signed byte; then simTime (s),
+// Dt (s), TSMCtrl (int32) and SMethQ (double).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct HostState {
+    std::vector<double> P, sat, x, y, z, label;
+};
+
+osr_status fetch_state(osr_grid *g, int med, HostState &h) {
+    const long n = g->cells;
+    const char *m = med ? "f." : "m.";
+    h.P.resize(3 * n);
+    h.sat.resize(3 * n);
+    h.x.resize((size_t)g->nc * n);
+    h.y.resize((size_t)g->nc * n);
+    h.z.resize((size_t)g->nc * n);
+    h.label.resize(n);
+    struct {
+        const char *k;
+        std::vector<double> *v;
+    } f[] = {{"P", &h.P}, {"sat", &h.sat}, {"x", &h.x}, {"y", &h.y}, {"z", &h.z}, {"label", &h.label}};
+    for (auto &it : f) {
+        const std::string name = std::string(m) + it.k;
+        osr_status rc = osr_grid_get(g, name.c_str(), it.v->data());
+        if (rc != OSR_OK) return rc;
+    }
+    return OSR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+osr_status osr_sim_write_restart(osr_sim *s, const char *path, double smethq) {
+    if (!s || !path) return OSR_ERR_ARG;
+    osr_grid *g = s->g;
+    const int nx = g->nx, ny = g->ny, nz = g->nz, nc = g->nc;
+    const long n = g->cells;
+    HostState st[2];
+    for (int m = 0; m < 2; m++) {
+        osr_status rc = fetch_state(g, m, st[m]);
+        if (rc != OSR_OK) return rc;
+    }
+    std::vector<unsigned char> buf;
+    auto put = [&](const void *p, size_t b) {
+        const unsigned char *c = (const unsigned char *)p;
+        buf.insert(buf.end(), c, c + b);
+    };
+    for (int m = 0; m < 2; m++) {
+        std::vector<double> halo((size_t)(nx + 2) * (ny + 2) * (nz + 2) * 3, 0.0);
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++)
+                for (int iz = 0; iz < nz; iz++) {
+                    const long c = ix + (long)nx * (iy + (long)ny * iz);
+                    const size_t h = (((size_t)(ix + 1) * (ny + 2) + (iy + 1)) * (nz + 2) + (iz + 1)) * 3;
+                    for (int ph = 0; ph < 3; ph++) halo[h + ph] = st[m].P[(size_t)ph * n + c];
+                }
+        put(halo.data(), halo.size() * 8);
+    }
+    for (int m = 0; m < 2; m++)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++)
+                for (int iz = 0; iz < nz; iz++) {
+                    const long c = ix + (long)nx * (iy + (long)ny * iz);
+                    for (int q = 0; q < 3; q++) put(&st[m].sat[(size_t)q * n + c], 8);
+                    for (int i = 0; i < nc; i++) {
+                        put(&st[m].x[(size_t)i * n + c], 8);
+                        put(&st[m].y[(size_t)i * n + c], 8);
+                    }
+                    const signed char lab = (signed char)st[m].label[c];
+                    put(&lab, 1);
+                }
+    const int tsm = s->tsm_ctrl;
+    put(&s->sim_time, 8);
+    put(&s->dt, 8);
+    put(&tsm, 4);
+    put(&smethq, 8);
+    FILE *fp = std::fopen(path, "wb");
+    if (!fp) return OSR_ERR_ARG;
+    const bool ok = std::fwrite(buf.data(), 1, buf.size(), fp) == buf.size();
+    return (std::fclose(fp) == 0 && ok) ? OSR_OK : OSR_ERR_ARG;
+}
+
+osr_status osr_sim_read_restart(osr_sim *s, const char *path, double *smethq) {
+    if (!s || !path) return OSR_ERR_ARG;
+    osr_grid *g = s->g;
+    const int nx = g->nx, ny = g->ny, nz = g->nz, nc = g->nc;
+    const long n = g->cells;
+    const size_t halo = (size_t)(nx + 2) * (ny + 2) * (nz + 2) * 3 * 8, rec = 24 + 16 * (size_t)nc + 1;
+    const size_t want = 2 * halo + 2 * rec * (size_t)n + 28;
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return OSR_ERR_ARG;
+    std::vector<unsigned char> buf(want + 1);
+    const size_t got = std::fread(buf.data(), 1, buf.size(), fp);
+    std::fclose(fp);
+    if (got != want) return OSR_ERR_ARG;   // not a restart file of this grid and component count
+    size_t off = 0;
+    auto get = [&](void *p, size_t b) {
+        std::memcpy(p, buf.data() + off, b);
+        off += b;
+    };
+    HostState st[2];
+    for (int m = 0; m < 2; m++) {
+        osr_status rc = fetch_state(g, m, st[m]);   // the overall compositions stay the grid's
+        if (rc != OSR_OK) return rc;
+    }
+    for (int m = 0; m < 2; m++) {
+        for (int ix = 0; ix < nx + 2; ix++)
+            for (int iy = 0; iy < ny + 2; iy++)
+                for (int iz = 0; iz < nz + 2; iz++)
+                    for (int ph = 0; ph < 3; ph++) {
+                        double v;
+                        get(&v, 8);
+                        if (ix >= 1 && ix <= nx && iy >= 1 && iy <= ny && iz >= 1 && iz <= nz) {
+                            const long c = (ix - 1) + (long)nx * ((iy - 1) + (long)ny * (iz - 1));
+                            st[m].P[(size_t)ph * n + c] = v;
+                        }
+                    }
+    }
+    std::vector<signed char> labs[2] = {std::vector<signed char>(n), std::vector<signed char>(n)};
+    for (int m = 0; m < 2; m++)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++)
+                for (int iz = 0; iz < nz; iz++) {
+                    const long c = ix + (long)nx * (iy + (long)ny * iz);
+                    for (int q = 0; q < 3; q++) get(&st[m].sat[(size_t)q * n + c], 8);
+                    for (int i = 0; i < nc; i++) {
+                        get(&st[m].x[(size_t)i * n + c], 8);
+                        get(&st[m].y[(size_t)i * n + c], 8);
+                    }
+                    get(&labs[m][c], 1);
+                }
+    double t, dt, sm;
+    int tsm;
+    get(&t, 8);
+    get(&dt, 8);
+    get(&tsm, 4);
+    get(&sm, 8);
+    // ReadRST followed by UpdateDependencies(true) (compsim/PrimeSim.cpp:84-85)
+    for (int m = 0; m < 2; m++) {
+        osr_status rc = osr_grid_set_state(g, m, st[m].P.data() + n, st[m].sat.data(), st[m].x.data(),
+                                           st[m].y.data(), st[m].z.data(), labs[m].data(), nullptr);
+        if (rc == OSR_OK) rc = osr_grid_set_pressures(g, m, st[m].P.data());
+        if (rc != OSR_OK) return rc;
+    }
+    osr_status rc = osr_grid_phase_ctrl(g, nullptr);
+    if (rc == OSR_OK) rc = osr_grid_refresh_layout(g, nullptr);
+    if (rc == OSR_OK) rc = osr_grid_update_dependencies(g, nullptr);
+    if (rc == OSR_OK) rc = osr_sim_restart(s, t, dt, tsm);
+    if (rc == OSR_OK && smethq) *smethq = sm;
+    return rc;
+}
+
+osr_status osr_grid_write_listing(osr_grid *g, const char *path, double sim_time, int first_call) {
+    if (!g || !path) return OSR_ERR_ARG;
+    const int nx = g->nx, ny = g->ny, nz = g->nz, nc = g->nc;
+    const long n = g->cells;
+    HostState st[2];
+    for (int m = 0; m < 2; m++) {
+        osr_status rc = fetch_state(g, m, st[m]);
+        if (rc != OSR_OK) return rc;
+    }
+    std::string out(80, '-');
+    char num[64];
+    out += "\n";
+    std::snprintf(num, sizeof num, first_call ? "%g" : "%.20g", sim_time / 3600);
+    out += num;
+    out += "\nX\tY\tZ\tP\t\t\tSw\t\t\tSo\t\t\tSg\t\t\t";
+    for (int i = 0; i < nc; i++) out += "Xo[" + std::to_string(i) + "]\t\t\t";
+    for (int i = 0; i < nc; i++) out += "Yg[" + std::to_string(i) + "]\t\t\t";
+    for (int m = 0; m < 2; m++) {
+        out += m ? "\nF\n" : "\nM\n";
+        const HostState &h = st[m];
+        long c = 0;
+        for (int iz = 0; iz < nz; iz++)
+            for (int iy = 0; iy < ny; iy++)
+                for (int ix = 0; ix < nx; ix++, c++) {
+                    char line[256];
+                    std::snprintf(line, sizeof line, "\n%d\t%d\t%d\t%.20g\t%.20g\t%.20g\t%.20g", ix, iy, iz, h.P[n + c],
+                                  h.sat[c], h.sat[n + c], h.sat[2 * n + c]);
+                    out += line;
+                    for (int i = 0; i < nc; i++) {
+                        std::snprintf(num, sizeof num, "\t%.20g\t", h.x[(size_t)i * n + c]);
+                        out += num;
+                    }
+                    for (int i = 0; i < nc; i++) {
+                        std::snprintf(num, sizeof num, "%.20g\t", h.y[(size_t)i * n + c]);
+                        out += num;
+                    }
+                }
+    }
+    out += "\n\n\n";
+    FILE *fp = std::fopen(path, "ab");
+    if (!fp) return OSR_ERR_ARG;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), fp) == out.size();
+    return (std::fclose(fp) == 0 && ok) ? OSR_OK : OSR_ERR_ARG;
 }
 
 }  // extern "C"
