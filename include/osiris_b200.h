@@ -643,6 +643,14 @@ osr_status osr_grid_jacobian_apply_transpose(osr_grid *grid, const double *d_val
 osr_status osr_grid_ksp_solve(osr_grid *grid, const double *d_vals, const double *d_rhs, double *d_sol,
                               const osr_ksp_opts *opts, osr_ksp_info *info, void *stream);
 
+/* Solve J^T d_sol = d_rhs (the adjoint system of the Newton step) from a zero
+ * initial guess: the same left-preconditioned BiCGStab with J^T in the
+ * products (the transposed product of osr_grid_jacobian_apply_transpose)
+ * and the transposed inverse diagonal blocks as preconditioner.  Options,
+ * outcome and synchronisation as osr_grid_ksp_solve. */
+osr_status osr_grid_ksp_solve_transpose(osr_grid *grid, const double *d_vals, const double *d_rhs, double *d_sol,
+                                        const osr_ksp_opts *opts, osr_ksp_info *info, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Distributed linear solve over z-slabs (the multi-rank KSPSolve of the
  * reference: PETSc's KSPBCGS + PCVPBJACOBI over CreateAllocationTable's row

@@ -840,6 +840,17 @@ class Grid:
                                         None if stream is None else _vp(stream)), "osr_grid_ksp_solve")
         return {"reason": info.reason, "its": info.its, "rnorm0": info.rnorm0, "rnorm": info.rnorm}
 
+    def ksp_solve_transpose(self, vals, d_rhs, d_sol, stream=None, **opts) -> dict:
+        """Solve J^T d_sol = d_rhs (osr_grid_ksp_solve_transpose; the adjoint
+        system of the Newton step)."""
+        o = ksp_opts(**opts)
+        info = KspInfo()
+        _check(lib().osr_grid_ksp_solve_transpose(self._h, _vp(vals.data_ptr()), _vp(d_rhs.data_ptr()),
+                                                  _vp(d_sol.data_ptr()), ctypes.byref(o), ctypes.byref(info),
+                                                  None if stream is None else _vp(stream)),
+               "osr_grid_ksp_solve_transpose")
+        return {"reason": info.reason, "its": info.its, "rnorm0": info.rnorm0, "rnorm": info.rnorm}
+
     def get(self, name: str) -> np.ndarray:
         L = lib()
         n = L.osr_grid_field_size(self._h, name.encode())

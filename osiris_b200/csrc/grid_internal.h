@@ -61,6 +61,9 @@ double peaceman_re(const double *di, const double *dj, int nx, int ny, int ix, i
 osr_status grid_assembly_init(osr_grid &g, const osr_model *md);
 void grid_assembly_free(osr_grid &g);
 void ksp_free(osr_grid &g);
+// y = J^T x (MatMultTranspose) on the compact Jacobian, y zeroed first.
+osr_status jacobian_transpose_apply(const osr_grid &g, const double *vals, const double *x, double *y,
+                                    cudaStream_t st);
 // PJac / CalcPCoeff launched on `st` without reading the row count and PCoeff
 // back (they stay in rowoff[2 cells] and pmax).
 osr_status relayout_launch(osr_grid &g, cudaStream_t st);

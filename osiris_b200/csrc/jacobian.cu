@@ -239,6 +239,20 @@ __global__ void jacobian_transpose_kernel(int N, int nx, int ny, int nz, long n,
     }
 }
 
+// y = J^T x on `st` (y zeroed first).
+osr_status jacobian_transpose_apply(const osr_grid &g, const double *vals, const double *x, double *y,
+                                    cudaStream_t st) {
+    const osrj::Layout L(g.nc);
+    JAC_CUDA(cudaMemsetAsync(y, 0, (size_t)g.n_rows * 8, st));
+    const long total = (2 * g.cells + 31) / 32 * 32 * L.ET;
+    long blocks = (total + 255) / 256;
+    if (blocks > 148L * 32) blocks = 148L * 32;
+    jacobian_transpose_kernel<<<(unsigned)blocks, 256, 0, st>>>(g.nc, g.nx, g.ny, g.nz, g.cells, g.rowoff,
+                                                                g.m[0].label, g.m[1].label, L.ET, vals, x, y);
+    JAC_CUDA(cudaGetLastError());
+    return OSR_OK;
+}
+
 static osr_status ensure_jacobian_scratch(osr_grid &g) {
     if (g.jw_q) return OSR_OK;
     const long nb = 2 * g.cells;
@@ -293,17 +307,7 @@ osr_status osr_grid_block_columns(osr_grid *g, long *out) {
 osr_status osr_grid_jacobian_apply_transpose(osr_grid *g, const double *d_vals, const double *d_lambda, double *d_y,
                                             void *stream) {
     if (!g || !d_vals || !d_lambda || !d_y || !g->rowoff || g->n_rows <= 0) return OSR_ERR_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
-    const osrj::Layout L(g->nc);
-    JAC_CUDA(cudaMemsetAsync(d_y, 0, (size_t)g->n_rows * 8, st));
-    const long total = (2 * g->cells + 31) / 32 * 32 * L.ET;
-    long blocks = (total + 255) / 256;
-    if (blocks > 148L * 32) blocks = 148L * 32;
-    jacobian_transpose_kernel<<<(unsigned)blocks, 256, 0, st>>>(g->nc, g->nx, g->ny, g->nz, g->cells, g->rowoff,
-                                                                g->m[0].label, g->m[1].label, L.ET, d_vals, d_lambda,
-                                                                d_y);
-    JAC_CUDA(cudaGetLastError());
-    return OSR_OK;
+    return osr::jacobian_transpose_apply(*g, d_vals, d_lambda, d_y, (cudaStream_t)stream);
 }
 
 osr_status osr_grid_jacobian_pattern(osr_grid *g, long *d_row, long *d_col, void *stream) {

@@ -392,6 +392,50 @@ static osr_status solve_n(osr_grid &g, const double *vals, const double *b, doub
     return OSR_OK;
 }
 
+// The solve with the transposed matrix, J^T x = b (the adjoint system of
+// the Newton step): the same left-preconditioned BiCGStab with J^T in the
+// products (osr::jacobian_transpose_apply, atomic additions) and the
+// transposed inverse blocks as preconditioner; direct launches, the state
+// read back every `every` iterations.
+template <int N>
+static osr_status solve_t_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
+                            osr_ksp_info *info, cudaStream_t st) {
+    osr_status rc = ksp_ensure(g);
+    if (rc != OSR_OK) return rc;
+    osr_ksp_work &k = *g.ksp;
+    const SolvePlan<N> p = solve_plan<N>(g, vals, b, x);
+    ksp_set_host(k, o);
+    const int every = o.check_every > 0 ? o.check_every : 8;
+    KSP_CUDA(cudaMemcpyAsync(k.scal, k.host, sizeof(osrk::KspScal), cudaMemcpyHostToDevice, st));
+    osrk::bjac_invert_kernel<N><<<p.ib, p.tpb, 0, st>>>(p.v, k.inv, k.scal);
+    osrk::bjac_apply_kernel<N, 0, false, true><<<p.ab, p.atb, 0, st>>>(p.v, k.inv, b, k.r, nullptr, k.part, k.scal);
+    osrk::bcgs_setup_kernel<<<p.vbk, 256, 0, st>>>(p.n, k.r, k.r0, k.p, k.v, x);
+    KSP_CUDA(cudaGetLastError());
+    int launched = 0;
+    for (;;) {
+        const int c = every < o.max_it - launched ? every : o.max_it - launched;
+        for (int q = 0; q < c; q++) {
+            osrk::bcgs_p_kernel<<<p.vbk, 256, 0, st>>>(p.n, k.r, k.p, k.v, k.scal);
+            if ((rc = jacobian_transpose_apply(g, vals, k.p, k.t, st)) != OSR_OK) return rc;
+            osrk::bjac_apply_kernel<N, 1, false, true><<<p.ab, p.atb, 0, st>>>(p.v, k.inv, k.t, k.v, k.r0, k.part,
+                                                                               k.scal);
+            osrk::bcgs_s_kernel<<<p.vbk, 256, 0, st>>>(p.n, k.r, k.v, k.s, k.scal);
+            if ((rc = jacobian_transpose_apply(g, vals, k.s, k.w, st)) != OSR_OK) return rc;
+            osrk::bjac_apply_kernel<N, 2, false, true><<<p.ab, p.atb, 0, st>>>(p.v, k.inv, k.w, k.t, k.s, k.part,
+                                                                               k.scal);
+            osrk::bcgs_xr_kernel<<<p.xb, osrk::kRedThreads, 0, st>>>(p.n, x, k.p, k.s, k.t, k.r, k.r0, k.part,
+                                                                      k.scal);
+        }
+        launched += c;
+        KSP_CUDA(cudaGetLastError());
+        KSP_CUDA(cudaMemcpyAsync(k.host, k.scal, sizeof(osrk::KspScal), cudaMemcpyDeviceToHost, st));
+        KSP_CUDA(cudaStreamSynchronize(st));
+        if (k.host->reason != osrk::kItersRunning || launched >= o.max_it) break;
+    }
+    ksp_read_host(k, info);
+    return OSR_OK;
+}
+
 template <int N>
 static osr_status step_graph_n(osr_grid &g, const double *vals, const double *b, double *x, const osr_ksp_opts &o,
                                const std::function<void(cudaStream_t)> &pre,
@@ -588,6 +632,16 @@ osr_status osr_dksp_info(osr_dksp *d, osr_ksp_info *info, void *stream) {
     info->rnorm0 = d->host->rnorm0;
     info->rnorm = d->host->rnorm;
     return OSR_OK;
+}
+
+osr_status osr_grid_ksp_solve_transpose(osr_grid *g, const double *d_vals, const double *d_rhs, double *d_sol,
+                                        const osr_ksp_opts *opts, osr_ksp_info *info, void *stream) {
+    if (!g || !d_vals || !d_rhs || !d_sol || !g->rowoff || g->n_rows <= 0) return OSR_ERR_ARG;
+    osr_ksp_opts o;
+    osr_ksp_default_opts(&o);
+    if (opts) o = *opts;
+    if (o.max_it < 0 || !(o.rtol >= 0) || !(o.atol >= 0)) return OSR_ERR_ARG;
+    KSP_SWITCH(osr::solve_t_n<K>(*g, d_vals, d_rhs, d_sol, o, info, (cudaStream_t)stream))
 }
 
 osr_status osr_grid_ksp_solve(osr_grid *g, const double *d_vals, const double *d_rhs, double *d_sol,

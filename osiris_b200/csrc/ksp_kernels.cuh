@@ -444,7 +444,9 @@ struct Owned {
 // DIST: the distributed form (one slab): the dot products are summed over
 // the owned block rows only and written to dots[] for the host to sum over
 // the slabs; the scalar step is left to dksp_scalar_kernel.
-template <int N, int MODE, bool DIST = false>
+// TR: apply the transposed inverse blocks (the preconditioner of a solve
+// with the transposed matrix).
+template <int N, int MODE, bool DIST = false, bool TR = false>
 __global__ void __launch_bounds__(kApplyThreads) bjac_apply_kernel(const KView v, const double *__restrict__ inv,
                                                                     const double *__restrict__ r,
                                                                     double *__restrict__ z,
@@ -470,7 +472,7 @@ __global__ void __launch_bounds__(kApplyThreads) bjac_apply_kernel(const KView v
             if (j >= bs) break;
 #pragma unroll
             for (int i = 0; i < BS; i++)
-                if (i < bs) zv[i] += __ldg(ib + 32 * (j * BS + i)) * rv[j];
+                if (i < bs) zv[i] += __ldg(ib + 32 * (TR ? (i * BS + j) : (j * BS + i))) * rv[j];
         }
         const bool count = !DIST || own.block(b);
 #pragma unroll
