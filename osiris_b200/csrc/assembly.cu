@@ -321,7 +321,10 @@ static osr_status update_all_n(osr_grid &g, const double *x, cudaStream_t st) {
 template <int N>
 static osr_status residual_n(osr_grid &g, double *f, double *fscale, double t, cudaStream_t st) {
     AsmArgs<N> A = asm_args<N>(g, f, fscale, t);
-    residual_kernel<N><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(A);
+    if (fscale)
+        residual_kernel<N, true><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(A);
+    else
+        residual_kernel<N, false><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(A);
     ASM_CUDA(cudaGetLastError());
     return OSR_OK;
 }

@@ -723,35 +723,54 @@ __global__ void well_terms_kernel(const __grid_constant__ AsmArgs<N> A, double *
     }
 }
 
-// Fugacity of component i in one phase at the phase's own pressure with Z
-// taken from the stored density, as the two-phase rows evaluate it
-// (compsim/Petsc_Functions.cpp:4559-4621).
+// Fugacity coefficients of one phase at the phase's own pressure with Z taken
+// from the stored density, as the two-phase rows evaluate them
+// (compsim/Petsc_Functions.cpp:4559-4621).  The reference recomputes the
+// mixing sums for every component row; they do not depend on the row, so they
+// are formed once per phase here, with the same operations in the same order
+// as the per-row evaluation.  s[k] is the
+// k-th attraction row sum sum_j w_j sa_k sa_j (1 - kij), which is also the
+// component's own t_i.
 template <int N>
-__device__ double phase_fugacity_coeff(const GridFluid<N> &g, const double *w, long n, long c, double P, double rho,
-                                       int i) {
-    const FluidTable<N> &f = g.f;
-    const double rt = kR * g.T;
-    double A = 0, B = 0, ti = 0;
-    for (int k = 0; k < N; k++) {
-        const double wk = w[(long)k * n + c];
-        B += wk * f.b[k];
-        double sk = 0;
-        for (int j = 0; j < N; j++) sk += w[(long)j * n + c] * g.sa[k] * g.sa[j] * f.bic[k * N + j];
-        A += wk * sk;
+struct PhaseFug {
+    double s[N];
+    double Ca, Cb, Z, DD, FF, lzb;
+
+    __device__ __forceinline__ PhaseFug(const GridFluid<N> &g, const double *w, long n, long c, double P, double rho) {
+        const FluidTable<N> &f = g.f;
+        const double rt = kR * g.T;
+        double wv[N];
+#pragma unroll
+        for (int k = 0; k < N; k++) wv[k] = w[(long)k * n + c];
+        double A = 0, B = 0;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            B += wv[k] * f.b[k];
+            double sk = 0;
+#pragma unroll
+            for (int j = 0; j < N; j++) sk += wv[j] * g.sa[k] * g.sa[j] * f.bic[k * N + j];
+            s[k] = sk;
+            A += wv[k] * sk;
+        }
+        Ca = A;
+        Cb = B;
+        A *= P / (rt * rt);
+        B *= P / rt;
+        Z = P / (rho * rt);
+        const bool srk = f.srk != 0;
+        const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
+        DD = A / (B * (d1 - d2));
+        FF = log((Z + d2 * B) / (Z + d1 * B));
+        lzb = log(Z - B);
     }
-    for (int j = 0; j < N; j++) ti += w[(long)j * n + c] * g.sa[i] * g.sa[j] * f.bic[i * N + j];
-    const double Ca = A, Cb = B;
-    A *= P / (rt * rt);
-    B *= P / rt;
-    const double Z = P / (rho * rt);
-    const bool srk = f.srk != 0;
-    const double d1 = srk ? 1.0 : 1 + kSqrt2, d2 = srk ? 0.0 : 1 - kSqrt2;
-    const double t1 = f.b[i] / Cb;
-    const double EE = 2 * ti / Ca - t1;
-    const double DD = A / (B * (d1 - d2));
-    const double FF = log((Z + d2 * B) / (Z + d1 * B));
-    return exp(t1 * (Z - 1) - log(Z - B) + DD * EE * FF);
-}
+
+    // fugacity coefficient of component i
+    __device__ __forceinline__ double coeff(const FluidTable<N> &f, int i) const {
+        const double t1 = f.b[i] / Cb;
+        const double EE = 2 * s[i] / Ca - t1;
+        return exp(t1 * (Z - 1) - lzb + DD * EE * FF);
+    }
+};
 
 // One face of a cell: neighbour index, distances, areas.
 struct Face {
@@ -784,7 +803,8 @@ __device__ __forceinline__ double porpor_at(const MediumFields &F, const GridSca
     return F.por[c] * (1 + s.cpor * dp + s.dcpor * dp * dp);
 }
 
-template <int N>
+// SCALE: the row scales (sum of |terms| of each row) are written to A.fscale.
+template <int N, bool SCALE>
 __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const __grid_constant__ AsmArgs<N> A) {
     const GridScalars &s = A.a.s;
     const GridGeom &geo = A.a.geo;
@@ -799,7 +819,7 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         const signed char lab = F.label[c];
         const int rows = block_rows(lab, N);
         double *fo = A.f + row0;
-        double *so = A.fscale ? A.fscale + row0 : nullptr;
+        double *so = SCALE ? A.fscale + row0 : nullptr;
         if (F.por[c] < kPorTiny) {
             for (int r = 0; r < rows; r++) {
                 fo[r] = 0;
@@ -816,10 +836,13 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         // ---- two-phase fugacity rows
         int r = 0;
         if (lab == 0) {
+            const double Po = F.P[n + c], Pg = F.P[2 * n + c];
+            const PhaseFug<N> fl(A.a.g, F.x, n, c, Po, F.rho[c]);
+            const PhaseFug<N> fg(A.a.g, F.y, n, c, Pg, F.rho[n + c]);
+#pragma unroll
             for (int i = 0; i < N; i++) {
-                const double Po = F.P[n + c], Pg = F.P[2 * n + c];
-                const double phiL = phase_fugacity_coeff<N>(A.a.g, F.x, n, c, Po, F.rho[c], i);
-                const double phiG = phase_fugacity_coeff<N>(A.a.g, F.y, n, c, Pg, F.rho[n + c], i);
+                const double phiL = fl.coeff(A.a.g.f, i);
+                const double phiG = fg.coeff(A.a.g.f, i);
                 const double a1 = F.x[(long)i * n + c] * Po * phiL, a2 = F.y[(long)i * n + c] * Pg * phiG;
                 fo[r] = a1 - a2;
                 if (so) so[r] = fabs(a1) + fabs(a2);
@@ -831,7 +854,8 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         const int nf = cell_faces<N>(A, c, ix, iy, iz, fc);
         double KP[2][6], KG[2][6];
         long up[2][6];
-        double KW[6];
+        // the water row's face terms, summed in face order as the row adds them
+        double RW = 0, SW = 0;
         for (int q = 0; q < nf; q++) {
             const Face &e = fc[q];
             const long plane = (long)e.d * n + e.tc;
@@ -853,7 +877,9 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
             }
             const double Tw = F.wtran[plane];
             const double dPw = e.sgn > 0 ? F.P[e.nb] - F.P[c] : F.P[c] - F.P[e.nb];
-            KW[q] = e.sgn * (Tw * dPw + kGAcc * s.wat_ro * Tw * dH);
+            const double kw = e.sgn * (Tw * dPw + kGAcc * s.wat_ro * Tw * dH);
+            RW += kw;
+            SW += fabs(kw);
         }
         // ---- matrix-fracture advective transfer (identical value, opposite sign)
         const double sgnT = med == 0 ? 1.0 : -1.0;
@@ -880,12 +906,36 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         const double dfo = SF3 * Vb * Fpor / tor * Fr.sat[n + c] * Fr.rho[c];
         const double dfg = SF3 * Vb * Fpor / tor * Fr.sat[2 * n + c] * Fr.rho[n + c];
         const double dCoefl = lab == -1 ? 0.0 : 1.0, dCoefg = lab == 1 ? 0.0 : 1.0;
+        // ---- intra-continuum diffusion: the factor of each (face, phase)
+        // that does not depend on the component, AAd / BBd * NNd of the
+        // reference's DTran = AAd / BBd * NNd * Dup (formed once here, applied
+        // per component row below with the same evaluation order)
+        double DB[2][6];
+        bool Dzero[2][6], Dinact[6];
+        for (int q = 0; q < nf; q++) {
+            const Face &e = fc[q];
+            const long nb = e.nb;
+            const double porpor2 = porpor_at(F, s, nb);
+            const double NNd = e.area2 / (e.dn + e.dl);
+            const signed char lnb = F.label[nb];
+            Dinact[q] = F.por[c] < kPorTiny || F.por[nb] < kPorTiny;
+            for (int p = 0; p < 2; p++) {
+                const double Coef = p ? (lnb == 1 ? 0.0 : 1.0) : (lnb == -1 ? 0.0 : 1.0);
+                const double dC = p ? dCoefg : dCoefl;
+                double AAd = F.rho[p * n + nb] * e.dn * Coef + F.rho[p * n + c] * e.dl * dC;
+                AAd *= (F.sat[(1 + p) * n + nb] * e.dn * Coef + F.sat[(1 + p) * n + c] * e.dl * dC) / (e.dn + e.dl);
+                const double tn = med == 0 ? A.tor[nb] : 1.0, tc_ = med == 0 ? tor : 1.0;
+                const double BBd = tn * e.dn * Coef / porpor2 + tc_ * e.dl * dC / porpor;
+                DB[p][q] = AAd / BBd * NNd;
+                Dzero[p][q] = Coef == 0 && dC == 0;
+            }
+        }
         // ---- component balances (first N-1 components)
         for (int i = 0; i < N - 1; i++, r++) {
             double R = 0, sc = 0;
             auto add = [&](double v) {
                 R += v;
-                sc += fabs(v);
+                if (SCALE) sc += fabs(v);
             };
             for (int p = 0; p < 2; p++) {
                 const double *w = p ? F.y : F.x;
@@ -936,27 +986,18 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
             for (int q = 0; q < nf; q++) {
                 const Face &e = fc[q];
                 const long nb = e.nb;
-                const double porpor2 = porpor_at(F, s, nb);
-                const double NNd = e.area2 / (e.dn + e.dl);
                 for (int p = 0; p < 2; p++) {
                     const double *w = p ? F.y : F.x;
-                    const signed char lnb = F.label[nb];
-                    const double Coef = p ? (lnb == 1 ? 0.0 : 1.0) : (lnb == -1 ? 0.0 : 1.0);
-                    const double dC = p ? dCoefg : dCoefl;
                     const double wn = w[(long)i * n + nb], wc = w[(long)i * n + c];
                     double Dup = wn > wc ? F.diff[(long)(2 * i + p) * n + nb] : F.diff[(long)(2 * i + p) * n + c];
-                    if (F.por[c] < kPorTiny || F.por[nb] < kPorTiny) Dup = 0;
-                    double AAd = F.rho[p * n + nb] * e.dn * Coef + F.rho[p * n + c] * e.dl * dC;
-                    AAd *= (F.sat[(1 + p) * n + nb] * e.dn * Coef + F.sat[(1 + p) * n + c] * e.dl * dC) / (e.dn + e.dl);
-                    const double tn = med == 0 ? A.tor[nb] : 1.0, tc_ = med == 0 ? tor : 1.0;
-                    const double BBd = tn * e.dn * Coef / porpor2 + tc_ * e.dl * dC / porpor;
-                    double DTran = AAd / BBd * NNd * Dup;
-                    if (Coef == 0 && dC == 0) DTran = 0;
+                    if (Dinact[q]) Dup = 0;
+                    double DTran = DB[p][q] * Dup;
+                    if (Dzero[p][q]) DTran = 0;
                     add(e.sgn > 0 ? DTran * (wn - wc) : -(DTran * (wc - wn)));
                 }
             }
             fo[r] = 0 - R;   // LSide: the accumulation at the linearisation point minus itself
-            if (so) so[r] = sc;
+            if (SCALE) so[r] = sc;
         }
         // ---- total hydrocarbon
         {
@@ -978,11 +1019,7 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         }
         // ---- water
         {
-            double R = 0, sc = 0;
-            for (int q = 0; q < nf; q++) {
-                R += KW[q];
-                sc += fabs(KW[q]);
-            }
+            double R = RW, sc = SW;
             R += sgnT * conv_w;
             sc += fabs(conv_w);
             R += wr.Qw;
