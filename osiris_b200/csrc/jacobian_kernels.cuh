@@ -1425,6 +1425,22 @@ OSR_HD inline void fugacity_rows(const JacView &v, const Cell &q, const Out &out
     const double DDl = Al / (Bl * (d1 - d2)), DDg = Ag / (Bg * (d1 - d2));
     const double FFl = log((Zl + d2 * Bl) / (Zl + d1 * Bl)), FFg = log((Zg + d2 * Bg) / (Zg + d1 * Bg));
     const double lZBl = log(Zl - Bl), lZBg = log(Zg - Bg);
+    // Denominators of the composition derivatives that do not depend on the
+    // entry, inverted once per cell (the reference divides in every entry).
+    const double iCb2l = 1 / (Cbl * Cbl), iCb2g = 1 / (Cbg * Cbg), iCbl = 1 / Cbl, iCbg = 1 / Cbg;
+    const double iBB2l = 1 / (Bl * Bl * (d1 - d2)), iBB2g = 1 / (Bg * Bg * (d1 - d2));
+    const double iZd2l = 1 / (Zl + d2 * Bl), iZd2g = 1 / (Zg + d2 * Bg);
+    const double iZd1l = 1 / (Zl + d1 * Bl), iZd1g = 1 / (Zg + d1 * Bg);
+    const double iZBl = 1 / (Zl - Bl), iZBg = 1 / (Zg - Bg);
+    const double iCal = 1 / Cal, iCag = 1 / Cag;
+    const double iPCal2 = 1 / (Pl * Cal * Cal), iPCag2 = 1 / (Pg * Cag * Cag);
+    const double ZZPl = Zl * Zl / Pl, ZZPg = Zg * Zg / Pg;
+    // d Z / d w_k of each phase (the reference's -dE RT Z^2 / P)
+    double dzl[kMaxNc], dzg[kMaxNc];
+    for (int k = 0; k < N; k++) {
+        dzl[k] = -q.dE(k, 0) * RT * ZZPl;
+        dzg[k] = -q.dE(k, 1) * RT * ZZPg;
+    }
     for (int i = 0; i < N; i++) {
         const double t1l = v.b[i] / Cbl, t1g = v.b[i] / Cbg;
         const double EEl = 2 * tl[i] / Cal - t1l, EEg = 2 * tg[i] / Cag - t1g;
@@ -1439,19 +1455,20 @@ OSR_HD inline void fugacity_rows(const JacView &v, const Cell &q, const Out &out
         const double dPhig = phiG * (dAAg + dBBg + EEg * (dDDg * FFg + DDg * dFFg));
         const double xi = xl[i], yi = yg[i];
         out.st(L.f(i, 2 * N), jpc(v) * (xi * (phiL + Pl * dPhil) - yi * (phiG + Pg * dPhig)));
+        const double bi = v.b[i], tli = tl[i], tgi = tg[i];
         for (int k = 0; k < N; k++) {
             const double dAl = tl[k] * (2 * Pl / (RT * RT)), dAg = tg[k] * (2 * Pg / (RT * RT));
             const double dBl = v.b[k] * Pl / RT, dBg = v.b[k] * Pg / RT;
-            const double dZl = -q.dE(k, 0) * RT * Zl * Zl / Pl, dZg = -q.dE(k, 1) * RT * Zg * Zg / Pg;
-            const double dAAxl = -v.b[k] * v.b[i] * (Zl - 1) / (Cbl * Cbl) + v.b[i] * dZl / Cbl;
-            const double dAAxg = -v.b[k] * v.b[i] * (Zg - 1) / (Cbg * Cbg) + v.b[i] * dZg / Cbg;
-            const double dBBxl = (dBl - dZl) / (Zl - Bl), dBBxg = (dBg - dZg) / (Zg - Bg);
-            const double dDDxl = (dAl * Bl - dBl * Al) / (Bl * Bl * (d1 - d2)), dDDxg = (dAg * Bg - dBg * Ag) / (Bg * Bg * (d1 - d2));
-            const double dFFxl = (dZl + d2 * dBl) / (Zl + d2 * Bl) - (dZl + d1 * dBl) / (Zl + d1 * Bl);
-            const double dFFxg = (dZg + d2 * dBg) / (Zg + d2 * Bg) - (dZg + d1 * dBg) / (Zg + d1 * Bg);
+            const double dZl = dzl[k], dZg = dzg[k];
+            const double dAAxl = -v.b[k] * bi * (Zl - 1) * iCb2l + bi * dZl * iCbl;
+            const double dAAxg = -v.b[k] * bi * (Zg - 1) * iCb2g + bi * dZg * iCbg;
+            const double dBBxl = (dBl - dZl) * iZBl, dBBxg = (dBg - dZg) * iZBg;
+            const double dDDxl = (dAl * Bl - dBl * Al) * iBB2l, dDDxg = (dAg * Bg - dBg * Ag) * iBB2g;
+            const double dFFxl = (dZl + d2 * dBl) * iZd2l - (dZl + d1 * dBl) * iZd1l;
+            const double dFFxg = (dZg + d2 * dBg) * iZd2g - (dZg + d1 * dBg) * iZd1g;
             const double tik = v.sa[i] * v.sa[k] * v.bic[i * N + k];
-            const double dEEl = 2 * (tik / Cal - dAl * RT * RT * tl[i] / (Pl * Cal * Cal)) + v.b[i] * v.b[k] / (Cbl * Cbl);
-            const double dEEg = 2 * (tik / Cag - dAg * RT * RT * tg[i] / (Pg * Cag * Cag)) + v.b[i] * v.b[k] / (Cbg * Cbg);
+            const double dEEl = 2 * (tik * iCal - dAl * RT * RT * tli * iPCal2) + bi * v.b[k] * iCb2l;
+            const double dEEg = 2 * (tik * iCag - dAg * RT * RT * tgi * iPCag2) + bi * v.b[k] * iCb2g;
             const double dPxl = phiL * (dAAxl + dBBxl + dDDxl * EEl * FFl + DDl * dEEl * FFl + DDl * EEl * dFFxl);
             const double dPxg = phiG * (dAAxg + dBBxg + dDDxg * EEg * FFg + DDg * dEEg * FFg + DDg * EEg * dFFxg);
             if (i == k) {
