@@ -1,6 +1,7 @@
 // Host side of the residual path: row layout, unknown maps, well constants
 // and the FormFunction entry points of the C ABI.
 #include <cuda_runtime.h>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -320,11 +321,13 @@ static osr_status update_all_n(osr_grid &g, const double *x, cudaStream_t st) {
 
 template <int N>
 static osr_status residual_n(osr_grid &g, double *f, double *fscale, double t, cudaStream_t st) {
+    // the kernel's face tables hold cell indices in 32 bits
+    if (2 * g.cells >= (long)INT_MAX) return OSR_ERR_ARG;
     AsmArgs<N> A = asm_args<N>(g, f, fscale, t);
     if (fscale)
-        residual_kernel<N, true><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(A);
+        residual_kernel<N, true><<<(unsigned)grid_blocks(2 * g.cells), kResThreads, 0, st>>>(A);
     else
-        residual_kernel<N, false><<<(unsigned)grid_blocks(2 * g.cells), 128, 0, st>>>(A);
+        residual_kernel<N, false><<<(unsigned)grid_blocks(2 * g.cells), kResThreads, 0, st>>>(A);
     ASM_CUDA(cudaGetLastError());
     return OSR_OK;
 }

@@ -803,9 +803,29 @@ __device__ __forceinline__ double porpor_at(const MediumFields &F, const GridSca
     return F.por[c] * (1 + s.cpor * dp + s.dcpor * dp * dp);
 }
 
+// Threads per CTA of the residual kernel.
+constexpr int kResThreads = 128;
+
+// Per-thread face tables of the residual kernel in shared memory, entry e of
+// thread t at [e][t] (a warp reads consecutive words): the advective and
+// gravity factors and upstream cell of each (phase, face), the diffusion
+// factor of each (phase, face), the neighbour of each face, and bits: 1 << q
+// a + face, 1 << (6 + q) an inactive neighbour, 1 << (12 + 6 p + q) no
+// diffusive flux.  The component rows read these once per row; as a local
+// array the thread's frame (about 800 bytes, 512 threads per SM) exceeds L1.
+// Cell indices fit 32 bits (the host checks the grid size).
+struct ResFaces {
+    double kp[12][kResThreads], kg[12][kResThreads], db[12][kResThreads];
+    int up[12][kResThreads], nb[6][kResThreads];
+    unsigned bits[kResThreads];
+};
+
 // SCALE: the row scales (sum of |terms| of each row) are written to A.fscale.
+// Launched with kResThreads threads per CTA.
 template <int N, bool SCALE>
-__global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const __grid_constant__ AsmArgs<N> A) {
+__global__ void __launch_bounds__(kResThreads, OSR_RES_MIN_BLOCKS) residual_kernel(const __grid_constant__ AsmArgs<N> A) {
+    __shared__ ResFaces sf;
+    const int t = threadIdx.x;
     const GridScalars &s = A.a.s;
     const GridGeom &geo = A.a.geo;
     const long n = s.cells;
@@ -852,12 +872,13 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         // ---- faces: advective factors per phase (oil 0, gas 1)
         Face fc[6];
         const int nf = cell_faces<N>(A, c, ix, iy, iz, fc);
-        double KP[2][6], KG[2][6];
-        long up[2][6];
+        unsigned bits = 0;
         // the water row's face terms, summed in face order as the row adds them
         double RW = 0, SW = 0;
         for (int q = 0; q < nf; q++) {
             const Face &e = fc[q];
+            sf.nb[q][t] = (int)e.nb;
+            if (e.sgn > 0) bits |= 1u << q;
             const long plane = (long)e.d * n + e.tc;
             const double dH = e.sgn > 0 ? geo.blockH[e.nb] - geo.blockH[c] : geo.blockH[c] - geo.blockH[e.nb];
             for (int p = 0; p < 2; p++) {
@@ -865,14 +886,15 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
                 const double Tg = F.trans[(long)((2 + p) * 3) * n + plane];
                 const double Pc_ = F.P[(1 + p) * n + c], Pn_ = F.P[(1 + p) * n + e.nb];
                 const int tS = F.transS[(long)(p * 3) * n + plane];
+                const int pq = p * 6 + q;
                 if (e.sgn > 0) {
-                    KP[p][q] = Tp * (Pn_ - Pc_);
-                    KG[p][q] = Tg * dH;
-                    up[p][q] = tS ? e.nb : c;
+                    sf.kp[pq][t] = Tp * (Pn_ - Pc_);
+                    sf.kg[pq][t] = Tg * dH;
+                    sf.up[pq][t] = (int)(tS ? e.nb : c);
                 } else {
-                    KP[p][q] = -(Tp * (Pc_ - Pn_));
-                    KG[p][q] = -(Tg * dH);
-                    up[p][q] = tS ? c : e.nb;
+                    sf.kp[pq][t] = -(Tp * (Pc_ - Pn_));
+                    sf.kg[pq][t] = -(Tg * dH);
+                    sf.up[pq][t] = (int)(tS ? c : e.nb);
                 }
             }
             const double Tw = F.wtran[plane];
@@ -910,15 +932,13 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
         // that does not depend on the component, AAd / BBd * NNd of the
         // reference's DTran = AAd / BBd * NNd * Dup (formed once here, applied
         // per component row below with the same evaluation order)
-        double DB[2][6];
-        bool Dzero[2][6], Dinact[6];
         for (int q = 0; q < nf; q++) {
             const Face &e = fc[q];
             const long nb = e.nb;
             const double porpor2 = porpor_at(F, s, nb);
             const double NNd = e.area2 / (e.dn + e.dl);
             const signed char lnb = F.label[nb];
-            Dinact[q] = F.por[c] < kPorTiny || F.por[nb] < kPorTiny;
+            if (F.por[c] < kPorTiny || F.por[nb] < kPorTiny) bits |= 1u << (6 + q);
             for (int p = 0; p < 2; p++) {
                 const double Coef = p ? (lnb == 1 ? 0.0 : 1.0) : (lnb == -1 ? 0.0 : 1.0);
                 const double dC = p ? dCoefg : dCoefl;
@@ -926,8 +946,8 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
                 AAd *= (F.sat[(1 + p) * n + nb] * e.dn * Coef + F.sat[(1 + p) * n + c] * e.dl * dC) / (e.dn + e.dl);
                 const double tn = med == 0 ? A.tor[nb] : 1.0, tc_ = med == 0 ? tor : 1.0;
                 const double BBd = tn * e.dn * Coef / porpor2 + tc_ * e.dl * dC / porpor;
-                DB[p][q] = AAd / BBd * NNd;
-                Dzero[p][q] = Coef == 0 && dC == 0;
+                sf.db[p * 6 + q][t] = AAd / BBd * NNd;
+                if (Coef == 0 && dC == 0) bits |= 1u << (12 + p * 6 + q);
             }
         }
         // ---- component balances (first N-1 components)
@@ -939,11 +959,11 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
             };
             for (int p = 0; p < 2; p++) {
                 const double *w = p ? F.y : F.x;
-                for (int q = 0; q < nf; q++) add(w[(long)i * n + up[p][q]] * KP[p][q]);
+                for (int q = 0; q < nf; q++) add(w[(long)i * n + sf.up[p * 6 + q][t]] * sf.kp[p * 6 + q][t]);
             }
             for (int p = 0; p < 2; p++) {
                 const double *w = p ? F.y : F.x;
-                for (int q = 0; q < nf; q++) add(w[(long)i * n + up[p][q]] * KG[p][q]);
+                for (int q = 0; q < nf; q++) add(w[(long)i * n + sf.up[p * 6 + q][t]] * sf.kg[p * 6 + q][t]);
             }
             add(sgnT * M.x[(long)i * n + c] * conv_o);
             add(sgnT * M.y[(long)i * n + c] * conv_g);
@@ -984,16 +1004,15 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
             add(oComp * wr.Qo + gComp * wr.Qg);
             // intra-continuum diffusion
             for (int q = 0; q < nf; q++) {
-                const Face &e = fc[q];
-                const long nb = e.nb;
+                const long nb = sf.nb[q][t];
                 for (int p = 0; p < 2; p++) {
                     const double *w = p ? F.y : F.x;
                     const double wn = w[(long)i * n + nb], wc = w[(long)i * n + c];
                     double Dup = wn > wc ? F.diff[(long)(2 * i + p) * n + nb] : F.diff[(long)(2 * i + p) * n + c];
-                    if (Dinact[q]) Dup = 0;
-                    double DTran = DB[p][q] * Dup;
-                    if (Dzero[p][q]) DTran = 0;
-                    add(e.sgn > 0 ? DTran * (wn - wc) : -(DTran * (wc - wn)));
+                    if (bits & (1u << (6 + q))) Dup = 0;
+                    double DTran = sf.db[p * 6 + q][t] * Dup;
+                    if (bits & (1u << (12 + p * 6 + q))) DTran = 0;
+                    add((bits & (1u << q)) ? DTran * (wn - wc) : -(DTran * (wc - wn)));
                 }
             }
             fo[r] = 0 - R;   // LSide: the accumulation at the linearisation point minus itself
@@ -1007,9 +1026,9 @@ __global__ void __launch_bounds__(128, OSR_RES_MIN_BLOCKS) residual_kernel(const
                 sc += fabs(v);
             };
             for (int p = 0; p < 2; p++)
-                for (int q = 0; q < nf; q++) add(KP[p][q]);
+                for (int q = 0; q < nf; q++) add(sf.kp[p * 6 + q][t]);
             for (int p = 0; p < 2; p++)
-                for (int q = 0; q < nf; q++) add(KG[p][q]);
+                for (int q = 0; q < nf; q++) add(sf.kg[p * 6 + q][t]);
             add(sgnT * conv_o);
             add(sgnT * conv_g);
             add(wr.Qo + wr.Qg);
