@@ -19,10 +19,19 @@ static osr_status jfail(cudaError_t) { return OSR_ERR_CUDA; }
     } while (0)
 
 constexpr int kRowThreads = 128;
-// Resident CTAs per SM the row kernels are compiled for (bounds their registers).
+// Resident CTAs per SM the row kernels are compiled for (bounds their
+// registers): the composition-column and fugacity kinds (4: 128 registers),
+// and the pressure-saturation kinds, whose four shared row sums per row and
+// longer per-face state spill heavily at 128 registers (3: 168 registers).
+// On the 128x128x32 PR-8 Jacobian: 3 / 4 CTAs for the pressure-saturation
+// kinds 20.8 / 21.9 ms, 2 CTAs 22.9 ms; 3 CTAs for the column kinds 22.6 ms.
 #ifndef OSR_JAC_MIN_BLOCKS
 #define OSR_JAC_MIN_BLOCKS 4
 #endif
+#ifndef OSR_JAC_PS_MIN_BLOCKS
+#define OSR_JAC_PS_MIN_BLOCKS 3
+#endif
+constexpr int jac_min_blocks(int kind) { return kind == 2 || kind == 3 ? OSR_JAC_PS_MIN_BLOCKS : OSR_JAC_MIN_BLOCKS; }
 
 template <int N>
 __global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_constant__ osrj::JacView v) {
@@ -36,7 +45,7 @@ __global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_cons
 // task.  Each thread's per-row sums: 3N (columns) or 4N (pressure and
 // saturations) doubles of dynamic shared memory.
 template <int KIND>
-__global__ void __launch_bounds__(kRowThreads, OSR_JAC_MIN_BLOCKS) jacobian_rows_kernel(const __grid_constant__ osrj::JacView v,
+__global__ void __launch_bounds__(kRowThreads, jac_min_blocks(KIND)) jacobian_rows_kernel(const __grid_constant__ osrj::JacView v,
                                                                    long chunk0, long chunks) {
     extern __shared__ double s_acc[];
     const int T = KIND <= 1 ? v.nc : 1;
