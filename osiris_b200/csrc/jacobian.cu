@@ -20,18 +20,26 @@ static osr_status jfail(cudaError_t) { return OSR_ERR_CUDA; }
 
 constexpr int kRowThreads = 128;
 // Resident CTAs per SM the row kernels are compiled for (bounds their
-// registers): the composition-column and fugacity kinds (4: 128 registers),
-// and the pressure-saturation kinds, whose four shared row sums per row and
-// longer per-face state spill heavily at 128 registers (3: 168 registers).
-// On the 128x128x32 PR-8 Jacobian: 3 / 4 CTAs for the pressure-saturation
-// kinds 20.8 / 21.9 ms, 2 CTAs 22.9 ms; 3 CTAs for the column kinds 22.6 ms.
+// registers): the composition-column kinds (4: 128 registers), the
+// pressure-saturation kinds, whose four shared row sums per row and longer
+// per-face state spill heavily at 128 registers (3: 168 registers), and the
+// fugacity / water / constraint kind, whose per-cell arrays sit in local
+// memory anyway and which gains from occupancy (6: 80 registers).  On the
+// 128x128x32 PR-8 Jacobian: pressure-saturation kinds at 2 / 3 / 4 CTAs
+// 22.9 / 20.8 / 21.9 ms; column kinds at 3 CTAs 22.6 ms; the fugacity kind
+// at 3 / 4 / 5 / 6 / 8 CTAs 21.6 / 21.5 / 21.7 / 20.8 / 21.9 ms.
 #ifndef OSR_JAC_MIN_BLOCKS
 #define OSR_JAC_MIN_BLOCKS 4
 #endif
 #ifndef OSR_JAC_PS_MIN_BLOCKS
 #define OSR_JAC_PS_MIN_BLOCKS 3
 #endif
-constexpr int jac_min_blocks(int kind) { return kind == 2 || kind == 3 ? OSR_JAC_PS_MIN_BLOCKS : OSR_JAC_MIN_BLOCKS; }
+#ifndef OSR_JAC_ROW_MIN_BLOCKS
+#define OSR_JAC_ROW_MIN_BLOCKS 6
+#endif
+constexpr int jac_min_blocks(int kind) {
+    return kind == 2 || kind == 3 ? OSR_JAC_PS_MIN_BLOCKS : kind == 4 ? OSR_JAC_ROW_MIN_BLOCKS : OSR_JAC_MIN_BLOCKS;
+}
 
 template <int N>
 __global__ void __launch_bounds__(kRowThreads) jac_prep_kernel(const __grid_constant__ osrj::JacView v) {
